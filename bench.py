@@ -1,0 +1,348 @@
+#!/usr/bin/env python
+"""FDTD benchmark: 3-D 256^3 FP32 Yee step with CPML on B200.
+
+Workload (one "step" = one leapfrog time step of the whole grid, H then E,
+soft-source injection and a running-DFT monitor, all in the fused
+``dn_fdtd3d_run`` kernel): 256^3 cells, dl = 25 nm, 12-cell CPML, Courant
+0.4, FP32; eps = SiO2 substrate / 500 nm Si slab / air with a 128x128x40
+design block of seeded filtered noise in [2.085, 12.1]; Ex-polarised
+Gaussian-pulse plane source at 1.55 um; Ey DFT monitor on a 64x64 plane.
+Inputs are synthetic (seeded), the state (2 x 6 x 67 MB + 67 MB) is larger
+than the 126 MB L2, so no flush is needed between steps.
+
+Prints one JSON line (rank 0).  ``--impl reference`` times the CPU FP64
+restatement of the reference's algorithm (the oracle) on the host cores on
+the same grid instead.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import torch
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SHAPE = (256, 256, 256)
+DL, COURANT, PML, T_SOLVE = 25.0, 0.4, 12, 4000
+Z_SRC, Z_MON = 40, 200
+BYTES_PER_CELL_STEP = 52  # FP32: read Ex Ey Ez Hx Hy Hz dt/eps, write the six fields
+WORKLOAD = "3d_yee_256cube_cpml12_fp32"
+METRIC = "FDTD Gcell-updates/s"
+UNIT = "Gcell-updates/s"
+
+
+def workload():
+    from diffnano_b200.workloads import gaussian_pulse_for_band, slab_eps_3d
+
+    eps = slab_eps_3d(SHAPE, dl=DL, design=(40, 128, 128), seed=1)
+    src = gaussian_pulse_for_band(1550.0, 200.0)
+    src.update(plane="xy", z=Z_SRC, component="Ex")
+    mons = [{"name": "out", "component": "Ey", "plane": "xy", "z": Z_MON,
+             "extent": [[96, 160], [96, 160]], "wavelengths_nm": [1550.0]}]
+    return eps, src, mons
+
+
+def config_dict(extra=None):
+    c = {"workload": WORKLOAD, "grid": list(SHAPE), "dl_nm": DL, "pml_layers": PML,
+         "courant": COURANT, "n_steps_per_solve": T_SOLVE,
+         "source": "Ex plane-wave Gaussian pulse, 1550 nm, 200 nm band, plane z=40",
+         "monitor": "Ey DFT on a 64x64 plane at z=200, 1550 nm",
+         "l2": "inputs larger than L2 (state 940 MB ping-pong + 67 MB coefficients)",
+         "parallelism": "replicas (one independent grid per GPU)"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+def measured_peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_per_launch():
+    p = os.path.join(ROOT, "profiles", "fdtd3d_256_traffic.json")
+    try:
+        with open(p) as fh:
+            return float(json.load(fh)["dram_bytes_per_launch"])
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-i", str(self.idx)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+        else:
+            self.lines = []
+
+    def summary(self):
+        if not self.lines:
+            return None
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except (ValueError, IndexError):
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(x: float, ws: int, dev) -> float:
+    if ws == 1:
+        return x
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle (FP64 torch CPU restatement of the reference)
+# ---------------------------------------------------------------------------
+def cpu_baseline(eps, n_steps_hint: int | None = None, budget_s: float = 15.0):
+    from oracle import fdtd_ref as R
+
+    threads = os.cpu_count() or 1
+    torch.set_num_threads(threads)
+    D, H, W = SHAPE
+    dt = COURANT * DL / math.sqrt(3.0)
+    prof = (*R.cpml_profile(W, PML, DL, dt), *R.cpml_profile(H, PML, DL, dt),
+            *R.cpml_profile(D, PML, DL, dt))
+    gen = torch.Generator().manual_seed(0)
+    f = [1e-3 * torch.randn(D, H, W, dtype=torch.float64, generator=gen) for _ in range(6)]
+    t = time.perf_counter()
+    f = list(R.step_3d(*f, eps, prof, dt, DL))  # warm-up
+    t1 = time.perf_counter() - t
+    n = n_steps_hint or max(2, min(20, int(budget_s / max(t1, 1e-3))))
+    t = time.perf_counter()
+    for _ in range(n):
+        f = list(R.step_3d(*f, eps, prof, dt, DL))
+    el = time.perf_counter() - t
+    return {"value": D * H * W * n / el / 1e9, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n} time steps of the full 256^3 grid, FP64 torch-CPU restatement of "
+                      f"fdtd3d.py:_time_step (oracle/fdtd_ref.py), {threads} threads"}
+
+
+def run_reference(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import fdtd_ref as R
+
+    threads = os.cpu_count() or 1
+    torch.set_num_threads(threads)
+    eps, _, _ = workload()
+    D, H, W = SHAPE
+    # bounded sample (about a minute on 8 cores): full grid while K+W <= 16
+    # steps, else a z-slab of the same grid
+    total = args.steps + args.warmup
+    dz = D if total <= 16 else max(8, int(D * 16 / total))
+    dt = COURANT * DL / math.sqrt(3.0)
+    # the slab keeps all three CPML profiles (cubic "reference" broadcasting)
+    prof = (*R.cpml_profile(W, PML, DL, dt), *R.cpml_profile(H, PML, DL, dt),
+            *R.cpml_profile(W, PML, DL, dt))
+    e = eps[:dz].contiguous()
+    gen = torch.Generator().manual_seed(0)
+    f = [1e-3 * torch.randn(dz, H, W, dtype=torch.float64, generator=gen) for _ in range(6)]
+
+    def step(f):
+        return list(R.step_3d(*f, e, prof, dt, DL))
+
+    for _ in range(args.warmup):
+        f = step(f)
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        f = step(f)
+    el = time.perf_counter() - t
+    v = dz * H * W * args.steps / el / 1e9
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": config_dict({"reference_sample": f"z-slab {dz}x{H}x{W} per step"}),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{args.steps} steps of a {dz}x{H}x{W} slab of the "
+                                       "256^3 grid, FP64 torch-CPU restatement of the "
+                                       "reference's fdtd3d.py:_time_step"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    ws, rank, local = dist_setup()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    import diffnano_b200 as dn
+
+    eps, src, mons = workload()
+    D, H, W = SHAPE
+    cells = D * H * W
+    K, Wm = args.steps, args.warmup
+    n_total = max(T_SOLVE, K + Wm)
+    solver = dn.FDTDSolver3D(grid_shape=SHAPE, dl=DL, wavelength_nm=1550.0, pml_layers=PML,
+                             n_steps=n_total, courant=COURANT, device=dev, dtype=torch.float32)
+    eng = solver._make_engine(n_total, src, mons)
+    eng.set_eps(eps.to(dev))
+    eng.run(0, Wm)
+    torch.cuda.synchronize(dev)
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(ws)
+    torch.cuda.synchronize(dev)
+    with ClockSampler(local) as cs:
+        e0.record(stream)
+        eng.run(Wm, K)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+    barrier(ws)
+    el = e0.elapsed_time(e1) / 1e3
+    eng.check_status()
+    el_max = max_over_ranks(el, ws, dev)
+    value = ws * cells * K / el_max / 1e9
+    launch_s = el / K
+    peak, peak_kind = measured_peak_hbm()
+    achieved = BYTES_PER_CELL_STEP * cells / launch_s / 1e9
+    traffic = traffic_per_launch()
+    del eng
+    torch.cuda.empty_cache()
+
+    # end to end through the public API with host buffers (reference device="cpu")
+    e2e = None
+    if not args.no_e2e:
+        s_host = dn.FDTDSolver3D(grid_shape=SHAPE, dl=DL, wavelength_nm=1550.0, pml_layers=PML,
+                                 n_steps=T_SOLVE, courant=COURANT, device="cpu",
+                                 dtype=torch.float32)
+        eps_pinned = eps.to(torch.float32).pin_memory()
+        r = s_host.forward(eps_pinned, source=dict(src), monitors=mons)  # warm-up
+        barrier(ws)
+        t = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            r = s_host.forward(eps_pinned, source=dict(src), monitors=mons)
+        e2e_el = (time.perf_counter() - t) / args.e2e_steps
+        e2e_el = max_over_ranks(e2e_el, ws, dev)
+        d2h = r.field.numel() * r.field.element_size() + sum(
+            m["dft"].numel() * m["dft"].element_size() for m in r.metadata["monitors"])
+        e2e = {"value": ws * cells * T_SOLVE / e2e_el / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": eps_pinned.numel() * eps_pinned.element_size(),
+               "d2h_bytes_per_step": d2h,
+               "step": f"one FDTDSolver3D.forward(device='cpu') solve of {T_SOLVE} time steps "
+                       f"(host eps in, host field + monitor DFT out), mean of {args.e2e_steps}"}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(eps)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K,
+                "warmup": Wm, "ms_per_step": el_max / K * 1e3, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": config_dict(),
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": traffic,
+                             "peak_source": f"hbm_gbs of {peak_kind}",
+                             "algorithmic_bytes_per_launch": BYTES_PER_CELL_STEP * cells,
+                             "kernel": "k_fdtd3d (one launch per time step)"},
+                "cpu_baseline": cpu, "e2e": e2e, "clocks": cs.summary(), "gpu_launches": K}
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,126 @@
+"""ctypes binding of the C ABI in ``include/dn_fdtd.h`` (``_native/libdn_fdtd.so``).
+
+The library is built in-tree by ``diffnano_b200/build.py``.  There is no
+fallback: if the library is missing, :func:`lib` raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_native", "libdn_fdtd.so")
+
+# status codes (dn_fdtd.h)
+DN_OK, DN_EINVAL, DN_ENOMEM, DN_ECUDA, DN_ETIMEOUT, DN_ENONFINITE, DN_EUNSUPPORTED = range(7)
+DN_F32, DN_F64 = 0, 1
+DN_EX, DN_EY, DN_EZ, DN_HX, DN_HY, DN_HZ = range(6)
+DN_NONE = -1
+DN_TM, DN_TE = 0, 1
+DN_AXES_REFERENCE, DN_AXES_PHYSICAL = 0, 1
+DN_MAX_MONITORS = 4
+DN_MAX_FREQS = 16
+
+COMPONENTS = {"Ex": DN_EX, "Ey": DN_EY, "Ez": DN_EZ, "Hx": DN_HX, "Hy": DN_HY, "Hz": DN_HZ}
+
+c_int32, c_int64, c_double, c_void_p = ctypes.c_int32, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p
+
+
+class DnBox(ctypes.Structure):
+    _fields_ = [("lo", c_int32 * 3), ("hi", c_int32 * 3)]
+
+
+class DnGrid(ctypes.Structure):
+    _fields_ = [("D", c_int32), ("H", c_int32), ("W", c_int32), ("dtype", c_int32),
+                ("pitch_y", c_int64), ("pitch_z", c_int64), ("dt", c_double), ("dl", c_double),
+                ("axes", c_int32), ("pol", c_int32)]
+
+
+class DnCpml(ctypes.Structure):
+    _fields_ = [("b", c_void_p * 3), ("c", c_void_p * 3)]
+
+
+class DnSource(ctypes.Structure):
+    _fields_ = [("component", c_int32), ("box", DnBox), ("wave", c_void_p)]
+
+
+class DnMonitor(ctypes.Structure):
+    _fields_ = [("component", c_int32), ("box", DnBox), ("n_freq", c_int32),
+                ("phase", c_void_p), ("acc", c_void_p)]
+
+
+class DnProbe(ctypes.Structure):
+    _fields_ = [("component", c_int32), ("pos", c_int32 * 3), ("out", c_void_p)]
+
+
+PTR6 = c_void_p * 6
+_P6 = ctypes.POINTER(c_void_p)  # a PTR6 instance (or None) is passed here
+
+# name -> (restype, argtypes); every symbol include/dn_fdtd.h declares
+SIGNATURES = {
+    "dn_strerror": (ctypes.c_char_p, [c_int32]),
+    "dn_version": (c_int32, []),
+    "dn_last_cuda_error": (c_int32, []),
+    "dn_fdtd2d_run": (c_int32, [ctypes.POINTER(DnGrid), _P6, _P6, c_void_p,
+                                ctypes.POINTER(DnCpml), ctypes.POINTER(DnSource),
+                                ctypes.POINTER(DnMonitor), c_int32, ctypes.POINTER(DnProbe), c_int32,
+                                c_int32, c_void_p, c_void_p, ctypes.POINTER(c_int32)]),
+    "dn_fdtd3d_run": (c_int32, [ctypes.POINTER(DnGrid), _P6, _P6, c_void_p,
+                                ctypes.POINTER(DnCpml), ctypes.POINTER(DnSource),
+                                ctypes.POINTER(DnMonitor), c_int32, ctypes.POINTER(DnProbe), c_int32,
+                                c_int32, c_void_p, c_void_p, ctypes.POINTER(c_int32)]),
+}
+
+
+class DNError(RuntimeError):
+    """A dn_* call returned a non-OK status."""
+
+    def __init__(self, fn: str, status: int, msg: str):
+        super().__init__(f"{fn} failed: {msg} (status {status})")
+        self.status = status
+
+
+_lock = threading.Lock()
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load the CUDA library (once).  Raises if it has not been built."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise ImportError(
+                    f"diffnano_b200 CUDA library not built ({LIB_PATH} missing); run "
+                    "`python -c 'import __graft_entry__ as g; g.build()'` or "
+                    "`python diffnano_b200/build.py`")
+            L = ctypes.CDLL(LIB_PATH)
+            for name, (res, args) in SIGNATURES.items():
+                f = getattr(L, name)
+                f.restype = res
+                f.argtypes = args
+            _lib = L
+    return _lib
+
+
+def check(fn: str, status: int) -> None:
+    """Raise for a non-OK status (``ValueError`` for bad arguments)."""
+    if status == DN_OK:
+        return
+    L = lib()
+    msg = L.dn_strerror(status).decode()
+    if status == DN_ECUDA:
+        msg += f" (cuda error {L.dn_last_cuda_error()})"
+    if status == DN_EINVAL:
+        raise ValueError(f"{fn}: {msg}")
+    raise DNError(fn, status, msg)
+
+
+def box(lo, hi) -> DnBox:
+    b = DnBox()
+    for a in range(3):
+        b.lo[a] = int(lo[a])
+        b.hi[a] = int(hi[a])
+    return b

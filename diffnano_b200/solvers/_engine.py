@@ -1,0 +1,207 @@
+"""Device state and kernel driver shared by the 2-D and 3-D solvers.
+
+An :class:`Engine` owns, on one CUDA device, everything the C ABI needs for
+one solver configuration: two ping-pong field sets ``(6, D, H, Wp)`` (rows
+padded to ``Wp``, a multiple of 32 elements, so every row starts 128-byte
+aligned and TMA boxes are legal), the per-cell coefficient ``dt/eps``, the
+CPML profiles, the source waveform table, DFT-monitor phase tables and FP64
+accumulators, and a probe buffer.  It runs steps through
+``dn_fdtd2d_run`` / ``dn_fdtd3d_run`` on the current torch stream.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import torch
+
+from diffnano_b200 import _lib
+from diffnano_b200.solvers import _setup
+
+F64 = torch.float64
+
+
+def compute_device(device) -> torch.device:
+    """CUDA device the kernels run on for a solver built with ``device``.
+
+    The reference runs wherever ``device`` says, CPU included.  These
+    kernels exist only for CUDA (sm_100a): a CUDA ``device`` is used as is;
+    any other ``device`` names where inputs and results live, and the
+    computation runs on the current CUDA device.  There is no CPU path.
+    """
+    dev = torch.device(device)
+    if not torch.cuda.is_available():
+        raise RuntimeError(
+            "diffnano_b200 runs its FDTD kernels on a CUDA GPU (sm_100a) and has no CPU path; "
+            "no CUDA device is visible")
+    if dev.type == "cuda":
+        return dev if dev.index is not None else torch.device("cuda", torch.cuda.current_device())
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+def padded_width(W: int) -> int:
+    return (W + 31) // 32 * 32
+
+
+@dataclass
+class MonitorSpec:
+    name: str
+    component: int
+    box: tuple  # ((z0,z1),(y0,y1),(x0,x1))
+    wavelengths: list
+    cells: int = field(init=False)
+
+    def __post_init__(self):
+        self.cells = 1
+        for a, b in self.box:
+            self.cells *= b - a
+
+    @property
+    def shape(self):
+        return tuple(b - a for a, b in self.box)
+
+
+class Engine:
+    """Device state + launcher for one grid / source / monitor configuration."""
+
+    def __init__(self, *, is3d: bool, shape, dl: float, dt: float, pml_layers: int,
+                 dtype: torch.dtype, device: torch.device, n_steps: int, wave: torch.Tensor,
+                 src_box, src_comp: int, monitors=(), probe=None, pol: int = _lib.DN_TM,
+                 axes: int = _lib.DN_AXES_REFERENCE):
+        if dtype not in (torch.float32, torch.float64):
+            raise ValueError(f"dtype must be torch.float32 or torch.float64, got {dtype}")
+        self.is3d = is3d
+        self.shape3 = tuple(int(v) for v in (shape if is3d else (1, *shape)))
+        D, H, W = self.shape3
+        self.Wp = padded_width(W)
+        self.dtype, self.device = dtype, device
+        self.dl, self.dt, self.n_steps = float(dl), float(dt), int(n_steps)
+        self.pol, self.axes = pol, axes
+        kw = dict(dtype=dtype, device=device)
+        self.A = torch.zeros((6, D, H, self.Wp), **kw)
+        self.B = torch.zeros((6, D, H, self.Wp), **kw)
+        self.ce = torch.zeros((D, H, self.Wp), **kw)
+        self.cur_b = False
+
+        # CPML profiles: axis 0 = z (D), 1 = y (H), 2 = x (W)
+        self.prof = []
+        for a, n in enumerate(self.shape3):
+            if a == 0 and not is3d:
+                self.prof.append(None)
+                continue
+            b, c = _setup.cpml_profile(n, pml_layers, dl, dt)
+            self.prof.append((b.to(device), c.to(device)))
+        self.cpml = _lib.DnCpml()
+        for a in range(3):
+            if self.prof[a] is not None:
+                self.cpml.b[a] = self.prof[a][0].data_ptr()
+                self.cpml.c[a] = self.prof[a][1].data_ptr()
+
+        self.grid = _lib.DnGrid(D=D, H=H, W=W, dtype=_lib.DN_F32 if dtype == torch.float32 else _lib.DN_F64,
+                                pitch_y=self.Wp, pitch_z=H * self.Wp, dt=self.dt, dl=self.dl,
+                                axes=axes, pol=pol)
+
+        # source
+        self.wave = wave.to(device=device, dtype=dtype).contiguous()
+        self.src = _lib.DnSource(component=_lib.DN_NONE)
+        if src_box is not None and src_comp != _lib.DN_NONE:
+            self.src.component = src_comp
+            self.src.box = _lib.box([a for a, _ in src_box], [b for _, b in src_box])
+            self.src.wave = self.wave.data_ptr()
+
+        # monitors
+        if len(monitors) > _lib.DN_MAX_MONITORS:
+            raise ValueError(f"at most {_lib.DN_MAX_MONITORS} monitors per solve")
+        self.monitors = list(monitors)
+        self.phases, self.accs = [], []
+        self.mon_arr = (_lib.DnMonitor * max(1, len(self.monitors)))()
+        for m, spec in enumerate(self.monitors):
+            if not 1 <= len(spec.wavelengths) <= _lib.DN_MAX_FREQS:
+                raise ValueError(f"a monitor takes 1..{_lib.DN_MAX_FREQS} wavelengths")
+            ph = _setup.dft_phase_table(self.n_steps, self.dt, spec.wavelengths).to(device)
+            acc = torch.zeros((len(spec.wavelengths), spec.cells, 2), dtype=F64, device=device)
+            self.phases.append(ph)
+            self.accs.append(acc)
+            M = self.mon_arr[m]
+            M.component = spec.component
+            M.box = _lib.box([a for a, _ in spec.box], [b for _, b in spec.box])
+            M.n_freq = len(spec.wavelengths)
+            M.phase = ph.data_ptr()
+            M.acc = acc.data_ptr()
+
+        # probe
+        self.probe = _lib.DnProbe(component=_lib.DN_NONE)
+        self.probe_out = None
+        if probe is not None:
+            comp, pos = probe
+            self.probe_out = torch.zeros(self.n_steps, **kw)
+            self.probe.component = comp
+            for a in range(3):
+                self.probe.pos[a] = int(pos[a])
+            self.probe.out = self.probe_out.data_ptr()
+
+        self.status = torch.zeros(1, dtype=torch.int32, device=device)
+
+    # ------------------------------------------------------------------
+    def set_eps(self, eps: torch.Tensor) -> None:
+        """Per-cell coefficient dt/eps (computed in FP64, stored in the dtype)."""
+        e = eps.to(device=self.device).reshape(self.shape3)
+        self.ce[..., : self.shape3[2]] = (self.dt / e.to(F64)).to(self.dtype)
+
+    def current(self) -> torch.Tensor:
+        return self.B if self.cur_b else self.A
+
+    def field(self, comp: int) -> torch.Tensor:
+        """View ``(D, H, W)`` of a component of the current state."""
+        return self.current()[comp, :, :, : self.shape3[2]]
+
+    def reset(self) -> None:
+        self.A.zero_()
+        self.B.zero_()
+        self.cur_b = False
+        for a in self.accs:
+            a.zero_()
+        if self.probe_out is not None:
+            self.probe_out.zero_()
+        self.status.zero_()
+
+    def load_state(self, state: torch.Tensor) -> None:
+        self.current().copy_(state)
+
+    @staticmethod
+    def _ptrs(t: torch.Tensor):
+        return _lib.PTR6(*[t[c].data_ptr() for c in range(6)])
+
+    def run(self, t0: int, nsteps: int) -> None:
+        """Advance ``nsteps`` steps starting at absolute step ``t0``."""
+        if nsteps <= 0:
+            return
+        if t0 + nsteps > self.n_steps:
+            raise ValueError("step range beyond the precomputed source/monitor tables")
+        L = _lib.lib()
+        fa, fb = (self.B, self.A) if self.cur_b else (self.A, self.B)
+        out = ctypes.c_int32(0)
+        fn_name = "dn_fdtd3d_run" if self.is3d else "dn_fdtd2d_run"
+        with torch.cuda.device(self.device):
+            stream = torch.cuda.current_stream(self.device).cuda_stream
+            rc = getattr(L, fn_name)(
+                ctypes.byref(self.grid), self._ptrs(fa), self._ptrs(fb), self.ce.data_ptr(),
+                ctypes.byref(self.cpml), ctypes.byref(self.src), self.mon_arr, len(self.monitors),
+                ctypes.byref(self.probe), int(t0), int(nsteps), self.status.data_ptr(),
+                ctypes.c_void_p(stream), ctypes.byref(out))
+        _lib.check(fn_name, rc)
+        if out.value:
+            self.cur_b = not self.cur_b
+
+    def check_status(self) -> None:
+        """Raise if a kernel recorded a device-side error (synchronises)."""
+        s = int(self.status.item())
+        if s != _lib.DN_OK:
+            _lib.check("device status", s)
+
+    def monitor_dft(self, m: int) -> torch.Tensor:
+        """Complex ``(L, *box_shape)`` DFT of monitor ``m`` (FP64 -> complex128)."""
+        spec = self.monitors[m]
+        acc = self.accs[m]
+        return torch.view_as_complex(acc).reshape(len(spec.wavelengths), *spec.shape)

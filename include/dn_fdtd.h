@@ -1,0 +1,155 @@
+/*
+ * dn_fdtd.h -- C ABI of the B200 (sm_100a) Yee-FDTD library (libdn_fdtd.so).
+ *
+ * Plain C: raw device pointers, sizes and strides, int status codes, no C++
+ * exceptions and no torch types cross this boundary.  All buffers are owned
+ * by the caller (the Python layer allocates them with PyTorch); every call is
+ * asynchronous on the given CUDA stream (passed as `void*`, a cudaStream_t;
+ * NULL = legacy default stream) unless its comment says otherwise.
+ *
+ * Layout: a field is a (D, H, W) array, W (x, index k) fastest, then H (y,
+ * index j), then D (z, index i).  Rows are `pitch_y` elements apart and
+ * planes `pitch_z` elements apart; for the 3-D kernels pitch_y * element size
+ * must be a multiple of 16 bytes and every field base 16-byte aligned (the
+ * Python layer pads rows to 32 elements).  2-D grids use D = 1, index (j, k)
+ * = (row, column) and ignore pitch_z.
+ *
+ * Reference interfaces replaced (DiffNano, paths relative to its checkout):
+ *   dn_fdtd2d_run  <- FDTDSolver2D._run_steps loop body: _time_step_tm /
+ *                     _time_step_te + `field + mask*waveform`
+ *                     (diffnano/solvers/fdtd2d.py:233-303, 330-357)
+ *   dn_fdtd3d_run  <- FDTDSolver3D._run_steps loop body: _time_step +
+ *                     `Ez + mask*waveform` (diffnano/solvers/fdtd3d.py:378-465,
+ *                     490-502)
+ */
+#ifndef DN_FDTD_H
+#define DN_FDTD_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define DN_OK            0
+#define DN_EINVAL        1  /* bad argument (shape, pointer, alignment, size) */
+#define DN_ENOMEM        2  /* a limit of a fixed-size resource was exceeded   */
+#define DN_ECUDA         3  /* a CUDA runtime/driver call failed               */
+#define DN_ETIMEOUT      4  /* a bounded device-side wait gave up              */
+#define DN_ENONFINITE    5  /* a NaN/Inf was detected                          */
+#define DN_EUNSUPPORTED  6  /* no kernel for this configuration / device       */
+
+/* ---- enums ------------------------------------------------------------- */
+#define DN_F32 0
+#define DN_F64 1
+
+/* field components; also the index into the 6-pointer field sets */
+#define DN_EX 0
+#define DN_EY 1
+#define DN_EZ 2
+#define DN_HX 3
+#define DN_HY 4
+#define DN_HZ 5
+#define DN_NONE (-1)
+
+/* 2-D polarisations */
+#define DN_TM 0 /* Ez, Hx, Hy  (fdtd2d.py:233-267) */
+#define DN_TE 1 /* Hz, Ex, Ey  (fdtd2d.py:269-303) */
+
+/* 3-D CPML axis mapping */
+#define DN_AXES_REFERENCE 0 /* the reference's broadcasting (fdtd3d.py:402-463); cubic grids */
+#define DN_AXES_PHYSICAL  1 /* every profile indexed along its own axis; any (D, H, W)       */
+
+#define DN_MAX_MONITORS 4
+#define DN_MAX_FREQS 16
+
+/* half-open index box, axis order (z, y, x); 2-D uses z = [0, 1) */
+typedef struct {
+  int32_t lo[3];
+  int32_t hi[3];
+} dn_box;
+
+typedef struct {
+  int32_t D, H, W;
+  int32_t dtype;   /* DN_F32 / DN_F64: element type of fields, coefficients, wave table */
+  int64_t pitch_y; /* elements between rows   (>= W)         */
+  int64_t pitch_z; /* elements between planes (>= H*pitch_y) */
+  double dt;       /* time step (c = 1, nm units)            */
+  double dl;       /* cell size (nm)                         */
+  int32_t axes;    /* 3-D only: DN_AXES_*                     */
+  int32_t pol;     /* 2-D only: DN_TM / DN_TE                 */
+} dn_grid;
+
+/* CPML profiles (FP64, device): index 0 = z (length D), 1 = y (H), 2 = x (W).
+ * b = exp(-(s+a)dt), c = s(b-1)/(s+a) as in fdtd2d.py:67-88.  2-D uses y, x. */
+typedef struct {
+  const double* b[3];
+  const double* c[3];
+} dn_cpml;
+
+/* soft source: after each full step, field[component][box] += wave[t]
+ * (fdtd2d.py:333,351; fdtd3d.py:502).  `wave` is indexed by the absolute
+ * step t and has the grid's dtype.  component = DN_NONE disables it. */
+typedef struct {
+  int32_t component;
+  dn_box box;
+  const void* wave;
+} dn_source;
+
+/* running-DFT monitor (extension, no reference counterpart):
+ * acc[f][cell][0..1] += v_t(cell) * phase[t][f][0..1] on every step t, where
+ * v_t is the component's value after step t (source included) and
+ * phase[t][f] = (cos(w_f t dt) dt, -sin(w_f t dt) dt).  Cells are the box's
+ * cells in (z, y, x) row-major order.  FP64 accumulators. */
+typedef struct {
+  int32_t component;
+  dn_box box;
+  int32_t n_freq;
+  const double* phase; /* [T][n_freq][2] device */
+  double* acc;         /* [n_freq][cells][2] device, caller zeroes it */
+} dn_monitor;
+
+/* single-cell probe (fdtd2d.py:335-337 snapshots, fdtd3d.py:698 time_series):
+ * out[t] = value of `component` at (pos[0], pos[1], pos[2]) = (z, y, x) after
+ * step t (source included).  `out` has the grid dtype and is indexed by the
+ * absolute step t.  component = DN_NONE disables it. */
+typedef struct {
+  int32_t component;
+  int32_t pos[3];
+  void* out;
+} dn_probe;
+
+/* ---- library information ------------------------------------------------ */
+const char* dn_strerror(int32_t status);
+int32_t dn_version(void);
+/* last CUDA error code seen by the library on this thread (0 if none) */
+int32_t dn_last_cuda_error(void);
+
+/* ---- forward time stepping --------------------------------------------- */
+/*
+ * Run `nsteps` leapfrog steps t = t0 .. t0+nsteps-1 of the 2-D TM/TE solver.
+ * Fields ping-pong: step t reads set `fa` when (t - t0) is even and writes
+ * `fb`, and the reverse when odd; *final_in_b tells where the result is.
+ * Field sets are 6 pointers indexed by DN_EX..DN_HZ; only the polarisation's
+ * three are used.  `ce` is the per-cell coefficient dt/eps_r (grid dtype,
+ * same layout as the fields).  `src`, `mons` and `probe` may be NULL.  `status`
+ * (device int32, may be NULL) receives device-side error codes and is never
+ * cleared by the library.
+ */
+int32_t dn_fdtd2d_run(const dn_grid* g, void* const fa[6], void* const fb[6], const void* ce,
+                      const dn_cpml* cpml, const dn_source* src, const dn_monitor* mons,
+                      int32_t n_mon, const dn_probe* probe, int32_t t0, int32_t nsteps,
+                      int32_t* status, void* stream, int32_t* final_in_b);
+
+/* 3-D analogue (all six components), same ping-pong and status contract. */
+int32_t dn_fdtd3d_run(const dn_grid* g, void* const fa[6], void* const fb[6], const void* ce,
+                      const dn_cpml* cpml, const dn_source* src, const dn_monitor* mons,
+                      int32_t n_mon, const dn_probe* probe, int32_t t0, int32_t nsteps,
+                      int32_t* status, void* stream, int32_t* final_in_b);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DN_FDTD_H */

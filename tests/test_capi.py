@@ -1,0 +1,111 @@
+"""The C-ABI library loads and exports every symbol include/*.h declares;
+argument validation rejects bad calls on the host (no GPU work)."""
+
+from __future__ import annotations
+
+import ctypes
+import glob
+import os
+import re
+
+import pytest
+from conftest import ROOT
+
+from diffnano_b200 import _lib
+
+
+def _declared_symbols():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names |= set(re.findall(r"\b(dn_[a-z0-9_]+)\s*\(", text))
+    return sorted(names)
+
+
+def test_library_exports_every_declared_symbol():
+    L = _lib.lib()
+    declared = _declared_symbols()
+    assert "dn_fdtd3d_run" in declared and "dn_fdtd2d_run" in declared
+    for name in declared:
+        assert hasattr(L, name), f"{name} declared in include/ but not exported"
+    assert set(declared) <= set(_lib.SIGNATURES), "ctypes signatures missing for some symbols"
+
+
+def test_strerror_and_version():
+    L = _lib.lib()
+    assert L.dn_version() >= 1
+    assert L.dn_strerror(_lib.DN_OK) == b"ok"
+    assert L.dn_strerror(_lib.DN_ETIMEOUT).startswith(b"bounded")
+    assert L.dn_strerror(12345) == b"unknown status"
+
+
+@pytest.mark.parametrize("fn", ["dn_fdtd2d_run", "dn_fdtd3d_run"])
+def test_null_grid_rejected(fn):
+    L = _lib.lib()
+    out = ctypes.c_int32(-1)
+    rc = getattr(L, fn)(None, None, None, None, None, None, None, 0, None, 0, 1, None, None,
+                        ctypes.byref(out))
+    assert rc == _lib.DN_EINVAL
+
+
+def _grid(**kw):
+    g = dict(D=1, H=8, W=8, dtype=_lib.DN_F32, pitch_y=32, pitch_z=256, dt=1.0, dl=2.0, axes=0,
+             pol=0)
+    g.update(kw)
+    return _lib.DnGrid(**g)
+
+
+@pytest.mark.parametrize("bad", [dict(H=0), dict(pitch_y=4), dict(dt=0.0), dict(dl=-1.0),
+                                 dict(dtype=7), dict(pol=9), dict(D=2)])
+def test_2d_bad_grid_rejected_before_any_launch(bad):
+    L = _lib.lib()
+    g = _grid(**bad)
+    fake = _lib.PTR6(*([16] * 6))  # never dereferenced: validation fails first
+    cp = _lib.DnCpml()
+    for a in range(3):
+        cp.b[a] = cp.c[a] = 16
+    out = ctypes.c_int32(-1)
+    rc = L.dn_fdtd2d_run(ctypes.byref(g), fake, fake, 16, ctypes.byref(cp), None, None, 0, None,
+                         0, 1, None, None, ctypes.byref(out))
+    assert rc == _lib.DN_EINVAL
+
+
+def test_3d_reference_axes_needs_cubic_grid():
+    L = _lib.lib()
+    g = _grid(D=4, H=8, W=8, pitch_z=256, axes=_lib.DN_AXES_REFERENCE)
+    fake = _lib.PTR6(*([256] * 6))
+    cp = _lib.DnCpml()
+    for a in range(3):
+        cp.b[a] = cp.c[a] = 256
+    out = ctypes.c_int32(-1)
+    rc = L.dn_fdtd3d_run(ctypes.byref(g), fake, fake, 256, ctypes.byref(cp), None, None, 0,
+                         None, 0, 1, None, None, ctypes.byref(out))
+    assert rc == _lib.DN_EINVAL
+
+
+def test_source_box_outside_grid_rejected():
+    L = _lib.lib()
+    g = _grid()
+    fake = _lib.PTR6(*([16] * 6))
+    cp = _lib.DnCpml()
+    for a in range(3):
+        cp.b[a] = cp.c[a] = 16
+    src = _lib.DnSource(component=_lib.DN_EZ, box=_lib.box((0, 0, 0), (1, 9, 8)), wave=16)
+    out = ctypes.c_int32(-1)
+    rc = L.dn_fdtd2d_run(ctypes.byref(g), fake, fake, 16, ctypes.byref(cp), ctypes.byref(src),
+                         None, 0, None, 0, 1, None, None, ctypes.byref(out))
+    assert rc == _lib.DN_EINVAL
+    # a TE-only component on a TM grid is rejected too
+    src = _lib.DnSource(component=_lib.DN_HZ, box=_lib.box((0, 0, 0), (1, 1, 1)), wave=16)
+    rc = L.dn_fdtd2d_run(ctypes.byref(g), fake, fake, 16, ctypes.byref(cp), ctypes.byref(src),
+                         None, 0, None, 0, 1, None, None, ctypes.byref(out))
+    assert rc == _lib.DN_EINVAL
+
+
+def test_check_maps_status_to_exceptions():
+    with pytest.raises(ValueError):
+        _lib.check("x", _lib.DN_EINVAL)
+    with pytest.raises(_lib.DNError):
+        _lib.check("x", _lib.DN_ETIMEOUT)
+    _lib.check("x", _lib.DN_OK)
