@@ -18,7 +18,8 @@ from oracle import fdtd_ref as R
 
 
 @pytest.mark.parametrize("name,courant,dl,T", [("tm2d_cfg0", 0.5, 20.0, 2000),
-                                               ("te2d", 0.5, 20.0, 300),
+                                               ("te2d", 0.5, 20.0, 40),
+                                               ("te2d_long", 0.5, 20.0, 300),
                                                ("tm2d_cont", 0.6, 15.0, 250)])
 def test_waveform_table_matches_reference(name, courant, dl, T):
     g = load_golden(name)

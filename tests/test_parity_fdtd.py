@@ -35,11 +35,14 @@ def test_tm2d_cfg0_vs_reference(cuda, dtype):
     assert rel_l2(series, g["series"]) < TOL[dtype]
 
 
-@pytest.mark.parametrize("dtype", DTYPES)
-def test_te2d_vs_reference(cuda, dtype):
-    g = load_golden("te2d")
-    s = dn.FDTDSolver2D(grid_shape=(48, 40), polarization="TE", pml_layers=6, n_steps=300,
-                        device=cuda, dtype=dtype)
+@pytest.mark.parametrize("name,dtype", [("te2d", torch.float32), ("te2d", torch.float64),
+                                        ("te2d_long", torch.float64)])
+def test_te2d_vs_reference(cuda, name, dtype):
+    """The reference's TE scheme grows exponentially (to ~1e87 in the long
+    fixture, beyond FP32's range), so FP32 is checked on the 40-step run."""
+    g = load_golden(name)
+    s = dn.FDTDSolver2D(grid_shape=(48, 40), polarization="TE", pml_layers=6,
+                        n_steps=int(g["n_steps"]), device=cuda, dtype=dtype)
     r = s.forward(torch.tensor(g["eps"]), source=dict(g["source"]))
     assert rel_l2(r.field[0], g["hz"]) < TOL[dtype]
     assert rel_l2(torch.stack(r.metadata["snapshots"]), g["series"]) < TOL[dtype]
@@ -153,10 +156,11 @@ def test_2d_monitors_vs_oracle(cuda, pol):
     comp = "Ez" if pol == "TM" else "Hz"
     wl = [1450.0, 1550.0, 1650.0]
     src = {"type": "gaussian_pulse", "row": 6}
+    T = 250 if pol == "TM" else 40  # the reference's TE scheme grows exponentially
     o = R.run_2d(eps, dl=15.0, dt=DT2(0.6, 15.0), omega=OMEGA, pml_layers=4, polarization=pol,
-                 n_steps=250, source=src,
+                 n_steps=T, source=src,
                  monitors=[dict(component=comp, box=((30, 31), (0, 36)), wavelengths_nm=wl)])
-    s = dn.FDTDSolver2D(grid_shape=(40, 36), polarization=pol, pml_layers=4, n_steps=250,
+    s = dn.FDTDSolver2D(grid_shape=(40, 36), polarization=pol, pml_layers=4, n_steps=T,
                         dl=15.0, courant=0.6, device=cuda, dtype=torch.float64)
     r = s.forward(eps, source=dict(src), monitors=[{"component": comp, "row": 30,
                                                     "wavelengths_nm": wl}])
