@@ -201,7 +201,8 @@ class Engine:
             _lib.check("device status", s)
 
     def monitor_dft(self, m: int) -> torch.Tensor:
-        """Complex ``(L, *box_shape)`` DFT of monitor ``m`` (FP64 -> complex128)."""
+        """Complex ``(L, *box_shape)`` DFT of monitor ``m`` (complex128); 2-D
+        boxes drop their z extent, so a 2-D shape is ``(L, rows, cols)``."""
         spec = self.monitors[m]
-        acc = self.accs[m]
-        return torch.view_as_complex(acc).reshape(len(spec.wavelengths), *spec.shape)
+        shape = spec.shape if self.is3d else spec.shape[1:]
+        return torch.view_as_complex(self.accs[m]).reshape(len(spec.wavelengths), *shape)
