@@ -33,7 +33,7 @@ sys.path.insert(0, ROOT)
 
 SHAPE = (256, 256, 256)
 DL, COURANT, PML, T_SOLVE = 25.0, 0.4, 12, 4000
-Z_SRC, Z_MON = 40, 200
+Z_SRC = 40
 BYTES_PER_CELL_STEP = 52  # FP32: read Ex Ey Ez Hx Hy Hz dt/eps, write the six fields
 WORKLOAD = "3d_yee_256cube_cpml12_fp32"
 METRIC = "FDTD Gcell-updates/s"
@@ -41,21 +41,25 @@ UNIT = "Gcell-updates/s"
 
 
 def workload():
+    """eps, source dict and monitor spec of the cubic grid SHAPE."""
     from diffnano_b200.workloads import gaussian_pulse_for_band, slab_eps_3d
 
+    n = SHAPE[0]
     eps = slab_eps_3d(SHAPE, dl=DL, design=(40, 128, 128), seed=1)
     src = gaussian_pulse_for_band(1550.0, 200.0)
     src.update(plane="xy", z=Z_SRC, component="Ex")
-    mons = [{"name": "out", "component": "Ey", "plane": "xy", "z": Z_MON,
-             "extent": [[96, 160], [96, 160]], "wavelengths_nm": [1550.0]}]
+    c = n // 2
+    mons = [{"name": "out", "component": "Ey", "plane": "xy", "z": n - 56,
+             "extent": [[c - 32, c + 32], [c - 32, c + 32]], "wavelengths_nm": [1550.0]}]
     return eps, src, mons
 
 
 def config_dict(extra=None):
-    c = {"workload": WORKLOAD, "grid": list(SHAPE), "dl_nm": DL, "pml_layers": PML,
+    c = {"workload": WORKLOAD if SHAPE[0] == 256 else f"3d_yee_{SHAPE[0]}cube_cpml12_fp32",
+         "grid": list(SHAPE), "dl_nm": DL, "pml_layers": PML,
          "courant": COURANT, "n_steps_per_solve": T_SOLVE,
          "source": "Ex plane-wave Gaussian pulse, 1550 nm, 200 nm band, plane z=40",
-         "monitor": "Ey DFT on a 64x64 plane at z=200, 1550 nm",
+         "monitor": f"Ey DFT on a 64x64 plane at z={SHAPE[0] - 56}, 1550 nm",
          "l2": "inputs larger than L2 (state 940 MB ping-pong + 67 MB coefficients)",
          "parallelism": "replicas (one independent grid per GPU)"}
     if extra:
@@ -336,7 +340,11 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--grid", type=int, default=256,
+                    help="cubic grid side (256 is the benchmark; smaller sides are for profiling)")
     args = ap.parse_args()
+    global SHAPE
+    SHAPE = (args.grid,) * 3
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":

@@ -59,11 +59,16 @@ struct alignas(64) TmapSet {
   CUtensorMap m[NARR];
 };
 
+// Work split: CTA b owns tile (b % ntiles) for z in [split*D/nsplit,
+// (split+1)*D/nsplit), split = b / ntiles.  Consecutive CTAs are neighbouring
+// tiles at the same z range, so CTAs that run together march through z in
+// lockstep and the halo rows/columns one CTA fetches are L2 hits for its
+// neighbours.
 struct Plan {
-  long long total;  // tile-planes
-  int chunk;        // planes per CTA range
-  int ntx;          // tiles along x
-  int maxj;         // job-list capacity
+  int ntx;     // tiles along x
+  int ntiles;  // tiles per plane
+  int nsplit;  // z ranges per tile
+  int maxj;    // job-list capacity
 };
 
 __device__ __forceinline__ long long fidx(const long long pz, const long long py, int i, int j,
@@ -99,19 +104,19 @@ __global__ void __launch_bounds__(NT3, Cfg<T>::MINB)
   const int D = p.D, H = p.H, W = p.W;
   const long long py = p.py, pz = p.pz;
   const T dt = p.dt, idl = p.inv_dl;
-  const long long L0 = (long long)blockIdx.x * plan.chunk;
-  const long long L1 = min(L0 + plan.chunk, plan.total);
+  const int tile = blockIdx.x % plan.ntiles;
+  const int split = blockIdx.x / plan.ntiles;
+  const int zA = (int)((long long)split * D / plan.nsplit);
+  const int zB = (int)((long long)(split + 1) * D / plan.nsplit);
 
   if (tid == 0) {
+    // jobs = planes whose inputs this CTA loads, in consumption order: the
+    // warm-up plane zA-1 (new Hx, Hy below the range), zA..zB-1, and plane zB
+    // (E only, for the forward differences of plane zB-1)
     int nj = 0;
-    for (long long L = L0; L < L1;) {
-      const int t = (int)(L / D), z0 = (int)(L % D);
-      const int z1 = (int)min((long long)D, z0 + (L1 - L));
-      if (z0 > 0) jobs[nj++] = make_int2(t, z0 - 1);
-      for (int z = z0; z < z1; ++z) jobs[nj++] = make_int2(t, z);
-      if (z1 < D) jobs[nj++] = make_int2(t, z1);
-      L += z1 - z0;
-    }
+    if (zA > 0) jobs[nj++] = make_int2(tile, zA - 1);
+    for (int z = zA; z < zB; ++z) jobs[nj++] = make_int2(tile, z);
+    if (zB < D) jobs[nj++] = make_int2(tile, zB);
     // a previous launch that recorded an error turns this one into a no-op
     const bool skip = p.status != nullptr && *reinterpret_cast<volatile int*>(p.status) != 0;
     s_nj = skip ? 0 : nj;
@@ -155,15 +160,13 @@ __global__ void __launch_bounds__(NT3, Cfg<T>::MINB)
   };
 
   bool failed = false;
-  for (long long L = nj > 0 ? L0 : L1; L < L1 && !failed;) {
-    const int t = (int)(L / D), z0 = (int)(L % D);
-    const int z1 = (int)min((long long)D, z0 + (L1 - L));
-    L += z1 - z0;
+  do {
+    if (nj == 0) break;
+    const int t = tile, z0 = zA, z1 = zB;
     const int tyi = t / plan.ntx, txi = t % plan.ntx;
     const int k0 = txi * TX, j0 = tyi * TY;
     const int kk = lane, k = k0 + kk;
 
-    __syncthreads();  // previous segment's readers of the tables are done
     for (int e = tid; e < TY + 2; e += NT3) {
       const int j = j0 - 1 + e;
       const bool ok = j >= 0 && j < H;
@@ -347,7 +350,7 @@ __global__ void __launch_bounds__(NT3, Cfg<T>::MINB)
       ++rel;
       ++q;
     }
-  }
+  } while (false);
 
   if (failed) {
     if (tid == 0) {
@@ -449,7 +452,7 @@ int run3d(const dn_grid* g, void* const fa[6], void* const fb[6], const void* ce
   Plan plan;
   plan.ntx = (g->W + TX - 1) / TX;
   const int nty = (g->H + TY - 1) / TY;
-  plan.total = (long long)plan.ntx * nty * g->D;
+  plan.ntiles = plan.ntx * nty;
 
   int dev = 0, nsm = 0;
   DN_CUDA_CHECK(cudaGetDevice(&dev));
@@ -458,13 +461,16 @@ int run3d(const dn_grid* g, void* const fa[6], void* const fb[6], const void* ce
   const size_t fixed = ((size_t)(C::S * C::STAGE_BYTES + C::SH_BYTES + C::TAB_BYTES + 15) / 16) *
                            16 +
                        C::S * sizeof(uint64_t) + 2 * sizeof(int) + 128;
-  const int per_sm = C::MINB;
-  long long nctas = (long long)nsm * per_sm;
-  long long chunk = (plan.total + nctas - 1) / nctas;
-  if (chunk < MIN_CHUNK) chunk = MIN_CHUNK;
-  nctas = (plan.total + chunk - 1) / chunk;
-  plan.chunk = (int)chunk;
-  plan.maxj = (int)(chunk + 2 * (chunk / g->D + 2));
+  // as many z ranges per tile as keep every CTA resident at once, each at
+  // least MIN_CHUNK planes long
+  const long long capacity = (long long)nsm * C::MINB;
+  long long nsplit = capacity / plan.ntiles;
+  if (nsplit > g->D / MIN_CHUNK) nsplit = g->D / MIN_CHUNK;
+  if (nsplit < 1) nsplit = 1;
+  plan.nsplit = (int)nsplit;
+  const long long nctas = (long long)plan.ntiles * nsplit;
+  if (nctas > 0x7fffffffLL) return DN_EUNSUPPORTED;
+  plan.maxj = (g->D + nsplit - 1) / nsplit + 2;
   const size_t smem = fixed + (size_t)plan.maxj * sizeof(int2);
   if (smem > 227 * 1024) return DN_EUNSUPPORTED;
 
