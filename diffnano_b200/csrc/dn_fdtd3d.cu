@@ -11,18 +11,22 @@
 //   DN_AXES_PHYSICAL   each profile indexed along its own axis.
 //
 // Design (memory bound, 52 B per cell-step in FP32: 7 arrays read, 6 written):
-//  * a CTA owns a 16 (y) x 32 (x) column of cells and marches along z over a
-//    contiguous range of planes; the ranges of all CTAs tile the
-//    (tile, plane) space evenly, so the persistent grid is balanced;
-//  * each plane's inputs (Ex, Ey, Ez, Hx, Hy, Hz, dt/eps) arrive by 3-D TMA
-//    boxes (x from k0-4 so the start is 16-byte aligned, y from j0-1) into a
-//    ring of shared-memory stages tracked by mbarriers, several planes ahead;
-//  * new H of the plane is computed for the tile plus the one-cell low halo
-//    (recomputed, not exchanged) into shared memory; new Hx, Hy of the plane
-//    below stay in registers (the z sliding window);
-//  * E of the plane is updated from those, the source and the running DFT
-//    monitors are applied in registers, and all six results are stored to the
-//    other ping-pong buffer (neighbouring CTAs still read the old one).
+//  * a CTA owns a 16 (y) x 32 (x) column of cells over a range of planes and
+//    marches along z; consecutive CTAs are neighbouring tiles over the same
+//    z range, so CTAs that run together stay in lockstep and the halo rows /
+//    columns one CTA fetches are L2 hits for its neighbours;
+//  * a producer warp streams each plane's inputs (Ex, Ey, Ez, Hx, Hy, Hz,
+//    dt/eps) with 3-D TMA boxes (x from k0-4 so the start is 16-byte aligned,
+//    y from j0-1) into a ring of shared-memory stages guarded by "full"
+//    (transaction-count) and "empty" (consumer-release) mbarriers, several
+//    planes ahead of the consumers;
+//  * eight consumer warps each own two rows of the tile and never synchronise
+//    with each other: a warp recomputes the new H of the row above its pair
+//    (instead of exchanging it), takes the x-1 neighbour by warp shuffle (two
+//    lanes compute the k0-1 halo column), keeps new Hx, Hy of the plane below
+//    in registers (the z sliding window), updates E, applies the source, DFT
+//    monitors and probe in registers, and stores all six results to the other
+//    ping-pong buffer (neighbouring CTAs still read the old one).
 #include <cuda.h>
 
 #include <mutex>
@@ -32,26 +36,25 @@
 namespace dn {
 namespace {
 
-constexpr int TX = 32;           // tile x (one warp)
-constexpr int TY = 16;           // tile y
-constexpr int NT3 = 256;         // 8 warps
-constexpr int RW = TY / 8;       // rows per thread
-constexpr int BX = TX + 8;       // box x: k0-4 .. k0+TX+3
-constexpr int BY = TY + 2;       // box y: j0-1 .. j0+TY
-constexpr int NARR = 7;          // Ex Ey Ez Hx Hy Hz ce
+constexpr int TX = 32;                // tile x (one warp)
+constexpr int TY = 16;                // tile y
+constexpr int NCW = TY / 2;           // consumer warps, two rows each
+constexpr int NT3 = (NCW + 1) * 32;   // + one producer warp
+constexpr int BX = TX + 8;            // box x: k0-4 .. k0+TX+3
+constexpr int BY = TY + 2;            // box y: j0-1 .. j0+TY
+constexpr int NARR = 7;               // Ex Ey Ez Hx Hy Hz ce
 constexpr int A_CE = 6;
-constexpr int MIN_CHUNK = 8;     // min planes per CTA range
-constexpr uint32_t WAIT_PROBES = 1u << 20;  // ~1 s of probing at most
+constexpr int MIN_CHUNK = 8;          // min planes per CTA range
+constexpr uint32_t WAIT_PROBES = 1u << 20;  // bound on mbarrier probes per wait
 
 template <typename T>
 struct Cfg {
-  static constexpr int S = sizeof(T) == 4 ? 4 : 3;  // stages
+  static constexpr int S = sizeof(T) == 4 ? 5 : 3;  // ring stages
   static constexpr int MINB = sizeof(T) == 4 ? 2 : 1;
   static constexpr int BOX_BYTES = BX * BY * (int)sizeof(T);
   static constexpr int ARR_BYTES = (BOX_BYTES + 127) / 128 * 128;
   static constexpr int STAGE_BYTES = NARR * ARR_BYTES;
   static constexpr int TX_BYTES = NARR * BOX_BYTES;
-  static constexpr int SH_BYTES = 3 * (TY + 1) * (TX + 1) * (int)sizeof(T);
   static constexpr int TAB_BYTES = (2 * (TY + 2) + 2 * (TX + 2)) * (int)sizeof(T);
 };
 
@@ -60,10 +63,7 @@ struct alignas(64) TmapSet {
 };
 
 // Work split: CTA b owns tile (b % ntiles) for z in [split*D/nsplit,
-// (split+1)*D/nsplit), split = b / ntiles.  Consecutive CTAs are neighbouring
-// tiles at the same z range, so CTAs that run together march through z in
-// lockstep and the halo rows/columns one CTA fetches are L2 hits for its
-// neighbours.
+// (split+1)*D/nsplit), split = b / ntiles.
 struct Plan {
   int ntx;     // tiles along x
   int ntiles;  // tiles per plane
@@ -71,9 +71,56 @@ struct Plan {
   int maxj;    // job-list capacity
 };
 
-__device__ __forceinline__ long long fidx(const long long pz, const long long py, int i, int j,
-                                          int k) {
-  return i * pz + j * py + k;
+constexpr unsigned FULL_MASK = 0xffffffffu;
+
+// bounded wait on an mbarrier phase that also gives up when another warp has
+// flagged an abort
+__device__ __forceinline__ bool wait_phase(uint64_t* bar, uint32_t parity, volatile int* abort) {
+  for (uint32_t n = 0; n < WAIT_PROBES; ++n) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((n & 63u) == 63u && *abort) return false;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// source / DFT monitors / probe on one cell's six new values (kept in
+// registers: components are selected, never indexed)
+template <typename T>
+__device__ __forceinline__ T pick(int c, T ex, T ey, T ez, T hx, T hy, T hz) {
+  return c == DN_EX ? ex : c == DN_EY ? ey : c == DN_EZ ? ez : c == DN_HX ? hx : c == DN_HY ? hy : hz;
+}
+
+template <typename T>
+__device__ __forceinline__ void special_cell(const StepParams<T>& p, int i, int j, int k, T& ex,
+                                             T& ey, T& ez, T& hx, T& hy, T& hz) {
+  if (p.src.comp >= 0 && p.src.box.contains(i, j, k)) {
+    const T w = p.src.wave[p.t];
+    const int c = p.src.comp;
+    ex += c == DN_EX ? w : T(0);
+    ey += c == DN_EY ? w : T(0);
+    ez += c == DN_EZ ? w : T(0);
+    hx += c == DN_HX ? w : T(0);
+    hy += c == DN_HY ? w : T(0);
+    hz += c == DN_HZ ? w : T(0);
+  }
+  for (int m = 0; m < p.n_mon; ++m) {
+    const MonDev& M = p.mon[m];
+    if (!M.box.contains(i, j, k)) continue;
+    const double x = static_cast<double>(pick(M.comp, ex, ey, ez, hx, hy, hz));
+    const long long cell = M.box.offset(i, j, k);
+    const double* ph = M.phase + (long long)p.t * M.nf * 2;
+    for (int f = 0; f < M.nf; ++f) {
+      double* a = M.acc + ((long long)f * M.ncell + cell) * 2;
+      a[0] = fma(x, ph[2 * f + 0], a[0]);
+      a[1] = fma(x, ph[2 * f + 1], a[1]);
+    }
+  }
+  if (p.probe.comp >= 0 && i == p.probe.pos[0] && j == p.probe.pos[1] && k == p.probe.pos[2])
+    p.probe.out[p.t] = pick(p.probe.comp, ex, ey, ez, hx, hy, hz);
 }
 
 template <typename T, int AXES>
@@ -86,19 +133,16 @@ __global__ void __launch_bounds__(NT3, Cfg<T>::MINB)
   unsigned char* smem = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~static_cast<uintptr_t>(127));
   unsigned char* stages = smem;
-  T* sHx = reinterpret_cast<T*>(smem + S * C::STAGE_BYTES);
-  T* sHy = sHx + (TY + 1) * (TX + 1);
-  T* sHz = sHy + (TY + 1) * (TX + 1);
-  T* sbJ = sHz + (TY + 1) * (TX + 1);
+  T* sbJ = reinterpret_cast<T*>(smem + S * C::STAGE_BYTES);
   T* sgJ = sbJ + (TY + 2);
   T* sbK = sgJ + (TY + 2);
   T* sgK = sbK + (TX + 2);
   uint64_t* full = reinterpret_cast<uint64_t*>(
-      smem + ((S * C::STAGE_BYTES + C::SH_BYTES + C::TAB_BYTES + 15) / 16) * 16);
-  int* s_flags = reinterpret_cast<int*>(full + S);  // [0] job count, [1] failure flag
+      smem + ((S * C::STAGE_BYTES + C::TAB_BYTES + 15) / 16) * 16);
+  uint64_t* empty = full + S;
+  int* s_flags = reinterpret_cast<int*>(empty + S);  // [0] job count, [1] abort flag
   int2* jobs = reinterpret_cast<int2*>(s_flags + 2);
-  int& s_nj = s_flags[0];
-  int& s_fail = s_flags[1];
+  volatile int* s_abort = s_flags + 1;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int D = p.D, H = p.H, W = p.W;
@@ -106,265 +150,273 @@ __global__ void __launch_bounds__(NT3, Cfg<T>::MINB)
   const T dt = p.dt, idl = p.inv_dl;
   const int tile = blockIdx.x % plan.ntiles;
   const int split = blockIdx.x / plan.ntiles;
-  const int zA = (int)((long long)split * D / plan.nsplit);
-  const int zB = (int)((long long)(split + 1) * D / plan.nsplit);
+  const int z0 = (int)((long long)split * D / plan.nsplit);
+  const int z1 = (int)((long long)(split + 1) * D / plan.nsplit);
+  const int tyi = tile / plan.ntx, txi = tile % plan.ntx;
+  const int k0 = txi * TX, j0 = tyi * TY;
 
   if (tid == 0) {
     // jobs = planes whose inputs this CTA loads, in consumption order: the
-    // warm-up plane zA-1 (new Hx, Hy below the range), zA..zB-1, and plane zB
-    // (E only, for the forward differences of plane zB-1)
+    // warm-up plane z0-1 (new Hx, Hy below the range), z0..z1-1, and plane z1
+    // (E only, for the forward z-differences of plane z1-1)
     int nj = 0;
-    if (zA > 0) jobs[nj++] = make_int2(tile, zA - 1);
-    for (int z = zA; z < zB; ++z) jobs[nj++] = make_int2(tile, z);
-    if (zB < D) jobs[nj++] = make_int2(tile, zB);
+    if (z0 > 0) jobs[nj++] = make_int2(tile, z0 - 1);
+    for (int z = z0; z < z1; ++z) jobs[nj++] = make_int2(tile, z);
+    if (z1 < D) jobs[nj++] = make_int2(tile, z1);
     // a previous launch that recorded an error turns this one into a no-op
     const bool skip = p.status != nullptr && *reinterpret_cast<volatile int*>(p.status) != 0;
-    s_nj = skip ? 0 : nj;
-    s_fail = 0;
-    for (int s = 0; s < S; ++s) mbar_init(&full[s], 1);
+    s_flags[0] = skip ? 0 : nj;
+    s_flags[1] = 0;
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], NCW);
+    }
     fence_barrier_init();
   }
-  __syncthreads();
-  const int nj = s_nj;
+  for (int e = tid; e < TY + 2; e += NT3) {
+    const int j = j0 - 1 + e;
+    const bool ok = j >= 0 && j < H;
+    sbJ[e] = ok ? static_cast<T>(p.b[1][j]) : T(1);
+    sgJ[e] = ok ? static_cast<T>(1.0 + p.c[1][j]) : T(1);
+  }
+  for (int e = tid; e < TX + 2; e += NT3) {
+    const int kx = k0 - 1 + e;
+    const bool ok = kx >= 0 && kx < W;
+    sbK[e] = ok ? static_cast<T>(p.b[2][kx]) : T(1);
+    sgK[e] = ok ? static_cast<T>(1.0 + p.c[2][kx]) : T(1);
+  }
+  __syncthreads();  // the only CTA-wide barrier
+  const int nj = s_flags[0];
+  if (nj == 0) return;
 
   auto stage_arr = [&](int q, int a) -> const T* {
     return reinterpret_cast<const T*>(stages + (q % S) * C::STAGE_BYTES + a * C::ARR_BYTES);
   };
-  auto issue = [&](int q) {
-    const int2 jb = jobs[q];
-    const int tyi = jb.x / plan.ntx, txi = jb.x % plan.ntx;
-    const int k0 = txi * TX, j0 = tyi * TY;
-    uint64_t* bar = &full[q % S];
-    fence_proxy_async_smem();
-    mbar_arrive_expect_tx(bar, C::TX_BYTES);
-    unsigned char* dst = stages + (q % S) * C::STAGE_BYTES;
-    for (int a = 0; a < NARR; ++a)
-      tma_load_3d(dst + a * C::ARR_BYTES, &tm.m[a], bar, k0 - 4, j0 - 1, jb.y);
-  };
 
-  int issued = 0, rel = 0, q = 0;
-  if (tid == 0)
-    for (; issued < min(nj, S); ++issued) issue(issued);
-
-  // wait for jobs q (and q+1); every thread waits so every thread acquires
-  // the TMA writes; any timeout makes the whole CTA leave together.
-  auto wait_jobs = [&](int qa, bool two) -> bool {
-    bool ok = mbar_wait_bounded(&full[qa % S], (qa / S) & 1, WAIT_PROBES);
-    if (two && ok) ok = mbar_wait_bounded(&full[(qa + 1) % S], ((qa + 1) / S) & 1, WAIT_PROBES);
-    if (!ok) s_fail = 1;
-    __syncthreads();
-    if (s_fail) return false;
-    if (tid == 0)
-      for (; issued < nj && issued < rel + S; ++issued) issue(issued);
-    return true;
-  };
-
-  bool failed = false;
-  do {
-    if (nj == 0) break;
-    const int t = tile, z0 = zA, z1 = zB;
-    const int tyi = t / plan.ntx, txi = t % plan.ntx;
-    const int k0 = txi * TX, j0 = tyi * TY;
-    const int kk = lane, k = k0 + kk;
-
-    for (int e = tid; e < TY + 2; e += NT3) {
-      const int j = j0 - 1 + e;
-      const bool ok = j >= 0 && j < H;
-      sbJ[e] = ok ? static_cast<T>(p.b[1][j]) : T(1);
-      sgJ[e] = ok ? static_cast<T>(1.0 + p.c[1][j]) : T(1);
+  // ======================= producer warp ====================================
+  if (warp == NCW) {
+    if (lane == 0) {
+      bool ok = true;
+      int issued = 0;
+      for (int q = 0; q < nj && ok; ++q) {
+        if (q >= S) ok = wait_phase(&empty[q % S], ((q / S) - 1) & 1, s_abort);
+        if (!ok) break;
+        const int2 jb = jobs[q];
+        uint64_t* bar = &full[q % S];
+        unsigned char* dst = stages + (q % S) * C::STAGE_BYTES;
+        fence_proxy_async_smem();
+        mbar_arrive_expect_tx(bar, C::TX_BYTES);
+        for (int a = 0; a < NARR; ++a)
+          tma_load_3d(dst + a * C::ARR_BYTES, &tm.m[a], bar, k0 - 4, j0 - 1, jb.y);
+        issued = q + 1;
+      }
+      // stay until the consumers released the last stages, so no copy can
+      // still be in flight when the CTA's shared memory is given back
+      for (int q = max(0, nj - S); q < nj && ok; ++q)
+        ok = wait_phase(&empty[q % S], (q / S) & 1, s_abort);
+      if (!ok) {
+        report_status(p.status, DN_ETIMEOUT);
+        *s_abort = 1;
+        for (int q = max(0, issued - S); q < issued; ++q)
+          (void)mbar_wait_bounded(&full[q % S], (q / S) & 1, WAIT_PROBES);
+      }
     }
-    for (int e = tid; e < TX + 2; e += NT3) {
-      const int kx = k0 - 1 + e;
-      const bool ok = kx >= 0 && kx < W;
-      sbK[e] = ok ? static_cast<T>(p.b[2][kx]) : T(1);
-      sgK[e] = ok ? static_cast<T>(1.0 + p.c[2][kx]) : T(1);
-    }
-    // (tables become visible at the next barrier inside wait_jobs)
-
-    T prevHx[RW], prevHy[RW];
-#pragma unroll
-    for (int r = 0; r < RW; ++r) prevHx[r] = prevHy[r] = T(0);
-
-    // ---- warm-up: new Hx, Hy of plane z0-1 for the owned cells -----------
-    if (z0 > 0) {
-      if (!wait_jobs(q, true)) {
-        failed = true;
-        break;
-      }
-      const int i = z0 - 1;
-      T bI = T(1), gI = T(1);
-      if (AXES == DN_AXES_PHYSICAL) {
-        bI = static_cast<T>(__ldg(p.b[0] + i));
-        gI = static_cast<T>(1.0 + __ldg(p.c[0] + i));
-      }
-      const T* cEx = stage_arr(q, DN_EX);
-      const T* cEy = stage_arr(q, DN_EY);
-      const T* cEz = stage_arr(q, DN_EZ);
-      const T* cHx = stage_arr(q, DN_HX);
-      const T* cHy = stage_arr(q, DN_HY);
-      const T* nEx = stage_arr(q + 1, DN_EX);
-      const T* nEy = stage_arr(q + 1, DN_EY);
-#pragma unroll
-      for (int r = 0; r < RW; ++r) {
-        const int jj = warp + 8 * r, j = j0 + jj;
-        if (j >= H || k >= W) continue;
-        const int e = (jj + 1) * BX + kk + 4;
-        const T bj = sbJ[jj + 1], gj = sgJ[jj + 1], bk = sbK[kk + 1], gk = sgK[kk + 1];
-        const T dEz_j = (j < H - 1) ? cEz[e + BX] - cEz[e] : T(0);
-        const T dEy_i = nEy[e] - cEy[e];
-        const T dEx_i = nEx[e] - cEx[e];
-        const T dEz_k = (k < W - 1) ? cEz[e + 1] - cEz[e] : T(0);
-        const T hx_g2 = AXES == DN_AXES_REFERENCE ? gk : gI;
-        const T hy_b = AXES == DN_AXES_REFERENCE ? bk : bI;
-        const T hy_g1 = AXES == DN_AXES_REFERENCE ? gk : gI;
-        const T hy_g2 = AXES == DN_AXES_REFERENCE ? gj : gk;
-        prevHx[r] = bj * cHx[e] - dt * (gj * (dEz_j * idl) - hx_g2 * (dEy_i * idl));
-        prevHy[r] = hy_b * cHy[e] - dt * (hy_g1 * (dEx_i * idl) - hy_g2 * (dEz_k * idl));
-      }
-      ++rel;
-      ++q;
-    }
-
-    // ---- march -----------------------------------------------------------
-    for (int i = z0; i < z1; ++i) {
-      const bool has_next = (i + 1 < D);
-      if (!wait_jobs(q, has_next)) {
-        failed = true;
-        break;
-      }
-      T bI = T(1), gI = T(1);
-      if (AXES == DN_AXES_PHYSICAL) {
-        bI = static_cast<T>(__ldg(p.b[0] + i));
-        gI = static_cast<T>(1.0 + __ldg(p.c[0] + i));
-      }
-      const T* cEx = stage_arr(q, DN_EX);
-      const T* cEy = stage_arr(q, DN_EY);
-      const T* cEz = stage_arr(q, DN_EZ);
-      const T* cHx = stage_arr(q, DN_HX);
-      const T* cHy = stage_arr(q, DN_HY);
-      const T* cHz = stage_arr(q, DN_HZ);
-      const T* cCe = stage_arr(q, A_CE);
-      const T* nEx = stage_arr(q + 1, DN_EX);
-      const T* nEy = stage_arr(q + 1, DN_EY);
-
-      // new H at one cell; `e` is its stage offset, (jt, kt) its table index
-      auto h_update = [&](int e, int j, int kx, int jt, int kt, bool want_hx, bool want_hy,
-                          bool want_hz, T& hx, T& hy, T& hz) {
-        const T bj = sbJ[jt], gj = sgJ[jt], bk = sbK[kt], gk = sgK[kt];
-        if (want_hx) {
-          const T dEz_j = (j < H - 1) ? cEz[e + BX] - cEz[e] : T(0);
-          const T dEy_i = has_next ? nEy[e] - cEy[e] : T(0);
-          const T g2 = AXES == DN_AXES_REFERENCE ? gk : gI;
-          hx = bj * cHx[e] - dt * (gj * (dEz_j * idl) - g2 * (dEy_i * idl));
-        }
-        if (want_hy) {
-          const T dEx_i = has_next ? nEx[e] - cEx[e] : T(0);
-          const T dEz_k = (kx < W - 1) ? cEz[e + 1] - cEz[e] : T(0);
-          const T b = AXES == DN_AXES_REFERENCE ? bk : bI;
-          const T g1 = AXES == DN_AXES_REFERENCE ? gk : gI;
-          const T g2 = AXES == DN_AXES_REFERENCE ? gj : gk;
-          hy = b * cHy[e] - dt * (g1 * (dEx_i * idl) - g2 * (dEz_k * idl));
-        }
-        if (want_hz) {
-          const T dEy_k = (kx < W - 1) ? cEy[e + 1] - cEy[e] : T(0);
-          const T dEx_j = (j < H - 1) ? cEx[e + BX] - cEx[e] : T(0);
-          hz = bk * cHz[e] - dt * (gk * (dEy_k * idl) - gj * (dEx_j * idl));
-        }
-      };
-
-      // ---- step A: new H of plane i (tile + low halo) -> shared -----------
-      T ownHx[RW], ownHy[RW], ownHz[RW];
-#pragma unroll
-      for (int r = 0; r < RW; ++r) {
-        const int jj = warp + 8 * r, j = j0 + jj;
-        ownHx[r] = ownHy[r] = ownHz[r] = T(0);
-        if (j < H && k < W)
-          h_update((jj + 1) * BX + kk + 4, j, k, jj + 1, kk + 1, true, true, true, ownHx[r],
-                   ownHy[r], ownHz[r]);
-        const int s = (jj + 1) * (TX + 1) + kk + 1;
-        sHx[s] = ownHx[r];
-        sHy[s] = ownHy[r];
-        sHz[s] = ownHz[r];
-      }
-      if (warp == 0) {  // row halo j0-1: Hx, Hz
-        T hx = T(0), hy = T(0), hz = T(0);
-        if (j0 > 0 && k < W) h_update(kk + 4, j0 - 1, k, 0, kk + 1, true, false, true, hx, hy, hz);
-        sHx[kk + 1] = hx;
-        sHz[kk + 1] = hz;
-      } else if (warp == 1 && lane < TY) {  // column halo k0-1: Hy, Hz
-        const int jj = lane, j = j0 + jj;
-        T hx = T(0), hy = T(0), hz = T(0);
-        if (k0 > 0 && j < H)
-          h_update((jj + 1) * BX + 3, j, k0 - 1, jj + 1, 0, false, true, true, hx, hy, hz);
-        sHy[(jj + 1) * (TX + 1)] = hy;
-        sHz[(jj + 1) * (TX + 1)] = hz;
-      }
-      __syncthreads();
-
-      // ---- step B: new E of plane i, source, monitors, stores ------------
-      const bool special = any_special(p, i);
-#pragma unroll
-      for (int r = 0; r < RW; ++r) {
-        const int jj = warp + 8 * r, j = j0 + jj;
-        if (j < H && k < W) {
-          const int e = (jj + 1) * BX + kk + 4;
-          const int s = (jj + 1) * (TX + 1) + kk + 1;
-          const T bj = sbJ[jj + 1], gj = sgJ[jj + 1], bk = sbK[kk + 1], gk = sgK[kk + 1];
-          const T ce = cCe[e];
-          const T hx = sHx[s], hy = sHy[s], hz = sHz[s];
-          const T dHz_j = (j > 0) ? hz - sHz[s - (TX + 1)] : T(0);
-          const T dHy_i = (i > 0) ? hy - prevHy[r] : T(0);
-          const T dHx_i = (i > 0) ? hx - prevHx[r] : T(0);
-          const T dHz_k = (k > 0) ? hz - sHz[s - 1] : T(0);
-          const T dHy_k = (k > 0) ? hy - sHy[s - 1] : T(0);
-          const T dHx_j = (j > 0) ? hx - sHx[s - (TX + 1)] : T(0);
-          T v[6];
-          if (AXES == DN_AXES_REFERENCE) {
-            v[DN_EX] = bj * bk * cEx[e] + ce * (gj * (dHz_j * idl) - gk * (dHy_i * idl));
-            v[DN_EY] = bk * bj * cEy[e] + ce * (gk * (dHx_i * idl) - gj * (dHz_k * idl));
-          } else {
-            v[DN_EX] = bj * bI * cEx[e] + ce * (gj * (dHz_j * idl) - gI * (dHy_i * idl));
-            v[DN_EY] = bI * bk * cEy[e] + ce * (gI * (dHx_i * idl) - gk * (dHz_k * idl));
-          }
-          v[DN_EZ] = bk * bj * cEz[e] + ce * (gk * (dHy_k * idl) - gj * (dHx_j * idl));
-          v[DN_HX] = hx;
-          v[DN_HY] = hy;
-          v[DN_HZ] = hz;
-          if (special) {
-            inject_source(p, i, j, k, v);
-            accumulate_monitors(p, i, j, k, v);
-            record_probe(p, i, j, k, v);
-          }
-          const long long o = fidx(pz, py, i, j, k);
-#pragma unroll
-          for (int a = 0; a < 6; ++a) p.out[a][o] = v[a];
-        }
-        prevHx[r] = ownHx[r];
-        prevHy[r] = ownHy[r];
-      }
-      ++rel;
-      ++q;
-    }
-    if (failed) break;
-    if (z1 < D) {  // the E-only job of plane z1 was consumed as "next"
-      ++rel;
-      ++q;
-    }
-  } while (false);
-
-  if (failed) {
-    if (tid == 0) {
-      report_status(p.status, DN_ETIMEOUT);
-      // let copies still in flight land before the CTA's shared memory goes
-      for (int qq = q; qq < issued; ++qq)
-        (void)mbar_wait_bounded(&full[qq % S], (qq / S) & 1, WAIT_PROBES);
-    }
-    __syncthreads();
+    return;
   }
+
+  // ======================= consumer warps ===================================
+  const int w = warp;
+  const int ja = j0 + 2 * w;  // first owned row; rows ja, ja+1 owned, ja-1 recomputed
+  const int k = k0 + lane;
+  const bool kin = k < W;
+  // K-profile coefficients of the own column and of the k0-1 halo column
+  const T bK = sbK[lane + 1], gK = sgK[lane + 1];
+  const T bKh = sbK[0], gKh = sgK[0];
+  // J-profile coefficients of rows ja-1, ja, ja+1 (table index 2w + r)
+  T bJ[3], gJ[3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    bJ[r] = sbJ[2 * w + r];
+    gJ[r] = sgJ[2 * w + r];
+  }
+  T prevHx[2] = {T(0), T(0)}, prevHy[2] = {T(0), T(0)};
+  int q = 0;
+  bool ok = true;
+
+  auto wait_full = [&](int qa) -> bool {
+    const bool r = wait_phase(&full[qa % S], (qa / S) & 1, s_abort);
+    __syncwarp();
+    return r;
+  };
+  auto release = [&](int qa) {
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[qa % S]);
+  };
+  auto fail = [&]() {
+    if (lane == 0) {
+      report_status(p.status, DN_ETIMEOUT);
+      *s_abort = 1;
+    }
+  };
+
+  // ---- warm-up: new Hx, Hy of plane z0-1 for the owned rows ----------------
+  if (z0 > 0) {
+    ok = wait_full(q) && wait_full(q + 1);
+    if (!ok) {
+      fail();
+      return;
+    }
+    T bI = T(1), gI = T(1);
+    if (AXES == DN_AXES_PHYSICAL) {
+      bI = static_cast<T>(__ldg(p.b[0] + (z0 - 1)));
+      gI = static_cast<T>(1.0 + __ldg(p.c[0] + (z0 - 1)));
+    }
+    const T* cEx = stage_arr(q, DN_EX);
+    const T* cEy = stage_arr(q, DN_EY);
+    const T* cEz = stage_arr(q, DN_EZ);
+    const T* cHx = stage_arr(q, DN_HX);
+    const T* cHy = stage_arr(q, DN_HY);
+    const T* nEx = stage_arr(q + 1, DN_EX);
+    const T* nEy = stage_arr(q + 1, DN_EY);
+#pragma unroll
+    for (int r = 1; r < 3; ++r) {
+      const int j = ja + r - 1;
+      const int e = (2 * w + r) * BX + lane + 4;
+      const T dEz_j = (j < H - 1) ? cEz[e + BX] - cEz[e] : T(0);
+      const T dEy_i = nEy[e] - cEy[e];
+      const T dEx_i = nEx[e] - cEx[e];
+      const T dEz_k = (k < W - 1) ? cEz[e + 1] - cEz[e] : T(0);
+      const T hx_g2 = AXES == DN_AXES_REFERENCE ? gK : gI;
+      const T hy_b = AXES == DN_AXES_REFERENCE ? bK : bI;
+      const T hy_g1 = AXES == DN_AXES_REFERENCE ? gK : gI;
+      const T hy_g2 = AXES == DN_AXES_REFERENCE ? gJ[r] : gK;
+      prevHx[r - 1] = bJ[r] * cHx[e] - dt * (gJ[r] * (dEz_j * idl) - hx_g2 * (dEy_i * idl));
+      prevHy[r - 1] = hy_b * cHy[e] - dt * (hy_g1 * (dEx_i * idl) - hy_g2 * (dEz_k * idl));
+    }
+    release(q);
+    ++q;
+  }
+
+  // ---- march -----------------------------------------------------------------
+  for (int i = z0; i < z1; ++i) {
+    const bool has_next = (i + 1 < D);
+    ok = wait_full(q) && (!has_next || wait_full(q + 1));
+    if (!ok) {
+      fail();
+      return;
+    }
+    T bI = T(1), gI = T(1);
+    if (AXES == DN_AXES_PHYSICAL) {
+      bI = static_cast<T>(__ldg(p.b[0] + i));
+      gI = static_cast<T>(1.0 + __ldg(p.c[0] + i));
+    }
+    const T* cEx = stage_arr(q, DN_EX);
+    const T* cEy = stage_arr(q, DN_EY);
+    const T* cEz = stage_arr(q, DN_EZ);
+    const T* cHx = stage_arr(q, DN_HX);
+    const T* cHy = stage_arr(q, DN_HY);
+    const T* cHz = stage_arr(q, DN_HZ);
+    const T* cCe = stage_arr(q, A_CE);
+    const T* nEx = stage_arr(q + 1, DN_EX);
+    const T* nEy = stage_arr(q + 1, DN_EY);
+
+    // coefficient roles that depend on the mapping
+    const T hx_g2 = AXES == DN_AXES_REFERENCE ? gK : gI;
+    const T hy_b = AXES == DN_AXES_REFERENCE ? bK : bI;
+    const T hy_g1 = AXES == DN_AXES_REFERENCE ? gK : gI;
+
+    // ---- new H of rows ja-1 (Hx, Hz), ja, ja+1 (all three) at column k ----
+    T Hx[3], Hy[3], Hz[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      const int j = ja + r - 1;
+      const int e = (2 * w + r) * BX + lane + 4;
+      const T ey = cEy[e], ex = cEx[e], ez = cEz[e];
+      const T dEz_j = (j < H - 1) ? cEz[e + BX] - ez : T(0);
+      const T dEy_i = has_next ? nEy[e] - ey : T(0);
+      Hx[r] = bJ[r] * cHx[e] - dt * (gJ[r] * (dEz_j * idl) - hx_g2 * (dEy_i * idl));
+      const T dEy_k = (k < W - 1) ? cEy[e + 1] - ey : T(0);
+      const T dEx_j = (j < H - 1) ? cEx[e + BX] - ex : T(0);
+      Hz[r] = bK * cHz[e] - dt * (gK * (dEy_k * idl) - gJ[r] * (dEx_j * idl));
+      if (r > 0) {
+        const T dEx_i = has_next ? nEx[e] - ex : T(0);
+        const T dEz_k = (k < W - 1) ? cEz[e + 1] - ez : T(0);
+        const T hy_g2 = AXES == DN_AXES_REFERENCE ? gJ[r] : gK;
+        Hy[r] = hy_b * cHy[e] - dt * (hy_g1 * (dEx_i * idl) - hy_g2 * (dEz_k * idl));
+      } else {
+        Hy[r] = T(0);
+      }
+    }
+
+    // ---- k0-1 halo column of rows ja, ja+1 (lanes 0 and 1) ----------------
+    T haloHy = T(0), haloHz = T(0);
+    if (lane < 2 && k0 > 0) {
+      const int r = 1 + lane;
+      const int j = ja + lane;
+      const int e = (2 * w + r) * BX + 3;
+      const T ex = cEx[e], ey = cEy[e], ez = cEz[e];
+      const T dEx_i = has_next ? nEx[e] - ex : T(0);
+      const T dEz_k = cEz[e + 1] - ez;
+      const T b = AXES == DN_AXES_REFERENCE ? bKh : bI;
+      const T g1 = AXES == DN_AXES_REFERENCE ? gKh : gI;
+      const T g2 = AXES == DN_AXES_REFERENCE ? gJ[r] : gKh;
+      haloHy = b * cHy[e] - dt * (g1 * (dEx_i * idl) - g2 * (dEz_k * idl));
+      const T dEy_k = cEy[e + 1] - ey;
+      const T dEx_j = (j < H - 1) ? cEx[e + BX] - ex : T(0);
+      haloHz = bKh * cHz[e] - dt * (gKh * (dEy_k * idl) - gJ[r] * (dEx_j * idl));
+    }
+    const T hHy[2] = {__shfl_sync(FULL_MASK, haloHy, 0), __shfl_sync(FULL_MASK, haloHy, 1)};
+    const T hHz[2] = {__shfl_sync(FULL_MASK, haloHz, 0), __shfl_sync(FULL_MASK, haloHz, 1)};
+
+    // ---- new E of rows ja, ja+1, source, monitors, stores -----------------
+    const bool special = any_special(p, i);
+#pragma unroll
+    for (int r = 1; r < 3; ++r) {
+      const int j = ja + r - 1;
+      T hyL = __shfl_up_sync(FULL_MASK, Hy[r], 1);
+      T hzL = __shfl_up_sync(FULL_MASK, Hz[r], 1);
+      if (lane == 0) {
+        hyL = hHy[r - 1];
+        hzL = hHz[r - 1];
+      }
+      if (j < H && kin) {
+        const int e = (2 * w + r) * BX + lane + 4;
+        const T ce = cCe[e];
+        const T dHz_j = (j > 0) ? Hz[r] - Hz[r - 1] : T(0);
+        const T dHx_j = (j > 0) ? Hx[r] - Hx[r - 1] : T(0);
+        const T dHy_i = (i > 0) ? Hy[r] - prevHy[r - 1] : T(0);
+        const T dHx_i = (i > 0) ? Hx[r] - prevHx[r - 1] : T(0);
+        const T dHz_k = (k > 0) ? Hz[r] - hzL : T(0);
+        const T dHy_k = (k > 0) ? Hy[r] - hyL : T(0);
+        T ex, ey;
+        if (AXES == DN_AXES_REFERENCE) {
+          ex = bJ[r] * bK * cEx[e] + ce * (gJ[r] * (dHz_j * idl) - gK * (dHy_i * idl));
+          ey = bK * bJ[r] * cEy[e] + ce * (gK * (dHx_i * idl) - gJ[r] * (dHz_k * idl));
+        } else {
+          ex = bJ[r] * bI * cEx[e] + ce * (gJ[r] * (dHz_j * idl) - gI * (dHy_i * idl));
+          ey = bI * bK * cEy[e] + ce * (gI * (dHx_i * idl) - gK * (dHz_k * idl));
+        }
+        T ez = bK * bJ[r] * cEz[e] + ce * (gK * (dHy_k * idl) - gJ[r] * (dHx_j * idl));
+        T hx = Hx[r], hy = Hy[r], hz = Hz[r];
+        if (special) special_cell(p, i, j, k, ex, ey, ez, hx, hy, hz);
+        const long long o = i * pz + j * py + k;
+        p.out[DN_EX][o] = ex;
+        p.out[DN_EY][o] = ey;
+        p.out[DN_EZ][o] = ez;
+        p.out[DN_HX][o] = hx;
+        p.out[DN_HY][o] = hy;
+        p.out[DN_HZ][o] = hz;
+      }
+      prevHx[r - 1] = Hx[r];
+      prevHy[r - 1] = Hy[r];
+    }
+    release(q);
+    ++q;
+  }
+  if (z1 < D) release(q);  // the E-only job of plane z1 was read as "next"
 }
 
 // ---------------------------------------------------------------------------
-// host side
 // ---------------------------------------------------------------------------
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
                                   const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
@@ -458,9 +510,8 @@ int run3d(const dn_grid* g, void* const fa[6], void* const fb[6], const void* ce
   DN_CUDA_CHECK(cudaGetDevice(&dev));
   DN_CUDA_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   // first guess of the shared-memory need, for the occupancy query
-  const size_t fixed = ((size_t)(C::S * C::STAGE_BYTES + C::SH_BYTES + C::TAB_BYTES + 15) / 16) *
-                           16 +
-                       C::S * sizeof(uint64_t) + 2 * sizeof(int) + 128;
+  const size_t fixed = ((size_t)(C::S * C::STAGE_BYTES + C::TAB_BYTES + 15) / 16) * 16 +
+                       2 * C::S * sizeof(uint64_t) + 2 * sizeof(int) + 128;
   // as many z ranges per tile as keep every CTA resident at once, each at
   // least MIN_CHUNK planes long
   const long long capacity = (long long)nsm * C::MINB;
