@@ -45,7 +45,8 @@ constexpr int BY = TY + 2;            // box y: j0-1 .. j0+TY
 constexpr int NARR = 7;               // Ex Ey Ez Hx Hy Hz ce
 constexpr int A_CE = 6;
 constexpr int MIN_CHUNK = 8;          // min planes per CTA range
-constexpr uint32_t WAIT_PROBES = 1u << 20;  // bound on mbarrier probes per wait
+constexpr uint32_t WAIT_PROBES = 1u << 16;  // bound on mbarrier probes per wait
+constexpr uint32_t SLEEP_NS = 20000;        // suspend-time hint per probe (~1.3 s bound)
 
 template <typename T>
 struct Cfg {
@@ -77,8 +78,8 @@ constexpr unsigned FULL_MASK = 0xffffffffu;
 // flagged an abort
 __device__ __forceinline__ bool wait_phase(uint64_t* bar, uint32_t parity, volatile int* abort) {
   for (uint32_t n = 0; n < WAIT_PROBES; ++n) {
-    if (mbar_try_wait(bar, parity)) return true;
-    if ((n & 63u) == 63u && *abort) return false;
+    if (mbar_try_wait_sleep(bar, parity, SLEEP_NS)) return true;
+    if ((n & 15u) == 15u && *abort) return false;
   }
   return false;
 }
@@ -226,22 +227,31 @@ __global__ void __launch_bounds__(NT3, Cfg<T>::MINB)
 
   // ======================= consumer warps ===================================
   const int w = warp;
-  const int ja = j0 + 2 * w;  // first owned row; rows ja, ja+1 owned, ja-1 recomputed
+  const int ja = j0 + 2 * w;  // rows ja, ja+1 are owned; row ja-1 is recomputed
   const int k = k0 + lane;
   const bool kin = k < W;
-  // K-profile coefficients of the own column and of the k0-1 halo column
+  const T dti = dt * idl;
+  // Per-lane coefficients with the boundary rules folded in: a forward
+  // difference on the last index and a backward difference on the first one
+  // get a zero coefficient.  The neighbour read there is a zero-filled TMA
+  // element or an in-range finite value, so 0 * value == 0 exactly.
   const T bK = sbK[lane + 1], gK = sgK[lane + 1];
   const T bKh = sbK[0], gKh = sgK[0];
-  // J-profile coefficients of rows ja-1, ja, ja+1 (table index 2w + r)
-  T bJ[3], gJ[3];
+  const T kf = (k < W - 1) ? T(1) : T(0);
+  const T kb = (k > 0) ? T(1) : T(0);
+  const T cKf = kf * dti * gK;  // dt (1+c_k)/dl on a forward x difference
+  const T cKb = kb * gK * idl;  // (1+c_k)/dl on a backward x difference
+  T bJ[3], gJ[3], cJf[3], cJb[3];
 #pragma unroll
   for (int r = 0; r < 3; ++r) {
+    const int j = ja + r - 1;
     bJ[r] = sbJ[2 * w + r];
     gJ[r] = sgJ[2 * w + r];
+    cJf[r] = (j < H - 1) ? dti * gJ[r] : T(0);  // dt (1+c_j)/dl, forward y
+    cJb[r] = (j > 0) ? gJ[r] * idl : T(0);       // (1+c_j)/dl, backward y
   }
   T prevHx[2] = {T(0), T(0)}, prevHy[2] = {T(0), T(0)};
   int q = 0;
-  bool ok = true;
 
   auto wait_full = [&](int qa) -> bool {
     const bool r = wait_phase(&full[qa % S], (qa / S) & 1, s_abort);
@@ -258,19 +268,33 @@ __global__ void __launch_bounds__(NT3, Cfg<T>::MINB)
       *s_abort = 1;
     }
   };
+  // coefficients of the z (i) roles: per lane for the reference mapping,
+  // per plane for the physical one
+  auto i_roles = [&](int i, T& hx_c2, T& hy_b, T& hy_c1, T& e_ci, T& bI) {
+    if (AXES == DN_AXES_REFERENCE) {
+      hx_c2 = dti * gK;
+      hy_b = bK;
+      hy_c1 = dti * gK;
+      e_ci = gK * idl;
+      bI = T(1);
+    } else {
+      bI = static_cast<T>(__ldg(p.b[0] + i));
+      const T gI = static_cast<T>(1.0 + __ldg(p.c[0] + i));
+      hx_c2 = dti * gI;
+      hy_b = bI;
+      hy_c1 = dti * gI;
+      e_ci = gI * idl;
+    }
+  };
 
   // ---- warm-up: new Hx, Hy of plane z0-1 for the owned rows ----------------
   if (z0 > 0) {
-    ok = wait_full(q) && wait_full(q + 1);
-    if (!ok) {
+    if (!(wait_full(q) && wait_full(q + 1))) {
       fail();
       return;
     }
-    T bI = T(1), gI = T(1);
-    if (AXES == DN_AXES_PHYSICAL) {
-      bI = static_cast<T>(__ldg(p.b[0] + (z0 - 1)));
-      gI = static_cast<T>(1.0 + __ldg(p.c[0] + (z0 - 1)));
-    }
+    T hx_c2, hy_b, hy_c1, e_ci, bI;
+    i_roles(z0 - 1, hx_c2, hy_b, hy_c1, e_ci, bI);
     const T* cEx = stage_arr(q, DN_EX);
     const T* cEy = stage_arr(q, DN_EY);
     const T* cEz = stage_arr(q, DN_EZ);
@@ -280,18 +304,11 @@ __global__ void __launch_bounds__(NT3, Cfg<T>::MINB)
     const T* nEy = stage_arr(q + 1, DN_EY);
 #pragma unroll
     for (int r = 1; r < 3; ++r) {
-      const int j = ja + r - 1;
       const int e = (2 * w + r) * BX + lane + 4;
-      const T dEz_j = (j < H - 1) ? cEz[e + BX] - cEz[e] : T(0);
-      const T dEy_i = nEy[e] - cEy[e];
-      const T dEx_i = nEx[e] - cEx[e];
-      const T dEz_k = (k < W - 1) ? cEz[e + 1] - cEz[e] : T(0);
-      const T hx_g2 = AXES == DN_AXES_REFERENCE ? gK : gI;
-      const T hy_b = AXES == DN_AXES_REFERENCE ? bK : bI;
-      const T hy_g1 = AXES == DN_AXES_REFERENCE ? gK : gI;
-      const T hy_g2 = AXES == DN_AXES_REFERENCE ? gJ[r] : gK;
-      prevHx[r - 1] = bJ[r] * cHx[e] - dt * (gJ[r] * (dEz_j * idl) - hx_g2 * (dEy_i * idl));
-      prevHy[r - 1] = hy_b * cHy[e] - dt * (hy_g1 * (dEx_i * idl) - hy_g2 * (dEz_k * idl));
+      const T hy_c2 = AXES == DN_AXES_REFERENCE ? kf * dti * gJ[r] : cKf;
+      const T ez = cEz[e];
+      prevHx[r - 1] = bJ[r] * cHx[e] - cJf[r] * (cEz[e + BX] - ez) + hx_c2 * (nEy[e] - cEy[e]);
+      prevHy[r - 1] = hy_b * cHy[e] - hy_c1 * (nEx[e] - cEx[e]) + hy_c2 * (cEz[e + 1] - ez);
     }
     release(q);
     ++q;
@@ -300,16 +317,13 @@ __global__ void __launch_bounds__(NT3, Cfg<T>::MINB)
   // ---- march -----------------------------------------------------------------
   for (int i = z0; i < z1; ++i) {
     const bool has_next = (i + 1 < D);
-    ok = wait_full(q) && (!has_next || wait_full(q + 1));
-    if (!ok) {
+    // plane i was already waited for as "next" unless it is the very first
+    if ((i == 0 && !wait_full(q)) || (has_next && !wait_full(q + 1))) {
       fail();
       return;
     }
-    T bI = T(1), gI = T(1);
-    if (AXES == DN_AXES_PHYSICAL) {
-      bI = static_cast<T>(__ldg(p.b[0] + i));
-      gI = static_cast<T>(1.0 + __ldg(p.c[0] + i));
-    }
+    T hx_c2, hy_b, hy_c1, e_ci, bI;
+    i_roles(i, hx_c2, hy_b, hy_c1, e_ci, bI);
     const T* cEx = stage_arr(q, DN_EX);
     const T* cEy = stage_arr(q, DN_EY);
     const T* cEz = stage_arr(q, DN_EZ);
@@ -317,32 +331,21 @@ __global__ void __launch_bounds__(NT3, Cfg<T>::MINB)
     const T* cHy = stage_arr(q, DN_HY);
     const T* cHz = stage_arr(q, DN_HZ);
     const T* cCe = stage_arr(q, A_CE);
-    const T* nEx = stage_arr(q + 1, DN_EX);
-    const T* nEy = stage_arr(q + 1, DN_EY);
-
-    // coefficient roles that depend on the mapping
-    const T hx_g2 = AXES == DN_AXES_REFERENCE ? gK : gI;
-    const T hy_b = AXES == DN_AXES_REFERENCE ? bK : bI;
-    const T hy_g1 = AXES == DN_AXES_REFERENCE ? gK : gI;
+    // on the last plane the forward z difference is 0: read "next" = current
+    const T* nEx = has_next ? stage_arr(q + 1, DN_EX) : cEx;
+    const T* nEy = has_next ? stage_arr(q + 1, DN_EY) : cEy;
 
     // ---- new H of rows ja-1 (Hx, Hz), ja, ja+1 (all three) at column k ----
     T Hx[3], Hy[3], Hz[3];
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
-      const int j = ja + r - 1;
       const int e = (2 * w + r) * BX + lane + 4;
       const T ey = cEy[e], ex = cEx[e], ez = cEz[e];
-      const T dEz_j = (j < H - 1) ? cEz[e + BX] - ez : T(0);
-      const T dEy_i = has_next ? nEy[e] - ey : T(0);
-      Hx[r] = bJ[r] * cHx[e] - dt * (gJ[r] * (dEz_j * idl) - hx_g2 * (dEy_i * idl));
-      const T dEy_k = (k < W - 1) ? cEy[e + 1] - ey : T(0);
-      const T dEx_j = (j < H - 1) ? cEx[e + BX] - ex : T(0);
-      Hz[r] = bK * cHz[e] - dt * (gK * (dEy_k * idl) - gJ[r] * (dEx_j * idl));
+      Hx[r] = bJ[r] * cHx[e] - cJf[r] * (cEz[e + BX] - ez) + hx_c2 * (nEy[e] - ey);
+      Hz[r] = bK * cHz[e] - cKf * (cEy[e + 1] - ey) + cJf[r] * (cEx[e + BX] - ex);
       if (r > 0) {
-        const T dEx_i = has_next ? nEx[e] - ex : T(0);
-        const T dEz_k = (k < W - 1) ? cEz[e + 1] - ez : T(0);
-        const T hy_g2 = AXES == DN_AXES_REFERENCE ? gJ[r] : gK;
-        Hy[r] = hy_b * cHy[e] - dt * (hy_g1 * (dEx_i * idl) - hy_g2 * (dEz_k * idl));
+        const T hy_c2 = AXES == DN_AXES_REFERENCE ? kf * dti * gJ[r] : cKf;
+        Hy[r] = hy_b * cHy[e] - hy_c1 * (nEx[e] - ex) + hy_c2 * (cEz[e + 1] - ez);
       } else {
         Hy[r] = T(0);
       }
@@ -352,21 +355,23 @@ __global__ void __launch_bounds__(NT3, Cfg<T>::MINB)
     T haloHy = T(0), haloHz = T(0);
     if (lane < 2 && k0 > 0) {
       const int r = 1 + lane;
-      const int j = ja + lane;
       const int e = (2 * w + r) * BX + 3;
       const T ex = cEx[e], ey = cEy[e], ez = cEz[e];
-      const T dEx_i = has_next ? nEx[e] - ex : T(0);
-      const T dEz_k = cEz[e + 1] - ez;
       const T b = AXES == DN_AXES_REFERENCE ? bKh : bI;
-      const T g1 = AXES == DN_AXES_REFERENCE ? gKh : gI;
-      const T g2 = AXES == DN_AXES_REFERENCE ? gJ[r] : gKh;
-      haloHy = b * cHy[e] - dt * (g1 * (dEx_i * idl) - g2 * (dEz_k * idl));
-      const T dEy_k = cEy[e + 1] - ey;
-      const T dEx_j = (j < H - 1) ? cEx[e + BX] - ex : T(0);
-      haloHz = bKh * cHz[e] - dt * (gKh * (dEy_k * idl) - gJ[r] * (dEx_j * idl));
+      const T c1 = AXES == DN_AXES_REFERENCE ? dti * gKh : hy_c1;
+      const T c2 = AXES == DN_AXES_REFERENCE ? dti * gJ[r] : dti * gKh;
+      haloHy = b * cHy[e] - c1 * (nEx[e] - ex) + c2 * (cEz[e + 1] - ez);
+      haloHz = bKh * cHz[e] - dti * gKh * (cEy[e + 1] - ey) + cJf[r] * (cEx[e + BX] - ex);
     }
-    const T hHy[2] = {__shfl_sync(FULL_MASK, haloHy, 0), __shfl_sync(FULL_MASK, haloHy, 1)};
-    const T hHz[2] = {__shfl_sync(FULL_MASK, haloHz, 0), __shfl_sync(FULL_MASK, haloHz, 1)};
+    const T hHy0 = __shfl_sync(FULL_MASK, haloHy, 0), hHy1 = __shfl_sync(FULL_MASK, haloHy, 1);
+    const T hHz0 = __shfl_sync(FULL_MASK, haloHz, 0), hHz1 = __shfl_sync(FULL_MASK, haloHz, 1);
+
+    if (i == 0) {  // the backward z difference is 0 on the first plane
+      prevHx[0] = Hx[1];
+      prevHx[1] = Hx[2];
+      prevHy[0] = Hy[1];
+      prevHy[1] = Hy[2];
+    }
 
     // ---- new E of rows ja, ja+1, source, monitors, stores -----------------
     const bool special = any_special(p, i);
@@ -376,27 +381,18 @@ __global__ void __launch_bounds__(NT3, Cfg<T>::MINB)
       T hyL = __shfl_up_sync(FULL_MASK, Hy[r], 1);
       T hzL = __shfl_up_sync(FULL_MASK, Hz[r], 1);
       if (lane == 0) {
-        hyL = hHy[r - 1];
-        hzL = hHz[r - 1];
+        hyL = r == 1 ? hHy0 : hHy1;
+        hzL = r == 1 ? hHz0 : hHz1;
       }
       if (j < H && kin) {
         const int e = (2 * w + r) * BX + lane + 4;
         const T ce = cCe[e];
-        const T dHz_j = (j > 0) ? Hz[r] - Hz[r - 1] : T(0);
-        const T dHx_j = (j > 0) ? Hx[r] - Hx[r - 1] : T(0);
-        const T dHy_i = (i > 0) ? Hy[r] - prevHy[r - 1] : T(0);
-        const T dHx_i = (i > 0) ? Hx[r] - prevHx[r - 1] : T(0);
-        const T dHz_k = (k > 0) ? Hz[r] - hzL : T(0);
-        const T dHy_k = (k > 0) ? Hy[r] - hyL : T(0);
-        T ex, ey;
-        if (AXES == DN_AXES_REFERENCE) {
-          ex = bJ[r] * bK * cEx[e] + ce * (gJ[r] * (dHz_j * idl) - gK * (dHy_i * idl));
-          ey = bK * bJ[r] * cEy[e] + ce * (gK * (dHx_i * idl) - gJ[r] * (dHz_k * idl));
-        } else {
-          ex = bJ[r] * bI * cEx[e] + ce * (gJ[r] * (dHz_j * idl) - gI * (dHy_i * idl));
-          ey = bI * bK * cEy[e] + ce * (gI * (dHx_i * idl) - gK * (dHz_k * idl));
-        }
-        T ez = bK * bJ[r] * cEz[e] + ce * (gK * (dHy_k * idl) - gJ[r] * (dHx_j * idl));
+        const T ex_b = AXES == DN_AXES_REFERENCE ? bJ[r] * bK : bJ[r] * bI;
+        const T ey_b = AXES == DN_AXES_REFERENCE ? bK * bJ[r] : bI * bK;
+        const T ey_c2 = AXES == DN_AXES_REFERENCE ? kb * gJ[r] * idl : cKb;
+        T ex = ex_b * cEx[e] + ce * (cJb[r] * (Hz[r] - Hz[r - 1]) - e_ci * (Hy[r] - prevHy[r - 1]));
+        T ey = ey_b * cEy[e] + ce * (e_ci * (Hx[r] - prevHx[r - 1]) - ey_c2 * (Hz[r] - hzL));
+        T ez = bK * bJ[r] * cEz[e] + ce * (cKb * (Hy[r] - hyL) - cJb[r] * (Hx[r] - Hx[r - 1]));
         T hx = Hx[r], hy = Hy[r], hz = Hz[r];
         if (special) special_cell(p, i, j, k, ex, ey, ez, hx, hy, hz);
         const long long o = i * pz + j * py + k;
