@@ -122,11 +122,15 @@ __device__ __forceinline__ void record_probe(const StepParams<T>& p, int i, int 
     p.probe.out[p.t] = v[p.probe.comp];
 }
 
+// Does plane i hold a source, monitor or probe cell?  (Unrolled over the
+// fixed monitor capacity so the parameter array is never indexed at run time,
+// which would move it to local memory.)
 template <typename T>
 __device__ __forceinline__ bool any_special(const StepParams<T>& p, int i) {
   bool any = p.src.comp >= 0 && p.src.box.has_plane(i);
   any |= p.probe.comp >= 0 && p.probe.pos[0] == i;
-  for (int m = 0; m < p.n_mon; ++m) any |= p.mon[m].box.has_plane(i);
+#pragma unroll
+  for (int m = 0; m < DN_MAX_MONITORS; ++m) any |= m < p.n_mon && p.mon[m].box.has_plane(i);
   return any;
 }
 

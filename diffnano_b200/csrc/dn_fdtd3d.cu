@@ -108,7 +108,9 @@ __device__ __forceinline__ void special_cell(const StepParams<T>& p, int i, int 
     hy += c == DN_HY ? w : T(0);
     hz += c == DN_HZ ? w : T(0);
   }
-  for (int m = 0; m < p.n_mon; ++m) {
+#pragma unroll
+  for (int m = 0; m < DN_MAX_MONITORS; ++m) {
+    if (m >= p.n_mon) break;
     const MonDev& M = p.mon[m];
     if (!M.box.contains(i, j, k)) continue;
     const double x = static_cast<double>(pick(M.comp, ex, ey, ez, hx, hy, hz));
@@ -193,6 +195,7 @@ __global__ void __launch_bounds__(NT3, Cfg<T>::MINB)
   auto stage_arr = [&](int q, int a) -> const T* {
     return reinterpret_cast<const T*>(stages + (q % S) * C::STAGE_BYTES + a * C::ARR_BYTES);
   };
+  constexpr int AE = C::ARR_BYTES / (int)sizeof(T);  // elements between staged arrays
 
   // ======================= producer warp ====================================
   if (warp == NCW) {
@@ -324,22 +327,26 @@ __global__ void __launch_bounds__(NT3, Cfg<T>::MINB)
     }
     T hx_c2, hy_b, hy_c1, e_ci, bI;
     i_roles(i, hx_c2, hy_b, hy_c1, e_ci, bI);
-    const T* cEx = stage_arr(q, DN_EX);
-    const T* cEy = stage_arr(q, DN_EY);
-    const T* cEz = stage_arr(q, DN_EZ);
-    const T* cHx = stage_arr(q, DN_HX);
-    const T* cHy = stage_arr(q, DN_HY);
-    const T* cHz = stage_arr(q, DN_HZ);
-    const T* cCe = stage_arr(q, A_CE);
-    // on the last plane the forward z difference is 0: read "next" = current
-    const T* nEx = has_next ? stage_arr(q + 1, DN_EX) : cEx;
-    const T* nEy = has_next ? stage_arr(q + 1, DN_EY) : cEy;
+    // this lane's element of row ja-1 in the stage of plane i and of plane i+1
+    // (on the last plane the forward z difference is 0: "next" = current);
+    // every other access is a compile-time offset from these two pointers
+    const T* cur = stage_arr(q, 0) + 2 * w * BX + lane + 4;
+    const T* nxt = has_next ? stage_arr(q + 1, 0) + 2 * w * BX + lane + 4 : cur;
+    const T* cEx = cur + DN_EX * AE;
+    const T* cEy = cur + DN_EY * AE;
+    const T* cEz = cur + DN_EZ * AE;
+    const T* cHx = cur + DN_HX * AE;
+    const T* cHy = cur + DN_HY * AE;
+    const T* cHz = cur + DN_HZ * AE;
+    const T* cCe = cur + A_CE * AE;
+    const T* nEx = nxt + DN_EX * AE;
+    const T* nEy = nxt + DN_EY * AE;
 
     // ---- new H of rows ja-1 (Hx, Hz), ja, ja+1 (all three) at column k ----
     T Hx[3], Hy[3], Hz[3];
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
-      const int e = (2 * w + r) * BX + lane + 4;
+      const int e = r * BX;
       const T ey = cEy[e], ex = cEx[e], ez = cEz[e];
       Hx[r] = bJ[r] * cHx[e] - cJf[r] * (cEz[e + BX] - ez) + hx_c2 * (nEy[e] - ey);
       Hz[r] = bK * cHz[e] - cKf * (cEy[e + 1] - ey) + cJf[r] * (cEx[e + BX] - ex);
@@ -355,7 +362,7 @@ __global__ void __launch_bounds__(NT3, Cfg<T>::MINB)
     T haloHy = T(0), haloHz = T(0);
     if (lane < 2 && k0 > 0) {
       const int r = 1 + lane;
-      const int e = (2 * w + r) * BX + 3;
+      const int e = r * BX - 1 - lane;  // column k0-1 of row ja-1+r (pointers sit at k0+lane)
       const T ex = cEx[e], ey = cEy[e], ez = cEz[e];
       const T b = AXES == DN_AXES_REFERENCE ? bKh : bI;
       const T c1 = AXES == DN_AXES_REFERENCE ? dti * gKh : hy_c1;
@@ -375,6 +382,7 @@ __global__ void __launch_bounds__(NT3, Cfg<T>::MINB)
 
     // ---- new E of rows ja, ja+1, source, monitors, stores -----------------
     const bool special = any_special(p, i);
+    const long long o_plane = i * pz + (long long)ja * py + k;
 #pragma unroll
     for (int r = 1; r < 3; ++r) {
       const int j = ja + r - 1;
@@ -385,7 +393,7 @@ __global__ void __launch_bounds__(NT3, Cfg<T>::MINB)
         hzL = r == 1 ? hHz0 : hHz1;
       }
       if (j < H && kin) {
-        const int e = (2 * w + r) * BX + lane + 4;
+        const int e = r * BX;
         const T ce = cCe[e];
         const T ex_b = AXES == DN_AXES_REFERENCE ? bJ[r] * bK : bJ[r] * bI;
         const T ey_b = AXES == DN_AXES_REFERENCE ? bK * bJ[r] : bI * bK;
@@ -395,7 +403,7 @@ __global__ void __launch_bounds__(NT3, Cfg<T>::MINB)
         T ez = bK * bJ[r] * cEz[e] + ce * (cKb * (Hy[r] - hyL) - cJb[r] * (Hx[r] - Hx[r - 1]));
         T hx = Hx[r], hy = Hy[r], hz = Hz[r];
         if (special) special_cell(p, i, j, k, ex, ey, ez, hx, hy, hz);
-        const long long o = i * pz + j * py + k;
+        const long long o = o_plane + (r - 1) * py;
         p.out[DN_EX][o] = ex;
         p.out[DN_EY][o] = ey;
         p.out[DN_EZ][o] = ez;
