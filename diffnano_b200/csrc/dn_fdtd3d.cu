@@ -361,14 +361,17 @@ __global__ void __launch_bounds__(NT3, Cfg<T>::MINB)
     // ---- k0-1 halo column of rows ja, ja+1 (lanes 0 and 1) ----------------
     T haloHy = T(0), haloHz = T(0);
     if (lane < 2 && k0 > 0) {
-      const int r = 1 + lane;
-      const int e = r * BX - 1 - lane;  // column k0-1 of row ja-1+r (pointers sit at k0+lane)
+      // lane 0 takes row ja, lane 1 row ja+1 (selected, not indexed, so the
+      // coefficient arrays stay in registers)
+      const T gJr = lane == 0 ? gJ[1] : gJ[2];
+      const T cJfr = lane == 0 ? cJf[1] : cJf[2];
+      const int e = (1 + lane) * BX - 1 - lane;  // column k0-1 (pointers sit at k0+lane)
       const T ex = cEx[e], ey = cEy[e], ez = cEz[e];
       const T b = AXES == DN_AXES_REFERENCE ? bKh : bI;
       const T c1 = AXES == DN_AXES_REFERENCE ? dti * gKh : hy_c1;
-      const T c2 = AXES == DN_AXES_REFERENCE ? dti * gJ[r] : dti * gKh;
+      const T c2 = AXES == DN_AXES_REFERENCE ? dti * gJr : dti * gKh;
       haloHy = b * cHy[e] - c1 * (nEx[e] - ex) + c2 * (cEz[e + 1] - ez);
-      haloHz = bKh * cHz[e] - dti * gKh * (cEy[e + 1] - ey) + cJf[r] * (cEx[e + BX] - ex);
+      haloHz = bKh * cHz[e] - dti * gKh * (cEy[e + 1] - ey) + cJfr * (cEx[e + BX] - ex);
     }
     const T hHy0 = __shfl_sync(FULL_MASK, haloHy, 0), hHy1 = __shfl_sync(FULL_MASK, haloHy, 1);
     const T hHz0 = __shfl_sync(FULL_MASK, haloHz, 0), hHz1 = __shfl_sync(FULL_MASK, haloHz, 1);
