@@ -55,6 +55,11 @@ class DnProbe(ctypes.Structure):
     _fields_ = [("component", c_int32), ("pos", c_int32 * 3), ("out", c_void_p)]
 
 
+class DnCurlRecord(ctypes.Structure):
+    _fields_ = [("curl", c_void_p * 3), ("step_stride", c_int64), ("t0", c_int32),
+                ("nslots", c_int32)]
+
+
 PTR6 = c_void_p * 6
 _P6 = ctypes.POINTER(c_void_p)  # a PTR6 instance (or None) is passed here
 
@@ -65,12 +70,22 @@ SIGNATURES = {
     "dn_last_cuda_error": (c_int32, []),
     "dn_fdtd2d_run": (c_int32, [ctypes.POINTER(DnGrid), _P6, _P6, c_void_p,
                                 ctypes.POINTER(DnCpml), ctypes.POINTER(DnSource),
-                                ctypes.POINTER(DnMonitor), c_int32, ctypes.POINTER(DnProbe), c_int32,
-                                c_int32, c_void_p, c_void_p, ctypes.POINTER(c_int32)]),
+                                ctypes.POINTER(DnMonitor), c_int32, ctypes.POINTER(DnProbe),
+                                ctypes.POINTER(DnCurlRecord), c_int32, c_int32, c_void_p,
+                                c_void_p, ctypes.POINTER(c_int32)]),
     "dn_fdtd3d_run": (c_int32, [ctypes.POINTER(DnGrid), _P6, _P6, c_void_p,
                                 ctypes.POINTER(DnCpml), ctypes.POINTER(DnSource),
-                                ctypes.POINTER(DnMonitor), c_int32, ctypes.POINTER(DnProbe), c_int32,
-                                c_int32, c_void_p, c_void_p, ctypes.POINTER(c_int32)]),
+                                ctypes.POINTER(DnMonitor), c_int32, ctypes.POINTER(DnProbe),
+                                ctypes.POINTER(DnCurlRecord), c_int32, c_int32, c_void_p,
+                                c_void_p, ctypes.POINTER(c_int32)]),
+    "dn_fdtd2d_adjoint": (c_int32, [ctypes.POINTER(DnGrid), _P6, _P6, c_void_p,
+                                    ctypes.POINTER(DnCpml), ctypes.POINTER(DnCurlRecord),
+                                    c_void_p, ctypes.POINTER(DnMonitor), c_int32, c_int32,
+                                    c_int32, c_void_p, c_void_p, ctypes.POINTER(c_int32)]),
+    "dn_fdtd3d_adjoint": (c_int32, [ctypes.POINTER(DnGrid), _P6, _P6, c_void_p,
+                                    ctypes.POINTER(DnCpml), ctypes.POINTER(DnCurlRecord),
+                                    c_void_p, ctypes.POINTER(DnMonitor), c_int32, c_int32,
+                                    c_int32, c_void_p, c_void_p, ctypes.POINTER(c_int32)]),
 }
 
 

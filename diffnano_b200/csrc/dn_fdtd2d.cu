@@ -30,8 +30,16 @@ constexpr int TI2 = 16;  // tile rows (y)
 constexpr int NT2 = 256;
 constexpr int R2 = TI2 / (NT2 / 32);  // rows per thread
 
-template <typename T, int POL>
-__global__ void __launch_bounds__(NT2) k_fdtd2d_step(const StepParams<T> p) {
+// curl record for the adjoint replay (see dn_curl_record)
+template <typename T>
+struct CurlRec2 {
+  T* curl[3];
+  long long stride;
+  int t0;
+};
+
+template <typename T, int POL, bool REC>
+__global__ void __launch_bounds__(NT2) k_fdtd2d_step(const StepParams<T> p, const CurlRec2<T> rec) {
   __shared__ T s_f[TI2 + 2][TJ2 + 2];
   __shared__ T s_a[TI2 + 1][TJ2 + 1];
   __shared__ T s_b[TI2 + 1][TJ2 + 1];
@@ -122,8 +130,15 @@ __global__ void __launch_bounds__(NT2) k_fdtd2d_step(const StepParams<T> p) {
         const T hz = s_f[ii + 1][jj + 1];
         const T dj = (j > 0) ? hz - s_f[ii + 1][jj] : T(0);
         const T di = (i > 0) ? hz - s_f[ii][jj + 1] : T(0);
-        a_own[r] = s_bx[jj + 1] * p.in[DN_EX][o] + ce * s_gx[jj + 1] * (dj * idl);
-        b_own[r] = s_by[ii + 1] * p.in[DN_EY][o] - ce * s_gy[ii + 1] * (di * idl);
+        const T curl_x = s_gx[jj + 1] * (dj * idl);
+        const T curl_y = -(s_gy[ii + 1] * (di * idl));
+        a_own[r] = s_bx[jj + 1] * p.in[DN_EX][o] + ce * curl_x;
+        b_own[r] = s_by[ii + 1] * p.in[DN_EY][o] + ce * curl_y;
+        if (REC) {
+          const long long oc = (long long)(p.t - rec.t0) * rec.stride + o;
+          rec.curl[0][oc] = curl_x;
+          rec.curl[1][oc] = curl_y;
+        }
       }
       s_a[ii][jj] = a_own[r];
       s_b[ii][jj] = b_own[r];
@@ -163,7 +178,9 @@ __global__ void __launch_bounds__(NT2) k_fdtd2d_step(const StepParams<T> p) {
     if (POL == DN_TM) {
       const T dHy = (i > 0) ? s_b[ii + 1][jj] - s_b[ii][jj] : T(0);
       const T dHx = (j > 0) ? s_a[ii][jj + 1] - s_a[ii][jj] : T(0);
-      v[DN_EZ] = bb * fo + p.ce[o] * (s_gx[jj + 1] * (dHy * idl) - s_gy[ii + 1] * (dHx * idl));
+      const T curl_z = s_gx[jj + 1] * (dHy * idl) - s_gy[ii + 1] * (dHx * idl);
+      v[DN_EZ] = bb * fo + p.ce[o] * curl_z;
+      if (REC) rec.curl[2][(long long)(p.t - rec.t0) * rec.stride + o] = curl_z;
       v[DN_HX] = a_own[r];
       v[DN_HY] = b_own[r];
       v[DN_HZ] = v[DN_EX] = v[DN_EY] = T(0);
@@ -193,21 +210,41 @@ __global__ void __launch_bounds__(NT2) k_fdtd2d_step(const StepParams<T> p) {
 template <typename T>
 int run2d(const dn_grid* g, void* const fa[6], void* const fb[6], const void* ce,
           const dn_cpml* cpml, const dn_source* src, const dn_monitor* mons, int32_t n_mon,
-          const dn_probe* probe, int32_t t0, int32_t nsteps, int32_t* status, void* stream, int32_t* final_in_b) {
+          const dn_probe* probe, const dn_curl_record* crec, int32_t t0, int32_t nsteps,
+          int32_t* status, void* stream, int32_t* final_in_b) {
   StepParams<T> p;
   int rc = build_params<T>(false, g, fa, fb, ce, cpml, src, mons, n_mon, probe, status, &p);
   if (rc != DN_OK) return rc;
   if (t0 < 0 || nsteps < 0 || !final_in_b) return DN_EINVAL;
+  CurlRec2<T> rec{};
+  const bool record = crec != nullptr;
+  if (record) {
+    const bool tm = g->pol == DN_TM;
+    if ((tm && !crec->curl[2]) || (!tm && (!crec->curl[0] || !crec->curl[1]))) return DN_EINVAL;
+    if (crec->step_stride < (int64_t)g->H * g->pitch_y || crec->t0 < 0 || t0 < crec->t0 ||
+        t0 + nsteps > crec->t0 + crec->nslots)
+      return DN_EINVAL;
+    for (int c = 0; c < 3; ++c) rec.curl[c] = static_cast<T*>(crec->curl[c]);
+    rec.stride = crec->step_stride;
+    rec.t0 = crec->t0;
+  }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const dim3 grid((g->W + TJ2 - 1) / TJ2, (g->H + TI2 - 1) / TI2);
   for (int n = 0; n < nsteps; ++n) {
     const bool even = (n % 2) == 0;
     set_io(&p, even ? fa : fb, even ? fb : fa);
     p.t = t0 + n;
-    if (g->pol == DN_TM)
-      k_fdtd2d_step<T, DN_TM><<<grid, NT2, 0, s>>>(p);
-    else
-      k_fdtd2d_step<T, DN_TE><<<grid, NT2, 0, s>>>(p);
+    if (g->pol == DN_TM) {
+      if (record)
+        k_fdtd2d_step<T, DN_TM, true><<<grid, NT2, 0, s>>>(p, rec);
+      else
+        k_fdtd2d_step<T, DN_TM, false><<<grid, NT2, 0, s>>>(p, rec);
+    } else {
+      if (record)
+        k_fdtd2d_step<T, DN_TE, true><<<grid, NT2, 0, s>>>(p, rec);
+      else
+        k_fdtd2d_step<T, DN_TE, false><<<grid, NT2, 0, s>>>(p, rec);
+    }
   }
   DN_CUDA_CHECK(cudaGetLastError());
   *final_in_b = nsteps % 2;
@@ -220,14 +257,15 @@ int run2d(const dn_grid* g, void* const fa[6], void* const fb[6], const void* ce
 extern "C" int32_t dn_fdtd2d_run(const dn_grid* g, void* const fa[6], void* const fb[6],
                                  const void* ce, const dn_cpml* cpml, const dn_source* src,
                                  const dn_monitor* mons, int32_t n_mon,
-                                 const dn_probe* probe, int32_t t0, int32_t nsteps,
-                                 int32_t* status, void* stream, int32_t* final_in_b) {
+                                 const dn_probe* probe, const dn_curl_record* rec, int32_t t0,
+                                 int32_t nsteps, int32_t* status, void* stream,
+                                 int32_t* final_in_b) {
   if (!g) return DN_EINVAL;
   if (g->dtype == DN_F32)
-    return dn::run2d<float>(g, fa, fb, ce, cpml, src, mons, n_mon, probe, t0, nsteps, status, stream,
+    return dn::run2d<float>(g, fa, fb, ce, cpml, src, mons, n_mon, probe, rec, t0, nsteps, status, stream,
                             final_in_b);
   if (g->dtype == DN_F64)
-    return dn::run2d<double>(g, fa, fb, ce, cpml, src, mons, n_mon, probe, t0, nsteps, status, stream,
+    return dn::run2d<double>(g, fa, fb, ce, cpml, src, mons, n_mon, probe, rec, t0, nsteps, status, stream,
                              final_in_b);
   return DN_EINVAL;
 }

@@ -10,83 +10,44 @@
 //                      every profile is indexed by j or k, none by i;
 //   DN_AXES_PHYSICAL   each profile indexed along its own axis.
 //
-// Design (memory bound, 52 B per cell-step in FP32: 7 arrays read, 6 written):
-//  * a CTA owns a 16 (y) x 32 (x) column of cells over a range of planes and
-//    marches along z; consecutive CTAs are neighbouring tiles over the same
-//    z range, so CTAs that run together stay in lockstep and the halo rows /
-//    columns one CTA fetches are L2 hits for its neighbours;
-//  * a producer warp streams each plane's inputs (Ex, Ey, Ez, Hx, Hy, Hz,
-//    dt/eps) with 3-D TMA boxes (x from k0-4 so the start is 16-byte aligned,
-//    y from j0-1) into a ring of shared-memory stages guarded by "full"
-//    (transaction-count) and "empty" (consumer-release) mbarriers, several
-//    planes ahead of the consumers;
-//  * eight consumer warps each own two rows of the tile and never synchronise
-//    with each other: a warp recomputes the new H of the row above its pair
-//    (instead of exchanging it), takes the x-1 neighbour by warp shuffle (two
-//    lanes compute the k0-1 halo column), keeps new Hx, Hy of the plane below
-//    in registers (the z sliding window), updates E, applies the source, DFT
-//    monitors and probe in registers, and stores all six results to the other
-//    ping-pong buffer (neighbouring CTAs still read the old one).
-#include <cuda.h>
-
-#include <mutex>
-
-#include "dn_host.cuh"
+// Design (memory bound, 52 B per cell-step in FP32: 7 arrays read, 6 written),
+// on the z-march pipeline of dn_zmarch.cuh:
+//  * a producer warp streams each plane's Ex, Ey, Ez, Hx, Hy, Hz and dt/eps
+//    into a ring of shared-memory stages with 3-D TMA boxes;
+//  * eight consumer warps each own two rows of the 16 x 32 tile and never
+//    synchronise with each other: a warp recomputes the new H of the row
+//    above its pair (instead of exchanging it), takes the x-1 neighbour by
+//    warp shuffle (two lanes compute the k0-1 halo column), keeps new Hx, Hy
+//    of the plane below in registers (the z sliding window), updates E,
+//    applies the source, DFT monitors and probe in registers, and stores all
+//    six results to the other ping-pong buffer (neighbouring CTAs still read
+//    the old one);
+//  * optionally (adjoint replay) the curl term of each E update is recorded.
+#include "dn_zmarch.cuh"
 
 namespace dn {
 namespace {
 
-constexpr int TX = 32;                // tile x (one warp)
-constexpr int TY = 16;                // tile y
-constexpr int NCW = TY / 2;           // consumer warps, two rows each
-constexpr int NT3 = (NCW + 1) * 32;   // + one producer warp
-constexpr int BX = TX + 8;            // box x: k0-4 .. k0+TX+3
-constexpr int BY = TY + 2;            // box y: j0-1 .. j0+TY
-constexpr int NARR = 7;               // Ex Ey Ez Hx Hy Hz ce
+using namespace zm;
+
+constexpr int NRING_F = 7;  // Ex Ey Ez Hx Hy Hz ce
 constexpr int A_CE = 6;
-constexpr int MIN_CHUNK = 8;          // min planes per CTA range
-constexpr uint32_t WAIT_PROBES = 1u << 16;  // bound on mbarrier probes per wait
-constexpr uint32_t SLEEP_NS = 20000;        // suspend-time hint per probe (~1.3 s bound)
 
 template <typename T>
-struct Cfg {
-  static constexpr int S = sizeof(T) == 4 ? 5 : 3;  // ring stages
+struct FwdCfg {
+  static constexpr int S = sizeof(T) == 4 ? 4 : 3;
   static constexpr int MINB = sizeof(T) == 4 ? 2 : 1;
-  static constexpr int BOX_BYTES = BX * BY * (int)sizeof(T);
-  static constexpr int ARR_BYTES = (BOX_BYTES + 127) / 128 * 128;
-  static constexpr int STAGE_BYTES = NARR * ARR_BYTES;
-  static constexpr int TX_BYTES = NARR * BOX_BYTES;
-  static constexpr int TAB_BYTES = (2 * (TY + 2) + 2 * (TX + 2)) * (int)sizeof(T);
+  using L = Layout<T, NRING_F, 0, S>;
 };
 
-struct alignas(64) TmapSet {
-  CUtensorMap m[NARR];
+// curl record for the adjoint replay: curl[c][slot * stride + cell] holds the
+// bracket term of the E_c update of step t0 + slot
+template <typename T>
+struct CurlRec {
+  T* curl[3];
+  long long stride;
+  int t0;
 };
-
-// Work split: CTA b owns tile (b % ntiles) for z in [split*D/nsplit,
-// (split+1)*D/nsplit), split = b / ntiles.
-struct Plan {
-  int ntx;     // tiles along x
-  int ntiles;  // tiles per plane
-  int nsplit;  // z ranges per tile
-  int maxj;    // job-list capacity
-};
-
-constexpr unsigned FULL_MASK = 0xffffffffu;
-
-// bounded wait on an mbarrier phase that also gives up when another warp has
-// flagged an abort
-__device__ __forceinline__ bool wait_phase(uint64_t* bar, uint32_t parity, volatile int* abort) {
-  for (uint32_t n = 0; n < WAIT_PROBES; ++n) {
-    if (mbar_try_wait_sleep(bar, parity, SLEEP_NS)) return true;
-    if ((n & 15u) == 15u && *abort) return false;
-  }
-  return false;
-}
-
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
 
 // source / DFT monitors / probe on one cell's six new values (kept in
 // registers: components are selected, never indexed)
@@ -126,109 +87,33 @@ __device__ __forceinline__ void special_cell(const StepParams<T>& p, int i, int 
     p.probe.out[p.t] = pick(p.probe.comp, ex, ey, ez, hx, hy, hz);
 }
 
-template <typename T, int AXES>
-__global__ void __launch_bounds__(NT3, Cfg<T>::MINB)
-    k_fdtd3d(const StepParams<T> p, const __grid_constant__ TmapSet tm, const Plan plan) {
-  using C = Cfg<T>;
-  constexpr int S = C::S;
+template <typename T, int AXES, bool REC>
+__global__ void __launch_bounds__(NT, FwdCfg<T>::MINB)
+    k_fdtd3d(const StepParams<T> p, const __grid_constant__ TmapSet tm, const Plan plan,
+             const CurlRec<T> rec) {
+  using L = typename FwdCfg<T>::L;
+  constexpr int S = L::S;
+  constexpr int AE = L::RING_ARR / (int)sizeof(T);  // elements between staged arrays
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  // TMA destinations must be 128-byte aligned: align the carve explicitly
-  unsigned char* smem = reinterpret_cast<unsigned char*>(
-      (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~static_cast<uintptr_t>(127));
-  unsigned char* stages = smem;
-  T* sbJ = reinterpret_cast<T*>(smem + S * C::STAGE_BYTES);
-  T* sgJ = sbJ + (TY + 2);
-  T* sbK = sgJ + (TY + 2);
-  T* sgK = sbK + (TX + 2);
-  uint64_t* full = reinterpret_cast<uint64_t*>(
-      smem + ((S * C::STAGE_BYTES + C::TAB_BYTES + 15) / 16) * 16);
-  uint64_t* empty = full + S;
-  int* s_flags = reinterpret_cast<int*>(empty + S);  // [0] job count, [1] abort flag
-  int2* jobs = reinterpret_cast<int2*>(s_flags + 2);
-  volatile int* s_abort = s_flags + 1;
-
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const Smem<T, L> sm(smem_raw);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int D = p.D, H = p.H, W = p.W;
   const long long py = p.py, pz = p.pz;
   const T dt = p.dt, idl = p.inv_dl;
-  const int tile = blockIdx.x % plan.ntiles;
-  const int split = blockIdx.x / plan.ntiles;
-  const int z0 = (int)((long long)split * D / plan.nsplit);
-  const int z1 = (int)((long long)(split + 1) * D / plan.nsplit);
-  const int tyi = tile / plan.ntx, txi = tile % plan.ntx;
-  const int k0 = txi * TX, j0 = tyi * TY;
+  const Range R(plan, D);
+  const int z0 = R.z0, z1 = R.z1, k0 = R.k0, j0 = R.j0;
 
-  if (tid == 0) {
-    // jobs = planes whose inputs this CTA loads, in consumption order: the
-    // warm-up plane z0-1 (new Hx, Hy below the range), z0..z1-1, and plane z1
-    // (E only, for the forward z-differences of plane z1-1)
-    int nj = 0;
-    if (z0 > 0) jobs[nj++] = make_int2(tile, z0 - 1);
-    for (int z = z0; z < z1; ++z) jobs[nj++] = make_int2(tile, z);
-    if (z1 < D) jobs[nj++] = make_int2(tile, z1);
-    // a previous launch that recorded an error turns this one into a no-op
-    const bool skip = p.status != nullptr && *reinterpret_cast<volatile int*>(p.status) != 0;
-    s_flags[0] = skip ? 0 : nj;
-    s_flags[1] = 0;
-    for (int s = 0; s < S; ++s) {
-      mbar_init(&full[s], 1);
-      mbar_init(&empty[s], NCW);
-    }
-    fence_barrier_init();
-  }
-  for (int e = tid; e < TY + 2; e += NT3) {
-    const int j = j0 - 1 + e;
-    const bool ok = j >= 0 && j < H;
-    sbJ[e] = ok ? static_cast<T>(p.b[1][j]) : T(1);
-    sgJ[e] = ok ? static_cast<T>(1.0 + p.c[1][j]) : T(1);
-  }
-  for (int e = tid; e < TX + 2; e += NT3) {
-    const int kx = k0 - 1 + e;
-    const bool ok = kx >= 0 && kx < W;
-    sbK[e] = ok ? static_cast<T>(p.b[2][kx]) : T(1);
-    sgK[e] = ok ? static_cast<T>(1.0 + p.c[2][kx]) : T(1);
-  }
-  __syncthreads();  // the only CTA-wide barrier
-  const int nj = s_flags[0];
+  const int nj = pipe_setup(sm, R, D, H, W, p.b, p.c, p.status);
   if (nj == 0) return;
 
-  auto stage_arr = [&](int q, int a) -> const T* {
-    return reinterpret_cast<const T*>(stages + (q % S) * C::STAGE_BYTES + a * C::ARR_BYTES);
-  };
-  constexpr int AE = C::ARR_BYTES / (int)sizeof(T);  // elements between staged arrays
-
-  // ======================= producer warp ====================================
-  if (warp == NCW) {
-    if (lane == 0) {
-      bool ok = true;
-      int issued = 0;
-      for (int q = 0; q < nj && ok; ++q) {
-        if (q >= S) ok = wait_phase(&empty[q % S], ((q / S) - 1) & 1, s_abort);
-        if (!ok) break;
-        const int2 jb = jobs[q];
-        uint64_t* bar = &full[q % S];
-        unsigned char* dst = stages + (q % S) * C::STAGE_BYTES;
-        fence_proxy_async_smem();
-        mbar_arrive_expect_tx(bar, C::TX_BYTES);
-        for (int a = 0; a < NARR; ++a)
-          tma_load_3d(dst + a * C::ARR_BYTES, &tm.m[a], bar, k0 - 4, j0 - 1, jb.y);
-        issued = q + 1;
-      }
-      // stay until the consumers released the last stages, so no copy can
-      // still be in flight when the CTA's shared memory is given back
-      for (int q = max(0, nj - S); q < nj && ok; ++q)
-        ok = wait_phase(&empty[q % S], (q / S) & 1, s_abort);
-      if (!ok) {
-        report_status(p.status, DN_ETIMEOUT);
-        *s_abort = 1;
-        for (int q = max(0, issued - S); q < issued; ++q)
-          (void)mbar_wait_bounded(&full[q % S], (q / S) & 1, WAIT_PROBES);
-      }
-    }
+  if (warp == NCW) {  // producer warp
+    if (lane == 0)
+      producer_run<T, L, NRING_F, 0>(sm, tm, R, nj, p.status, [](int) { return 0; });
     return;
   }
 
   // ======================= consumer warps ===================================
+  volatile int* s_abort = sm.flags + 1;
   const int w = warp;
   const int ja = j0 + 2 * w;  // rows ja, ja+1 are owned; row ja-1 is recomputed
   const int k = k0 + lane;
@@ -238,8 +123,8 @@ __global__ void __launch_bounds__(NT3, Cfg<T>::MINB)
   // difference on the last index and a backward difference on the first one
   // get a zero coefficient.  The neighbour read there is a zero-filled TMA
   // element or an in-range finite value, so 0 * value == 0 exactly.
-  const T bK = sbK[lane + 1], gK = sgK[lane + 1];
-  const T bKh = sbK[0], gKh = sgK[0];
+  const T bK = sm.sbK[lane + 1], gK = sm.sgK[lane + 1];
+  const T bKh = sm.sbK[0], gKh = sm.sgK[0];
   const T kf = (k < W - 1) ? T(1) : T(0);
   const T kb = (k > 0) ? T(1) : T(0);
   const T cKf = kf * dti * gK;  // dt (1+c_k)/dl on a forward x difference
@@ -248,8 +133,8 @@ __global__ void __launch_bounds__(NT3, Cfg<T>::MINB)
 #pragma unroll
   for (int r = 0; r < 3; ++r) {
     const int j = ja + r - 1;
-    bJ[r] = sbJ[2 * w + r];
-    gJ[r] = sgJ[2 * w + r];
+    bJ[r] = sm.sbJ[2 * w + r];
+    gJ[r] = sm.sgJ[2 * w + r];
     cJf[r] = (j < H - 1) ? dti * gJ[r] : T(0);  // dt (1+c_j)/dl, forward y
     cJb[r] = (j > 0) ? gJ[r] * idl : T(0);       // (1+c_j)/dl, backward y
   }
@@ -257,13 +142,13 @@ __global__ void __launch_bounds__(NT3, Cfg<T>::MINB)
   int q = 0;
 
   auto wait_full = [&](int qa) -> bool {
-    const bool r = wait_phase(&full[qa % S], (qa / S) & 1, s_abort);
+    const bool r = wait_phase(&sm.full[qa % S], (qa / S) & 1, s_abort);
     __syncwarp();
     return r;
   };
   auto release = [&](int qa) {
     __syncwarp();
-    if (lane == 0) mbar_arrive(&empty[qa % S]);
+    if (lane == 0) mbar_arrive(&sm.empty[qa % S]);
   };
   auto fail = [&]() {
     if (lane == 0) {
@@ -298,20 +183,18 @@ __global__ void __launch_bounds__(NT3, Cfg<T>::MINB)
     }
     T hx_c2, hy_b, hy_c1, e_ci, bI;
     i_roles(z0 - 1, hx_c2, hy_b, hy_c1, e_ci, bI);
-    const T* cEx = stage_arr(q, DN_EX);
-    const T* cEy = stage_arr(q, DN_EY);
-    const T* cEz = stage_arr(q, DN_EZ);
-    const T* cHx = stage_arr(q, DN_HX);
-    const T* cHy = stage_arr(q, DN_HY);
-    const T* nEx = stage_arr(q + 1, DN_EX);
-    const T* nEy = stage_arr(q + 1, DN_EY);
+    const T* cur = sm.arr(q, 0) + 2 * w * BX + lane + 4;
+    const T* nxt = sm.arr(q + 1, 0) + 2 * w * BX + lane + 4;
 #pragma unroll
     for (int r = 1; r < 3; ++r) {
-      const int e = (2 * w + r) * BX + lane + 4;
+      const int e = r * BX;
       const T hy_c2 = AXES == DN_AXES_REFERENCE ? kf * dti * gJ[r] : cKf;
-      const T ez = cEz[e];
-      prevHx[r - 1] = bJ[r] * cHx[e] - cJf[r] * (cEz[e + BX] - ez) + hx_c2 * (nEy[e] - cEy[e]);
-      prevHy[r - 1] = hy_b * cHy[e] - hy_c1 * (nEx[e] - cEx[e]) + hy_c2 * (cEz[e + 1] - ez);
+      const T ez = cur[DN_EZ * AE + e];
+      prevHx[r - 1] = bJ[r] * cur[DN_HX * AE + e] - cJf[r] * (cur[DN_EZ * AE + e + BX] - ez) +
+                      hx_c2 * (nxt[DN_EY * AE + e] - cur[DN_EY * AE + e]);
+      prevHy[r - 1] = hy_b * cur[DN_HY * AE + e] -
+                      hy_c1 * (nxt[DN_EX * AE + e] - cur[DN_EX * AE + e]) +
+                      hy_c2 * (cur[DN_EZ * AE + e + 1] - ez);
     }
     release(q);
     ++q;
@@ -327,11 +210,11 @@ __global__ void __launch_bounds__(NT3, Cfg<T>::MINB)
     }
     T hx_c2, hy_b, hy_c1, e_ci, bI;
     i_roles(i, hx_c2, hy_b, hy_c1, e_ci, bI);
-    // this lane's element of row ja-1 in the stage of plane i and of plane i+1
-    // (on the last plane the forward z difference is 0: "next" = current);
+    // this lane's element of row ja-1 in the stage of plane i and of plane
+    // i+1 (on the last plane the forward z difference is 0: "next" = current);
     // every other access is a compile-time offset from these two pointers
-    const T* cur = stage_arr(q, 0) + 2 * w * BX + lane + 4;
-    const T* nxt = has_next ? stage_arr(q + 1, 0) + 2 * w * BX + lane + 4 : cur;
+    const T* cur = sm.arr(q, 0) + 2 * w * BX + lane + 4;
+    const T* nxt = has_next ? sm.arr(q + 1, 0) + 2 * w * BX + lane + 4 : cur;
     const T* cEx = cur + DN_EX * AE;
     const T* cEy = cur + DN_EY * AE;
     const T* cEz = cur + DN_EZ * AE;
@@ -401,9 +284,12 @@ __global__ void __launch_bounds__(NT3, Cfg<T>::MINB)
         const T ex_b = AXES == DN_AXES_REFERENCE ? bJ[r] * bK : bJ[r] * bI;
         const T ey_b = AXES == DN_AXES_REFERENCE ? bK * bJ[r] : bI * bK;
         const T ey_c2 = AXES == DN_AXES_REFERENCE ? kb * gJ[r] * idl : cKb;
-        T ex = ex_b * cEx[e] + ce * (cJb[r] * (Hz[r] - Hz[r - 1]) - e_ci * (Hy[r] - prevHy[r - 1]));
-        T ey = ey_b * cEy[e] + ce * (e_ci * (Hx[r] - prevHx[r - 1]) - ey_c2 * (Hz[r] - hzL));
-        T ez = bK * bJ[r] * cEz[e] + ce * (cKb * (Hy[r] - hyL) - cJb[r] * (Hx[r] - Hx[r - 1]));
+        const T curl_x = cJb[r] * (Hz[r] - Hz[r - 1]) - e_ci * (Hy[r] - prevHy[r - 1]);
+        const T curl_y = e_ci * (Hx[r] - prevHx[r - 1]) - ey_c2 * (Hz[r] - hzL);
+        const T curl_z = cKb * (Hy[r] - hyL) - cJb[r] * (Hx[r] - Hx[r - 1]);
+        T ex = ex_b * cEx[e] + ce * curl_x;
+        T ey = ey_b * cEy[e] + ce * curl_y;
+        T ez = bK * bJ[r] * cEz[e] + ce * curl_z;
         T hx = Hx[r], hy = Hy[r], hz = Hz[r];
         if (special) special_cell(p, i, j, k, ex, ey, ez, hx, hy, hz);
         const long long o = o_plane + (r - 1) * py;
@@ -413,6 +299,12 @@ __global__ void __launch_bounds__(NT3, Cfg<T>::MINB)
         p.out[DN_HX][o] = hx;
         p.out[DN_HY][o] = hy;
         p.out[DN_HZ][o] = hz;
+        if (REC) {
+          const long long oc = (long long)(p.t - rec.t0) * rec.stride + o;
+          rec.curl[0][oc] = curl_x;
+          rec.curl[1][oc] = curl_y;
+          rec.curl[2][oc] = curl_z;
+        }
       }
       prevHx[r - 1] = Hx[r];
       prevHy[r - 1] = Hy[r];
@@ -424,52 +316,13 @@ __global__ void __launch_bounds__(NT3, Cfg<T>::MINB)
 }
 
 // ---------------------------------------------------------------------------
+// host side
 // ---------------------------------------------------------------------------
-typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
-                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
-                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
-                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiledFn get_encode() {
-  static EncodeTiledFn fn = nullptr;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    void* f = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) ==
-            cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<EncodeTiledFn>(f);
-  });
-  return fn;
-}
-
-template <typename T>
-int encode(CUtensorMap* m, const void* base, const dn_grid* g) {
-  EncodeTiledFn fn = get_encode();
-  if (!fn) return DN_ECUDA;
-  const cuuint64_t dims[3] = {(cuuint64_t)g->W, (cuuint64_t)g->H, (cuuint64_t)g->D};
-  const cuuint64_t strides[2] = {(cuuint64_t)g->pitch_y * sizeof(T),
-                                 (cuuint64_t)g->pitch_z * sizeof(T)};
-  const cuuint32_t box[3] = {BX, BY, 1};
-  const cuuint32_t es[3] = {1, 1, 1};
-  const CUresult r =
-      fn(m, sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
-         3, const_cast<void*>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) {
-    set_last_cuda_error(static_cast<int>(r));
-    return DN_ECUDA;
-  }
-  return DN_OK;
-}
-
-template <typename T, int AXES>
+template <typename T, int AXES, bool REC>
 int launch_all(const StepParams<T>& base, const TmapSet& ta, const TmapSet& tb, void* const fa[6],
                void* const fb[6], int t0, int nsteps, const Plan& plan, int nctas, size_t smem,
-               cudaStream_t s) {
-  auto kern = k_fdtd3d<T, AXES>;
+               const CurlRec<T>& rec, cudaStream_t s) {
+  auto kern = k_fdtd3d<T, AXES, REC>;
   DN_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)smem));
   StepParams<T> p = base;
@@ -477,7 +330,7 @@ int launch_all(const StepParams<T>& base, const TmapSet& ta, const TmapSet& tb, 
     const bool even = (n % 2) == 0;
     set_io(&p, even ? fa : fb, even ? fb : fa);
     p.t = t0 + n;
-    kern<<<nctas, NT3, smem, s>>>(p, even ? ta : tb, plan);
+    kern<<<nctas, NT, smem, s>>>(p, even ? ta : tb, plan, rec);
   }
   DN_CUDA_CHECK(cudaGetLastError());
   return DN_OK;
@@ -486,57 +339,64 @@ int launch_all(const StepParams<T>& base, const TmapSet& ta, const TmapSet& tb, 
 template <typename T>
 int run3d(const dn_grid* g, void* const fa[6], void* const fb[6], const void* ce,
           const dn_cpml* cpml, const dn_source* src, const dn_monitor* mons, int32_t n_mon,
-          const dn_probe* probe, int32_t t0, int32_t nsteps, int32_t* status, void* stream, int32_t* final_in_b) {
-  using C = Cfg<T>;
+          const dn_probe* probe, const dn_curl_record* crec, int32_t t0, int32_t nsteps,
+          int32_t* status, void* stream, int32_t* final_in_b) {
+  using L = typename FwdCfg<T>::L;
   StepParams<T> p;
   int rc = build_params<T>(true, g, fa, fb, ce, cpml, src, mons, n_mon, probe, status, &p);
   if (rc != DN_OK) return rc;
   if (t0 < 0 || nsteps < 0 || !final_in_b) return DN_EINVAL;
-  // TMA constraints: 16-byte aligned bases and byte strides
-  if ((g->pitch_y * (int64_t)sizeof(T)) % 16 || (g->pitch_z * (int64_t)sizeof(T)) % 16)
-    return DN_EINVAL;
-  for (int c = 0; c < 6; ++c)
-    if ((reinterpret_cast<uintptr_t>(fa[c]) | reinterpret_cast<uintptr_t>(fb[c])) & 15)
+  const void* ptrs[13];
+  for (int c = 0; c < 6; ++c) {
+    ptrs[c] = fa[c];
+    ptrs[6 + c] = fb[c];
+  }
+  ptrs[12] = ce;
+  if (!tma_ok(g, sizeof(T), ptrs, 13)) return DN_EINVAL;
+
+  CurlRec<T> rec{};
+  const bool record = crec != nullptr;
+  if (record) {
+    for (int c = 0; c < 3; ++c) {
+      if (!crec->curl[c]) return DN_EINVAL;
+      rec.curl[c] = static_cast<T*>(crec->curl[c]);
+    }
+    if (crec->step_stride < g->pitch_z * (int64_t)g->D || crec->t0 < 0 || t0 < crec->t0 ||
+        t0 + nsteps > crec->t0 + crec->nslots)
       return DN_EINVAL;
-  if (reinterpret_cast<uintptr_t>(ce) & 15) return DN_EINVAL;
+    rec.stride = crec->step_stride;
+    rec.t0 = crec->t0;
+  }
 
   TmapSet ta, tb;
   for (int c = 0; c < 6; ++c) {
-    if ((rc = encode<T>(&ta.m[c], fa[c], g)) != DN_OK) return rc;
-    if ((rc = encode<T>(&tb.m[c], fb[c], g)) != DN_OK) return rc;
+    if ((rc = encode_ring(&ta.m[c], fa[c], g, sizeof(T))) != DN_OK) return rc;
+    if ((rc = encode_ring(&tb.m[c], fb[c], g, sizeof(T))) != DN_OK) return rc;
   }
-  if ((rc = encode<T>(&ta.m[A_CE], ce, g)) != DN_OK) return rc;
+  if ((rc = encode_ring(&ta.m[A_CE], ce, g, sizeof(T))) != DN_OK) return rc;
   tb.m[A_CE] = ta.m[A_CE];
-
-  Plan plan;
-  plan.ntx = (g->W + TX - 1) / TX;
-  const int nty = (g->H + TY - 1) / TY;
-  plan.ntiles = plan.ntx * nty;
 
   int dev = 0, nsm = 0;
   DN_CUDA_CHECK(cudaGetDevice(&dev));
   DN_CUDA_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  // first guess of the shared-memory need, for the occupancy query
-  const size_t fixed = ((size_t)(C::S * C::STAGE_BYTES + C::TAB_BYTES + 15) / 16) * 16 +
-                       2 * C::S * sizeof(uint64_t) + 2 * sizeof(int) + 128;
-  // as many z ranges per tile as keep every CTA resident at once, each at
-  // least MIN_CHUNK planes long
-  const long long capacity = (long long)nsm * C::MINB;
-  long long nsplit = capacity / plan.ntiles;
-  if (nsplit > g->D / MIN_CHUNK) nsplit = g->D / MIN_CHUNK;
-  if (nsplit < 1) nsplit = 1;
-  plan.nsplit = (int)nsplit;
-  const long long nctas = (long long)plan.ntiles * nsplit;
+  long long nctas = 0;
+  const Plan plan = make_plan(g, (long long)nsm * FwdCfg<T>::MINB, &nctas);
   if (nctas > 0x7fffffffLL) return DN_EUNSUPPORTED;
-  plan.maxj = (g->D + nsplit - 1) / nsplit + 2;
-  const size_t smem = fixed + (size_t)plan.maxj * sizeof(int2);
+  const size_t smem = L::bytes(plan.maxj);
   if (smem > 227 * 1024) return DN_EUNSUPPORTED;
 
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int n = (int)nctas;
   if (g->axes == DN_AXES_REFERENCE)
-    rc = launch_all<T, DN_AXES_REFERENCE>(p, ta, tb, fa, fb, t0, nsteps, plan, (int)nctas, smem, s);
+    rc = record ? launch_all<T, DN_AXES_REFERENCE, true>(p, ta, tb, fa, fb, t0, nsteps, plan, n,
+                                                         smem, rec, s)
+                : launch_all<T, DN_AXES_REFERENCE, false>(p, ta, tb, fa, fb, t0, nsteps, plan, n,
+                                                          smem, rec, s);
   else
-    rc = launch_all<T, DN_AXES_PHYSICAL>(p, ta, tb, fa, fb, t0, nsteps, plan, (int)nctas, smem, s);
+    rc = record ? launch_all<T, DN_AXES_PHYSICAL, true>(p, ta, tb, fa, fb, t0, nsteps, plan, n,
+                                                        smem, rec, s)
+                : launch_all<T, DN_AXES_PHYSICAL, false>(p, ta, tb, fa, fb, t0, nsteps, plan, n,
+                                                         smem, rec, s);
   if (rc != DN_OK) return rc;
   *final_in_b = nsteps % 2;
   return DN_OK;
@@ -547,15 +407,15 @@ int run3d(const dn_grid* g, void* const fa[6], void* const fb[6], const void* ce
 
 extern "C" int32_t dn_fdtd3d_run(const dn_grid* g, void* const fa[6], void* const fb[6],
                                  const void* ce, const dn_cpml* cpml, const dn_source* src,
-                                 const dn_monitor* mons, int32_t n_mon,
-                                 const dn_probe* probe, int32_t t0, int32_t nsteps,
+                                 const dn_monitor* mons, int32_t n_mon, const dn_probe* probe,
+                                 const dn_curl_record* rec, int32_t t0, int32_t nsteps,
                                  int32_t* status, void* stream, int32_t* final_in_b) {
   if (!g) return DN_EINVAL;
   if (g->dtype == DN_F32)
-    return dn::run3d<float>(g, fa, fb, ce, cpml, src, mons, n_mon, probe, t0, nsteps, status, stream,
-                            final_in_b);
+    return dn::run3d<float>(g, fa, fb, ce, cpml, src, mons, n_mon, probe, rec, t0, nsteps, status,
+                            stream, final_in_b);
   if (g->dtype == DN_F64)
-    return dn::run3d<double>(g, fa, fb, ce, cpml, src, mons, n_mon, probe, t0, nsteps, status, stream,
-                             final_in_b);
+    return dn::run3d<double>(g, fa, fb, ce, cpml, src, mons, n_mon, probe, rec, t0, nsteps,
+                             status, stream, final_in_b);
   return DN_EINVAL;
 }

@@ -1,0 +1,243 @@
+// Shared machinery of the 3-D z-marching kernels (forward step and adjoint
+// step): tile geometry, the TMA tensor maps, the work split, the staged
+// shared-memory ring with its producer warp, and bounded mbarrier waits.
+//
+// A CTA owns a 16 (y) x 32 (x) tile over a range of z planes.  Per plane it
+// stages NRING arrays as 40 x 18 boxes (x from k0-4, y from j0-1: the tile
+// plus a one-cell ring, x start 16-byte aligned for TMA) and NTILE arrays as
+// 32 x 16 tile boxes, through a ring of S stages filled by one producer warp
+// and drained by eight consumer warps (two rows each).
+#pragma once
+
+#include <cuda.h>
+
+#include "dn_host.cuh"
+
+namespace dn {
+namespace zm {
+
+constexpr int TX = 32;               // tile x (one warp)
+constexpr int TY = 16;               // tile y
+constexpr int NCW = TY / 2;          // consumer warps, two rows each
+constexpr int NT = (NCW + 1) * 32;   // + one producer warp
+constexpr int BX = TX + 8;           // ring box x: k0-4 .. k0+TX+3
+constexpr int BY = TY + 2;           // ring box y: j0-1 .. j0+TY
+constexpr int MIN_CHUNK = 8;         // min planes per CTA range
+constexpr uint32_t WAIT_PROBES = 1u << 16;  // bound on mbarrier probes per wait
+constexpr uint32_t SLEEP_NS = 20000;        // suspend-time hint per probe (~1.3 s bound)
+constexpr unsigned FULL_MASK = 0xffffffffu;
+constexpr int MAX_MAPS = 10;
+
+// Shared-memory layout of one kernel configuration.
+template <typename T, int NRING, int NTILE, int S_>
+struct Layout {
+  static constexpr int S = S_;
+  static constexpr int RING_BYTES = BX * BY * (int)sizeof(T);
+  static constexpr int TILE_BYTES = TX * TY * (int)sizeof(T);
+  static constexpr int RING_ARR = (RING_BYTES + 127) / 128 * 128;
+  static constexpr int TILE_ARR = (TILE_BYTES + 127) / 128 * 128;
+  static constexpr int STAGE_BYTES = NRING * RING_ARR + NTILE * TILE_ARR;
+  static constexpr int TX_BYTES = NRING * RING_BYTES + NTILE * TILE_BYTES;
+  static constexpr int TAB_ELEMS = 2 * (TY + 2) + 2 * (TX + 2);
+  static constexpr int TAB_BYTES = TAB_ELEMS * (int)sizeof(T);
+  static constexpr int BAR_OFF = ((S * STAGE_BYTES + TAB_BYTES + 15) / 16) * 16;
+  // bytes of dynamic shared memory for a job list of `maxj` entries
+  static size_t bytes(int maxj) {
+    return (size_t)BAR_OFF + 2 * S * sizeof(uint64_t) + 2 * sizeof(int) +
+           (size_t)maxj * sizeof(int2) + 128;
+  }
+};
+
+struct alignas(64) TmapSet {
+  CUtensorMap m[MAX_MAPS];
+};
+
+// Work split: CTA b owns tile (b % ntiles) for z in [split*D/nsplit,
+// (split+1)*D/nsplit), split = b / ntiles.  Consecutive CTAs are neighbouring
+// tiles over the same z range, so CTAs that run together march through z in
+// lockstep and the halo rows/columns one CTA fetches are L2 hits for its
+// neighbours.
+struct Plan {
+  int ntx;     // tiles along x
+  int ntiles;  // tiles per plane
+  int nsplit;  // z ranges per tile
+  int maxj;    // job-list capacity
+};
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// bounded wait on an mbarrier phase that also gives up when another warp has
+// flagged an abort
+__device__ __forceinline__ bool wait_phase(uint64_t* bar, uint32_t parity, volatile int* abort) {
+  for (uint32_t n = 0; n < WAIT_PROBES; ++n) {
+    if (mbar_try_wait_sleep(bar, parity, SLEEP_NS)) return true;
+    if ((n & 15u) == 15u && *abort) return false;
+  }
+  return false;
+}
+
+// 4-D tiled TMA load (x, y, z, w); same alignment rule as the 3-D one.
+__device__ __forceinline__ void tma_load_4d(void* dst, const void* tmap, uint64_t* bar, int x,
+                                            int y, int z, int w) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4, %5, %6}], [%2];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(tmap)), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z), "r"(w)
+      : "memory");
+}
+
+// Pointers into the carved dynamic shared memory of one CTA.
+template <typename T, typename L>
+struct Smem {
+  unsigned char* stages;
+  T* sbJ;  // b_y of rows j0-1 .. j0+TY
+  T* sgJ;  // 1 + c_y of the same rows
+  T* sbK;  // b_x of columns k0-1 .. k0+TX
+  T* sgK;  // 1 + c_x of the same columns
+  uint64_t* full;
+  uint64_t* empty;
+  int* flags;  // [0] job count, [1] abort flag
+  int2* jobs;
+
+  __device__ explicit Smem(unsigned char* raw) {
+    // TMA destinations must be 128-byte aligned: align the carve explicitly
+    unsigned char* s = reinterpret_cast<unsigned char*>(
+        (reinterpret_cast<uintptr_t>(raw) + 127) & ~static_cast<uintptr_t>(127));
+    stages = s;
+    sbJ = reinterpret_cast<T*>(s + L::S * L::STAGE_BYTES);
+    sgJ = sbJ + (TY + 2);
+    sbK = sgJ + (TY + 2);
+    sgK = sbK + (TX + 2);
+    full = reinterpret_cast<uint64_t*>(s + L::BAR_OFF);
+    empty = full + L::S;
+    flags = reinterpret_cast<int*>(empty + L::S);
+    jobs = reinterpret_cast<int2*>(flags + 2);
+  }
+  // ring array a of job q's stage
+  __device__ const T* arr(int q, int a) const {
+    return reinterpret_cast<const T*>(stages + (q % L::S) * L::STAGE_BYTES + a * L::RING_ARR);
+  }
+  // tile array t (after the nring ring arrays) of job q's stage
+  __device__ const T* tile_arr(int q, int nring, int t) const {
+    return reinterpret_cast<const T*>(stages + (q % L::S) * L::STAGE_BYTES +
+                                      nring * L::RING_ARR + t * L::TILE_ARR);
+  }
+};
+
+// Per-CTA geometry derived from the plan.
+struct Range {
+  int tile, z0, z1, k0, j0;
+  __device__ Range(const Plan& plan, int D) {
+    tile = blockIdx.x % plan.ntiles;
+    const int split = blockIdx.x / plan.ntiles;
+    z0 = (int)((long long)split * D / plan.nsplit);
+    z1 = (int)((long long)(split + 1) * D / plan.nsplit);
+    k0 = (tile % plan.ntx) * TX;
+    j0 = (tile / plan.ntx) * TY;
+  }
+};
+
+// Thread 0 builds the job list (planes whose inputs this CTA stages, in
+// consumption order: warm-up plane z0-1, z0..z1-1, and plane z1 read only as
+// the "next" plane), initialises the barriers; all threads fill the CPML
+// profile tables of the tile.  Ends with the kernel's only CTA-wide barrier.
+// Returns the job count (0 when a previous launch recorded an error, which
+// turns this launch into a no-op).
+template <typename T, typename L>
+__device__ int pipe_setup(const Smem<T, L>& sm, const Range& R, int D, int H, int W,
+                          const double* const b[3], const double* const c[3],
+                          const int* status) {
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    int nj = 0;
+    if (R.z0 > 0) sm.jobs[nj++] = make_int2(R.tile, R.z0 - 1);
+    for (int z = R.z0; z < R.z1; ++z) sm.jobs[nj++] = make_int2(R.tile, z);
+    if (R.z1 < D) sm.jobs[nj++] = make_int2(R.tile, R.z1);
+    const bool skip = status != nullptr && *reinterpret_cast<const volatile int*>(status) != 0;
+    sm.flags[0] = skip ? 0 : nj;
+    sm.flags[1] = 0;
+    for (int s = 0; s < L::S; ++s) {
+      mbar_init(&sm.full[s], 1);
+      mbar_init(&sm.empty[s], NCW);
+    }
+    fence_barrier_init();
+  }
+  for (int e = tid; e < TY + 2; e += blockDim.x) {
+    const int j = R.j0 - 1 + e;
+    const bool ok = j >= 0 && j < H;
+    sm.sbJ[e] = ok ? static_cast<T>(b[1][j]) : T(1);
+    sm.sgJ[e] = ok ? static_cast<T>(1.0 + c[1][j]) : T(1);
+  }
+  for (int e = tid; e < TX + 2; e += blockDim.x) {
+    const int kx = R.k0 - 1 + e;
+    const bool ok = kx >= 0 && kx < W;
+    sm.sbK[e] = ok ? static_cast<T>(b[2][kx]) : T(1);
+    sm.sgK[e] = ok ? static_cast<T>(1.0 + c[2][kx]) : T(1);
+  }
+  __syncthreads();
+  return sm.flags[0];
+}
+
+// Producer (lane 0 of the last warp): stream job q's NRING ring boxes and
+// NTILE tile boxes into stage q % S once the consumers released the stage's
+// previous job; tile maps are 4-D (x, y, z, slot) with the slot coordinate
+// `tile_slot(z)`.  Stays until the consumers released the last stages so no
+// copy is still in flight when the shared memory is given back.
+template <typename T, typename L, int NRING, int NTILE, typename SlotFn>
+__device__ void producer_run(const Smem<T, L>& sm, const TmapSet& tm, const Range& R, int nj,
+                             int* status, SlotFn tile_slot) {
+  volatile int* abort = sm.flags + 1;
+  bool ok = true;
+  int issued = 0;
+  for (int q = 0; q < nj && ok; ++q) {
+    if (q >= L::S) ok = wait_phase(&sm.empty[q % L::S], ((q / L::S) - 1) & 1, abort);
+    if (!ok) break;
+    const int z = sm.jobs[q].y;
+    uint64_t* bar = &sm.full[q % L::S];
+    unsigned char* dst = sm.stages + (q % L::S) * L::STAGE_BYTES;
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(bar, L::TX_BYTES);
+#pragma unroll
+    for (int a = 0; a < NRING; ++a)
+      tma_load_3d(dst + a * L::RING_ARR, &tm.m[a], bar, R.k0 - 4, R.j0 - 1, z);
+#pragma unroll
+    for (int a = 0; a < NTILE; ++a)
+      tma_load_4d(dst + NRING * L::RING_ARR + a * L::TILE_ARR, &tm.m[NRING + a], bar, R.k0, R.j0,
+                  z, tile_slot(z));
+    issued = q + 1;
+  }
+  for (int q = max(0, nj - L::S); q < nj && ok; ++q)
+    ok = wait_phase(&sm.empty[q % L::S], (q / L::S) & 1, abort);
+  if (!ok) {
+    report_status(status, DN_ETIMEOUT);
+    *abort = 1;
+    for (int q = max(0, issued - L::S); q < issued; ++q)
+      (void)mbar_wait_bounded(&sm.full[q % L::S], (q / L::S) & 1, WAIT_PROBES);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host helpers
+// ---------------------------------------------------------------------------
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn get_encode();
+
+// ring (40 x 18 x 1) map over a (D, H, W) field with the grid's pitches
+int encode_ring(CUtensorMap* m, const void* base, const dn_grid* g, int elem_bytes);
+// tile (32 x 16 x 1 x 1) map over `nslots` fields of the grid's shape,
+// `slot_stride` elements apart
+int encode_tile4(CUtensorMap* m, const void* base, const dn_grid* g, int elem_bytes, int nslots,
+                 long long slot_stride);
+// work split for `capacity` resident CTAs
+Plan make_plan(const dn_grid* g, long long capacity, long long* nctas);
+// TMA constraints: 16-byte aligned bases and byte strides
+bool tma_ok(const dn_grid* g, int elem_bytes, const void* const* ptrs, int n);
+
+}  // namespace zm
+}  // namespace dn

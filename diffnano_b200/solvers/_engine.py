@@ -173,8 +173,13 @@ class Engine:
     def _ptrs(t: torch.Tensor):
         return _lib.PTR6(*[t[c].data_ptr() for c in range(6)])
 
-    def run(self, t0: int, nsteps: int) -> None:
-        """Advance ``nsteps`` steps starting at absolute step ``t0``."""
+    def run(self, t0: int, nsteps: int, record=None, outputs: bool = True) -> None:
+        """Advance ``nsteps`` steps starting at absolute step ``t0``.
+
+        ``record`` (a ``DnCurlRecord``) stores each step's curl terms for the
+        adjoint; ``outputs=False`` skips the monitors and the probe (used when
+        a segment is replayed for the adjoint, whose DFTs are already known).
+        """
         if nsteps <= 0:
             return
         if t0 + nsteps > self.n_steps:
@@ -183,16 +188,61 @@ class Engine:
         fa, fb = (self.B, self.A) if self.cur_b else (self.A, self.B)
         out = ctypes.c_int32(0)
         fn_name = "dn_fdtd3d_run" if self.is3d else "dn_fdtd2d_run"
+        no_probe = _lib.DnProbe(component=_lib.DN_NONE)
         with torch.cuda.device(self.device):
             stream = torch.cuda.current_stream(self.device).cuda_stream
             rc = getattr(L, fn_name)(
                 ctypes.byref(self.grid), self._ptrs(fa), self._ptrs(fb), self.ce.data_ptr(),
-                ctypes.byref(self.cpml), ctypes.byref(self.src), self.mon_arr, len(self.monitors),
-                ctypes.byref(self.probe), int(t0), int(nsteps), self.status.data_ptr(),
-                ctypes.c_void_p(stream), ctypes.byref(out))
+                ctypes.byref(self.cpml), ctypes.byref(self.src), self.mon_arr,
+                len(self.monitors) if outputs else 0,
+                ctypes.byref(self.probe if outputs else no_probe),
+                ctypes.byref(record) if record is not None else None, int(t0), int(nsteps),
+                self.status.data_ptr(), ctypes.c_void_p(stream), ctypes.byref(out))
         _lib.check(fn_name, rc)
         if out.value:
             self.cur_b = not self.cur_b
+
+    # ------------------------------------------------------------------
+    # adjoint support
+    # ------------------------------------------------------------------
+    def eps_components(self):
+        """Components whose update carries dt/eps (and so a curl record)."""
+        if self.is3d:
+            return (_lib.DN_EX, _lib.DN_EY, _lib.DN_EZ)
+        return (_lib.DN_EZ,) if self.pol == _lib.DN_TM else (_lib.DN_EX, _lib.DN_EY)
+
+    def curl_buffer(self, nslots: int) -> torch.Tensor:
+        """``(3, nslots, D, H, Wp)`` curl storage (only the slots of the
+        components that carry eps are written)."""
+        D, H, _ = self.shape3
+        ncomp = 3 if self.is3d else len(self.eps_components())
+        return torch.empty((ncomp, nslots, D, H, self.Wp), dtype=self.dtype, device=self.device)
+
+    def curl_record(self, buf: torch.Tensor, t0: int, nslots: int):
+        rec = _lib.DnCurlRecord(step_stride=buf.shape[2] * buf.shape[3] * buf.shape[4], t0=int(t0),
+                                nslots=int(nslots))
+        comps = self.eps_components()
+        for n, c in enumerate(comps):
+            slot = c if self.is3d else (2 if c == _lib.DN_EZ else c)
+            rec.curl[slot] = buf[n].data_ptr()
+        return rec
+
+    def adjoint(self, la: torch.Tensor, lb: torch.Tensor, rec, grad_ce: torch.Tensor, mon_arr,
+                n_mon: int, t_end: int, nsteps: int) -> bool:
+        """Reverse steps t_end-1 .. t_end-nsteps on adjoint sets la/lb (la
+        holds the current adjoint).  Returns True when the result ends in lb."""
+        L = _lib.lib()
+        out = ctypes.c_int32(0)
+        fn_name = "dn_fdtd3d_adjoint" if self.is3d else "dn_fdtd2d_adjoint"
+        with torch.cuda.device(self.device):
+            stream = torch.cuda.current_stream(self.device).cuda_stream
+            rc = getattr(L, fn_name)(
+                ctypes.byref(self.grid), self._ptrs(la), self._ptrs(lb), self.ce.data_ptr(),
+                ctypes.byref(self.cpml), ctypes.byref(rec), grad_ce.data_ptr(), mon_arr,
+                int(n_mon), int(t_end), int(nsteps), self.status.data_ptr(),
+                ctypes.c_void_p(stream), ctypes.byref(out))
+        _lib.check(fn_name, rc)
+        return bool(out.value)
 
     def check_status(self) -> None:
         """Raise if a kernel recorded a device-side error (synchronises)."""

@@ -120,6 +120,19 @@ typedef struct {
   void* out;
 } dn_probe;
 
+/* curl record (forward replay for the adjoint): during step t the bracket
+ * term of each eps-dependent update -- the part multiplied by dt/eps -- is
+ * stored at curl[c] + (t - t0) * step_stride + cell (cell = the field layout
+ * offset), for t0 <= t < t0 + nslots.  3-D records Ex, Ey, Ez (curl[0..2]);
+ * 2-D TM records Ez in curl[2]; 2-D TE records Ex, Ey in curl[0], curl[1].
+ * Grid dtype. */
+typedef struct {
+  void* curl[3];
+  int64_t step_stride;
+  int32_t t0;
+  int32_t nslots;
+} dn_curl_record;
+
 /* ---- library information ------------------------------------------------ */
 const char* dn_strerror(int32_t status);
 int32_t dn_version(void);
@@ -139,14 +152,40 @@ int32_t dn_last_cuda_error(void);
  */
 int32_t dn_fdtd2d_run(const dn_grid* g, void* const fa[6], void* const fb[6], const void* ce,
                       const dn_cpml* cpml, const dn_source* src, const dn_monitor* mons,
-                      int32_t n_mon, const dn_probe* probe, int32_t t0, int32_t nsteps,
-                      int32_t* status, void* stream, int32_t* final_in_b);
+                      int32_t n_mon, const dn_probe* probe, const dn_curl_record* rec,
+                      int32_t t0, int32_t nsteps, int32_t* status, void* stream,
+                      int32_t* final_in_b);
 
-/* 3-D analogue (all six components), same ping-pong and status contract. */
+/* 3-D analogue (all six components), same ping-pong and status contract.
+ * Field bases and ce must be 16-byte aligned, pitches multiples of 16 bytes. */
 int32_t dn_fdtd3d_run(const dn_grid* g, void* const fa[6], void* const fb[6], const void* ce,
                       const dn_cpml* cpml, const dn_source* src, const dn_monitor* mons,
-                      int32_t n_mon, const dn_probe* probe, int32_t t0, int32_t nsteps,
-                      int32_t* status, void* stream, int32_t* final_in_b);
+                      int32_t n_mon, const dn_probe* probe, const dn_curl_record* rec,
+                      int32_t t0, int32_t nsteps, int32_t* status, void* stream,
+                      int32_t* final_in_b);
+
+/* ---- adjoint (reverse) time stepping ------------------------------------
+ * Discrete adjoint of the steps above: runs reverse steps t = t_end-1 down
+ * to t_end-nsteps.  `la`/`lb` are 6-pointer sets of adjoint fields (the
+ * gradient of the loss with respect to each field after step t), ping-pong
+ * like the forward; on entry `la` holds the adjoint after step t_end-1.
+ * `curl` is the record of a forward replay covering those steps (see
+ * dn_curl_record).  `grad_ce` (FP64, field layout) accumulates
+ * dL/d(dt/eps) = sum_t lambda_E(t) . curl(t).  `mons` carry, in `acc`, the
+ * gradient of the loss with respect to each monitor's DFT (re, im); they are
+ * injected into the adjoint field before each reverse step.  The source term
+ * does not depend on eps and has no adjoint.
+ * Replaces the reference's backward passes: autograd through
+ * _time_step (diffnano/solvers/fdtd3d.py:378-465, fdtd2d.py:233-303) and
+ * _TimeReversalFDTD.backward (fdtd3d.py:166-219). */
+int32_t dn_fdtd2d_adjoint(const dn_grid* g, void* const la[6], void* const lb[6], const void* ce,
+                          const dn_cpml* cpml, const dn_curl_record* curl, double* grad_ce,
+                          const dn_monitor* mons, int32_t n_mon, int32_t t_end, int32_t nsteps,
+                          int32_t* status, void* stream, int32_t* final_in_b);
+int32_t dn_fdtd3d_adjoint(const dn_grid* g, void* const la[6], void* const lb[6], const void* ce,
+                          const dn_cpml* cpml, const dn_curl_record* curl, double* grad_ce,
+                          const dn_monitor* mons, int32_t n_mon, int32_t t_end, int32_t nsteps,
+                          int32_t* status, void* stream, int32_t* final_in_b);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,182 @@
+"""GPU gradients (hand-written discrete adjoint) against the reference's
+autograd (golden fixtures), the oracle's autograd and central finite
+differences of the FP64 kernels.
+
+Tolerances (relative L2 of dL/deps): FP64 kernels 1e-9 (same algorithm,
+rounding only); FP32 kernels 1e-4 (the target); finite differences 1e-4.
+"""
+
+from __future__ import annotations
+
+import pytest
+import torch
+from conftest import DT2, DT3, OMEGA, load_golden, rel_l2
+
+import diffnano_b200 as dn
+from oracle import fdtd_ref as R
+
+pytestmark = pytest.mark.gpu
+
+TOL = {torch.float32: 1e-4, torch.float64: 1e-9}
+DTYPES = [torch.float32, torch.float64]
+
+
+def _seeded(shape, seed, lo=1.5, span=2.0):
+    g = torch.Generator().manual_seed(seed)
+    return lo + span * torch.rand(*shape, dtype=torch.float64, generator=g)
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_grad2d_tm_vs_reference_autograd(cuda, dtype):
+    g = load_golden("grad2d")
+    s = dn.FDTDSolver2D(grid_shape=(24, 20), pml_layers=4, n_steps=60, device=cuda, dtype=dtype)
+    eps = torch.tensor(g["eps"]).to(cuda).requires_grad_(True)
+    r = s.forward(eps, source=dict(g["source"]))
+    (r.field.double() * torch.tensor(g["G"]).to(cuda)).sum().backward()
+    assert eps.grad.dtype == torch.float64
+    assert rel_l2(eps.grad, g["grad"]) < TOL[dtype]
+
+
+@pytest.mark.parametrize("mode", ["auto", "time_reversal", "checkpoint"])
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_grad3d_vs_reference_autograd(cuda, dtype, mode):
+    g = load_golden("grad3d")
+    kw = dict(use_checkpoint=True, checkpoint_segments=4) if mode == "checkpoint" else \
+        dict(backward=mode)
+    s = dn.FDTDSolver3D(grid_shape=(10, 10, 10), pml_layers=2, n_steps=30, courant=0.35,
+                        device=cuda, dtype=dtype, **kw)
+    eps = torch.tensor(g["eps"]).to(cuda).requires_grad_(True)
+    r = s.forward(eps, source=dict(g["source"]))
+    if mode == "time_reversal":
+        assert "TimeReversalFDTD" in type(r.field.grad_fn).__name__ or \
+            "TimeReversalFDTD" in str(r.field.grad_fn.next_functions)
+    (r.field.double() * torch.tensor(g["G"]).to(cuda)).sum().backward()
+    assert rel_l2(eps.grad, g["grad"]) < TOL[dtype]
+
+
+def test_grad_on_cpu_tensor_roundtrip(cuda):
+    """device='cpu' solver: eps and its gradient stay on the host."""
+    g = load_golden("grad3d")
+    s = dn.FDTDSolver3D(grid_shape=(10, 10, 10), pml_layers=2, n_steps=30, courant=0.35,
+                        dtype=torch.float64, backward="time_reversal")
+    eps = torch.tensor(g["eps"]).requires_grad_(True)
+    r = s.forward(eps, source=dict(g["source"]))
+    (r.field * torch.tensor(g["G"])).sum().backward()
+    assert eps.grad.device.type == "cpu"
+    assert rel_l2(eps.grad, g["grad"]) < 1e-9
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_grad2d_te_vs_oracle(cuda, dtype):
+    shape, T = (26, 34), 24
+    eps0 = _seeded(shape, 21)
+    src = {"type": "gaussian_pulse", "pos": [12, 15]}
+    G = torch.randn(*shape, dtype=torch.float64, generator=torch.Generator().manual_seed(22))
+    e = eps0.clone().requires_grad_(True)
+    o = R.run_2d(e, dl=20.0, dt=DT2(0.5, 20.0), omega=OMEGA, pml_layers=4, polarization="TE",
+                 n_steps=T, source=src)
+    (o["Hz"] * G).sum().backward()
+    s = dn.FDTDSolver2D(grid_shape=shape, polarization="TE", pml_layers=4, n_steps=T,
+                        device=cuda, dtype=dtype)
+    eps = eps0.clone().to(cuda).requires_grad_(True)
+    r = s.forward(eps, source=dict(src))
+    (r.field[0].double() * G.to(cuda)).sum().backward()
+    assert rel_l2(eps.grad, e.grad) < TOL[dtype] * 10  # TE grows exponentially
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+@pytest.mark.parametrize("shape,axes", [((18, 18, 18), "reference"), ((20, 24, 36), "physical"),
+                                        ((33, 40, 35), "physical")])
+def test_grad3d_vs_oracle(cuda, dtype, shape, axes):
+    """Multi-tile / ragged grids, both CPML mappings, Ex plane source,
+    several checkpoint segments (T not a multiple of the interval)."""
+    T = 29
+    eps0 = _seeded(shape, 23)
+    src = {"type": "gaussian_pulse", "plane": "xy", "z": 5, "component": "Ex",
+           "spread": 300.0, "t0": 900.0}
+    G = torch.randn(3, *shape, dtype=torch.float64, generator=torch.Generator().manual_seed(24))
+    e = eps0.clone().requires_grad_(True)
+    o = R.run_3d(e, dl=20.0, dt=DT3(0.4, 20.0), omega=OMEGA, pml_layers=4, n_steps=T,
+                 source=src, axes=axes, component="Ex")
+    (torch.stack([o["Ez"], o["Ex"], o["Ey"]]) * G).sum().backward()
+    s = dn.FDTDSolver3D(grid_shape=shape, pml_layers=4, n_steps=T, device=cuda, dtype=dtype,
+                        cpml_axes=axes)
+    eps = eps0.clone().to(cuda).requires_grad_(True)
+    r = s.forward(eps, source=dict(src))
+    (r.field.double() * G.to(cuda)).sum().backward()
+    assert rel_l2(eps.grad, e.grad) < TOL[dtype]
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_monitor_fom_gradient_vs_oracle(cuda, dtype):
+    """Loss = sum |DFT Ey|^2 over a plane monitor (the 3-D workload's FOM)."""
+    shape, T = (22, 22, 22), 60
+    eps0 = _seeded(shape, 25)
+    src = {"type": "gaussian_pulse", "plane": "xy", "z": 5, "component": "Ex",
+           "spread": 400.0, "t0": 1200.0}
+    wl = [1500.0, 1600.0]
+    e = eps0.clone().requires_grad_(True)
+    o = R.run_3d(e, dl=20.0, dt=DT3(0.4, 20.0), omega=OMEGA, pml_layers=3, n_steps=T,
+                 source=src, component="Ex",
+                 monitors=[dict(component="Ey", box=((16, 17), (4, 18), (3, 19)),
+                                wavelengths_nm=wl)])
+    R.fom_abs2(o["monitors"][0]).backward()
+    s = dn.FDTDSolver3D(grid_shape=shape, pml_layers=3, n_steps=T, device=cuda, dtype=dtype)
+    eps = eps0.clone().to(cuda).requires_grad_(True)
+    r = s.forward(eps, source=dict(src),
+                  monitors=[{"component": "Ey", "plane": "xy", "z": 16,
+                             "extent": [[4, 18], [3, 19]], "wavelengths_nm": wl}])
+    F = r.metadata["monitors"][0]["dft"]
+    (F.abs() ** 2).sum().backward()
+    assert rel_l2(eps.grad, e.grad) < TOL[dtype]
+
+
+def test_2d_monitor_gradient_vs_oracle(cuda):
+    shape, T = (40, 36), 120
+    eps0 = _seeded(shape, 26)
+    src = {"type": "gaussian_pulse", "row": 6}
+    wl = [1500.0, 1550.0, 1600.0]
+    e = eps0.clone().requires_grad_(True)
+    o = R.run_2d(e, dl=15.0, dt=DT2(0.6, 15.0), omega=OMEGA, pml_layers=4, n_steps=T, source=src,
+                 monitors=[dict(component="Ez", box=((30, 31), (0, 36)), wavelengths_nm=wl)])
+    R.fom_abs2(o["monitors"][0]).backward()
+    s = dn.FDTDSolver2D(grid_shape=shape, pml_layers=4, n_steps=T, dl=15.0, courant=0.6,
+                        device=cuda, dtype=torch.float64)
+    eps = eps0.clone().to(cuda).requires_grad_(True)
+    r = s.forward(eps, source=dict(src),
+                  monitors=[{"component": "Ez", "row": 30, "wavelengths_nm": wl}])
+    (r.metadata["monitors"][0]["dft"].abs() ** 2).sum().backward()
+    assert rel_l2(eps.grad, e.grad) < 1e-9
+
+
+def test_grad3d_central_finite_differences(cuda):
+    """dL/deps at 16 seeded voxels vs central differences (h = 1e-3) of the
+    FP64 kernels; L = sum |DFT Ey|^2 over a plane."""
+    shape, T = (20, 20, 20), 80
+    eps0 = _seeded(shape, 27)
+    src = {"type": "gaussian_pulse", "plane": "xy", "z": 4, "component": "Ex",
+           "spread": 400.0, "t0": 1200.0}
+    mons = [{"component": "Ey", "plane": "xy", "z": 15, "extent": [[3, 17], [3, 17]],
+             "wavelengths_nm": [1550.0]}]
+    s = dn.FDTDSolver3D(grid_shape=shape, pml_layers=3, n_steps=T, device=cuda,
+                        dtype=torch.float64)
+
+    def loss(e):
+        r = s.forward(e, source=dict(src), monitors=mons)
+        return (r.metadata["monitors"][0]["dft"].abs() ** 2).sum()
+
+    eps = eps0.clone().to(cuda).requires_grad_(True)
+    loss(eps).backward()
+    gen = torch.Generator().manual_seed(28)
+    idx = torch.randint(3, 17, (16, 3), generator=gen)
+    h = 1e-3
+    fd, ad = [], []
+    with torch.no_grad():
+        for z, y, x in idx.tolist():
+            ep = eps0.clone().to(cuda)
+            ep[z, y, x] += h
+            em = eps0.clone().to(cuda)
+            em[z, y, x] -= h
+            fd.append((loss(ep) - loss(em)).item() / (2 * h))
+            ad.append(eps.grad[z, y, x].item())
+    assert rel_l2(torch.tensor(ad), torch.tensor(fd)) < 1e-4

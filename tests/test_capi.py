@@ -44,7 +44,7 @@ def test_strerror_and_version():
 def test_null_grid_rejected(fn):
     L = _lib.lib()
     out = ctypes.c_int32(-1)
-    rc = getattr(L, fn)(None, None, None, None, None, None, None, 0, None, 0, 1, None, None,
+    rc = getattr(L, fn)(None, None, None, None, None, None, None, 0, None, None, 0, 1, None, None,
                         ctypes.byref(out))
     assert rc == _lib.DN_EINVAL
 
@@ -67,7 +67,7 @@ def test_2d_bad_grid_rejected_before_any_launch(bad):
         cp.b[a] = cp.c[a] = 16
     out = ctypes.c_int32(-1)
     rc = L.dn_fdtd2d_run(ctypes.byref(g), fake, fake, 16, ctypes.byref(cp), None, None, 0, None,
-                         0, 1, None, None, ctypes.byref(out))
+                         None, 0, 1, None, None, ctypes.byref(out))
     assert rc == _lib.DN_EINVAL
 
 
@@ -80,7 +80,7 @@ def test_3d_reference_axes_needs_cubic_grid():
         cp.b[a] = cp.c[a] = 256
     out = ctypes.c_int32(-1)
     rc = L.dn_fdtd3d_run(ctypes.byref(g), fake, fake, 256, ctypes.byref(cp), None, None, 0,
-                         None, 0, 1, None, None, ctypes.byref(out))
+                         None, None, 0, 1, None, None, ctypes.byref(out))
     assert rc == _lib.DN_EINVAL
 
 
@@ -94,12 +94,12 @@ def test_source_box_outside_grid_rejected():
     src = _lib.DnSource(component=_lib.DN_EZ, box=_lib.box((0, 0, 0), (1, 9, 8)), wave=16)
     out = ctypes.c_int32(-1)
     rc = L.dn_fdtd2d_run(ctypes.byref(g), fake, fake, 16, ctypes.byref(cp), ctypes.byref(src),
-                         None, 0, None, 0, 1, None, None, ctypes.byref(out))
+                         None, 0, None, None, 0, 1, None, None, ctypes.byref(out))
     assert rc == _lib.DN_EINVAL
     # a TE-only component on a TM grid is rejected too
     src = _lib.DnSource(component=_lib.DN_HZ, box=_lib.box((0, 0, 0), (1, 1, 1)), wave=16)
     rc = L.dn_fdtd2d_run(ctypes.byref(g), fake, fake, 16, ctypes.byref(cp), ctypes.byref(src),
-                         None, 0, None, 0, 1, None, None, ctypes.byref(out))
+                         None, 0, None, None, 0, 1, None, None, ctypes.byref(out))
     assert rc == _lib.DN_EINVAL
 
 
@@ -109,3 +109,25 @@ def test_check_maps_status_to_exceptions():
     with pytest.raises(_lib.DNError):
         _lib.check("x", _lib.DN_ETIMEOUT)
     _lib.check("x", _lib.DN_OK)
+
+
+@pytest.mark.parametrize("fn", ["dn_fdtd2d_adjoint", "dn_fdtd3d_adjoint"])
+def test_adjoint_rejects_missing_curl_record(fn):
+    L = _lib.lib()
+    is3d = fn.startswith("dn_fdtd3d")
+    g = _grid(D=8 if is3d else 1, H=8, W=8, pitch_y=32, pitch_z=256)
+    fake = _lib.PTR6(*([256] * 6))
+    cp = _lib.DnCpml()
+    for a in range(3):
+        cp.b[a] = cp.c[a] = 256
+    out = ctypes.c_int32(-1)
+    rc = getattr(L, fn)(ctypes.byref(g), fake, fake, 256, ctypes.byref(cp), None, 256, None, 0,
+                        4, 4, None, None, ctypes.byref(out))
+    assert rc == _lib.DN_EINVAL
+    # a record that does not cover the requested steps is rejected too
+    rec = _lib.DnCurlRecord(step_stride=8 * 256, t0=2, nslots=2)
+    for c in range(3):
+        rec.curl[c] = 256
+    rc = getattr(L, fn)(ctypes.byref(g), fake, fake, 256, ctypes.byref(cp), ctypes.byref(rec), 256,
+                        None, 0, 4, 4, None, None, ctypes.byref(out))
+    assert rc == _lib.DN_EINVAL
