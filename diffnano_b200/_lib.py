@@ -22,6 +22,7 @@ DN_TM, DN_TE = 0, 1
 DN_AXES_REFERENCE, DN_AXES_PHYSICAL = 0, 1
 DN_MAX_MONITORS = 4
 DN_MAX_FREQS = 16
+DN_NOALLOC_MAX_BYTES = 6 * 1024 * 1024
 
 COMPONENTS = {"Ex": DN_EX, "Ey": DN_EY, "Ez": DN_EZ, "Hx": DN_HX, "Hy": DN_HY, "Hz": DN_HZ}
 
@@ -86,6 +87,11 @@ SIGNATURES = {
                                     ctypes.POINTER(DnCpml), ctypes.POINTER(DnCurlRecord),
                                     c_void_p, ctypes.POINTER(DnMonitor), c_int32, c_int32,
                                     c_int32, c_void_p, c_void_p, ctypes.POINTER(c_int32)]),
+    "dn_fdtd2d_run_noalloc": (c_int32, [ctypes.POINTER(DnGrid), _P6, c_void_p,
+                                        ctypes.POINTER(DnCpml), ctypes.POINTER(DnSource),
+                                        ctypes.POINTER(DnMonitor), c_int32,
+                                        ctypes.POINTER(DnProbe), c_int32, c_int32, c_void_p,
+                                        c_void_p]),
 }
 
 

@@ -187,6 +187,25 @@ int32_t dn_fdtd3d_adjoint(const dn_grid* g, void* const la[6], void* const lb[6]
                           const dn_monitor* mons, int32_t n_mon, int32_t t_end, int32_t nsteps,
                           int32_t* status, void* stream, int32_t* final_in_b);
 
+/* ---- stepping without device allocation --------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory where they step the solver (a plugin inside an application that owns
+ * the whole device-memory budget, a loop whose policy forbids allocation):
+ * dn_fdtd2d_run with the second ping-pong set replaced by a file-scope device
+ * array of DN_NOALLOC_MAX_BYTES held by every GPU that loads the library.
+ * `f` (6 pointers, the polarisation's three used) is read and updated in
+ * place; the result is always in `f`.  Grids needing more than
+ * DN_NOALLOC_MAX_BYTES for three fields (H * pitch_y * element size each,
+ * rounded up to 256 bytes) return DN_ENOMEM.  The first call on a device
+ * looks up the array's address; make it before any stream capture.  All
+ * calls share the array: calls whose GPU work overlaps race.  Makes no
+ * cudaMalloc/cudaFree or other allocating call. */
+#define DN_NOALLOC_MAX_BYTES (6 * 1024 * 1024)
+int32_t dn_fdtd2d_run_noalloc(const dn_grid* g, void* const f[6], const void* ce,
+                              const dn_cpml* cpml, const dn_source* src, const dn_monitor* mons,
+                              int32_t n_mon, const dn_probe* probe, int32_t t0, int32_t nsteps,
+                              int32_t* status, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
