@@ -35,6 +35,9 @@ SHAPE = (256, 256, 256)
 DL, COURANT, PML, T_SOLVE = 25.0, 0.4, 12, 4000
 Z_SRC = 40
 BYTES_PER_CELL_STEP = 52  # FP32: read Ex Ey Ez Hx Hy Hz dt/eps, write the six fields
+# reverse step incl. its replay: replay 52 + 12 (curl record); adjoint reads 7
+# fields (28) + curl (12) + FP64 grad (8), writes 6 adjoint fields (24) + grad (8)
+ADJ_BYTES_PER_CELL_STEP = 144
 WORKLOAD = "3d_yee_256cube_cpml12_fp32"
 METRIC = "FDTD Gcell-updates/s"
 UNIT = "Gcell-updates/s"
@@ -286,6 +289,38 @@ def run_ours(args):
     del eng
     torch.cuda.empty_cache()
 
+    # adjoint: reverse sweep (segment replay with curl record + reverse steps)
+    adjoint = None
+    if not args.no_adjoint:
+        from diffnano_b200.solvers._adjoint import _Runner
+
+        Ta = args.adjoint_steps
+        eng_a = solver._make_engine(Ta, src, mons)
+        runner = _Runner(eng_a, ("Ez", "Ex", "Ey"), int(math.ceil(math.sqrt(Ta))))
+        with torch.no_grad():
+            runner.forward(eps.to(dev), True)
+        gen = torch.Generator(device=dev).manual_seed(0)
+        g_field = torch.randn((3, D, H, W), device=dev, generator=gen)
+        runner.adjoint(g_field, None)  # warm-up (also sizes the allocator's cache)
+        torch.cuda.synchronize(dev)
+        barrier(ws)
+        e0.record(stream)
+        runner.adjoint(g_field, None)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        el_a = max_over_ranks(e0.elapsed_time(e1) / 1e3, ws, dev)
+        rev_s = el_a / Ta
+        adjoint = {"value": ws * cells * Ta / el_a / 1e9, "unit": UNIT,
+                   "ms_per_step": rev_s * 1e3, "steps": Ta,
+                   "algorithmic_bytes_per_cell_step": ADJ_BYTES_PER_CELL_STEP,
+                   "achieved_GBs": ADJ_BYTES_PER_CELL_STEP * cells / rev_s / 1e9,
+                   "frac_of_hbm_peak": ADJ_BYTES_PER_CELL_STEP * cells / rev_s / 1e9 / peak,
+                   "what": f"reverse sweep of a {Ta}-step solve: per step one replay step with "
+                           "curl record (k_fdtd3d) + one reverse step (k_adj3d), "
+                           f"checkpoints every {runner.K} steps"}
+        del runner, eng_a
+        torch.cuda.empty_cache()
+
     # end to end through the public API with host buffers (reference device="cpu")
     e2e = None
     if not args.no_e2e:
@@ -308,6 +343,28 @@ def run_ours(args):
                "step": f"one FDTDSolver3D.forward(device='cpu') solve of {T_SOLVE} time steps "
                        f"(host eps in, host field + monitor DFT out), mean of {args.e2e_steps}"}
 
+    # full gradient of the monitor FOM through the public API, host buffers
+    grad_e2e = None
+    if not args.no_grad_e2e:
+        s_host = dn.FDTDSolver3D(grid_shape=SHAPE, dl=DL, wavelength_nm=1550.0, pml_layers=PML,
+                                 n_steps=T_SOLVE, courant=COURANT, device="cpu",
+                                 dtype=torch.float32, backward="time_reversal")
+        e_in = eps.to(torch.float32).pin_memory().requires_grad_(True)
+        barrier(ws)
+        t = time.perf_counter()
+        r = s_host.forward(e_in, source=dict(src), monitors=mons)
+        fom = (r.metadata["monitors"][0]["dft"].abs() ** 2).sum()
+        fom.backward()
+        g_el = max_over_ranks(time.perf_counter() - t, ws, dev)
+        grad_e2e = {"value": ws * cells * T_SOLVE / g_el / 1e9, "unit": UNIT, "wall_s": g_el,
+                    "h2d_bytes_per_step": e_in.numel() * e_in.element_size(),
+                    "d2h_bytes_per_step": e_in.grad.numel() * e_in.grad.element_size() + 8,
+                    "step": f"FOM = sum |DFT Ey|^2 and dFOM/deps of a {T_SOLVE}-step solve "
+                            "(forward with checkpoints, replay, reverse sweep), "
+                            "FDTDSolver3D(device='cpu', backward='time_reversal')"}
+        del r, fom, e_in
+        torch.cuda.empty_cache()
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(eps)
@@ -322,7 +379,8 @@ def run_ours(args):
                              "peak_source": f"hbm_gbs of {peak_kind}",
                              "algorithmic_bytes_per_launch": BYTES_PER_CELL_STEP * cells,
                              "kernel": "k_fdtd3d (one launch per time step)"},
-                "cpu_baseline": cpu, "e2e": e2e, "clocks": cs.summary(), "gpu_launches": K}
+                "cpu_baseline": cpu, "e2e": e2e, "adjoint": adjoint, "gradient_e2e": grad_e2e,
+                "clocks": cs.summary(), "gpu_launches": K}
         print(json.dumps(line), flush=True)
     if ws > 1:
         import torch.distributed as dist
@@ -340,6 +398,9 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--adjoint-steps", type=int, default=256)
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-grad-e2e", action="store_true")
     ap.add_argument("--grid", type=int, default=256,
                     help="cubic grid side (256 is the benchmark; smaller sides are for profiling)")
     args = ap.parse_args()
