@@ -87,6 +87,8 @@ SIGNATURES = {
                                     ctypes.POINTER(DnCpml), ctypes.POINTER(DnCurlRecord),
                                     c_void_p, ctypes.POINTER(DnMonitor), c_int32, c_int32,
                                     c_int32, c_void_p, c_void_p, ctypes.POINTER(c_int32)]),
+    "dn_fom_abs2_scratch_bytes": (c_int64, [c_int64]),
+    "dn_fom_abs2": (c_int32, [c_void_p, c_int64, c_void_p, c_void_p, c_int64, c_void_p]),
     "dn_fdtd2d_run_noalloc": (c_int32, [ctypes.POINTER(DnGrid), _P6, c_void_p,
                                         ctypes.POINTER(DnCpml), ctypes.POINTER(DnSource),
                                         ctypes.POINTER(DnMonitor), c_int32,

@@ -198,6 +198,12 @@ __global__ void __launch_bounds__(NT, AdjCfg<T>::MINB)
     const T fi_next = has_next ? T(1) : T(0);
     const T* cur = sm.arr(q, 0) + 2 * w * BX + lane + 4;
     const T* nxt = has_next ? sm.arr(q + 1, 0) + 2 * w * BX + lane + 4 : cur;
+    // issue the FP64 gradient loads now; they are consumed after lH'
+    const long long o_plane = i * pz + (long long)ja * py + k;
+    double gpre[2];
+#pragma unroll
+    for (int r = 1; r < 3; ++r)
+      gpre[r - 1] = (ja + r - 1 < H && kin) ? p.grad[o_plane + (r - 1) * py] : 0.0;
 
     // ---- lH' of rows ja-1, ja, ja+1 --------------------------------------
     T LHx[3], LHy[3], LHz[3];
@@ -238,7 +244,6 @@ __global__ void __launch_bounds__(NT, AdjCfg<T>::MINB)
     const T hvzk0 = __shfl_sync(FULL_MASK, hvzk, 0), hvzk1 = __shfl_sync(FULL_MASK, hvzk, 1);
 
     // ---- previous adjoint fields of rows ja, ja+1 ---------------------------
-    const long long o_plane = i * pz + (long long)ja * py + k;
     const T* ct = sm.tile_arr(q, NRING_A, 0) + (2 * w) * TX + lane;
     constexpr int TE = L::TILE_ARR / (int)sizeof(T);
 #pragma unroll
@@ -272,7 +277,7 @@ __global__ void __launch_bounds__(NT, AdjCfg<T>::MINB)
         const double gsum = static_cast<double>(lex) * static_cast<double>(ct[et]) +
                             static_cast<double>(ley) * static_cast<double>(ct[TE + et]) +
                             static_cast<double>(lez) * static_cast<double>(ct[2 * TE + et]);
-        p.grad[o] += gsum;
+        p.grad[o] = gpre[r - 1] + gsum;
         p.out[DN_EX][o] = nlex;
         p.out[DN_EY][o] = nley;
         p.out[DN_EZ][o] = nlez;

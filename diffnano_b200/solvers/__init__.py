@@ -14,7 +14,7 @@ import torch
 
 from diffnano_b200.solvers._result import SimResult
 
-__all__ = ["Solver", "SimResult", "FDTDSolver2D", "FDTDSolver3D"]
+__all__ = ["Solver", "SimResult", "FDTDSolver2D", "FDTDSolver3D", "fom_abs2"]
 
 
 @runtime_checkable
@@ -38,4 +38,8 @@ def __getattr__(name):
         from diffnano_b200.solvers.fdtd3d import FDTDSolver3D
 
         return FDTDSolver3D
+    if name == "fom_abs2":
+        from diffnano_b200.solvers._fom import fom_abs2
+
+        return fom_abs2
     raise AttributeError(f"module {__name__!r} has no attribute {name!r}")

@@ -187,6 +187,16 @@ int32_t dn_fdtd3d_adjoint(const dn_grid* g, void* const la[6], void* const lb[6]
                           const dn_monitor* mons, int32_t n_mon, int32_t t_end, int32_t nsteps,
                           int32_t* status, void* stream, int32_t* final_in_b);
 
+/* ---- figure of merit ----------------------------------------------------
+ * *out = sum_i |dft[i]|^2 over n_complex FP64 (re, im) pairs, reduced in FP64
+ * (warp-shuffle trees, per-block partials in `scratch`, deterministic final
+ * sum).  No reference counterpart (the reference has no monitors); it is the
+ * FOM of the design workloads (sum of |DFT E|^2 over a monitor).  `scratch`
+ * needs dn_fom_abs2_scratch_bytes(n_complex) bytes, 16-byte aligned. */
+int64_t dn_fom_abs2_scratch_bytes(int64_t n_complex);
+int32_t dn_fom_abs2(const double* dft, int64_t n_complex, double* out, void* scratch,
+                    int64_t scratch_bytes, void* stream);
+
 /* ---- stepping without device allocation --------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device
  * memory where they step the solver (a plugin inside an application that owns

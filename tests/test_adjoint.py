@@ -180,3 +180,37 @@ def test_grad3d_central_finite_differences(cuda):
             fd.append((loss(ep) - loss(em)).item() / (2 * h))
             ad.append(eps.grad[z, y, x].item())
     assert rel_l2(torch.tensor(ad), torch.tensor(fd)) < 1e-4
+
+
+def test_fom_kernel_matches_torch_and_is_deterministic(cuda):
+    from diffnano_b200.solvers import fom_abs2
+
+    g = torch.Generator().manual_seed(30)
+    for n in (1, 31, 4096, 300_001):
+        z = torch.complex(torch.randn(n, dtype=torch.float64, generator=g),
+                          torch.randn(n, dtype=torch.float64, generator=g)).to(cuda)
+        a = fom_abs2(z)
+        b = fom_abs2(z)
+        ref = (z.abs() ** 2).sum()
+        assert torch.equal(a, b)
+        assert abs(float(a) - float(ref)) <= 1e-12 * float(ref)
+
+
+def test_fom_kernel_gradient_drives_the_adjoint(cuda):
+    """The FOM kernel's backward feeds the monitor adjoint like torch's |F|^2."""
+    from diffnano_b200.solvers import fom_abs2
+
+    shape, T = (16, 16, 16), 40
+    eps0 = _seeded(shape, 31)
+    src = {"type": "gaussian_pulse", "plane": "xy", "z": 4, "component": "Ex",
+           "spread": 300.0, "t0": 900.0}
+    mons = [{"component": "Ey", "plane": "xy", "z": 12, "wavelengths_nm": [1550.0]}]
+    s = dn.FDTDSolver3D(grid_shape=shape, pml_layers=3, n_steps=T, device=cuda,
+                        dtype=torch.float64)
+    grads = []
+    for use_kernel in (True, False):
+        eps = eps0.clone().to(cuda).requires_grad_(True)
+        F = s.forward(eps, source=dict(src), monitors=mons).metadata["monitors"][0]["dft"]
+        (fom_abs2(F) if use_kernel else (F.abs() ** 2).sum()).backward()
+        grads.append(eps.grad)
+    assert rel_l2(grads[0], grads[1]) < 1e-12
