@@ -61,6 +61,25 @@ class DnCurlRecord(ctypes.Structure):
                 ("nslots", c_int32)]
 
 
+class DnBatch2dInst(ctypes.Structure):
+    _fields_ = [("H", c_int32), ("W", c_int32), ("pitch", c_int64), ("n_steps", c_int32),
+                ("src_comp", c_int32), ("src_box", DnBox), ("wave", c_void_p),
+                ("f", (c_void_p * 3) * 2), ("ce", c_void_p), ("b", c_void_p * 2),
+                ("c", c_void_p * 2), ("dt", c_double), ("dl", c_double), ("mon_comp", c_int32),
+                ("mon_box", DnBox), ("n_freq", c_int32), ("phase", c_void_p), ("acc", c_void_p),
+                ("ckpt", c_void_p), ("curl", c_void_p), ("lam", (c_void_p * 3) * 2),
+                ("grad", c_void_p), ("gmon", c_void_p)]
+
+
+class DnBatch2d(ctypes.Structure):
+    _fields_ = [("pol", c_int32), ("dtype", c_int32), ("n_inst", c_int32), ("K", c_int32),
+                ("tile_rows", c_int32), ("max_ctas", c_int32)]
+
+
+STRUCTS = {"dn_box": DnBox, "dn_grid": DnGrid, "dn_cpml": DnCpml, "dn_source": DnSource,
+           "dn_monitor": DnMonitor, "dn_probe": DnProbe, "dn_curl_record": DnCurlRecord,
+           "dn_batch2d_inst": DnBatch2dInst, "dn_batch2d": DnBatch2d}
+
 PTR6 = c_void_p * 6
 _P6 = ctypes.POINTER(c_void_p)  # a PTR6 instance (or None) is passed here
 
@@ -87,6 +106,12 @@ SIGNATURES = {
                                     ctypes.POINTER(DnCpml), ctypes.POINTER(DnCurlRecord),
                                     c_void_p, ctypes.POINTER(DnMonitor), c_int32, c_int32,
                                     c_int32, c_void_p, c_void_p, ctypes.POINTER(c_int32)]),
+    "dn_struct_size": (c_int64, [ctypes.c_char_p]),
+    "dn_batch2d_table_bytes": (c_int64, [ctypes.POINTER(DnBatch2d), ctypes.POINTER(DnBatch2dInst)]),
+    "dn_batch2d_pack": (c_int32, [ctypes.POINTER(DnBatch2d), ctypes.POINTER(DnBatch2dInst),
+                                  c_void_p, c_int64]),
+    "dn_batch2d_forward": (c_int32, [ctypes.POINTER(DnBatch2d), c_void_p, c_void_p, c_void_p]),
+    "dn_batch2d_backward": (c_int32, [ctypes.POINTER(DnBatch2d), c_void_p, c_void_p, c_void_p]),
     "dn_fom_abs2_scratch_bytes": (c_int64, [c_int64]),
     "dn_fom_abs2": (c_int32, [c_void_p, c_int64, c_void_p, c_void_p, c_int64, c_void_p]),
     "dn_fdtd2d_run_noalloc": (c_int32, [ctypes.POINTER(DnGrid), _P6, c_void_p,

@@ -1,0 +1,723 @@
+// Batched 2-D FDTD: many independent TMz / TE grids in one persistent launch.
+//
+// The reference runs one FDTDSolver2D object per grid, one Python step loop
+// each (diffnano/solvers/fdtd2d.py:309-357).  A design study (robust
+// erosion/dilation variants, wavelength sweeps) has many small-to-medium
+// grids of different sizes and step counts; launching each step of each grid
+// separately is launch-latency bound.  Here one cooperative kernel advances
+// all of them:
+//
+//   for each global step n:                       (forward kernel)
+//     every tile of every instance with n < n_steps is stepped
+//     (instances are sorted by step count, so the active tiles are a prefix
+//     of the tile list and are dealt round-robin to the CTAs);
+//     grid barrier (bounded spin, DN_ETIMEOUT)
+//
+// and the backward kernel walks the checkpoint segments from the last:
+// replay of the segment from its checkpoint with the curl record on, then the
+// segment's reverse steps (the same transpose as dn_adjoint2d.cu), with the
+// monitor-DFT gradient added to the adjoint field as it is loaded.  Field
+// loads bypass L1 (other SMs wrote them during the previous step).
+//
+// Tile: `TI` rows x 32 columns, 256 threads; the step arithmetic is that of
+// dn_fdtd2d.cu / dn_adjoint2d.cu (same equations, same boundary rules).
+#include <algorithm>
+#include <cstddef>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "dn_host.cuh"
+
+namespace dn {
+namespace {
+
+constexpr int TJ = 32;
+constexpr int NTB = 256;
+constexpr unsigned long long BAR_SPIN_LIMIT = 1ull << 24;  // x 64 ns ~ 1 s
+
+struct TableHeader {
+  int n_inst;
+  int total_tiles;
+  int max_steps;
+  int K;
+  int nseg;
+  int tile_rows;
+  int pad[2];
+  unsigned int bar[4];  // arrive count, generation, abort, unused
+};
+
+// table layout (all offsets 16-byte aligned):
+//   TableHeader | int tile_prefix[n+1] | int steps[n] (descending) |
+//   int2 tile_map[total_tiles] | dn_batch2d_inst inst[n] (sorted)
+struct TableView {
+  TableHeader* h;
+  const int* tile_prefix;
+  const int* steps;
+  const int2* tile_map;
+  const dn_batch2d_inst* inst;
+};
+
+__host__ __device__ inline size_t align16(size_t x) { return (x + 15) / 16 * 16; }
+
+__host__ __device__ inline void table_offsets(int n, int total_tiles, size_t* o_prefix,
+                                              size_t* o_steps, size_t* o_map, size_t* o_inst,
+                                              size_t* o_end) {
+  *o_prefix = align16(sizeof(TableHeader));
+  *o_steps = align16(*o_prefix + sizeof(int) * (n + 1));
+  *o_map = align16(*o_steps + sizeof(int) * n);
+  *o_inst = align16(*o_map + sizeof(int2) * (size_t)total_tiles);
+  *o_end = align16(*o_inst + sizeof(dn_batch2d_inst) * n);
+}
+
+__device__ TableView view(unsigned char* base) {
+  TableView v;
+  v.h = reinterpret_cast<TableHeader*>(base);
+  size_t op, os, om, oi, oe;
+  table_offsets(v.h->n_inst, v.h->total_tiles, &op, &os, &om, &oi, &oe);
+  v.tile_prefix = reinterpret_cast<const int*>(base + op);
+  v.steps = reinterpret_cast<const int*>(base + os);
+  v.tile_map = reinterpret_cast<const int2*>(base + om);
+  v.inst = reinterpret_cast<const dn_batch2d_inst*>(base + oi);
+  return v;
+}
+
+// tiles of the instances that still have a step at global step n
+__device__ int active_tiles(const TableView& v, int n) {
+  int lo = 0, hi = v.h->n_inst;  // first instance with steps <= n
+  while (lo < hi) {
+    const int mid = (lo + hi) / 2;
+    if (v.steps[mid] > n) lo = mid + 1; else hi = mid;
+  }
+  return v.tile_prefix[lo];
+}
+
+// grid barrier over all CTAs of the launch: arrive count + generation word,
+// bounded spin; returns false (and raises the abort word) on expiry or when
+// another CTA aborted
+__device__ bool grid_sync(unsigned int* bar, unsigned int& gen, int* status) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    __threadfence();
+    const unsigned int g = gen;
+    if (atomicAdd(&bar[0], 1u) == gridDim.x - 1) {
+      atomicExch(&bar[0], 0u);
+      __threadfence();
+      atomicExch(&bar[1], g + 1u);
+    } else {
+      unsigned long long spins = 0;
+      while (*reinterpret_cast<volatile unsigned int*>(&bar[1]) == g) {
+        if (*reinterpret_cast<volatile unsigned int*>(&bar[2])) {
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+        if (++spins > BAR_SPIN_LIMIT) {
+          ok = 0;
+          atomicExch(&bar[2], 1u);
+          report_status(status, DN_ETIMEOUT);
+          break;
+        }
+      }
+    }
+    gen = g + 1u;
+    __threadfence();
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+template <typename T>
+__device__ __forceinline__ T ld(const T* p) {
+  return __ldcg(p);
+}
+
+template <typename T, int TI>
+struct TileSmem {
+  T f[TI + 2][TJ + 2];
+  T a[TI + 1][TJ + 1];
+  T b[TI + 1][TJ + 1];
+  T bx[TJ + 2], gx[TJ + 2];
+  T by[TI + 2], gy[TI + 2];
+};
+
+template <typename T, int TI>
+__device__ void load_tables(TileSmem<T, TI>& s, const dn_batch2d_inst& I, int i0, int j0) {
+  for (int t = threadIdx.x; t < TJ + 2; t += NTB) {
+    const int j = j0 - 1 + t;
+    const bool ok = j >= 0 && j < I.W;
+    s.bx[t] = ok ? static_cast<T>(I.b[1][j]) : T(1);
+    s.gx[t] = ok ? static_cast<T>(1.0 + I.c[1][j]) : T(1);
+  }
+  for (int t = threadIdx.x; t < TI + 2; t += NTB) {
+    const int i = i0 - 1 + t;
+    const bool ok = i >= 0 && i < I.H;
+    s.by[t] = ok ? static_cast<T>(I.b[0][i]) : T(1);
+    s.gy[t] = ok ? static_cast<T>(1.0 + I.c[0][i]) : T(1);
+  }
+}
+
+__device__ __forceinline__ bool in_box(const dn_box& b, int i, int j) {
+  return i >= b.lo[1] && i < b.hi[1] && j >= b.lo[2] && j < b.hi[2];
+}
+
+__device__ __forceinline__ long long box_cell(const dn_box& b, int i, int j) {
+  return (long long)(i - b.lo[1]) * (b.hi[2] - b.lo[2]) + (j - b.lo[2]);
+}
+
+template <typename T>
+struct Sets {
+  T* p[3];
+};
+
+// ---------------------------------------------------------------------------
+// forward step of one tile.  zero_in: the input is the all-zero state.
+// ---------------------------------------------------------------------------
+template <typename T, int POL, int TI>
+__device__ void fwd_tile(TileSmem<T, TI>& s, const dn_batch2d_inst& I, int i0, int j0, int n,
+                         const Sets<T> in, bool zero_in, const Sets<T> out, const Sets<T> ckpt,
+                         bool save, const Sets<T> curl, bool record, bool monitors) {
+  constexpr int R = TI / (NTB / 32);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int H = I.H, W = I.W;
+  const long long py = I.pitch;
+  const T dt = static_cast<T>(I.dt), idl = static_cast<T>(1.0 / I.dl);
+  const T* ce = static_cast<const T*>(I.ce);
+  auto load = [&](int c, long long o) -> T { return zero_in ? T(0) : ld(in.p[c] + o); };
+
+  load_tables(s, I, i0, j0);
+  for (int t = threadIdx.x; t < (TI + 2) * (TJ + 2); t += NTB) {
+    const int r = t / (TJ + 2), c = t % (TJ + 2);
+    const int i = i0 - 1 + r, j = j0 - 1 + c;
+    s.f[r][c] = (i >= 0 && i < H && j >= 0 && j < W) ? load(0, i * py + j) : T(0);
+  }
+  __syncthreads();
+
+  const int jj = lane, j = j0 + jj;
+  T a_own[R], b_own[R], cx_own[R], cy_own[R];
+  if (POL == DN_TM) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int ii = warp + 8 * r, i = i0 + ii;
+      a_own[r] = b_own[r] = cx_own[r] = cy_own[r] = T(0);
+      if (i < H && j < W) {
+        const long long o = i * py + j;
+        const T ez = s.f[ii + 1][jj + 1];
+        const T dj = (j < W - 1) ? s.f[ii + 1][jj + 2] - ez : T(0);
+        const T di = (i < H - 1) ? s.f[ii + 2][jj + 1] - ez : T(0);
+        a_own[r] = s.by[ii + 1] * load(1, o) - dt * s.gy[ii + 1] * (dj * idl);
+        b_own[r] = s.bx[jj + 1] * load(2, o) + dt * s.gx[jj + 1] * (di * idl);
+      }
+      s.a[ii][jj + 1] = a_own[r];
+      s.b[ii + 1][jj] = b_own[r];
+    }
+    if (warp == 0 && lane < TI) {
+      const int ii = lane, i = i0 + ii, jh = j0 - 1;
+      T v = T(0);
+      if (jh >= 0 && i < H) {
+        const T dj = s.f[ii + 1][1] - s.f[ii + 1][0];
+        v = s.by[ii + 1] * load(1, i * py + jh) - dt * s.gy[ii + 1] * (dj * idl);
+      }
+      s.a[ii][0] = v;
+    } else if (warp == 1) {
+      const int ih = i0 - 1;
+      T v = T(0);
+      if (ih >= 0 && j < W) {
+        const T di = s.f[1][jj + 1] - s.f[0][jj + 1];
+        v = s.bx[jj + 1] * load(2, ih * py + j) + dt * s.gx[jj + 1] * (di * idl);
+      }
+      s.b[0][jj] = v;
+    }
+  } else {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int ii = warp + 8 * r, i = i0 + ii;
+      a_own[r] = b_own[r] = cx_own[r] = cy_own[r] = T(0);
+      if (i < H && j < W) {
+        const long long o = i * py + j;
+        const T hz = s.f[ii + 1][jj + 1];
+        const T dj = (j > 0) ? hz - s.f[ii + 1][jj] : T(0);
+        const T di = (i > 0) ? hz - s.f[ii][jj + 1] : T(0);
+        cx_own[r] = s.gx[jj + 1] * (dj * idl);
+        cy_own[r] = -(s.gy[ii + 1] * (di * idl));
+        const T c = ld(ce + o);
+        a_own[r] = s.bx[jj + 1] * load(1, o) + c * cx_own[r];
+        b_own[r] = s.by[ii + 1] * load(2, o) + c * cy_own[r];
+      }
+      s.a[ii][jj] = a_own[r];
+      s.b[ii][jj] = b_own[r];
+    }
+    if (warp == 0 && lane < TI) {
+      const int ii = lane, i = i0 + ii, jh = j0 + TJ;
+      T v = T(0);
+      if (jh < W && i < H) {
+        const long long o = i * py + jh;
+        const T dj = s.f[ii + 1][TJ + 1] - s.f[ii + 1][TJ];
+        v = s.bx[TJ + 1] * load(1, o) + ld(ce + o) * (s.gx[TJ + 1] * (dj * idl));
+      }
+      s.a[ii][TJ] = v;
+    } else if (warp == 1) {
+      const int ih = i0 + TI;
+      T v = T(0);
+      if (ih < H && j < W) {
+        const long long o = ih * py + j;
+        const T di = s.f[TI + 1][jj + 1] - s.f[TI][jj + 1];
+        v = s.by[TI + 1] * load(2, o) + ld(ce + o) * (-(s.gy[TI + 1] * (di * idl)));
+      }
+      s.b[TI][jj] = v;
+    }
+  }
+  __syncthreads();
+
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int ii = warp + 8 * r, i = i0 + ii;
+    if (i < H && j < W) {
+      const long long o = i * py + j;
+      const T fo = s.f[ii + 1][jj + 1];
+      const T bb = s.bx[jj + 1] * s.by[ii + 1];
+      T v0, cz = T(0);
+      if (POL == DN_TM) {
+        const T dHy = (i > 0) ? s.b[ii + 1][jj] - s.b[ii][jj] : T(0);
+        const T dHx = (j > 0) ? s.a[ii][jj + 1] - s.a[ii][jj] : T(0);
+        cz = s.gx[jj + 1] * (dHy * idl) - s.gy[ii + 1] * (dHx * idl);
+        v0 = bb * fo + ld(ce + o) * cz;
+      } else {
+        const T dEy = (i < H - 1) ? s.b[ii + 1][jj] - s.b[ii][jj] : T(0);
+        const T dEx = (j < W - 1) ? s.a[ii][jj + 1] - s.a[ii][jj] : T(0);
+        v0 = bb * fo + dt * (s.gx[jj + 1] * (dEy * idl) - s.gy[ii + 1] * (dEx * idl));
+      }
+      if (I.src_comp >= 0 && in_box(I.src_box, i, j))
+        v0 += static_cast<const T*>(I.wave)[n];
+      if (monitors && I.mon_comp >= 0 && in_box(I.mon_box, i, j)) {
+        const long long cell = box_cell(I.mon_box, i, j);
+        const long long ncell = (long long)(I.mon_box.hi[1] - I.mon_box.lo[1]) *
+                                (I.mon_box.hi[2] - I.mon_box.lo[2]);
+        const double x = static_cast<double>(v0);
+        const double* ph = I.phase + (long long)n * I.n_freq * 2;
+        for (int f = 0; f < I.n_freq; ++f) {
+          double* acc = I.acc + ((long long)f * ncell + cell) * 2;
+          acc[0] = fma(x, ph[2 * f], acc[0]);
+          acc[1] = fma(x, ph[2 * f + 1], acc[1]);
+        }
+      }
+      out.p[0][o] = v0;
+      out.p[1][o] = a_own[r];
+      out.p[2][o] = b_own[r];
+      if (save) {
+        ckpt.p[0][o] = v0;
+        ckpt.p[1][o] = a_own[r];
+        ckpt.p[2][o] = b_own[r];
+      }
+      if (record) {
+        if (POL == DN_TM) {
+          curl.p[0][o] = cz;
+        } else {
+          curl.p[0][o] = cx_own[r];
+          curl.p[1][o] = cy_own[r];
+        }
+      }
+    }
+  }
+  __syncthreads();  // shared memory is reused by the next tile
+}
+
+// monitor-DFT gradient added to the adjoint field at (i, j) for step n
+template <typename T>
+__device__ __forceinline__ T mon_inject(const dn_batch2d_inst& I, int i, int j, int n) {
+  if (!I.gmon || I.mon_comp < 0 || !in_box(I.mon_box, i, j)) return T(0);
+  const long long cell = box_cell(I.mon_box, i, j);
+  const long long ncell =
+      (long long)(I.mon_box.hi[1] - I.mon_box.lo[1]) * (I.mon_box.hi[2] - I.mon_box.lo[2]);
+  const double* ph = I.phase + (long long)n * I.n_freq * 2;
+  double g = 0.0;
+  for (int f = 0; f < I.n_freq; ++f) {
+    const double* a = I.gmon + ((long long)f * ncell + cell) * 2;
+    g = fma(a[0], ph[2 * f], fma(a[1], ph[2 * f + 1], g));
+  }
+  return static_cast<T>(g);
+}
+
+// ---------------------------------------------------------------------------
+// reverse step of one tile (transpose of fwd_tile; see dn_adjoint2d.cu)
+// ---------------------------------------------------------------------------
+template <typename T, int POL, int TI>
+__device__ void adj_tile(TileSmem<T, TI>& s, const dn_batch2d_inst& I, int i0, int j0, int n,
+                         const Sets<T> lin_s, const Sets<T> lout_s, const Sets<T> curl_s) {
+  T* const* lin = lin_s.p;
+  T* const* lout = lout_s.p;
+  T* const* curl = curl_s.p;
+  constexpr int R = TI / (NTB / 32);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int H = I.H, W = I.W;
+  const long long py = I.pitch;
+  const T dt = static_cast<T>(I.dt), idl = static_cast<T>(1.0 / I.dl);
+  const T* ce = static_cast<const T*>(I.ce);
+
+  load_tables(s, I, i0, j0);
+  for (int t = threadIdx.x; t < (TI + 2) * (TJ + 2); t += NTB) {
+    const int r = t / (TJ + 2), c = t % (TJ + 2);
+    const int i = i0 - 1 + r, j = j0 - 1 + c;
+    T v = T(0);
+    if (i >= 0 && i < H && j >= 0 && j < W) {
+      const long long o = i * py + j;
+      const T l0 = ld(lin[0] + o) + mon_inject<T>(I, i, j, n);
+      v = POL == DN_TM ? ld(ce + o) * l0 : l0;
+    }
+    s.f[r][c] = v;
+  }
+  __syncthreads();
+
+  const int jj = lane, j = j0 + jj;
+  T a_own[R], b_own[R];
+  if (POL == DN_TM) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int ii = warp + 8 * r, i = i0 + ii;
+      T vx = T(0), vy = T(0);
+      a_own[r] = b_own[r] = T(0);
+      if (i < H && j < W) {
+        const long long o = i * py + j;
+        const T u = s.f[ii + 1][jj + 1];
+        const T gy = s.gy[ii + 1] * idl, gx = s.gx[jj + 1] * idl;
+        a_own[r] = ld(lin[1] + o) - gy * ((j > 0 ? u : T(0)) - s.f[ii + 1][jj + 2]);
+        b_own[r] = ld(lin[2] + o) + gx * ((i > 0 ? u : T(0)) - s.f[ii + 2][jj + 1]);
+        vx = (j < W - 1) ? dt * gy * a_own[r] : T(0);
+        vy = (i < H - 1) ? dt * gx * b_own[r] : T(0);
+      }
+      s.a[ii][jj + 1] = vx;
+      s.b[ii + 1][jj] = vy;
+    }
+    if (warp == 0 && lane < TI) {
+      const int ii = lane, i = i0 + ii, jh = j0 - 1;
+      T v = T(0);
+      if (jh >= 0 && i < H) {
+        const T gy = s.gy[ii + 1] * idl;
+        const T u = s.f[ii + 1][0];
+        const T lh = ld(lin[1] + i * py + jh) - gy * ((jh > 0 ? u : T(0)) - s.f[ii + 1][1]);
+        v = dt * gy * lh;
+      }
+      s.a[ii][0] = v;
+    } else if (warp == 1) {
+      const int ih = i0 - 1;
+      T v = T(0);
+      if (ih >= 0 && j < W) {
+        const T gx = s.gx[jj + 1] * idl;
+        const T u = s.f[0][jj + 1];
+        const T lh = ld(lin[2] + ih * py + j) + gx * ((ih > 0 ? u : T(0)) - s.f[1][jj + 1]);
+        v = dt * gx * lh;
+      }
+      s.b[0][jj] = v;
+    }
+  } else {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int ii = warp + 8 * r, i = i0 + ii;
+      T ux = T(0), uy = T(0);
+      a_own[r] = b_own[r] = T(0);
+      if (i < H && j < W) {
+        const long long o = i * py + j;
+        const T lh = s.f[ii + 1][jj + 1];
+        const T cy = dt * s.gy[ii + 1] * idl, cx = dt * s.gx[jj + 1] * idl;
+        const T wj = (j < W - 1) ? cy * lh : T(0);
+        const T wjm = (j > 0) ? cy * s.f[ii + 1][jj] : T(0);
+        const T wi = (i < H - 1) ? cx * lh : T(0);
+        const T wim = (i > 0) ? cx * s.f[ii][jj + 1] : T(0);
+        a_own[r] = ld(lin[1] + o) + wj - wjm;
+        b_own[r] = ld(lin[2] + o) - wi + wim;
+        I.grad[o] += static_cast<double>(a_own[r]) * static_cast<double>(ld(curl[0] + o)) +
+                     static_cast<double>(b_own[r]) * static_cast<double>(ld(curl[1] + o));
+        const T c = ld(ce + o);
+        ux = (j > 0) ? c * s.gx[jj + 1] * idl * a_own[r] : T(0);
+        uy = (i > 0) ? c * s.gy[ii + 1] * idl * b_own[r] : T(0);
+      }
+      s.a[ii][jj] = ux;
+      s.b[ii][jj] = uy;
+    }
+    if (warp == 0 && lane < TI) {
+      const int ii = lane, i = i0 + ii, jh = j0 + TJ;
+      T v = T(0);
+      if (jh < W && i < H) {
+        const long long o = i * py + jh;
+        const T cy = dt * s.gy[ii + 1] * idl;
+        const T wj = (jh < W - 1) ? cy * s.f[ii + 1][TJ + 1] : T(0);
+        const T wjm = cy * s.f[ii + 1][TJ];
+        const T lex = ld(lin[1] + o) + wj - wjm;
+        v = ld(ce + o) * s.gx[TJ + 1] * idl * lex;
+      }
+      s.a[ii][TJ] = v;
+    } else if (warp == 1) {
+      const int ih = i0 + TI;
+      T v = T(0);
+      if (ih < H && j < W) {
+        const long long o = ih * py + j;
+        const T cx = dt * s.gx[jj + 1] * idl;
+        const T wi = (ih < H - 1) ? cx * s.f[TI + 1][jj + 1] : T(0);
+        const T wim = cx * s.f[TI][jj + 1];
+        const T ley = ld(lin[2] + o) - wi + wim;
+        v = ld(ce + o) * s.gy[TI + 1] * idl * ley;
+      }
+      s.b[TI][jj] = v;
+    }
+  }
+  __syncthreads();
+
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int ii = warp + 8 * r, i = i0 + ii;
+    if (i >= H || j >= W) continue;
+    const long long o = i * py + j;
+    const T bx = s.bx[jj + 1], by = s.by[ii + 1];
+    if (POL == DN_TM) {
+      const T lez = ld(lin[0] + o) + mon_inject<T>(I, i, j, n);
+      I.grad[o] += static_cast<double>(lez) * static_cast<double>(ld(curl[0] + o));
+      lout[0][o] = bx * by * lez + (s.a[ii][jj + 1] - s.a[ii][jj]) - (s.b[ii + 1][jj] - s.b[ii][jj]);
+      lout[1][o] = by * a_own[r];
+      lout[2][o] = bx * b_own[r];
+    } else {
+      const T lhz = s.f[ii + 1][jj + 1];
+      lout[0][o] = bx * by * lhz + (s.a[ii][jj] - s.a[ii][jj + 1]) - (s.b[ii][jj] - s.b[ii + 1][jj]);
+      lout[1][o] = bx * a_own[r];
+      lout[2][o] = by * b_own[r];
+    }
+  }
+  __syncthreads();
+}
+
+
+template <typename T>
+__device__ __forceinline__ Sets<T> field_set(void* const f[3]) {
+  return Sets<T>{{static_cast<T*>(f[0]), static_cast<T*>(f[1]), static_cast<T*>(f[2])}};
+}
+
+template <typename T>
+__device__ __forceinline__ Sets<T> slot_set(void* base, long long slot, long long field_elems,
+                                            int nfields) {
+  Sets<T> s{{nullptr, nullptr, nullptr}};
+  T* b = static_cast<T*>(base) + slot * nfields * field_elems;
+  for (int c = 0; c < nfields; ++c) s.p[c] = b + c * field_elems;
+  return s;
+}
+
+template <typename T, int POL, int TI>
+__global__ void __launch_bounds__(NTB) k_batch2d_fwd(unsigned char* table, int* status) {
+  __shared__ TileSmem<T, TI> s;
+  const TableView v = view(table);
+  __shared__ unsigned int s_gen;
+  if (threadIdx.x == 0) s_gen = *reinterpret_cast<volatile unsigned int*>(&v.h->bar[1]);
+  __syncthreads();
+  unsigned int gen = s_gen;
+  const int K = v.h->K;
+  for (int n = 0; n < v.h->max_steps; ++n) {
+    const int nt = active_tiles(v, n);
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+      const int2 m = v.tile_map[t];
+      const dn_batch2d_inst& I = v.inst[m.x];
+      const int ntx = (I.W + TJ - 1) / TJ;
+      const int i0 = (m.y / ntx) * TI, j0 = (m.y % ntx) * TJ;
+      const Sets<T> in = field_set<T>(I.f[n & 1]);
+      const Sets<T> out = field_set<T>(I.f[(n + 1) & 1]);
+      Sets<T> ck{{nullptr, nullptr, nullptr}};
+      const bool save = I.ckpt != nullptr && K > 0 && (n + 1) % K == 0 && (n + 1) < I.n_steps;
+      if (save) ck = slot_set<T>(I.ckpt, (n + 1) / K - 1, (long long)I.H * I.pitch, 3);
+      fwd_tile<T, POL, TI>(s, I, i0, j0, n, in, false, out, ck, save, ck, false, true);
+    }
+    if (!grid_sync(v.h->bar, gen, status)) return;
+  }
+}
+
+template <typename T, int POL, int TI>
+__global__ void __launch_bounds__(NTB) k_batch2d_bwd(unsigned char* table, int* status) {
+  __shared__ TileSmem<T, TI> s;
+  const TableView v = view(table);
+  __shared__ unsigned int s_gen;
+  if (threadIdx.x == 0) s_gen = *reinterpret_cast<volatile unsigned int*>(&v.h->bar[1]);
+  __syncthreads();
+  unsigned int gen = s_gen;
+  const int K = v.h->K;
+  constexpr int NCURL = POL == DN_TM ? 1 : 2;
+  for (int g = v.h->nseg - 1; g >= 0; --g) {
+    const int ta = g * K, tb = min(v.h->max_steps, ta + K);
+    // replay steps ta..tb-1 from the checkpoint at ta, curls recorded
+    for (int n = ta; n < tb; ++n) {
+      const int nt = active_tiles(v, n);
+      for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const int2 m = v.tile_map[t];
+        const dn_batch2d_inst& I = v.inst[m.x];
+        const int ntx = (I.W + TJ - 1) / TJ;
+        const int i0 = (m.y / ntx) * TI, j0 = (m.y % ntx) * TJ;
+        const long long fe = (long long)I.H * I.pitch;
+        const bool zero_in = n == ta && g == 0;
+        const Sets<T> in = n == ta ? (g == 0 ? field_set<T>(I.f[0]) : slot_set<T>(I.ckpt, g - 1, fe, 3))
+                                   : field_set<T>(I.f[n & 1]);
+        const Sets<T> out = field_set<T>(I.f[(n + 1) & 1]);
+        const Sets<T> cr = slot_set<T>(I.curl, n - ta, fe, NCURL);
+        fwd_tile<T, POL, TI>(s, I, i0, j0, n, in, zero_in, out, out, false, cr, true, false);
+      }
+      if (!grid_sync(v.h->bar, gen, status)) return;
+    }
+    // reverse steps tb-1 .. ta
+    for (int n = tb - 1; n >= ta; --n) {
+      const int nt = active_tiles(v, n);
+      for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const int2 m = v.tile_map[t];
+        const dn_batch2d_inst& I = v.inst[m.x];
+        const int ntx = (I.W + TJ - 1) / TJ;
+        const int i0 = (m.y / ntx) * TI, j0 = (m.y % ntx) * TJ;
+        const long long fe = (long long)I.H * I.pitch;
+        const Sets<T> lin = field_set<T>(I.lam[(n + 1) & 1]);
+        const Sets<T> lout = field_set<T>(I.lam[n & 1]);
+        const Sets<T> cr = slot_set<T>(I.curl, n - ta, fe, NCURL);
+        adj_tile<T, POL, TI>(s, I, i0, j0, n, lin, lout, cr);
+      }
+      if (!grid_sync(v.h->bar, gen, status)) return;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+int validate(const dn_batch2d* cfg, const dn_batch2d_inst* insts) {
+  if (!cfg || !insts || cfg->n_inst < 1) return DN_EINVAL;
+  if (cfg->pol != DN_TM && cfg->pol != DN_TE) return DN_EINVAL;
+  if (cfg->dtype != DN_F32 && cfg->dtype != DN_F64) return DN_EINVAL;
+  if (cfg->K < 1) return DN_EINVAL;
+  if (cfg->tile_rows != 8 && cfg->tile_rows != 16 && cfg->tile_rows != 32) return DN_EINVAL;
+  const int first = cfg->pol == DN_TM ? DN_EZ : DN_HZ;
+  for (int b = 0; b < cfg->n_inst; ++b) {
+    const dn_batch2d_inst& I = insts[b];
+    if (I.H < 1 || I.W < 1 || I.pitch < I.W || I.n_steps < 1) return DN_EINVAL;
+    if (!(I.dt > 0.0) || !(I.dl > 0.0) || !I.ce || !I.b[0] || !I.b[1] || !I.c[0] || !I.c[1])
+      return DN_EINVAL;
+    for (int s = 0; s < 2; ++s)
+      for (int c = 0; c < 3; ++c)
+        if (!I.f[s][c]) return DN_EINVAL;
+    if (I.src_comp != DN_NONE) {
+      if (I.src_comp != first || !I.wave || !box_ok(I.src_box, 1, I.H, I.W)) return DN_EINVAL;
+    }
+    if (I.mon_comp != DN_NONE) {
+      if (I.mon_comp != first || !box_ok(I.mon_box, 1, I.H, I.W) || I.n_freq < 1 ||
+          I.n_freq > DN_MAX_FREQS || !I.phase || !I.acc)
+        return DN_EINVAL;
+    }
+  }
+  return DN_OK;
+}
+
+int total_tiles_of(const dn_batch2d* cfg, const dn_batch2d_inst* insts) {
+  long long t = 0;
+  for (int b = 0; b < cfg->n_inst; ++b)
+    t += (long long)((insts[b].W + TJ - 1) / TJ) * ((insts[b].H + cfg->tile_rows - 1) / cfg->tile_rows);
+  return t > 0x7fffffffLL ? -1 : (int)t;
+}
+
+template <typename T, int POL, int TI>
+int launch(bool fwd, void* table, int* status, cudaStream_t s, int max_tiles) {
+  auto kern = fwd ? k_batch2d_fwd<T, POL, TI> : k_batch2d_bwd<T, POL, TI>;
+  int dev = 0, nsm = 0, per_sm = 0;
+  DN_CUDA_CHECK(cudaGetDevice(&dev));
+  DN_CUDA_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  DN_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NTB, 0));
+  if (per_sm < 1) return DN_EUNSUPPORTED;
+  int grid = nsm * per_sm;
+  if (grid > max_tiles) grid = max_tiles;
+  // the barrier words start from zero arrivals and no abort
+  DN_CUDA_CHECK(cudaMemsetAsync(static_cast<unsigned char*>(table) + offsetof(TableHeader, bar),
+                                0, sizeof(unsigned int) * 4, s));
+  void* args[] = {&table, &status};
+  DN_CUDA_CHECK(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(kern), dim3(grid), dim3(NTB),
+                                            args, 0, s));
+  return DN_OK;
+}
+
+template <typename T, int POL>
+int dispatch_rows(bool fwd, int rows, void* table, int* status, cudaStream_t s, int max_tiles) {
+  if (rows == 8) return launch<T, POL, 8>(fwd, table, status, s, max_tiles);
+  if (rows == 16) return launch<T, POL, 16>(fwd, table, status, s, max_tiles);
+  return launch<T, POL, 32>(fwd, table, status, s, max_tiles);
+}
+
+int run(bool fwd, const dn_batch2d* cfg, void* dev_table, int32_t* status, void* stream,
+        int max_tiles) {
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const bool tm = cfg->pol == DN_TM;
+  if (cfg->dtype == DN_F32)
+    return tm ? dispatch_rows<float, DN_TM>(fwd, cfg->tile_rows, dev_table, status, s, max_tiles)
+              : dispatch_rows<float, DN_TE>(fwd, cfg->tile_rows, dev_table, status, s, max_tiles);
+  return tm ? dispatch_rows<double, DN_TM>(fwd, cfg->tile_rows, dev_table, status, s, max_tiles)
+            : dispatch_rows<double, DN_TE>(fwd, cfg->tile_rows, dev_table, status, s, max_tiles);
+}
+
+}  // namespace
+}  // namespace dn
+
+extern "C" int64_t dn_batch2d_table_bytes(const dn_batch2d* cfg, const dn_batch2d_inst* insts) {
+  if (dn::validate(cfg, insts) != DN_OK) return -1;
+  const int tt = dn::total_tiles_of(cfg, insts);
+  if (tt < 0) return -1;
+  size_t op, os, om, oi, oe;
+  dn::table_offsets(cfg->n_inst, tt, &op, &os, &om, &oi, &oe);
+  return (int64_t)oe;
+}
+
+extern "C" int32_t dn_batch2d_pack(const dn_batch2d* cfg, const dn_batch2d_inst* insts,
+                                   void* host_table, int64_t bytes) {
+  int rc = dn::validate(cfg, insts);
+  if (rc != DN_OK) return rc;
+  if (!host_table || bytes < dn_batch2d_table_bytes(cfg, insts)) return DN_EINVAL;
+  const int n = cfg->n_inst;
+  const int tt = dn::total_tiles_of(cfg, insts);
+  std::vector<int> order(n);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return insts[a].n_steps > insts[b].n_steps; });
+  unsigned char* base = static_cast<unsigned char*>(host_table);
+  std::memset(base, 0, (size_t)bytes);
+  size_t op, os, om, oi, oe;
+  dn::table_offsets(n, tt, &op, &os, &om, &oi, &oe);
+  dn::TableHeader* h = reinterpret_cast<dn::TableHeader*>(base);
+  h->n_inst = n;
+  h->total_tiles = tt;
+  h->K = cfg->K;
+  h->tile_rows = cfg->tile_rows;
+  int* prefix = reinterpret_cast<int*>(base + op);
+  int* steps = reinterpret_cast<int*>(base + os);
+  int2* map = reinterpret_cast<int2*>(base + om);
+  dn_batch2d_inst* inst = reinterpret_cast<dn_batch2d_inst*>(base + oi);
+  int t = 0, max_steps = 0;
+  for (int k = 0; k < n; ++k) {
+    const dn_batch2d_inst& I = insts[order[k]];
+    inst[k] = I;
+    steps[k] = I.n_steps;
+    prefix[k] = t;
+    const int ntiles = ((I.W + dn::TJ - 1) / dn::TJ) * ((I.H + cfg->tile_rows - 1) / cfg->tile_rows);
+    for (int q = 0; q < ntiles; ++q) map[t++] = make_int2(k, q);
+    max_steps = std::max(max_steps, I.n_steps);
+  }
+  prefix[n] = t;
+  h->max_steps = max_steps;
+  h->nseg = (max_steps + cfg->K - 1) / cfg->K;
+  return DN_OK;
+}
+
+extern "C" int32_t dn_batch2d_forward(const dn_batch2d* cfg, void* dev_table, int32_t* status,
+                                      void* stream) {
+  if (!cfg || !dev_table || (reinterpret_cast<uintptr_t>(dev_table) & 15)) return DN_EINVAL;
+  if (cfg->tile_rows != 8 && cfg->tile_rows != 16 && cfg->tile_rows != 32) return DN_EINVAL;
+  if (cfg->pol != DN_TM && cfg->pol != DN_TE) return DN_EINVAL;
+  if (cfg->dtype != DN_F32 && cfg->dtype != DN_F64) return DN_EINVAL;
+  return dn::run(true, cfg, dev_table, status, stream, cfg->max_ctas > 0 ? cfg->max_ctas : 1 << 30);
+}
+
+extern "C" int32_t dn_batch2d_backward(const dn_batch2d* cfg, void* dev_table, int32_t* status,
+                                       void* stream) {
+  if (!cfg || !dev_table || (reinterpret_cast<uintptr_t>(dev_table) & 15)) return DN_EINVAL;
+  if (cfg->tile_rows != 8 && cfg->tile_rows != 16 && cfg->tile_rows != 32) return DN_EINVAL;
+  if (cfg->pol != DN_TM && cfg->pol != DN_TE) return DN_EINVAL;
+  if (cfg->dtype != DN_F32 && cfg->dtype != DN_F64) return DN_EINVAL;
+  return dn::run(false, cfg, dev_table, status, stream, cfg->max_ctas > 0 ? cfg->max_ctas : 1 << 30);
+}

@@ -24,4 +24,25 @@ extern "C" const char* dn_strerror(int32_t status) {
 
 extern "C" int32_t dn_version(void) { return 1; }
 
+#include <cstring>
+
+extern "C" int64_t dn_struct_size(const char* name) {
+  if (!name) return -1;
+  struct Entry {
+    const char* n;
+    int64_t s;
+  };
+  static const Entry table[] = {
+      {"dn_box", sizeof(dn_box)},         {"dn_grid", sizeof(dn_grid)},
+      {"dn_cpml", sizeof(dn_cpml)},       {"dn_source", sizeof(dn_source)},
+      {"dn_monitor", sizeof(dn_monitor)}, {"dn_probe", sizeof(dn_probe)},
+      {"dn_curl_record", sizeof(dn_curl_record)},
+      {"dn_batch2d_inst", sizeof(dn_batch2d_inst)},
+      {"dn_batch2d", sizeof(dn_batch2d)},
+  };
+  for (const Entry& e : table)
+    if (std::strcmp(e.n, name) == 0) return e.s;
+  return -1;
+}
+
 extern "C" int32_t dn_last_cuda_error(void) { return dn::last_cuda_error(); }

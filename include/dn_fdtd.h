@@ -135,6 +135,9 @@ typedef struct {
 
 /* ---- library information ------------------------------------------------ */
 const char* dn_strerror(int32_t status);
+/* sizeof of an ABI struct by name ("dn_grid", "dn_batch2d_inst", ...), -1 if
+ * unknown: lets a binding check its struct mirrors */
+int64_t dn_struct_size(const char* name);
 int32_t dn_version(void);
 /* last CUDA error code seen by the library on this thread (0 if none) */
 int32_t dn_last_cuda_error(void);
@@ -186,6 +189,72 @@ int32_t dn_fdtd3d_adjoint(const dn_grid* g, void* const la[6], void* const lb[6]
                           const dn_cpml* cpml, const dn_curl_record* curl, double* grad_ce,
                           const dn_monitor* mons, int32_t n_mon, int32_t t_end, int32_t nsteps,
                           int32_t* status, void* stream, int32_t* final_in_b);
+
+/* ---- batched 2-D instances in one persistent launch ----------------------
+ * Many independent 2-D grids of different sizes and step counts (robust-
+ * design variants, wavelength sweeps) advanced together by one persistent
+ * cooperative kernel: each global step processes every tile of every
+ * instance that still has steps left, then all CTAs meet at a grid barrier
+ * (bounded spin; DN_ETIMEOUT on expiry).  The backward kernel walks the
+ * checkpoint segments from the last: it replays each segment from its
+ * checkpoint with the curl record on, then runs the segment's reverse steps,
+ * injecting monitor-DFT gradients as it loads the adjoint field.
+ * No reference counterpart (the reference runs one solver object per grid).
+ *
+ * Per instance (host array, packed by dn_batch2d_pack into a device table):
+ * fields are the polarisation's three components in the order TM (Ez, Hx,
+ * Hy) / TE (Hz, Ex, Ey), each H x pitch elements, two ping-pong sets; after
+ * n_steps the state is in set n_steps % 2.  Checkpoints (states at steps K,
+ * 2K, ... < n_steps) are [slot-1][3][H*pitch]; the curl record of one segment
+ * is [K][ncurl][H*pitch] (TM: Ez; TE: Ex, Ey); adjoint sets likewise, the
+ * gradient of the final field goes into lam[n_steps % 2] before the backward
+ * launch, the result accumulates into grad (FP64 [H*pitch]). */
+typedef struct {
+  int32_t H, W;
+  int64_t pitch;
+  int32_t n_steps;
+  int32_t src_comp;           /* DN_EZ (TM) / DN_HZ (TE) / DN_NONE */
+  dn_box src_box;
+  const void* wave;           /* [n_steps] */
+  void* f[2][3];
+  const void* ce;
+  const double* b[2];         /* CPML: [0] rows (length H), [1] columns (length W) */
+  const double* c[2];
+  double dt, dl;
+  int32_t mon_comp;           /* DN_NONE or the polarisation's first field */
+  dn_box mon_box;
+  int32_t n_freq;
+  const double* phase;        /* [n_steps][n_freq][2] */
+  double* acc;                /* [n_freq][cells][2] */
+  void* ckpt;
+  void* curl;
+  void* lam[2][3];
+  double* grad;
+  const double* gmon;         /* [n_freq][cells][2], may be NULL */
+} dn_batch2d_inst;
+
+typedef struct {
+  int32_t pol;        /* DN_TM / DN_TE, all instances */
+  int32_t dtype;      /* DN_F32 / DN_F64 */
+  int32_t n_inst;
+  int32_t K;          /* checkpoint interval in steps (>= 1) */
+  int32_t tile_rows;  /* 8, 16 or 32 (tile = tile_rows x 32 cells) */
+  int32_t max_ctas;   /* upper bound on the persistent grid (0: as many as fit) */
+} dn_batch2d;
+
+/* bytes of the device table for this batch */
+int64_t dn_batch2d_table_bytes(const dn_batch2d* cfg, const dn_batch2d_inst* insts);
+/* pack the batch into `host_table` (dn_batch2d_table_bytes bytes); the caller
+ * copies it to device memory and passes that copy to the launches below */
+int32_t dn_batch2d_pack(const dn_batch2d* cfg, const dn_batch2d_inst* insts, void* host_table,
+                        int64_t bytes);
+/* forward: all steps of all instances (monitors accumulate, checkpoints are
+ * written when K < n_steps) in one persistent launch */
+int32_t dn_batch2d_forward(const dn_batch2d* cfg, void* dev_table, int32_t* status,
+                           void* stream);
+/* backward: replay + reverse sweep of all instances in one persistent launch */
+int32_t dn_batch2d_backward(const dn_batch2d* cfg, void* dev_table, int32_t* status,
+                            void* stream);
 
 /* ---- figure of merit ----------------------------------------------------
  * *out = sum_i |dft[i]|^2 over n_complex FP64 (re, im) pairs, reduced in FP64

@@ -1,0 +1,94 @@
+"""Batched 2-D path (one persistent launch for many grids) against the
+single-grid solver: fields, monitor DFTs and dL/deps of every instance, with
+ragged sizes, different step counts, several checkpoint segments, TM and TE,
+every tile height, and the CUDA-graph replay."""
+
+from __future__ import annotations
+
+import pytest
+import torch
+from conftest import rel_l2
+
+import diffnano_b200 as dn
+from diffnano_b200.solvers.batch2d import BatchInstance, FDTDBatch2D, autotune_tile_rows
+
+pytestmark = pytest.mark.gpu
+
+SHAPES = [(40, 36), (70, 50), (33, 90), (64, 64), (20, 24)]
+STEPS = [60, 45, 90, 30, 75]
+
+
+def _specs(pol, monitor=True):
+    out = []
+    for n, (shape, T) in enumerate(zip(SHAPES, STEPS)):
+        src = {"type": "gaussian_pulse", "row": 5 + n, "spread": 300.0, "t0": 900.0}
+        mon = {"row": shape[0] - 6, "wavelengths_nm": [1500.0, 1550.0 + 20 * n]} if monitor else None
+        out.append(BatchInstance(grid_shape=shape, n_steps=T, dl=20.0,
+                                 wavelength_nm=1450.0 + 40 * n, pml_layers=4, courant=0.5,
+                                 source=src, monitor=mon))
+    return out
+
+
+def _eps(seed):
+    g = torch.Generator().manual_seed(seed)
+    return [1.5 + 2.0 * torch.rand(*s, dtype=torch.float64, generator=g) for s in SHAPES]
+
+
+def _single(spec, pol, dtype, cuda, eps):
+    s = dn.FDTDSolver2D(grid_shape=spec.grid_shape, dl=spec.dl, wavelength_nm=spec.wavelength_nm,
+                        polarization=pol, pml_layers=spec.pml_layers, n_steps=spec.n_steps,
+                        courant=spec.courant, device=cuda, dtype=dtype)
+    comp = "Ez" if pol == "TM" else "Hz"
+    mons = [{"component": comp, **spec.monitor}] if spec.monitor else None
+    return s.forward(eps, source=dict(spec.source), monitors=mons)
+
+
+@pytest.mark.parametrize("rows", [8, 16, 32])
+@pytest.mark.parametrize("pol", ["TM", "TE"])
+def test_batched_forward_matches_single_grids(cuda, pol, rows):
+    specs = _specs(pol)
+    eps = _eps(1)
+    b = FDTDBatch2D(specs, pol, torch.float32, cuda, checkpoint_interval=16, tile_rows=rows)
+    fields, dfts = b.forward([e.to(cuda) for e in eps])
+    for spec, e, f, d in zip(specs, eps, fields, dfts):
+        r = _single(spec, pol, torch.float32, cuda, e.to(cuda))
+        assert rel_l2(f, r.field[0]) < 1e-6
+        assert rel_l2(torch.view_as_real(d), torch.view_as_real(r.metadata["monitors"][0]["dft"])) < 1e-6
+
+
+@pytest.mark.parametrize("pol", ["TM", "TE"])
+def test_batched_gradients_match_single_grids(cuda, pol):
+    specs = _specs(pol)
+    eps0 = _eps(2)
+    gen = torch.Generator().manual_seed(3)
+    G = [torch.randn(*s, dtype=torch.float64, generator=gen) for s in SHAPES]
+    b = FDTDBatch2D(specs, pol, torch.float64, cuda, checkpoint_interval=7, tile_rows=16)
+    eps = [e.clone().to(cuda).requires_grad_(True) for e in eps0]
+    fields, dfts = b.forward(eps)
+    loss = sum((f * g.to(cuda)).sum() + (d.abs() ** 2).sum() for f, g, d in zip(fields, G, dfts))
+    loss.backward()
+    for spec, e0, e, g in zip(specs, eps0, eps, G):
+        ref = e0.clone().to(cuda).requires_grad_(True)
+        r = _single(spec, pol, torch.float64, cuda, ref)
+        ((r.field[0] * g.to(cuda)).sum() + (r.metadata["monitors"][0]["dft"].abs() ** 2).sum()).backward()
+        assert rel_l2(e.grad, ref.grad) < 1e-9
+
+
+def test_batched_graph_replay_matches_direct(cuda):
+    specs = _specs("TM")
+    b = FDTDBatch2D(specs, "TM", torch.float32, cuda, tile_rows=16)
+    for seed in (4, 5):
+        eps = [e.to(cuda) for e in _eps(seed)]
+        f_graph, d_graph = b.forward_graphed(eps)
+        f_direct, d_direct = b.run_forward(eps)
+        for a, c in zip(f_graph, f_direct):
+            assert torch.equal(a, c)
+
+
+def test_autotuner_picks_a_candidate_and_caches(cuda, tmp_path, monkeypatch):
+    monkeypatch.setenv("XDG_CACHE_HOME", str(tmp_path))
+    b = FDTDBatch2D(_specs("TM", monitor=False), "TM", torch.float32, cuda)
+    rows = autotune_tile_rows(b)
+    assert rows in (8, 16, 32)
+    assert (tmp_path / "diffnano_b200" / "autotune.json").exists()
+    assert autotune_tile_rows(b) == rows

@@ -131,3 +131,20 @@ def test_adjoint_rejects_missing_curl_record(fn):
     rc = getattr(L, fn)(ctypes.byref(g), fake, fake, 256, ctypes.byref(cp), ctypes.byref(rec), 256,
                         None, 0, 4, 4, None, None, ctypes.byref(out))
     assert rc == _lib.DN_EINVAL
+
+
+@pytest.mark.parametrize("name", sorted(_lib.STRUCTS))
+def test_ctypes_struct_mirrors_match_the_c_abi(name):
+    assert _lib.lib().dn_struct_size(name.encode()) == ctypes.sizeof(_lib.STRUCTS[name])
+
+
+def test_batch2d_rejects_bad_configs():
+    L = _lib.lib()
+    cfg = _lib.DnBatch2d(pol=_lib.DN_TM, dtype=_lib.DN_F32, n_inst=1, K=0, tile_rows=16)
+    inst = (_lib.DnBatch2dInst * 1)()
+    assert L.dn_batch2d_table_bytes(ctypes.byref(cfg), inst) == -1  # K = 0
+    cfg.K = 8
+    cfg.tile_rows = 12
+    assert L.dn_batch2d_table_bytes(ctypes.byref(cfg), inst) == -1  # tile rows
+    cfg.tile_rows = 16
+    assert L.dn_batch2d_table_bytes(ctypes.byref(cfg), inst) == -1  # empty instance
