@@ -11,9 +11,10 @@ same step arithmetic as the single-grid kernels.  Each instance is described
 by the reference's own constructor arguments and source dict, plus one DFT
 line/point/box monitor on its injected field.
 
-``forward`` is differentiable with respect to every instance's eps; the
-launches can be recorded in a CUDA graph and replayed (``graph=True``) when
-the same batch is solved repeatedly (design iterations).  The tile height is
+``forward`` is differentiable with respect to every instance's eps;
+``forward_graphed`` records the eps upload, reset and persistent launch in a
+CUDA graph and replays it when the same batch is solved repeatedly (design
+iterations).  The tile height is
 chosen by ``autotune_tile_rows`` (measured, cached per device and batch
 signature).
 """
@@ -27,7 +28,6 @@ import math
 import os
 from dataclasses import dataclass, field
 
-import numpy as np
 import torch
 
 from diffnano_b200 import _lib
