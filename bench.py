@@ -389,6 +389,67 @@ def run_ours(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# secondary workload: 64 ragged 2-D instances, forward + adjoint, one
+# persistent launch each (not the default bench line)
+# ---------------------------------------------------------------------------
+BATCH_SIDES = (128, 192, 256, 384, 512, 768, 1024)
+
+
+def batch2d_workload(n_inst=64, seed=7):
+    from diffnano_b200.solvers.batch2d import BatchInstance
+    from diffnano_b200.workloads import blob_eps_2d, gaussian_pulse_for_band
+
+    g = torch.Generator().manual_seed(seed)
+    sides = [BATCH_SIDES[int(i)] for i in torch.randint(0, len(BATCH_SIDES), (n_inst,), generator=g)]
+    wls = torch.linspace(1450.0, 1650.0, 8).tolist()
+    specs, eps = [], []
+    for b, side in enumerate(sides):
+        T = int(round(1500 + (side - 128) * 4500 / 896))
+        wl = wls[b % 8]
+        src = gaussian_pulse_for_band(wl, 200.0)
+        src.update(row=30)
+        specs.append(BatchInstance(grid_shape=(side, side), n_steps=T, dl=20.0, wavelength_nm=wl,
+                                   pml_layers=20, courant=0.5, source=src,
+                                   monitor={"row": side - 30, "wavelengths_nm": [wl]}))
+        eps.append(blob_eps_2d(side, min(128, side - 64), seed=b // 3, variant=(b % 3) - 1))
+    return specs, eps
+
+
+def run_batch2d(args):
+    from diffnano_b200.solvers.batch2d import FDTDBatch2D
+
+    dev = torch.device("cuda", 0)
+    specs, eps = batch2d_workload()
+    cells_steps = sum(s.grid_shape[0] * s.grid_shape[1] * s.n_steps for s in specs)
+    batch = FDTDBatch2D(specs, "TM", torch.float32, dev)
+    e_dev = [e.to(dev).requires_grad_(True) for e in eps]
+    fields, dfts = batch.forward(e_dev)  # warm-up (also autotunes the tile height)
+    sum((d.abs() ** 2).sum() for d in dfts).backward()
+    torch.cuda.synchronize(dev)
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e_dev = [e.to(dev).requires_grad_(True) for e in eps]
+    e0.record()
+    fields, dfts = batch.forward(e_dev)
+    e1.record()
+    sum((d.abs() ** 2).sum() for d in dfts).backward()
+    e2.record()
+    torch.cuda.synchronize(dev)
+    f_s, b_s = e0.elapsed_time(e1) / 1e3, e1.elapsed_time(e2) / 1e3
+    line = {"metric": METRIC, "value": cells_steps / f_s / 1e9, "unit": UNIT, "n_gpus": 1,
+            "steps": 1, "warmup": 1, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "batched_2d_tm_64_instances", "instances": len(specs),
+                       "sides": sorted({s.grid_shape[0] for s in specs}),
+                       "cell_steps": cells_steps, "tile_rows": batch.tile_rows,
+                       "checkpoint_interval": batch.K},
+            "forward_s": f_s, "backward_s": b_s,
+            "backward_gcells": cells_steps / b_s / 1e9,
+            "kernels": "k_batch2d_fwd / k_batch2d_bwd (one persistent launch each)"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -401,6 +462,8 @@ def main():
     ap.add_argument("--adjoint-steps", type=int, default=256)
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-grad-e2e", action="store_true")
+    ap.add_argument("--workload", choices=["fdtd3d", "batch2d"], default="fdtd3d",
+                    help="fdtd3d: the benchmark (3-D 256^3); batch2d: 64 ragged 2-D instances")
     ap.add_argument("--grid", type=int, default=256,
                     help="cubic grid side (256 is the benchmark; smaller sides are for profiling)")
     args = ap.parse_args()
@@ -410,6 +473,8 @@ def main():
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batch2d":
+        return run_batch2d(args)
     return run_ours(args)
 
 
