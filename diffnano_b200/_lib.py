@@ -76,9 +76,29 @@ class DnBatch2d(ctypes.Structure):
                 ("tile_rows", c_int32), ("max_ctas", c_int32)]
 
 
+class DnGemmOperand(ctypes.Structure):
+    _fields_ = [("ptr", c_void_p), ("mn_major", c_int32), ("fold", c_int32), ("rows", c_int64),
+                ("k", c_int64), ("ld", c_int64), ("fold_stride", c_int64),
+                ("batch_stride", c_int64)]
+
+
+class DnGemm(ctypes.Structure):
+    _fields_ = [("M", c_int64), ("N", c_int64), ("batch", c_int32), ("n_seg", c_int32),
+                ("a", DnGemmOperand * 2), ("b", DnGemmOperand * 2), ("out", c_void_p),
+                ("out_dtype", c_int32), ("accumulate", c_int32), ("c_batch_stride", c_int64),
+                ("c_row_radix", c_int64), ("c_row_stride0", c_int64), ("c_row_stride1", c_int64),
+                ("c_col_radix", c_int64), ("c_col_stride0", c_int64), ("c_col_stride1", c_int64),
+                ("alpha", ctypes.c_float), ("act", c_int32), ("bias", c_void_p),
+                ("row_scale", c_void_p), ("batch_scale", c_void_p), ("addend", c_void_p),
+                ("addend_dtype", c_int32), ("aux_dtype", c_int32), ("aux", c_void_p),
+                ("pre", c_void_p), ("pre_dtype", c_int32), ("block_n", c_int32),
+                ("max_ctas", c_int32)]
+
+
 STRUCTS = {"dn_box": DnBox, "dn_grid": DnGrid, "dn_cpml": DnCpml, "dn_source": DnSource,
            "dn_monitor": DnMonitor, "dn_probe": DnProbe, "dn_curl_record": DnCurlRecord,
-           "dn_batch2d_inst": DnBatch2dInst, "dn_batch2d": DnBatch2d}
+           "dn_batch2d_inst": DnBatch2dInst, "dn_batch2d": DnBatch2d,
+           "dn_gemm_operand": DnGemmOperand, "dn_gemm": DnGemm}
 
 PTR6 = c_void_p * 6
 _P6 = ctypes.POINTER(c_void_p)  # a PTR6 instance (or None) is passed here
@@ -114,6 +134,7 @@ SIGNATURES = {
     "dn_batch2d_backward": (c_int32, [ctypes.POINTER(DnBatch2d), c_void_p, c_void_p, c_void_p]),
     "dn_fom_abs2_scratch_bytes": (c_int64, [c_int64]),
     "dn_fom_abs2": (c_int32, [c_void_p, c_int64, c_void_p, c_void_p, c_int64, c_void_p]),
+    "dn_gemm_run": (c_int32, [ctypes.POINTER(DnGemm), c_void_p, c_void_p]),
     "dn_fdtd2d_run_noalloc": (c_int32, [ctypes.POINTER(DnGrid), _P6, c_void_p,
                                         ctypes.POINTER(DnCpml), ctypes.POINTER(DnSource),
                                         ctypes.POINTER(DnMonitor), c_int32,

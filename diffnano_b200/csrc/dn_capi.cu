@@ -1,5 +1,6 @@
 // Library-wide C-ABI helpers: status strings, version, last CUDA error.
 #include "dn_common.cuh"
+#include "dn_fno.h"
 
 namespace dn {
 namespace {
@@ -39,6 +40,8 @@ extern "C" int64_t dn_struct_size(const char* name) {
       {"dn_curl_record", sizeof(dn_curl_record)},
       {"dn_batch2d_inst", sizeof(dn_batch2d_inst)},
       {"dn_batch2d", sizeof(dn_batch2d)},
+      {"dn_gemm_operand", sizeof(dn_gemm_operand)},
+      {"dn_gemm", sizeof(dn_gemm)},
   };
   for (const Entry& e : table)
     if (std::strcmp(e.n, name) == 0) return e.s;

@@ -1,0 +1,108 @@
+/*
+ * dn_fno.h -- C ABI of the surrogate kernels in libdn_fdtd.so: a BF16
+ * tensor-core GEMM (sm_100a tcgen05, FP32 accumulation in tensor memory) with
+ * a fused epilogue, the building block of the Fourier-neural-operator
+ * surrogate's training and inference passes.
+ *
+ * Same conventions as dn_fdtd.h: raw device pointers, element counts and
+ * strides, int status codes (DN_OK ...), asynchronous on the given stream.
+ *
+ * Reference interfaces replaced (DiffNano, paths relative to its checkout):
+ * the reference's surrogate is a small CNN trained with torch ops
+ * (diffnano/surrogate.py:78-285, NeuralSurrogate); it has no Fourier neural
+ * operator and no GEMM of its own.  dn_gemm_run is the one compute entry the
+ * surrogate's Python layer calls for every contraction of the operator
+ * (lifting, truncated 2-D DFT and its inverse, per-mode complex channel
+ * mixing, 1x1 channel mixing, readout) and their gradients.
+ */
+#ifndef DN_FNO_H
+#define DN_FNO_H
+
+#include <stdint.h>
+
+#include "dn_fdtd.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DN_BF16 2 /* element type code next to DN_F32 / DN_F64 */
+
+#define DN_ACT_NONE 0
+#define DN_ACT_GELU 1      /* y = gelu(v) (erf form); `pre` (optional) receives v */
+#define DN_ACT_GELU_GRAD 2 /* y = v * gelu'(aux), aux = the pre-activation       */
+
+/* One BF16 operand of C = A * B^T.  Element (r, k), r the row index (M for A,
+ * N for B) and k the contraction index, of GEMM batch z is at
+ *   K-major  (mn_major = 0): ptr + z*batch_stride + r*ld + k
+ *   MN-major (mn_major = 1): ptr + z*batch_stride + (r / fold)*fold_stride
+ *                                + k*ld + r % fold       (fold = 0: no fold)
+ * Rows r >= rows and k >= k extent read as zero.  ptr is 16-byte aligned;
+ * ld, fold_stride and batch_stride are multiples of 8 elements; fold is a
+ * multiple of 64; batch_stride = 0 shares the operand across batches. */
+typedef struct dn_gemm_operand {
+  const void* ptr;
+  int32_t mn_major;
+  int32_t fold;
+  int64_t rows;
+  int64_t k;
+  int64_t ld;
+  int64_t fold_stride;
+  int64_t batch_stride;
+} dn_gemm_operand;
+
+/* C[z] (M x N) = sum over segments s of A_s[z] * B_s[z]^T  (K_s = a[s].k =
+ * b[s].k), then the epilogue, per element (z, r, c):
+ *   v = alpha * acc * row_scale[r] * batch_scale[z] + bias[c] + addend[z,r,c]
+ *   y = v | gelu(v) | v * gelu'(aux[z,r,c])          (act)
+ *   out[z,r,c] = y   (or += y when accumulate, FP32 output only)
+ * with every optional pointer NULL to skip it.  out, addend, aux and pre
+ * share one index map:
+ *   off(z, r, c) = z*c_batch_stride + (r % c_row_radix)*c_row_stride0
+ *                + (r / c_row_radix)*c_row_stride1
+ *                + (c % c_col_radix)*c_col_stride0 + (c / c_col_radix)*c_col_stride1
+ * (radix 0 = no split).  c_col_radix, when set, is a multiple of 32. */
+typedef struct dn_gemm {
+  int64_t M;
+  int64_t N;
+  int32_t batch;
+  int32_t n_seg; /* 1 or 2 */
+  dn_gemm_operand a[2];
+  dn_gemm_operand b[2];
+  void* out;
+  int32_t out_dtype; /* DN_F32 or DN_BF16 */
+  int32_t accumulate;
+  int64_t c_batch_stride;
+  int64_t c_row_radix;
+  int64_t c_row_stride0;
+  int64_t c_row_stride1;
+  int64_t c_col_radix;
+  int64_t c_col_stride0;
+  int64_t c_col_stride1;
+  float alpha;
+  int32_t act;
+  const float* bias;
+  const float* row_scale;
+  const float* batch_scale;
+  const void* addend;
+  int32_t addend_dtype;
+  int32_t aux_dtype;
+  const void* aux;
+  void* pre;
+  int32_t pre_dtype;
+  int32_t block_n;  /* 0 = choose; else 64, 128 or 256 */
+  int32_t max_ctas; /* 0 = one per SM */
+} dn_gemm;
+
+/* Persistent warp-specialised kernel: a TMA producer warp (128-byte swizzled
+ * 128x64 / block_n x64 tiles), one thread issuing tcgen05.mma (M = 128, K =
+ * 16 each) into double-buffered tensor-memory accumulators, four epilogue
+ * warps.  Bounded waits; a wait that gives up stores DN_ETIMEOUT in *status
+ * (status may be NULL). */
+int32_t dn_gemm_run(const dn_gemm* g, int32_t* status, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DN_FNO_H */
