@@ -450,6 +450,74 @@ def run_batch2d(args):
     return 0
 
 
+def measured_peak_bf16():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d["bf16_tflops"]), float(d["bf16_tflops_sustained"]), "measured"
+    except Exception:
+        return 1590.0, 1400.0, "fallback"
+
+
+def run_fno(args):
+    """Learned surrogate: FDTD-labelled data, BF16 tensor-core training, held-out error."""
+    from diffnano_b200.surrogate.data import FDTDLabeler, TMzSetup, cell_steps, make_dataset
+    from diffnano_b200.surrogate.surrogate import FNOSurrogate
+
+    dev = torch.device("cuda", 0)
+    setup = TMzSetup()
+    lab = FDTDLabeler(setup, chunk=2048, device=dev)
+    n_train, n_test, epochs = args.fno_samples, args.fno_test, args.fno_epochs
+    make_dataset(64, 999, lab)  # warm-up: builds the solver, first launch
+    torch.cuda.synchronize(dev)
+    lab = FDTDLabeler(setup, chunk=2048, device=dev)
+    t0 = time.perf_counter()
+    designs, labels = make_dataset(n_train, 1, lab)
+    torch.cuda.synchronize(dev)
+    label_s = time.perf_counter() - t0
+    test_d, test_l = make_dataset(n_test, 10_000, lab)
+    sur = FNOSurrogate(lab, batch_size=256, lr=1e-3, device=dev, seed=0)
+    with ClockSampler(0) as clocks:
+        hist = sur.train_surrogate(n_epochs=epochs, designs=designs, labels=labels)
+    clk = clocks.summary()
+    acc = sur.accuracy(designs=test_d, labels=test_l)
+    steps = int(sur.timings["train_steps"])
+    flops = sur.net.gemm_flops(256) * steps
+    train_s = sur.timings["train_s"]
+    # inference throughput (prescreening rate), batch 256
+    x = test_d[:256]
+    sur.predict(x)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(10):
+        sur.predict(x)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    infer_s = e0.elapsed_time(e1) / 1e3 / 10
+    peak, peak_sus, kind = measured_peak_bf16()
+    tflops = flops / train_s / 1e12
+    line = {"metric": "FNO surrogate training throughput", "value": n_train * epochs / train_s,
+            "unit": "samples/s", "n_gpus": 1, "steps": steps, "warmup": 0,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16",
+            "data": "synthetic (seeded blob designs labelled by the batched FDTD)",
+            "config": {"workload": "fno_4layer_w64_m16_128x128_b256", "train_designs": n_train,
+                       "test_designs": n_test, "epochs": epochs, "batch": 256, "lr": 1e-3,
+                       "labels": "DFT Ez, 128-point monitor line, 1500/1550/1600 nm, "
+                                 "256x256 TMz FDTD 2000 steps"},
+            "label_s": label_s, "label_gcells": cell_steps(n_train, setup) / label_s / 1e9,
+            "train_s": train_s, "final_train_loss": hist[-1], "first_epoch_loss": hist[0],
+            "heldout": acc,
+            "gain_vs_no_network": acc["mean_predictor_rel_l2"] / acc["mean_rel_l2"],
+            "roofline": {"bound": "tensor", "achieved": tflops, "peak": peak_sus,
+                         "unit": "TFLOP/s", "frac": tflops / peak_sus,
+                         "peak_kind": f"{kind} sustained bf16"},
+            "infer_designs_per_s": 256 / infer_s, "clocks": clk}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -462,8 +530,12 @@ def main():
     ap.add_argument("--adjoint-steps", type=int, default=256)
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-grad-e2e", action="store_true")
-    ap.add_argument("--workload", choices=["fdtd3d", "batch2d"], default="fdtd3d",
-                    help="fdtd3d: the benchmark (3-D 256^3); batch2d: 64 ragged 2-D instances")
+    ap.add_argument("--workload", choices=["fdtd3d", "batch2d", "fno"], default="fdtd3d",
+                    help="fdtd3d: the benchmark (3-D 256^3); batch2d: 64 ragged 2-D instances; "
+                         "fno: surrogate data generation + training")
+    ap.add_argument("--fno-samples", type=int, default=20000)
+    ap.add_argument("--fno-test", type=int, default=1024)
+    ap.add_argument("--fno-epochs", type=int, default=50)
     ap.add_argument("--grid", type=int, default=256,
                     help="cubic grid side (256 is the benchmark; smaller sides are for profiling)")
     args = ap.parse_args()
@@ -475,6 +547,8 @@ def main():
         return run_reference(args)
     if args.workload == "batch2d":
         return run_batch2d(args)
+    if args.workload == "fno":
+        return run_fno(args)
     return run_ours(args)
 
 

@@ -135,6 +135,27 @@ SIGNATURES = {
     "dn_fom_abs2_scratch_bytes": (c_int64, [c_int64]),
     "dn_fom_abs2": (c_int32, [c_void_p, c_int64, c_void_p, c_void_p, c_int64, c_void_p]),
     "dn_gemm_run": (c_int32, [ctypes.POINTER(DnGemm), c_void_p, c_void_p]),
+    "dn_fno_features": (c_int32, [c_void_p, c_int64, c_int32, c_int32, ctypes.c_float,
+                                  ctypes.c_float, c_void_p, c_void_p]),
+    "dn_fno_features_bwd": (c_int32, [c_void_p, c_int64, ctypes.c_float, ctypes.c_float,
+                                      c_void_p, c_void_p]),
+    "dn_fno_readout": (c_int32, [c_void_p, c_void_p, c_int64, c_int32, c_int32, c_int32,
+                                 c_void_p, c_void_p]),
+    "dn_fno_readout_bwd": (c_int32, [c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_int32,
+                                     c_int32, c_void_p, c_void_p, c_void_p]),
+    "dn_colsum_scratch_elems": (c_int64, [c_int64, c_int64]),
+    "dn_colsum": (c_int32, [c_void_p, c_int32, c_int64, c_int64, c_int64, c_void_p, c_int32,
+                            c_void_p, c_int64, c_void_p]),
+    "dn_mse": (c_int32, [c_void_p, c_void_p, c_int64, c_int32, c_int32, ctypes.c_float,
+                         c_void_p, c_void_p, c_int32, c_void_p]),
+    "dn_adam": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, ctypes.c_float,
+                          ctypes.c_float, ctypes.c_float, ctypes.c_float, c_int32,
+                          ctypes.c_float, c_void_p, c_void_p]),
+    "dn_fno_pack_modes": (c_int32, [c_void_p, c_void_p, c_int64, c_int32, c_int32, c_void_p,
+                                    c_void_p]),
+    "dn_fno_unpack_mode_grads": (c_int32, [c_void_p, c_int64, c_int32, c_int32, c_void_p,
+                                           c_void_p, c_void_p]),
+    "dn_f32_to_bf16": (c_int32, [c_void_p, c_int64, c_void_p, c_void_p]),
     "dn_fdtd2d_run_noalloc": (c_int32, [ctypes.POINTER(DnGrid), _P6, c_void_p,
                                         ctypes.POINTER(DnCpml), ctypes.POINTER(DnSource),
                                         ctypes.POINTER(DnMonitor), c_int32,

@@ -1,0 +1,364 @@
+// Memory-bound helper kernels of the Fourier-neural-operator surrogate (the
+// contractions themselves run on the tcgen05 GEMM in dn_gemm.cu):
+//   * input features from a permittivity map, and their gradient back to eps
+//   * the readout that collapses the field's row axis with learned per-row,
+//     per-channel weights, and its backward pass
+//   * deterministic column sums (bias gradients, reductions of per-sample
+//     weight-gradient partials)
+//   * mean-squared-error loss with its BF16 gradient
+//   * Adam on an FP32 master copy with a BF16 mirror
+//   * packing of the complex per-mode weights into the real 2x2 block form the
+//     mixing GEMM reads, and the matching gradient unpacking
+// Layouts are channel-last (sample, row, column, channel) unless stated.
+#include <cuda_bf16.h>
+
+#include "dn_common.cuh"
+#include "dn_fno.h"
+
+namespace dn {
+namespace fa {
+
+__device__ __forceinline__ float bf2f(unsigned short h) {
+  return __uint_as_float(static_cast<uint32_t>(h) << 16);
+}
+__device__ __forceinline__ unsigned short f2bf(float v) {
+  return __bfloat16_as_ushort(__float2bfloat16_rn(v));
+}
+
+constexpr int FEAT = 8;  // features per pixel: eps (normalised), x, y, 5 zeros
+
+__global__ void k_features(const float* __restrict__ eps, long long n_img, int H, int W,
+                           float lo, float inv_span, unsigned short* __restrict__ feat) {
+  const long long n = n_img * H * W;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int w = (int)(i % W);
+    const int h = (int)((i / W) % H);
+    const float f0 = (eps[i] - lo) * inv_span;
+    const float fx = W > 1 ? (float)w / (float)(W - 1) : 0.0f;
+    const float fy = H > 1 ? (float)h / (float)(H - 1) : 0.0f;
+    uint4 u;
+    u.x = (uint32_t)f2bf(f0) | ((uint32_t)f2bf(fx) << 16);
+    u.y = (uint32_t)f2bf(fy);
+    u.z = 0u;
+    u.w = 0u;
+    reinterpret_cast<uint4*>(feat)[i] = u;
+  }
+}
+
+__global__ void k_features_bwd(const float* __restrict__ dfeat, long long n, float inv_span,
+                               float* __restrict__ deps) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    deps[i] = dfeat[i * FEAT] * inv_span;
+}
+
+// out[b, w, c] = sum_h r[h, c] * x[b, h, w, c]; one thread per (b, w, c)
+__global__ void k_readout(const unsigned short* __restrict__ x, const float* __restrict__ r,
+                          long long nb, int H, int W, int C, unsigned short* __restrict__ out) {
+  const long long n = nb * W * C;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(i % C);
+    const long long wc = i % ((long long)W * C);
+    const long long b = i / ((long long)W * C);
+    const unsigned short* xb = x + b * H * W * C + wc;
+    float s = 0.0f;
+    for (int h = 0; h < H; ++h) s = fmaf(r[h * C + c], bf2f(xb[(long long)h * W * C]), s);
+    out[i] = f2bf(s);
+  }
+}
+
+// dx[b, h, w, c] = r[h, c] * dR[b, w, c]            (one thread per element)
+__global__ void k_readout_bwd_x(const float* __restrict__ r, const unsigned short* __restrict__ dR,
+                                long long nb, int H, int W, int C, unsigned short* __restrict__ dx) {
+  const long long n = nb * H * W * C;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(i % C);
+    const long long wc = i % ((long long)W * C);
+    const int h = (int)((i / ((long long)W * C)) % H);
+    const long long b = i / ((long long)H * W * C);
+    dx[i] = f2bf(r[h * C + c] * bf2f(dR[b * W * C + wc]));
+  }
+}
+
+// dr_part[b, h, c] = sum_w dR[b, w, c] * x[b, h, w, c]   (one thread per (b, h, c))
+__global__ void k_readout_bwd_r(const unsigned short* __restrict__ x,
+                                const unsigned short* __restrict__ dR, long long nb, int H, int W,
+                                int C, float* __restrict__ dr_part) {
+  const long long n = nb * H * C;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(i % C);
+    const int h = (int)((i / C) % H);
+    const long long b = i / ((long long)H * C);
+    const unsigned short* xr = x + ((b * H + h) * W) * (long long)C + c;
+    const unsigned short* dr = dR + b * W * (long long)C + c;
+    float s = 0.0f;
+    for (int w = 0; w < W; ++w) s = fmaf(bf2f(dr[(long long)w * C]), bf2f(xr[(long long)w * C]), s);
+    dr_part[i] = s;
+  }
+}
+
+// column sums, pass 1: block (bx, by) sums rows [by*rpb, (by+1)*rpb) of
+// columns bx*256 + threadIdx.x into part[by, col]
+__global__ void k_colsum_part(const void* __restrict__ in, int bf16, long long rows,
+                              long long cols, long long ld, long long rpb,
+                              float* __restrict__ part) {
+  const long long col = blockIdx.x * 256LL + threadIdx.x;
+  if (col >= cols) return;
+  const long long r0 = blockIdx.y * rpb;
+  const long long r1 = r0 + rpb < rows ? r0 + rpb : rows;
+  float s = 0.0f;
+  if (bf16) {
+    const unsigned short* p = static_cast<const unsigned short*>(in);
+    for (long long r = r0; r < r1; ++r) s += bf2f(p[r * ld + col]);
+  } else {
+    const float* p = static_cast<const float*>(in);
+    for (long long r = r0; r < r1; ++r) s += p[r * ld + col];
+  }
+  part[blockIdx.y * cols + col] = s;
+}
+
+// pass 2: out[col] (+)= sum over the parts, in order
+__global__ void k_colsum_final(const float* __restrict__ part, long long nparts, long long cols,
+                               float* __restrict__ out, int accumulate) {
+  const long long col = blockIdx.x * 256LL + threadIdx.x;
+  if (col >= cols) return;
+  float s = 0.0f;
+  for (long long q = 0; q < nparts; ++q) s += part[q * cols + col];
+  out[col] = accumulate ? out[col] + s : s;
+}
+
+// MSE over the first `used` of `ld` columns; grad = scale * 2 (pred - target)
+// as BF16 (padding columns zero); per-block partial losses in double
+__global__ void k_mse(const float* __restrict__ pred, const float* __restrict__ target,
+                      long long rows, int ld, int used, float gscale,
+                      unsigned short* __restrict__ grad, double* __restrict__ part) {
+  __shared__ double s_w[8];
+  double acc = 0.0;
+  const long long n = rows * ld;
+  for (long long i = blockIdx.x * 256LL + threadIdx.x; i < n; i += (long long)gridDim.x * 256) {
+    const int c = (int)(i % ld);
+    float g = 0.0f;
+    if (c < used) {
+      const float d = pred[i] - target[i];
+      acc += (double)d * (double)d;
+      g = 2.0f * d * gscale;
+    }
+    grad[i] = f2bf(g);
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < 8; ++w) t += s_w[w];
+    part[blockIdx.x] = t;
+  }
+}
+
+__global__ void k_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                       float* __restrict__ v, long long n, float lr, float b1, float b2,
+                       float eps, float bc1, float bc2, float wd,
+                       unsigned short* __restrict__ mirror) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.0f - b1) * gi;
+    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    const float mh = mi / bc1, vh = vi / bc2;
+    const float pi = p[i] - lr * (mh / (sqrtf(vh) + eps) + wd * p[i]);
+    p[i] = pi;
+    if (mirror) mirror[i] = f2bf(pi);
+  }
+}
+
+// blk[m, (ro, o), (ri, i)] for ro, ri in {0, 1} (real, imaginary):
+//   [[wre, -wim], [wim, wre]] so that [yre; yim] = blk [zre; zim]
+__global__ void k_pack_modes(const float* __restrict__ wre, const float* __restrict__ wim,
+                             long long nm, int co, int ci, unsigned short* __restrict__ blk) {
+  const long long n = nm * 2 * co * 2 * ci;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const int col = (int)(idx % (2 * ci));
+    const int row = (int)((idx / (2 * ci)) % (2 * co));
+    const long long m = idx / ((long long)4 * co * ci);
+    const int ri = col / ci, i = col % ci, ro = row / co, o = row % co;
+    const long long w = (m * co + o) * ci + i;
+    float val;
+    if (ro == ri)
+      val = wre[w];
+    else
+      val = ro == 0 ? -wim[w] : wim[w];
+    blk[idx] = f2bf(val);
+  }
+}
+
+__global__ void k_unpack_mode_grads(const float* __restrict__ dblk, long long nm, int co, int ci,
+                                    float* __restrict__ dwre, float* __restrict__ dwim) {
+  const long long n = nm * co * ci;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(idx % ci);
+    const int o = (int)((idx / ci) % co);
+    const long long m = idx / ((long long)co * ci);
+    const float* b = dblk + m * 4LL * co * ci;
+    const long long ld = 2LL * ci;
+    dwre[idx] = b[o * ld + i] + b[(co + o) * ld + ci + i];
+    dwim[idx] = b[(co + o) * ld + i] - b[o * ld + ci + i];
+  }
+}
+
+__global__ void k_f32_to_bf16(const float* __restrict__ in, long long n,
+                              unsigned short* __restrict__ out) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = f2bf(in[i]);
+}
+
+unsigned grid_for(long long n, int threads = 256) {
+  long long b = (n + threads - 1) / threads;
+  const long long cap = 148LL * 16;
+  if (b > cap) b = cap;
+  if (b < 1) b = 1;
+  return (unsigned)b;
+}
+
+bool al16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+}  // namespace fa
+}  // namespace dn
+
+using namespace dn::fa;
+
+extern "C" int32_t dn_fno_features(const float* eps, int64_t n_img, int32_t H, int32_t W,
+                                   float eps_lo, float eps_hi, void* feat, void* stream) {
+  if (!eps || !feat || n_img < 1 || H < 1 || W < 1 || !(eps_hi > eps_lo) || !al16(feat))
+    return DN_EINVAL;
+  const long long n = n_img * (long long)H * W;
+  k_features<<<grid_for(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      eps, n_img, H, W, eps_lo, 1.0f / (eps_hi - eps_lo), static_cast<unsigned short*>(feat));
+  DN_CUDA_CHECK(cudaGetLastError());
+  return DN_OK;
+}
+
+extern "C" int32_t dn_fno_features_bwd(const float* dfeat, int64_t n_pix, float eps_lo,
+                                       float eps_hi, float* deps, void* stream) {
+  if (!dfeat || !deps || n_pix < 1 || !(eps_hi > eps_lo)) return DN_EINVAL;
+  k_features_bwd<<<grid_for(n_pix), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      dfeat, n_pix, 1.0f / (eps_hi - eps_lo), deps);
+  DN_CUDA_CHECK(cudaGetLastError());
+  return DN_OK;
+}
+
+extern "C" int32_t dn_fno_readout(const void* x, const float* r, int64_t nb, int32_t H,
+                                  int32_t W, int32_t C, void* out, void* stream) {
+  if (!x || !r || !out || nb < 1 || H < 1 || W < 1 || C < 1) return DN_EINVAL;
+  k_readout<<<grid_for(nb * W * C), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      static_cast<const unsigned short*>(x), r, nb, H, W, C, static_cast<unsigned short*>(out));
+  DN_CUDA_CHECK(cudaGetLastError());
+  return DN_OK;
+}
+
+extern "C" int32_t dn_fno_readout_bwd(const void* x, const float* r, const void* dR, int64_t nb,
+                                      int32_t H, int32_t W, int32_t C, void* dx, float* dr_part,
+                                      void* stream) {
+  if (!x || !r || !dR || nb < 1 || H < 1 || W < 1 || C < 1 || (!dx && !dr_part))
+    return DN_EINVAL;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (dx) {
+    k_readout_bwd_x<<<grid_for(nb * H * W * C), 256, 0, s>>>(
+        r, static_cast<const unsigned short*>(dR), nb, H, W, C, static_cast<unsigned short*>(dx));
+    DN_CUDA_CHECK(cudaGetLastError());
+  }
+  if (dr_part) {
+    k_readout_bwd_r<<<grid_for(nb * H * C), 256, 0, s>>>(
+        static_cast<const unsigned short*>(x), static_cast<const unsigned short*>(dR), nb, H, W, C,
+        dr_part);
+    DN_CUDA_CHECK(cudaGetLastError());
+  }
+  return DN_OK;
+}
+
+extern "C" int64_t dn_colsum_scratch_elems(int64_t rows, int64_t cols) {
+  if (rows < 1 || cols < 1) return 0;
+  const long long parts = rows < 512 ? rows : 512;
+  return parts * cols;
+}
+
+extern "C" int32_t dn_colsum(const void* in, int32_t dtype, int64_t rows, int64_t cols, int64_t ld,
+                             float* out, int32_t accumulate, float* scratch, int64_t scratch_elems,
+                             void* stream) {
+  if (!in || !out || !scratch || rows < 1 || cols < 1 || ld < cols) return DN_EINVAL;
+  if (dtype != DN_F32 && dtype != DN_BF16) return DN_EINVAL;
+  const long long parts = rows < 512 ? rows : 512;
+  if (scratch_elems < parts * cols) return DN_EINVAL;
+  const long long rpb = (rows + parts - 1) / parts;
+  const long long nparts = (rows + rpb - 1) / rpb;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const dim3 g1((unsigned)((cols + 255) / 256), (unsigned)nparts);
+  k_colsum_part<<<g1, 256, 0, s>>>(in, dtype == DN_BF16, rows, cols, ld, rpb, scratch);
+  DN_CUDA_CHECK(cudaGetLastError());
+  k_colsum_final<<<(unsigned)((cols + 255) / 256), 256, 0, s>>>(scratch, nparts, cols, out,
+                                                                  accumulate);
+  DN_CUDA_CHECK(cudaGetLastError());
+  return DN_OK;
+}
+
+extern "C" int32_t dn_mse(const float* pred, const float* target, int64_t rows, int32_t ld,
+                          int32_t used, float grad_scale, void* grad, double* loss_part,
+                          int32_t n_part, void* stream) {
+  if (!pred || !target || !grad || !loss_part || rows < 1 || ld < 1 || used < 1 || used > ld ||
+      n_part < 1)
+    return DN_EINVAL;
+  k_mse<<<n_part, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      pred, target, rows, ld, used, grad_scale, static_cast<unsigned short*>(grad), loss_part);
+  DN_CUDA_CHECK(cudaGetLastError());
+  return DN_OK;
+}
+
+extern "C" int32_t dn_adam(float* p, const float* g, float* m, float* v, int64_t n, float lr,
+                           float beta1, float beta2, float eps, int32_t step, float weight_decay,
+                           void* mirror_bf16, void* stream) {
+  if (!p || !g || !m || !v || n < 1 || step < 1) return DN_EINVAL;
+  const float bc1 = 1.0f - powf(beta1, (float)step);
+  const float bc2 = 1.0f - powf(beta2, (float)step);
+  k_adam<<<grid_for(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      p, g, m, v, n, lr, beta1, beta2, eps, bc1, bc2, weight_decay,
+      static_cast<unsigned short*>(mirror_bf16));
+  DN_CUDA_CHECK(cudaGetLastError());
+  return DN_OK;
+}
+
+extern "C" int32_t dn_fno_pack_modes(const float* wre, const float* wim, int64_t n_modes,
+                                     int32_t c_out, int32_t c_in, void* blk, void* stream) {
+  if (!wre || !wim || !blk || n_modes < 1 || c_out < 1 || c_in < 1) return DN_EINVAL;
+  k_pack_modes<<<grid_for(n_modes * 4LL * c_out * c_in), 256, 0,
+                 static_cast<cudaStream_t>(stream)>>>(wre, wim, n_modes, c_out, c_in,
+                                                      static_cast<unsigned short*>(blk));
+  DN_CUDA_CHECK(cudaGetLastError());
+  return DN_OK;
+}
+
+extern "C" int32_t dn_fno_unpack_mode_grads(const float* dblk, int64_t n_modes, int32_t c_out,
+                                            int32_t c_in, float* dwre, float* dwim,
+                                            void* stream) {
+  if (!dblk || !dwre || !dwim || n_modes < 1 || c_out < 1 || c_in < 1) return DN_EINVAL;
+  k_unpack_mode_grads<<<grid_for(n_modes * (long long)c_out * c_in), 256, 0,
+                        static_cast<cudaStream_t>(stream)>>>(dblk, n_modes, c_out, c_in, dwre,
+                                                             dwim);
+  DN_CUDA_CHECK(cudaGetLastError());
+  return DN_OK;
+}
+
+extern "C" int32_t dn_f32_to_bf16(const float* in, int64_t n, void* out, void* stream) {
+  if (!in || !out || n < 1) return DN_EINVAL;
+  k_f32_to_bf16<<<grid_for(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      in, n, static_cast<unsigned short*>(out));
+  DN_CUDA_CHECK(cudaGetLastError());
+  return DN_OK;
+}

@@ -62,7 +62,8 @@ class BatchInstance:
 class _Inst:
     """Device buffers of one instance."""
 
-    def __init__(self, spec: BatchInstance, pol: int, dtype, dev, K: int, grad: bool):
+    def __init__(self, spec: BatchInstance, pol: int, dtype, dev, K: int, grad: bool,
+                 shared: dict | None = None):
         H, W = spec.grid_shape
         self.spec, self.H, self.W = spec, H, W
         self.Wp = padded_width(W)
@@ -70,9 +71,20 @@ class _Inst:
         T = spec.n_steps
         self.f = torch.zeros((2, 3, H, self.Wp), **kw)
         self.ce = torch.zeros((H, self.Wp), **kw)
-        self.prof = [tuple(t.to(dev) for t in _setup.cpml_profile(n, spec.pml_layers, spec.dl, spec.dt))
-                     for n in (H, W)]
-        self.wave = _setup.waveform_table(T, spec.dt, spec.omega, spec.source).to(**kw)
+        # read-only tables, shared by instances with the same set-up
+        key = json.dumps([H, W, T, spec.pml_layers, spec.dl, spec.dt, spec.omega, str(dtype),
+                          spec.source, spec.monitor], sort_keys=True, default=str)
+        shared = {} if shared is None else shared
+        if key not in shared:
+            prof = [tuple(t.to(dev) for t in _setup.cpml_profile(n, spec.pml_layers, spec.dl,
+                                                                 spec.dt)) for n in (H, W)]
+            wave = _setup.waveform_table(T, spec.dt, spec.omega, spec.source).to(**kw)
+            phase = None
+            if spec.monitor is not None:
+                wl = [float(w) for w in spec.monitor.get("wavelengths_nm", [spec.wavelength_nm])]
+                phase = _setup.dft_phase_table(T, spec.dt, wl).to(dev)
+            shared[key] = (prof, wave, phase)
+        self.prof, self.wave, phase = shared[key]
         self.src_box = _setup.source_box_2d((H, W), spec.source)
         self.mon_box, self.phase, self.acc, self.nf = None, None, None, 0
         if spec.monitor is not None:
@@ -81,7 +93,7 @@ class _Inst:
             self.mon_box, self.nf = box, len(wl)
             self.mon_shape = tuple(b - a for a, b in box[1:])
             cells = self.mon_shape[0] * self.mon_shape[1]
-            self.phase = _setup.dft_phase_table(T, spec.dt, wl).to(dev)
+            self.phase = phase
             self.acc = torch.zeros((self.nf, cells, 2), dtype=F64, device=dev)
         self.grad_enabled = grad
         nck = max(0, math.ceil(T / K) - 1)
@@ -174,7 +186,9 @@ class FDTDBatch2D:
     def _build(self, grad: bool):
         if self._insts is not None and self._grad_alloc == grad:
             return
-        self._insts = [_Inst(s, self.pol, self.dtype, self.device, self.K, grad) for s in self.specs]
+        shared: dict = {}
+        self._insts = [_Inst(s, self.pol, self.dtype, self.device, self.K, grad, shared)
+                       for s in self.specs]
         self._grad_alloc = grad
         self._graph = None
         if self.tile_rows is None:

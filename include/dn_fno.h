@@ -9,7 +9,7 @@
  *
  * Reference interfaces replaced (DiffNano, paths relative to its checkout):
  * the reference's surrogate is a small CNN trained with torch ops
- * (diffnano/surrogate.py:78-285, NeuralSurrogate); it has no Fourier neural
+ * (diffnano/solvers/surrogate.py:78-285, NeuralSurrogate); it has no Fourier neural
  * operator and no GEMM of its own.  dn_gemm_run is the one compute entry the
  * surrogate's Python layer calls for every contraction of the operator
  * (lifting, truncated 2-D DFT and its inverse, per-mode complex channel
@@ -100,6 +100,61 @@ typedef struct dn_gemm {
  * warps.  Bounded waits; a wait that gives up stores DN_ETIMEOUT in *status
  * (status may be NULL). */
 int32_t dn_gemm_run(const dn_gemm* g, int32_t* status, void* stream);
+
+/* ---- memory-bound helpers of the operator's passes ----------------------
+ * Channel-last BF16 activations (sample, row, column, channel). */
+
+/* feat[i, 0..7] = ((eps - lo) / (hi - lo), column / (W-1), row / (H-1), 0 x 5)
+ * as BF16 for every pixel of n_img (H, W) FP32 maps; feat 16-byte aligned.
+ * Replaces the reference network's input reshaping
+ * (diffnano/solvers/surrogate.py:62-72, _SurrogateNet.forward). */
+int32_t dn_fno_features(const float* eps, int64_t n_img, int32_t H, int32_t W, float eps_lo,
+                        float eps_hi, void* feat, void* stream);
+/* deps[i] = dfeat[i, 0] / (hi - lo): dfeat FP32 (n_pix, 8) */
+int32_t dn_fno_features_bwd(const float* dfeat, int64_t n_pix, float eps_lo, float eps_hi,
+                            float* deps, void* stream);
+
+/* out[b, w, c] = sum_h r[h, c] * x[b, h, w, c]   (x, out BF16; r FP32 (H, C)) */
+int32_t dn_fno_readout(const void* x, const float* r, int64_t nb, int32_t H, int32_t W,
+                       int32_t C, void* out, void* stream);
+/* dx[b, h, w, c] = r[h, c] * dR[b, w, c] (BF16; NULL skips) and
+ * dr_part[b, h, c] = sum_w dR[b, w, c] * x[b, h, w, c] (FP32; NULL skips) */
+int32_t dn_fno_readout_bwd(const void* x, const float* r, const void* dR, int64_t nb, int32_t H,
+                           int32_t W, int32_t C, void* dx, float* dr_part, void* stream);
+
+/* out[c] (+)= sum_r in[r * ld + c], deterministic (fixed partition and order).
+ * in FP32 or BF16 (dtype); scratch: dn_colsum_scratch_elems(rows, cols) floats. */
+int64_t dn_colsum_scratch_elems(int64_t rows, int64_t cols);
+int32_t dn_colsum(const void* in, int32_t dtype, int64_t rows, int64_t cols, int64_t ld,
+                  float* out, int32_t accumulate, float* scratch, int64_t scratch_elems,
+                  void* stream);
+
+/* Squared error over the first `used` of `ld` columns of (rows, ld) FP32
+ * prediction and target: grad = grad_scale * 2 * (pred - target) as BF16
+ * (zero in the padding columns); loss_part[n_part] receives per-block sums of
+ * squares in FP64 (the caller adds them and divides).  Replaces the
+ * reference's mse_loss training criterion (diffnano/solvers/surrogate.py:193). */
+int32_t dn_mse(const float* pred, const float* target, int64_t rows, int32_t ld, int32_t used,
+               float grad_scale, void* grad, double* loss_part, int32_t n_part, void* stream);
+
+/* One Adam step (bias-corrected, decoupled weight decay) over n FP32
+ * parameters; writes the BF16 mirror when mirror_bf16 is not NULL.  Replaces
+ * torch.optim.Adam in the reference's surrogate training
+ * (diffnano/solvers/surrogate.py:128, 195-197). */
+int32_t dn_adam(float* p, const float* g, float* m, float* v, int64_t n, float lr, float beta1,
+                float beta2, float eps, int32_t step, float weight_decay, void* mirror_bf16,
+                void* stream);
+
+/* Complex per-mode weights w = wre + i*wim, (n_modes, c_out, c_in) FP32, to
+ * the real block matrix blk (n_modes, 2*c_out, 2*c_in) BF16 =
+ * [[wre, -wim], [wim, wre]]; and the gradient of that map. */
+int32_t dn_fno_pack_modes(const float* wre, const float* wim, int64_t n_modes, int32_t c_out,
+                          int32_t c_in, void* blk, void* stream);
+int32_t dn_fno_unpack_mode_grads(const float* dblk, int64_t n_modes, int32_t c_out, int32_t c_in,
+                                 float* dwre, float* dwim, void* stream);
+
+/* out[i] = bf16(in[i]) */
+int32_t dn_f32_to_bf16(const float* in, int64_t n, void* out, void* stream);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,111 @@
+"""Fourier-neural-operator surrogate: the DFT-matrix formulation against the
+FFT oracle (CPU, FP64), and the GPU forward pass, every parameter gradient and
+the input gradient against the oracle's FP32 autograd (GPU)."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from diffnano_b200.surrogate.fno import FNOConfig, dft_matrices, mode_table
+from oracle import fno_ref
+
+from conftest import rel_l2
+
+# BF16 activations, BF16 DFT matrices and BF16 weight mirrors against an FP32
+# FFT oracle fed the same BF16-rounded weights: a few BF16 roundings (2^-9)
+# per layer, accumulated over 4 layers
+TOL_FWD = 2e-2
+TOL_GRAD = 5e-2
+
+
+def test_dft_matrices_match_rfft2_irfft2():
+    cfg = FNOConfig(H=32, W=24, width=8, modes=4)
+    F2, G = dft_matrices(cfg)
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal((2, 32, 24, 8))
+    Z = np.einsum("mp,bpc->bmc", F2, x.reshape(2, 32 * 24, 8))
+    kh, kw = mode_table(cfg)
+    ref = np.fft.rfft2(x, axes=(1, 2))[:, kh, kw, :]
+    assert np.abs(Z[:, :cfg.n_modes] - ref.real).max() < 1e-10
+    assert np.abs(Z[:, cfg.n_modes:] - ref.imag).max() < 1e-10
+    wre = torch.randn(cfg.n_modes, 8, 8, dtype=torch.float64)
+    wim = torch.randn(cfg.n_modes, 8, 8, dtype=torch.float64)
+    s = fno_ref.spectral(torch.from_numpy(x), wre, wim, 4).numpy()
+    Yc = np.einsum("moi,bmi->bmo", (wre + 1j * wim).numpy(), ref)
+    xs = np.einsum("pm,bmc->bpc", G, np.concatenate([Yc.real, Yc.imag], axis=1))
+    assert np.abs(s - xs.reshape(s.shape)).max() < 1e-10
+
+
+def _bf16_round(params):
+    """The weights the GPU reads as BF16 GEMM operands, rounded the same way."""
+    out = {}
+    for k, v in params.items():
+        if k in ("P", "Q1", "Q2") or k.startswith(("W", "wre", "wim")):
+            v = v.to(torch.bfloat16).to(torch.float32)
+        out[k] = v
+    return out
+
+
+def _design_batch(B, seed):
+    from diffnano_b200.workloads import blob_eps_2d
+    eps = torch.stack([blob_eps_2d(256, 128, seed=seed + i, sigma_cells=2 + i % 5)[64:192, 64:192]
+                       for i in range(B)])
+    return eps.to(torch.float32)
+
+
+@pytest.mark.gpu
+def test_fno_forward_and_gradients_match_oracle(cuda):
+    from diffnano_b200.surrogate.fno import FNO2d
+    cfg = FNOConfig()
+    net = FNO2d(cfg, cuda, seed=3)
+    params = _bf16_round({k: v for k, v in net.state_dict().items()})
+    B = 4
+    eps = _design_batch(B, 11)
+    g = torch.Generator().manual_seed(5)
+    target = torch.randn(B, cfg.W, cfg.n_out, generator=g) * 0.1
+    kw = dict(layers=cfg.layers, modes=cfg.modes, n_out=cfg.n_out, lo=cfg.eps_lo, hi=cfg.eps_hi)
+    loss_ref, pred_ref, grads_ref, deps_ref = fno_ref.loss_and_grads(params, eps, target, **kw)
+
+    pred = net.forward(eps.to(cuda))
+    loss = net.loss(target.to(cuda))
+    net.ps.g.zero_()
+    deps = net.backward(B=B, want_input_grad=True)
+    torch.cuda.synchronize()
+    net.check_status()
+    assert rel_l2(pred, pred_ref) < TOL_FWD
+    assert abs(float(loss) - float(loss_ref)) / float(loss_ref) < TOL_FWD
+    for name, gref in grads_ref.items():
+        gg = net.ps.G(name).cpu()
+        if name == "P":
+            gg, gref = gg[:, :3], gref[:, :3]
+        if name in ("Q2", "q2"):
+            gg, gref = gg[:cfg.n_out], gref[:cfg.n_out]
+        err = rel_l2(gg, gref)
+        assert err < TOL_GRAD, f"gradient of {name}: rel-L2 {err:.3e}"
+    assert rel_l2(deps, deps_ref) < TOL_GRAD
+
+
+@pytest.mark.gpu
+def test_fno_adam_step_decreases_loss(cuda):
+    from diffnano_b200.surrogate.fno import FNO2d
+    cfg = FNOConfig()
+    net = FNO2d(cfg, cuda, seed=4)
+    B = 8
+    eps = _design_batch(B, 21)
+    # a learnable target: per-column fill fraction of the design, scaled per output
+    fill = ((eps - cfg.eps_lo) / (cfg.eps_hi - cfg.eps_lo)).mean(dim=1)  # (B, W)
+    scale = torch.linspace(-0.5, 0.5, cfg.n_out)
+    target = (fill[:, :, None] - 0.5) * scale[None, None, :]
+    eps, target = eps.to(cuda), target.to(cuda)
+    losses = []
+    for _ in range(30):
+        net.forward(eps)
+        losses.append(float(net.loss(target)))
+        net.ps.g.zero_()
+        net.backward(B=B)
+        net.adam_step(lr=2e-3)
+    torch.cuda.synchronize()
+    net.check_status()
+    assert losses[-1] < 0.5 * losses[0], losses
