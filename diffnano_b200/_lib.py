@@ -95,10 +95,17 @@ class DnGemm(ctypes.Structure):
                 ("max_ctas", c_int32)]
 
 
+class DnDensity(ctypes.Structure):
+    _fields_ = [("n_layers", c_int32), ("H", c_int32), ("W", c_int32), ("kind", c_int32),
+                ("radius", ctypes.c_float), ("beta", ctypes.c_float), ("eta", ctypes.c_float),
+                ("eps_lo", ctypes.c_float), ("eps_hi", ctypes.c_float)]
+
+
 STRUCTS = {"dn_box": DnBox, "dn_grid": DnGrid, "dn_cpml": DnCpml, "dn_source": DnSource,
            "dn_monitor": DnMonitor, "dn_probe": DnProbe, "dn_curl_record": DnCurlRecord,
            "dn_batch2d_inst": DnBatch2dInst, "dn_batch2d": DnBatch2d,
-           "dn_gemm_operand": DnGemmOperand, "dn_gemm": DnGemm}
+           "dn_gemm_operand": DnGemmOperand, "dn_gemm": DnGemm,
+           "dn_density": DnDensity}
 
 PTR6 = c_void_p * 6
 _P6 = ctypes.POINTER(c_void_p)  # a PTR6 instance (or None) is passed here
@@ -156,6 +163,14 @@ SIGNATURES = {
     "dn_fno_unpack_mode_grads": (c_int32, [c_void_p, c_int64, c_int32, c_int32, c_void_p,
                                            c_void_p, c_void_p]),
     "dn_f32_to_bf16": (c_int32, [c_void_p, c_int64, c_void_p, c_void_p]),
+    "dn_density_forward": (c_int32, [ctypes.POINTER(DnDensity), c_void_p, c_void_p, c_void_p,
+                                     c_void_p, c_void_p]),
+    "dn_density_backward": (c_int32, [ctypes.POINTER(DnDensity), c_void_p, c_void_p, c_void_p,
+                                      c_void_p, c_void_p]),
+    "dn_morph3": (c_int32, [c_void_p, c_int32, c_int32, c_int32, c_int32, c_void_p, c_void_p,
+                            c_void_p]),
+    "dn_morph3_backward": (c_int32, [c_void_p, c_void_p, c_int32, c_int32, c_int32, c_void_p,
+                                     c_void_p]),
     "dn_fdtd2d_run_noalloc": (c_int32, [ctypes.POINTER(DnGrid), _P6, c_void_p,
                                         ctypes.POINTER(DnCpml), ctypes.POINTER(DnSource),
                                         ctypes.POINTER(DnMonitor), c_int32,

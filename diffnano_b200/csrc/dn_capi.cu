@@ -1,6 +1,7 @@
 // Library-wide C-ABI helpers: status strings, version, last CUDA error.
 #include "dn_common.cuh"
 #include "dn_fno.h"
+#include "dn_design.h"
 
 namespace dn {
 namespace {
@@ -42,6 +43,7 @@ extern "C" int64_t dn_struct_size(const char* name) {
       {"dn_batch2d", sizeof(dn_batch2d)},
       {"dn_gemm_operand", sizeof(dn_gemm_operand)},
       {"dn_gemm", sizeof(dn_gemm)},
+      {"dn_density", sizeof(dn_density)},
   };
   for (const Entry& e : table)
     if (std::strcmp(e.n, name) == 0) return e.s;

@@ -152,9 +152,14 @@ def label_scale(labels: torch.Tensor) -> float:
     return float(torch.sqrt((labels.abs() ** 2).mean()))
 
 
+def _real_view(x: torch.Tensor) -> torch.Tensor:
+    return torch.view_as_real(x) if x.is_complex() else x
+
+
 def rel_l2_per_sample(pred: torch.Tensor, true: torch.Tensor) -> torch.Tensor:
-    d = (pred - true).reshape(pred.shape[0], -1).to(torch.float64)
-    t = true.reshape(true.shape[0], -1).to(torch.float64)
+    """||pred - true|| / ||true|| per sample (complex values count re and im)."""
+    d = _real_view(pred - true).reshape(pred.shape[0], -1).to(torch.float64)
+    t = _real_view(true).reshape(true.shape[0], -1).to(torch.float64)
     return d.norm(dim=1) / t.norm(dim=1).clamp_min(1e-300)
 
 

@@ -16,6 +16,7 @@ and ``dn_adam``.  Inputs are design-region permittivity maps ``(128, 128)``
 """
 from __future__ import annotations
 
+import math
 import time
 from typing import Dict, List, Optional
 
@@ -73,10 +74,18 @@ class FNOSurrogate:
     # ---- training -----------------------------------------------------------
     def train_surrogate(self, n_samples: int = 20000, n_epochs: int = 50, verbose: bool = False,
                         data_seed: int = 1, designs: Optional[torch.Tensor] = None,
-                        labels: Optional[torch.Tensor] = None) -> List[float]:
+                        labels: Optional[torch.Tensor] = None, schedule: str = "cosine",
+                        weight_decay: float = 0.0, mirror: bool = True) -> List[float]:
         """Generate ``n_samples`` labelled designs with the full solver (unless
         ``designs``/``labels`` are given) and train; returns the per-epoch
-        mean training loss."""
+        mean training loss.
+
+        ``schedule``: "constant" or "cosine" (decay of the learning rate to 0
+        over the run).  ``mirror``: each step flips a random half of the
+        batch left-right, design and monitor line together (the set-up is
+        mirror symmetric about the grid's centre column)."""
+        if schedule not in ("constant", "cosine"):
+            raise ValueError(f"schedule must be 'constant' or 'cosine', got {schedule!r}")
         dev = self._device
         if designs is None:
             torch.cuda.synchronize(dev)
@@ -95,16 +104,27 @@ class FNOSurrogate:
         history: List[float] = []
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
+        total = max(1, n_epochs * steps)
+        it = 0
         for epoch in range(n_epochs):
             perm = torch.randperm(n, device=dev, generator=g)
             acc = torch.zeros((), dtype=torch.float64, device=dev)
             for s in range(steps):
                 idx = perm[s * B:(s + 1) * B]
-                self.net.forward(designs[idx])
-                acc += self.net.loss(targets[idx])
+                x, y = designs[idx], targets[idx]
+                if mirror:
+                    flip = torch.rand(B, device=dev, generator=g) < 0.5
+                    x = torch.where(flip[:, None, None], x.flip(-1), x)
+                    y = torch.where(flip[:, None, None], y.flip(1), y)
+                self.net.forward(x)
+                acc += self.net.loss(y)
                 self.net.ps.g.zero_()
                 self.net.backward(B=B)
-                self.net.adam_step(lr=self.lr)
+                lr = self.lr
+                if schedule == "cosine":
+                    lr = 0.5 * self.lr * (1.0 + math.cos(math.pi * it / total))
+                self.net.adam_step(lr=lr, weight_decay=weight_decay)
+                it += 1
             history.append(float(acc) / max(1, steps))
             if verbose and epoch % 10 == 0:
                 print(f"epoch {epoch}: loss={history[-1]:.6f}")

@@ -38,8 +38,11 @@ def cfg0_eps(mask: np.ndarray) -> torch.Tensor:
 
 
 def rel_l2(a, b) -> float:
-    a = torch.as_tensor(a).detach().to("cpu", torch.float64)
-    b = torch.as_tensor(b).detach().to("cpu", torch.float64)
+    a, b = torch.as_tensor(a).detach().cpu(), torch.as_tensor(b).detach().cpu()
+    a = (torch.view_as_real(a.to(torch.complex128)) if a.is_complex() or b.is_complex()
+         else a.to(torch.float64))
+    b = (torch.view_as_real(b.to(torch.complex128)) if b.is_complex() or a.dim() > b.dim()
+         else b.to(torch.float64))
     return float(torch.linalg.vector_norm(a - b) / max(float(torch.linalg.vector_norm(b)), 1e-300))
 
 
