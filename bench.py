@@ -559,7 +559,10 @@ def run_design(args):
                        "plain": f"{args.design_iters} Adam iterations, FDTD forward+adjoint each",
                        "surrogate": f"FNO on the 2-D cross-section, {cfg.n_train} batched-FDTD "
                                     f"proxy labels, {cfg.n_candidates} candidates/iteration"},
-            "plain": {"wall_s": plain_s, "final_fom": target / plain["fom0"],
+            "plain": {"history": [{"n": r.verification, "t": round(r.wall_s, 2),
+                                   "fom": r.fom / plain["fom0"], "beta": round(r.beta, 2)}
+                                  for r in plain["history"]],
+                      "wall_s": plain_s, "final_fom": target / plain["fom0"],
                       "best_fom": plain["best_fom"] / plain["fom0"],
                       "s_per_iteration": plain_s / args.design_iters,
                       "gcells": setup.cell_steps() * args.design_iters / plain_s / 1e9},

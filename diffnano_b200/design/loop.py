@@ -10,17 +10,20 @@ inside a gradient loop:
   forward + adjoint and takes an Adam step on the density (``dn_adam``), with
   the projection sharpness beta raised from ``beta[0]`` to ``beta[1]``
   (``beta_continuation_schedule``).
-* :class:`SurrogateAssistedLoop` -- a Fourier neural operator trained on the
-  2-D proxy (labelled by the batched FDTD) runs Adam on its own prediction of
-  the focal intensity from the accepted design (``inner_steps`` steps,
-  beta ramped to the next outer value), keeps ``n_candidates`` snapshots of
-  that path, ranks them by predicted figure of merit in one batched inference
-  and sends the best to the 3-D FDTD forward + adjoint.  The verified design
-  is accepted when its FDTD figure of merit does not fall below the last
-  accepted one (within ``tolerance``); otherwise the loop falls back to a plain
-  Adam step from the accepted design with the FDTD gradient.  Every verified
-  sample also fine-tunes the network.  Wall time includes the proxy labelling
-  and the training.
+* :class:`SurrogateAssistedLoop` -- a Fourier neural operator S trained on the
+  2-D proxy (labelled by the batched FDTD) is corrected to first order at the
+  accepted design rho_k (model m(rho) = f_k + S(rho) - S(rho_k) + (g_k -
+  grad S(rho_k)) . (rho - rho_k), which matches the FDTD value f_k and
+  gradient g_k there: first-order model management, Alexandrov et al.,
+  Structural Optimization 15, 1998).  Adam on m from rho_k (beta ramped to the
+  next outer value) proposes a path; ``n_candidates`` snapshots of it are
+  ranked by m in one batched inference and the best goes to the 3-D FDTD
+  forward + adjoint.  It is accepted when its FDTD figure of merit does not
+  fall more than ``tolerance`` below the last accepted one; otherwise the loop
+  falls back to a plain Adam step from rho_k with g_k.  The inner step size is
+  a trust region: doubled when the FDTD gain is at least 3/4 of the predicted
+  one, quartered on a rejection.  Every verified sample also fine-tunes the
+  network.  Wall time includes the proxy labelling and the training.
 """
 from __future__ import annotations
 
@@ -101,11 +104,13 @@ class SurrogateConfig:
     batch: int = 256
     lr: float = 1e-3
     n_candidates: int = 32
-    inner_steps: int = 64
+    inner_steps: int = 32
     inner_lr: float = 0.02
+    max_inner_lr: float = 0.16
+    min_inner_lr: float = 1e-4
     outer_schedule: int = 10  # outer iterations over which beta reaches its end value
     max_verify: int = 40
-    tolerance: float = 0.0
+    tolerance: float = 0.02
     ft_steps: int = 10
     ft_lr: float = 2e-4
     fallback_lr: float = 0.02
@@ -173,27 +178,35 @@ class SurrogateAssistedLoop:
     def predict_fom(self, eps_design: torch.Tensor) -> torch.Tensor:
         return self._focal(self.net.forward(eps_design)) * self.scale ** 2
 
-    def _ascent(self, rho: torch.Tensor, b0: float, b1: float) -> List[torch.Tensor]:
-        """Adam on the predicted focal intensity; density snapshots along the path."""
-        c, s = self.cfg, self.problem.setup
-        opt = DensityAdam(rho, c.inner_lr)
-        every = max(1, c.inner_steps // c.n_candidates)
-        snaps = [opt.rho.clone()]
+    def _value_grad(self, rho: torch.Tensor, beta: float):
+        """Surrogate focal intensity S(rho) and dS/drho (FOM units)."""
+        s = self.problem.setup
         W = s.design_shape[1]
         li, fc = s.center_index, s.focus_col
-        for k in range(c.inner_steps):
-            b = b0 * (b1 / b0) ** ((k + 1) / c.inner_steps)
-            x = opt.rho.clone().requires_grad_(True)
-            eps = s.eps_design(x, b).unsqueeze(0)
-            pred = self.net.forward(eps.detach())
-            ws = self.net._bwd_workspace(1)
-            gout = torch.zeros(W, OUT_LD, device=x.device)
-            gout[fc, 2 * li] = -2.0 * pred[0, fc, 2 * li]
-            gout[fc, 2 * li + 1] = -2.0 * pred[0, fc, 2 * li + 1]
-            ws["gout"].copy_(gout.to(torch.bfloat16))
-            deps = self.net.backward(B=1, want_input_grad=True)
-            eps.backward(deps)
-            opt.ascend(-x.grad, 1.0)  # x.grad is d(-fom)/d rho
+        x = rho.detach().clone().requires_grad_(True)
+        eps = s.eps_design(x, beta).unsqueeze(0)
+        pred = self.net.forward(eps.detach())
+        value = self._focal(pred)[0] * self.scale ** 2
+        gout = torch.zeros(W, OUT_LD, device=x.device)
+        gout[fc, 2 * li] = -2.0 * pred[0, fc, 2 * li]
+        gout[fc, 2 * li + 1] = -2.0 * pred[0, fc, 2 * li + 1]
+        self.net._bwd_workspace(1)["gout"].copy_(gout.to(torch.bfloat16))
+        deps = self.net.backward(B=1, want_input_grad=True)  # d(-S/scale^2)/d eps
+        eps.backward(deps)
+        return float(value), -x.grad * self.scale ** 2
+
+    def _ascent(self, rho: torch.Tensor, b0: float, b1: float, corr: torch.Tensor,
+                steps: int, lr: float, fom_ref: float) -> List[torch.Tensor]:
+        """Adam (learning rate ``lr``) on the corrected model m = S + corr .
+        (rho - rho_k); density snapshots along the path (the candidates)."""
+        c = self.cfg
+        opt = DensityAdam(rho, lr)
+        every = max(1, steps // c.n_candidates)
+        snaps = []
+        for k in range(steps):
+            b = b0 * (b1 / b0) ** ((k + 1) / steps)
+            _, dS = self._value_grad(opt.rho, b)
+            opt.ascend(dS + corr, 1.0 / fom_ref)
             if (k + 1) % every == 0:
                 snaps.append(opt.rho.clone())
         return snaps[-c.n_candidates:]
@@ -235,27 +248,40 @@ class SurrogateAssistedLoop:
         fallback = DensityAdam(rho, c.fallback_lr)
         fom0 = fom
         reached = None
+        steps = c.inner_steps
+        lr = c.inner_lr  # trust region: the inner path's step size
         o = 0
         while len(hist) < c.max_verify:
             o += 1
             b_next = beta_continuation_schedule(o, c.outer_schedule, beta[0], beta[1])
-            snaps = self._ascent(rho, b, b_next)
+            # first-order correction: the model matches the FDTD value and
+            # gradient at the accepted design
+            s0, dS0 = self._value_grad(rho, b)
+            corr = grad - dS0
+            snaps = self._ascent(rho, b, b_next, corr, steps, lr, fom0)
             with torch.no_grad():
                 eps_c = torch.stack([s.eps_design(r, b_next) for r in snaps])
-                pred = self.predict_fom(eps_c)
-            best = int(torch.argmax(pred))
+                S = self.predict_fom(eps_c)
+                lin = torch.stack([(corr * (r - rho)).sum() for r in snaps])
+                model = fom + (S - s0) + lin
+            best = int(torch.argmax(model))
             cand = snaps[best]
             f_new, g_new, dft_new = p.evaluate(cand, b_next, grad=True)
             self._record_sample(eps_c[best], dft_new)
             ok = f_new >= (1.0 - c.tolerance) * fom
             hist.append(Record(len(hist) + 1, time.perf_counter() - t0, f_new, b_next,
                                "surrogate", ok))
-            cand_stats.append({"pred_best": float(pred[best]), "fdtd": f_new,
-                               "pred_spread": float(pred.max() - pred.min())})
+            predicted = float(model[best])
+            cand_stats.append({"model_best": predicted, "fdtd": f_new, "fom_before": fom,
+                               "inner_lr": lr, "pick": best})
+            gain_pred = predicted - fom
+            ratio = (f_new - fom) / gain_pred if gain_pred > 0 else 0.0
             if ok:
                 rho, fom, grad, b = cand.clone(), f_new, g_new, b_next
-                fallback.rho.copy_(rho)
+                if ratio > 0.75:
+                    lr = min(c.max_inner_lr, 2.0 * lr)
             else:
+                lr = max(c.min_inner_lr, 0.25 * lr)
                 # plain step from the accepted design with its FDTD gradient
                 fallback.rho.copy_(rho)
                 r2 = fallback.ascend(grad, 1.0 / fom0).clone()
