@@ -92,7 +92,7 @@ class DnGemm(ctypes.Structure):
                 ("row_scale", c_void_p), ("batch_scale", c_void_p), ("addend", c_void_p),
                 ("addend_dtype", c_int32), ("aux_dtype", c_int32), ("aux", c_void_p),
                 ("pre", c_void_p), ("pre_dtype", c_int32), ("block_n", c_int32),
-                ("max_ctas", c_int32)]
+                ("max_ctas", c_int32), ("col_scale", c_void_p), ("row_bias", c_void_p)]
 
 
 class DnDensity(ctypes.Structure):
@@ -163,6 +163,10 @@ SIGNATURES = {
     "dn_fno_unpack_mode_grads": (c_int32, [c_void_p, c_int64, c_int32, c_int32, c_void_p,
                                            c_void_p, c_void_p]),
     "dn_f32_to_bf16": (c_int32, [c_void_p, c_int64, c_void_p, c_void_p]),
+    "dn_fno_channel_sums": (c_int32, [c_void_p, c_int64, c_int32, c_int64, c_void_p, c_void_p,
+                                      c_void_p]),
+    "dn_fno_modes_rows": (c_int32, [c_void_p, c_void_p, c_int32, c_int64, c_int32, c_int32,
+                                    c_void_p]),
     "dn_density_forward": (c_int32, [ctypes.POINTER(DnDensity), c_void_p, c_void_p, c_void_p,
                                      c_void_p, c_void_p]),
     "dn_density_backward": (c_int32, [ctypes.POINTER(DnDensity), c_void_p, c_void_p, c_void_p,

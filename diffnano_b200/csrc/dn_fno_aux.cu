@@ -9,7 +9,7 @@
 //   * Adam on an FP32 master copy with a BF16 mirror
 //   * packing of the complex per-mode weights into the real 2x2 block form the
 //     mixing GEMM reads, and the matching gradient unpacking
-// Layouts are channel-last (sample, row, column, channel) unless stated.
+// Activations are channel-first (sample, channel, row, column) unless stated.
 #include <cuda_bf16.h>
 
 #include "dn_common.cuh"
@@ -53,51 +53,114 @@ __global__ void k_features_bwd(const float* __restrict__ dfeat, long long n, flo
     deps[i] = dfeat[i * FEAT] * inv_span;
 }
 
-// out[b, w, c] = sum_h r[h, c] * x[b, h, w, c]; one thread per (b, w, c)
+// out[b, w, c] = sum_h r[h, c] * x[b, c, h, w]; one thread per (b, c, w)
+// (x channel-first, out channel-last)
 __global__ void k_readout(const unsigned short* __restrict__ x, const float* __restrict__ r,
                           long long nb, int H, int W, int C, unsigned short* __restrict__ out) {
-  const long long n = nb * W * C;
+  const long long n = nb * C * W;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
-    const int c = (int)(i % C);
-    const long long wc = i % ((long long)W * C);
+    const int w = (int)(i % W);
+    const int c = (int)((i / W) % C);
     const long long b = i / ((long long)W * C);
-    const unsigned short* xb = x + b * H * W * C + wc;
+    const unsigned short* xp = x + (b * C + c) * (long long)H * W + w;
     float s = 0.0f;
-    for (int h = 0; h < H; ++h) s = fmaf(r[h * C + c], bf2f(xb[(long long)h * W * C]), s);
-    out[i] = f2bf(s);
+    for (int h = 0; h < H; ++h) s = fmaf(r[h * C + c], bf2f(xp[(long long)h * W]), s);
+    out[(b * W + w) * C + c] = f2bf(s);
   }
 }
 
-// dx[b, h, w, c] = r[h, c] * dR[b, w, c]            (one thread per element)
+// dx[b, c, h, w] = r[h, c] * dR[b, w, c]            (one thread per element)
 __global__ void k_readout_bwd_x(const float* __restrict__ r, const unsigned short* __restrict__ dR,
                                 long long nb, int H, int W, int C, unsigned short* __restrict__ dx) {
-  const long long n = nb * H * W * C;
+  const long long n = nb * C * H * W;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
-    const int c = (int)(i % C);
-    const long long wc = i % ((long long)W * C);
-    const int h = (int)((i / ((long long)W * C)) % H);
-    const long long b = i / ((long long)H * W * C);
-    dx[i] = f2bf(r[h * C + c] * bf2f(dR[b * W * C + wc]));
+    const int w = (int)(i % W);
+    const int h = (int)((i / W) % H);
+    const int c = (int)((i / ((long long)W * H)) % C);
+    const long long b = i / ((long long)C * H * W);
+    dx[i] = f2bf(r[h * C + c] * bf2f(dR[(b * W + w) * C + c]));
   }
 }
 
-// dr_part[b, h, c] = sum_w dR[b, w, c] * x[b, h, w, c]   (one thread per (b, h, c))
+// dr_part[b, h, c] = sum_w dR[b, w, c] * x[b, c, h, w]   (one thread per (b, c, h))
 __global__ void k_readout_bwd_r(const unsigned short* __restrict__ x,
                                 const unsigned short* __restrict__ dR, long long nb, int H, int W,
                                 int C, float* __restrict__ dr_part) {
-  const long long n = nb * H * C;
+  const long long n = nb * C * H;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
-    const int c = (int)(i % C);
-    const int h = (int)((i / C) % H);
+    const int h = (int)(i % H);
+    const int c = (int)((i / H) % C);
     const long long b = i / ((long long)H * C);
-    const unsigned short* xr = x + ((b * H + h) * W) * (long long)C + c;
+    const unsigned short* xr = x + ((b * C + c) * H + h) * (long long)W;
     const unsigned short* dr = dR + b * W * (long long)C + c;
     float s = 0.0f;
-    for (int w = 0; w < W; ++w) s = fmaf(bf2f(dr[(long long)w * C]), bf2f(xr[(long long)w * C]), s);
-    dr_part[i] = s;
+    for (int w = 0; w < W; ++w) s = fmaf(bf2f(dr[(long long)w * C]), bf2f(xr[w]), s);
+    dr_part[(b * H + h) * C + c] = s;
+  }
+}
+
+// channel sums, pass 1: block (c, q) sums samples q, q + 256, ... of channel c
+__global__ void k_channel_part(const unsigned short* __restrict__ x, long long nb, int C,
+                               long long npix, float* __restrict__ part) {
+  __shared__ float s_w[8];
+  const int c = blockIdx.x, q = blockIdx.y;
+  float s = 0.0f;
+  for (long long b = q; b < nb; b += gridDim.y) {
+    const uint4* row = reinterpret_cast<const uint4*>(x + (b * C + c) * npix);
+    for (long long i = threadIdx.x; i < npix / 8; i += blockDim.x) {
+      const uint4 u = row[i];
+      const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        s += __uint_as_float(w[e] << 16) + __uint_as_float(w[e] & 0xFFFF0000u);
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float t = 0.0f;
+    for (int w = 0; w < 8; ++w) t += s_w[w];
+    part[q * C + c] = t;
+  }
+}
+
+// mode-major <-> row-major spectra:
+//   modes (m, b, r, c): ((m * nb + b) * 2 + r) * C + c
+//   rows  (b, c, r, m): ((b * C + c) * 2 + r) * nm + m
+// tiled 32 x 32 transpose of the (m, c) plane of every (b, r)
+__global__ void k_modes_rows(const unsigned short* __restrict__ src, unsigned short* __restrict__ dst,
+                             int nm, long long nb, int C, int to_rows) {
+  __shared__ unsigned short tile[32][33];
+  const long long br = blockIdx.z;
+  const long long b = br >> 1;
+  const int r = (int)(br & 1);
+  const int m0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+  if (to_rows) {
+    for (int k = ty; k < 32; k += 8) {  // read rows m, columns c
+      const int m = m0 + k, c = c0 + tx;
+      if (m < nm && c < C) tile[k][tx] = src[((m * nb + b) * 2 + r) * C + c];
+    }
+    __syncthreads();
+    for (int k = ty; k < 32; k += 8) {  // write rows c, columns m
+      const int c = c0 + k, m = m0 + tx;
+      if (m < nm && c < C) dst[((b * C + c) * 2 + r) * nm + m] = tile[tx][k];
+    }
+  } else {
+    for (int k = ty; k < 32; k += 8) {  // read rows c, columns m
+      const int c = c0 + k, m = m0 + tx;
+      if (m < nm && c < C) tile[k][tx] = src[((b * C + c) * 2 + r) * nm + m];
+    }
+    __syncthreads();
+    for (int k = ty; k < 32; k += 8) {  // write rows m, columns c
+      const int m = m0 + k, c = c0 + tx;
+      if (m < nm && c < C) dst[((m * nb + b) * 2 + r) * C + c] = tile[tx][k];
+    }
   }
 }
 
@@ -258,7 +321,7 @@ extern "C" int32_t dn_fno_features_bwd(const float* dfeat, int64_t n_pix, float 
 extern "C" int32_t dn_fno_readout(const void* x, const float* r, int64_t nb, int32_t H,
                                   int32_t W, int32_t C, void* out, void* stream) {
   if (!x || !r || !out || nb < 1 || H < 1 || W < 1 || C < 1) return DN_EINVAL;
-  k_readout<<<grid_for(nb * W * C), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+  k_readout<<<grid_for(nb * C * W), 256, 0, static_cast<cudaStream_t>(stream)>>>(
       static_cast<const unsigned short*>(x), r, nb, H, W, C, static_cast<unsigned short*>(out));
   DN_CUDA_CHECK(cudaGetLastError());
   return DN_OK;
@@ -271,12 +334,12 @@ extern "C" int32_t dn_fno_readout_bwd(const void* x, const float* r, const void*
     return DN_EINVAL;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (dx) {
-    k_readout_bwd_x<<<grid_for(nb * H * W * C), 256, 0, s>>>(
+    k_readout_bwd_x<<<grid_for(nb * C * H * W), 256, 0, s>>>(
         r, static_cast<const unsigned short*>(dR), nb, H, W, C, static_cast<unsigned short*>(dx));
     DN_CUDA_CHECK(cudaGetLastError());
   }
   if (dr_part) {
-    k_readout_bwd_r<<<grid_for(nb * H * C), 256, 0, s>>>(
+    k_readout_bwd_r<<<grid_for(nb * C * H), 256, 0, s>>>(
         static_cast<const unsigned short*>(x), static_cast<const unsigned short*>(dR), nb, H, W, C,
         dr_part);
     DN_CUDA_CHECK(cudaGetLastError());
@@ -359,6 +422,33 @@ extern "C" int32_t dn_f32_to_bf16(const float* in, int64_t n, void* out, void* s
   if (!in || !out || n < 1) return DN_EINVAL;
   k_f32_to_bf16<<<grid_for(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(
       in, n, static_cast<unsigned short*>(out));
+  DN_CUDA_CHECK(cudaGetLastError());
+  return DN_OK;
+}
+
+extern "C" int32_t dn_fno_modes_rows(const void* src, void* dst, int32_t n_modes, int64_t nb,
+                                     int32_t C, int32_t to_rows, void* stream) {
+  if (!src || !dst || src == dst || n_modes < 1 || nb < 1 || C < 1) return DN_EINVAL;
+  if (nb * 2 > 65535) return DN_EUNSUPPORTED;
+  const dim3 grid((unsigned)((n_modes + 31) / 32), (unsigned)((C + 31) / 32), (unsigned)(nb * 2));
+  k_modes_rows<<<grid, dim3(32, 8), 0, static_cast<cudaStream_t>(stream)>>>(
+      static_cast<const unsigned short*>(src), static_cast<unsigned short*>(dst), n_modes, nb, C,
+      to_rows != 0);
+  DN_CUDA_CHECK(cudaGetLastError());
+  return DN_OK;
+}
+
+extern "C" int32_t dn_fno_channel_sums(const void* x, int64_t nb, int32_t C, int64_t n_pix,
+                                       float* out, float* scratch, void* stream) {
+  if (!x || !out || !scratch || nb < 1 || C < 1 || n_pix < 8 || n_pix % 8 || !al16(x))
+    return DN_EINVAL;
+  if (C > 65535) return DN_EUNSUPPORTED;
+  const int parts = nb < 256 ? (int)nb : 256;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  k_channel_part<<<dim3((unsigned)C, (unsigned)parts), 256, 0, s>>>(
+      static_cast<const unsigned short*>(x), nb, C, n_pix, scratch);
+  DN_CUDA_CHECK(cudaGetLastError());
+  k_colsum_final<<<(unsigned)((C + 255) / 256), 256, 0, s>>>(scratch, parts, C, out, 0);
   DN_CUDA_CHECK(cudaGetLastError());
   return DN_OK;
 }

@@ -6,8 +6,9 @@
 //   two-digit index map (so one GEMM can write a transposed or re-blocked
 //   layout that the next GEMM reads directly).
 //
-// Persistent CTAs (one per SM, 192 threads) walk the tile list
-// (m fastest, then n, then batch):
+// Persistent CTAs (one per SM, 192 threads) walk the tile list: per batch,
+// groups of 16 m tiles, n tiles inside a group, m fastest (neighbouring CTAs
+// share A rows and B columns in L2):
 //   warp 0, lane 0  TMA producer.  Per 64-wide k block it loads the 128 x 64
 //                   A tile and the BN x 64 B tile into one ring stage
 //                   (128-byte swizzle; a K-major operand is one box, an
@@ -77,6 +78,8 @@ struct Params {
   int act;
   const float* bias;
   const float* row_scale;
+  const float* row_bias;
+  const float* col_scale;
   const float* batch_scale;
   const char* addend;
   int addend_bf16;
@@ -92,6 +95,19 @@ __device__ __forceinline__ unsigned long long gtimer() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
+}
+
+// bounded spin (no suspend) for the producer / MMA hand-offs, where the
+// wake-up latency of a suspended wait shows in the throughput
+__device__ __forceinline__ bool gwait_spin(uint64_t* bar, uint32_t parity, volatile int* abort) {
+  const unsigned long long t0 = gtimer();
+  for (uint32_t n = 0;; ++n) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((n & 255) == 255) {
+      if (*abort) return false;
+      if (gtimer() - t0 > WAIT_NS) return false;
+    }
+  }
 }
 
 // bounded wait; false when it gave up or another role aborted
@@ -248,6 +264,21 @@ __device__ __forceinline__ void store32(char* base, int bf16, long long off, lon
   }
 }
 
+__device__ __forceinline__ void tile_coords(long long t, const Params& p, int& mt, int& nt,
+                                            int& bz) {
+  const long long per_batch = (long long)p.tiles_m * p.tiles_n;
+  bz = (int)(t / per_batch);
+  long long r = t % per_batch;
+  const int G = 16;
+  const long long gsize = (long long)G * p.tiles_n;
+  const int g = (int)(r / gsize);
+  const int m0 = g * G;
+  const int gm = p.tiles_m - m0 < G ? p.tiles_m - m0 : G;
+  r -= (long long)g * gsize;
+  mt = m0 + (int)(r % gm);
+  nt = (int)(r / gm);
+}
+
 template <int BN>
 __global__ void __launch_bounds__(NT, 1)
     k_gemm(const __grid_constant__ CUtensorMap ta0, const __grid_constant__ CUtensorMap tb0,
@@ -298,14 +329,12 @@ __global__ void __launch_bounds__(NT, 1)
       // ---- TMA producer ----------------------------------------------------
       long long g = 0;
       for (long long t = blockIdx.x; t < p.n_tiles && !*abort; t += gridDim.x) {
-        const int mt = (int)(t % p.tiles_m);
-        const long long rest = t / p.tiles_m;
-        const int nt = (int)(rest % p.tiles_n);
-        const int bz = (int)(rest / p.tiles_n);
+        int mt, nt, bz;
+        tile_coords(t, p, mt, nt, bz);
         bool ok = true;
         for (int kb = 0; kb < kb_total; ++kb, ++g) {
           const int s = (int)(g % S);
-          if (g >= S && !gwait(&empty[s], (uint32_t)(((g / S) - 1) & 1), abort)) {
+          if (g >= S && !gwait_spin(&empty[s], (uint32_t)(((g / S) - 1) & 1), abort)) {
             fail(abort, p.status);
             ok = false;
             break;
@@ -340,7 +369,7 @@ __global__ void __launch_bounds__(NT, 1)
       int it = 0;
       for (long long t = blockIdx.x; t < p.n_tiles && !*abort; t += gridDim.x, ++it) {
         const int buf = it & 1;
-        if (it >= 2 && !gwait(&tempty[buf], (uint32_t)(((it >> 1) - 1) & 1), abort)) {
+        if (it >= 2 && !gwait_spin(&tempty[buf], (uint32_t)(((it >> 1) - 1) & 1), abort)) {
           fail(abort, p.status);
           break;
         }
@@ -349,7 +378,7 @@ __global__ void __launch_bounds__(NT, 1)
         bool ok = true;
         for (int kb = 0; kb < kb_total; ++kb, ++g) {
           const int s = (int)(g % S);
-          if (!gwait(&full[s], (uint32_t)((g / S) & 1), abort)) {
+          if (!gwait_spin(&full[s], (uint32_t)((g / S) & 1), abort)) {
             fail(abort, p.status);
             ok = false;
             break;
@@ -405,14 +434,13 @@ __global__ void __launch_bounds__(NT, 1)
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const int mt = (int)(t % p.tiles_m);
-      const long long rest = t / p.tiles_m;
-      const int nt = (int)(rest % p.tiles_n);
-      const int bz = (int)(rest / p.tiles_n);
+      int mt, nt, bz;
+      tile_coords(t, p, mt, nt, bz);
       const long long row = (long long)mt * BM + quad * 32 + lane;
       const bool row_ok = row < p.M;
       float scale = p.alpha;
       if (row_ok && p.row_scale) scale *= p.row_scale[row];
+      const float rbias = (row_ok && p.row_bias) ? p.row_bias[row] : 0.0f;
       if (p.batch_scale) scale *= p.batch_scale[bz];
       const long long roff = (long long)bz * p.sb + (row % p.R0) * p.r0 + (row / p.R0) * p.r1;
 #pragma unroll 1
@@ -439,6 +467,15 @@ __global__ void __launch_bounds__(NT, 1)
           float v[32];
 #pragma unroll
           for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]) * scale;
+          if (p.col_scale) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+              if (j < nv) v[j] *= p.col_scale[col + j];
+          }
+          if (p.row_bias) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j) v[j] += rbias;
+          }
           if (p.bias) {
 #pragma unroll
             for (int j = 0; j < 32; ++j)
@@ -632,6 +669,8 @@ extern "C" int32_t dn_gemm_run(const dn_gemm* g, int32_t* status, void* stream) 
   p.act = g->act;
   p.bias = g->bias;
   p.row_scale = g->row_scale;
+  p.col_scale = g->col_scale;
+  p.row_bias = g->row_bias;
   p.batch_scale = g->batch_scale;
   p.addend = static_cast<const char*>(g->addend);
   p.addend_bf16 = g->addend_dtype == DN_BF16;

@@ -155,6 +155,11 @@ class FNO2d:
         self.Gm = torch.from_numpy(G).to(torch.bfloat16).to(self.dev).contiguous()
         self.blk = [torch.empty(c.n_modes, 2 * c.width, 2 * c.width, dtype=torch.bfloat16,
                                 device=self.dev) for _ in range(c.layers)]
+        # G = F2^T diag(cw): cw = c_kw / (H W) per mode row (c = 1 for kw = 0, else 2)
+        _, kw = mode_table(c)
+        cw = torch.from_numpy(np.where(kw == 0, 1.0, 2.0) / (c.H * c.W)).to(torch.float32)
+        self.cscale = torch.cat([cw, cw]).to(self.dev)
+        self.bscale = (1.0 / cw).to(self.dev)
         self.status = torch.zeros(1, dtype=torch.int32, device=self.dev)
         self._ws: Dict[int, Dict[str, torch.Tensor]] = {}
         self.refresh()
@@ -220,14 +225,16 @@ class FNO2d:
         if B in self._ws:
             return self._ws[B]
         c, d = self.cfg, self.dev
-        HW, C = c.H * c.W, c.width
+        HW, C, NM, NR = c.H * c.W, c.width, c.n_modes, c.n_mode_rows
         bf = dict(dtype=torch.bfloat16, device=d)
         ws = {
             "feat": torch.zeros(B, HW, FEAT, **bf),
-            "X": [torch.empty(B, HW, C, **bf) for _ in range(c.layers + 1)],
-            "pre": [torch.empty(B, HW, C, **bf) for _ in range(c.layers - 1)],
-            "Zm": [torch.empty(c.n_modes, B, 2 * C, **bf) for _ in range(c.layers)],
-            "Yh": torch.empty(B, c.n_mode_rows, C, **bf),
+            "X": [torch.empty(B, C, HW, **bf) for _ in range(c.layers + 1)],
+            "pre": [torch.empty(B, C, HW, **bf) for _ in range(c.layers - 1)],
+            "Zm": [torch.empty(NM, B, 2 * C, **bf) for _ in range(c.layers)],
+            "Ym": torch.empty(NM, B, 2 * C, **bf),
+            "Yt": torch.empty(B, C, NR, **bf),
+            "S": torch.empty(B, C, HW, **bf),
             "R": torch.empty(B, c.W, C, **bf),
             "U": torch.empty(B * c.W, c.hidden, **bf),
             "preU": torch.empty(B * c.W, c.hidden, **bf),
@@ -241,25 +248,32 @@ class FNO2d:
         if "gout" in ws:
             return ws
         c, d = self.cfg, self.dev
-        HW, C = c.H * c.W, c.width
+        HW, C, NM, NR = c.H * c.W, c.width, c.n_modes, c.n_mode_rows
         bf = dict(dtype=torch.bfloat16, device=d)
         f32 = dict(dtype=torch.float32, device=d)
-        rows_max = max(B * HW, B * c.W)
         ws.update({
             "gout": torch.zeros(B * c.W, OUT_LD, **bf),
             "dpreU": torch.empty(B * c.W, c.hidden, **bf),
             "dR": torch.empty(B * c.W, C, **bf),
-            "dA": torch.empty(B, HW, C, **bf),
-            "dB": torch.empty(B, HW, C, **bf),
-            "dYm": torch.empty(c.n_modes, B, 2 * C, **bf),
-            "dZ": torch.empty(B, c.n_mode_rows, C, **bf),
-            "dblk": torch.empty(c.n_modes, 2 * C, 2 * C, **f32),
+            "dA": torch.empty(B, C, HW, **bf),
+            "dB": torch.empty(B, C, HW, **bf),
+            "dXs": torch.empty(B, C, HW, **bf),
+            "dYt": torch.empty(B, C, NR, **bf),
+            "dYm": torch.empty(NM, B, 2 * C, **bf),
+            "dZm": torch.empty(NM, B, 2 * C, **bf),
+            "dZt": torch.empty(B, C, NR, **bf),
+            "dblk": torch.empty(NM, 2 * C, 2 * C, **f32),
             "part": torch.empty(B * max(c.H, c.hidden, OUT_LD) * max(C, c.hidden), **f32),
-            "scratch": torch.empty(int(self.L.dn_colsum_scratch_elems(rows_max, 4 * C * C)),
-                                   **f32),
+            "scratch": torch.empty(int(self.L.dn_colsum_scratch_elems(max(B * c.W, B),
+                                                                       4 * C * C)), **f32),
             "loss_part": torch.zeros(256, dtype=torch.float64, device=d),
         })
         return ws
+
+    def _modes_rows(self, src, dst, B, to_rows):
+        c = self.cfg
+        _lib.check("dn_fno_modes_rows", self.L.dn_fno_modes_rows(
+            _c(src), _c(dst), c.n_modes, B, c.width, int(to_rows), self._stream()))
 
     # ---- passes -----------------------------------------------------------
     def forward(self, eps: torch.Tensor) -> torch.Tensor:
@@ -275,34 +289,35 @@ class FNO2d:
 
     def _forward(self, eps, ws, B):
         c, ps, L, s = self.cfg, self.ps, self.L, self._stream()
-        HW, C, NM = c.H * c.W, c.width, c.n_modes
+        HW, C, NM, NR = c.H * c.W, c.width, c.n_modes, c.n_mode_rows
         st = self.status
         _lib.check("dn_fno_features", L.dn_fno_features(
             _c(eps), B, c.H, c.W, c.eps_lo, c.eps_hi, _c(ws["feat"]), s))
         X = ws["X"]
-        # lift
-        gemm(B * HW, C, [(kmajor(ws["feat"], B * HW, FEAT), kmajor(ps.B("P"), C, FEAT))], X[0],
-             OutMap.rowmajor(C), bias=ps.P("p"), status=st)
+        # lift, per sample X0[c, hw] = P feat^T + p (channel-first rows)
+        gemm(C, HW, [(kmajor(ps.B("P"), C, FEAT),
+                      kmajor(ws["feat"], HW, FEAT, batch_stride=HW * FEAT))],
+             X[0], OutMap.rowmajor(HW, batch=C * HW), batch=B, row_bias=ps.P("p"), status=st)
         zmap = OutMap(row_radix=NM, row0=B * 2 * C, row1=C, col_radix=C, col0=1, col1=2 * C)
-        ymap = OutMap(batch=C, row0=c.n_mode_rows * C, col_radix=C, col0=1, col1=NM * C)
         for l in range(c.layers):
-            # truncated DFT of every channel of every sample: Zm[m, b, (ri, c)]
-            gemm(c.n_mode_rows, B * C, [(kmajor(self.F2, c.n_mode_rows, HW),
-                                         mnmajor(X[l], B * C, HW, ld=C, fold=C,
-                                                 fold_stride=HW * C))],
+            # truncated DFT of every (sample, channel) row: Zm[m, b, (ri, c)]
+            gemm(NR, B * C, [(kmajor(self.F2, NR, HW), kmajor(X[l], B * C, HW))],
                  ws["Zm"][l], zmap, status=st)
-            # per-mode complex channel mixing: Yh[b, (ri, m), o]
+            # per-mode complex channel mixing: Ym[m, b, (ri, o)]
             gemm(B, 2 * C, [(kmajor(ws["Zm"][l], B, 2 * C, batch_stride=B * 2 * C),
                              kmajor(self.blk[l], 2 * C, 2 * C, batch_stride=4 * C * C))],
-                 ws["Yh"], ymap, batch=NM, status=st)
-            # inverse DFT + 1x1 mix + bias (+ GELU) in one GEMM
+                 ws["Ym"], OutMap.rowmajor(2 * C, batch=B * 2 * C), batch=NM, status=st)
+            self._modes_rows(ws["Ym"], ws["Yt"], B, True)
+            # inverse DFT: S[(b, o), hw]
+            gemm(B * C, HW, [(kmajor(ws["Yt"], B * C, NR), kmajor(self.Gm, HW, NR))],
+                 ws["S"], OutMap.rowmajor(HW), status=st)
+            # 1x1 mix + S + bias (+ GELU), per sample X'[o, hw] = W X[:, hw]
             last = l == c.layers - 1
-            gemm(HW, C, [(kmajor(self.Gm, HW, c.n_mode_rows),
-                          mnmajor(ws["Yh"], C, c.n_mode_rows, ld=C,
-                                  batch_stride=c.n_mode_rows * C)),
-                         (kmajor(X[l], HW, C, batch_stride=HW * C), kmajor(ps.B(f"W{l}"), C, C))],
-                 X[l + 1], OutMap.rowmajor(C, batch=HW * C), batch=B, bias=ps.P(f"b{l}"),
-                 act=0 if last else ACT_GELU, pre=None if last else ws["pre"][l], status=st)
+            gemm(C, HW, [(kmajor(ps.B(f"W{l}"), C, C),
+                          mnmajor(X[l], HW, C, ld=HW, batch_stride=C * HW))],
+                 X[l + 1], OutMap.rowmajor(HW, batch=C * HW), batch=B, row_bias=ps.P(f"b{l}"),
+                 addend=ws["S"], act=0 if last else ACT_GELU,
+                 pre=None if last else ws["pre"][l], status=st)
         _lib.check("dn_fno_readout", L.dn_fno_readout(
             _c(X[c.layers]), _c(ps.P("r")), B, c.H, c.W, C, _c(ws["R"]), s))
         gemm(B * c.W, c.hidden, [(kmajor(ws["R"], B * c.W, C), kmajor(ps.B("Q1"), c.hidden, C))],
@@ -316,6 +331,12 @@ class FNO2d:
         _lib.check("dn_colsum", self.L.dn_colsum(
             _c(src), dtype, rows, cols, cols, _c(dst), 0, _c(ws["scratch"]),
             ws["scratch"].numel(), self._stream()))
+
+    def _channel_sums(self, d, B, dst, ws):
+        """dst[c] = sum over samples and pixels of channel-first d (B, C, HW)."""
+        c = self.cfg
+        _lib.check("dn_fno_channel_sums", self.L.dn_fno_channel_sums(
+            _c(d), B, c.width, c.H * c.W, _c(dst), _c(ws["scratch"]), self._stream()))
 
     def backward(self, gout_bf16: Optional[torch.Tensor] = None, B: Optional[int] = None,
                  want_input_grad: bool = False) -> Optional[torch.Tensor]:
@@ -357,47 +378,53 @@ class FNO2d:
         _lib.check("dn_fno_readout_bwd", L.dn_fno_readout_bwd(
             _c(X[c.layers]), _c(ps.P("r")), _c(ws["dR"]), B, c.H, c.W, C, _c(dcur), _c(part), s))
         self._colsum(part, F32, B, c.H * C, ps.G("r"), ws)
-        zmap = OutMap(row_radix=NM, row0=B * 2 * C, row1=C, col_radix=C, col0=1, col1=2 * C)
-        ymap = OutMap(batch=C, row0=NR * C, col_radix=C, col0=1, col1=NM * C)
         for l in reversed(range(c.layers)):
-            # dpre_l = dcur
-            gemm(NR, B * C, [(mnmajor(self.Gm, NR, HW, ld=NR),
-                              mnmajor(dcur, B * C, HW, ld=C, fold=C, fold_stride=HW * C))],
-                 ws["dYm"], zmap, status=st)
+            # dcur = d loss / d pre_l, channel-first
+            # through the inverse DFT: dYt = dpre G = (dpre F2^T) diag(c/HW)
+            gemm(B * C, NR, [(kmajor(dcur, B * C, HW), kmajor(self.F2, NR, HW))],
+                 ws["dYt"], OutMap.rowmajor(NR), col_scale=self.cscale, status=st)
+            self._modes_rows(ws["dYt"], ws["dYm"], B, False)
+            # mode weights
             gemm(2 * C, 2 * C, [(mnmajor(ws["dYm"], 2 * C, B, ld=2 * C, batch_stride=B * 2 * C),
                                  mnmajor(ws["Zm"][l], 2 * C, B, ld=2 * C,
                                          batch_stride=B * 2 * C))],
                  ws["dblk"], OutMap.rowmajor(2 * C, batch=4 * C * C), batch=NM, status=st)
             _lib.check("dn_fno_unpack_mode_grads", L.dn_fno_unpack_mode_grads(
                 _c(ws["dblk"]), NM, C, C, _c(ps.G(f"wre{l}")), _c(ps.G(f"wim{l}")), s))
+            # back through the mixing; HW/c per mode turns G into F2^T below
             gemm(B, 2 * C, [(kmajor(ws["dYm"], B, 2 * C, batch_stride=B * 2 * C),
                              mnmajor(self.blk[l], 2 * C, 2 * C, ld=2 * C,
                                      batch_stride=4 * C * C))],
-                 ws["dZ"], ymap, batch=NM, status=st)
-            gemm(C, C, [(mnmajor(dcur, C, HW, ld=C, batch_stride=HW * C),
-                         mnmajor(X[l], C, HW, ld=C, batch_stride=HW * C))],
+                 ws["dZm"], OutMap.rowmajor(2 * C, batch=B * 2 * C), batch=NM,
+                 batch_scale=self.bscale, status=st)
+            self._modes_rows(ws["dZm"], ws["dZt"], B, True)
+            # through the DFT: dXs = dZ F2 = (dZ diag(HW/c)) G^T
+            gemm(B * C, HW, [(kmajor(ws["dZt"], B * C, NR), kmajor(self.Gm, HW, NR))],
+                 ws["dXs"], OutMap.rowmajor(HW), status=st)
+            # 1x1 weights and bias
+            gemm(C, C, [(kmajor(dcur, C, HW, batch_stride=C * HW),
+                         kmajor(X[l], C, HW, batch_stride=C * HW))],
                  part, OutMap.rowmajor(C, batch=C * C), batch=B, status=st)
             self._colsum(part, F32, B, C * C, ps.G(f"W{l}"), ws)
-            self._colsum(dcur, BF16, B * HW, C, ps.G(f"b{l}"), ws)
-            # dX_l through the DFT and the 1x1 mix; through GELU of layer l-1
+            self._channel_sums(dcur, B, ps.G(f"b{l}"), ws)
+            # dX_l = dXs + W^T dpre_l, through GELU of layer l-1
             act = ACT_GELU_GRAD if l > 0 else 0
-            gemm(HW, C, [(mnmajor(self.F2, HW, NR, ld=HW),
-                          mnmajor(ws["dZ"], C, NR, ld=C, batch_stride=NR * C)),
-                         (kmajor(dcur, HW, C, batch_stride=HW * C),
-                          mnmajor(ps.B(f"W{l}"), C, C, ld=C))],
-                 dnext, OutMap.rowmajor(C, batch=HW * C), batch=B, act=act,
-                 aux=ws["pre"][l - 1] if l > 0 else None, status=st)
+            gemm(C, HW, [(mnmajor(ps.B(f"W{l}"), C, C, ld=C),
+                          mnmajor(dcur, HW, C, ld=HW, batch_stride=C * HW))],
+                 dnext, OutMap.rowmajor(HW, batch=C * HW), batch=B, addend=ws["dXs"],
+                 act=act, aux=ws["pre"][l - 1] if l > 0 else None, status=st)
             dcur, dnext = dnext, dcur
         # lift (dcur = dX0)
-        gemm(C, FEAT, [(mnmajor(dcur, C, HW, ld=C, batch_stride=HW * C),
+        gemm(C, FEAT, [(kmajor(dcur, C, HW, batch_stride=C * HW),
                         mnmajor(ws["feat"], FEAT, HW, ld=FEAT, batch_stride=HW * FEAT))],
              part, OutMap.rowmajor(FEAT, batch=C * FEAT), batch=B, status=st)
         self._colsum(part, F32, B, C * FEAT, ps.G("P"), ws)
-        self._colsum(dcur, BF16, B * HW, C, ps.G("p"), ws)
+        self._channel_sums(dcur, B, ps.G("p"), ws)
         if not want_input_grad:
             return None
         dfeat = torch.empty(B * HW, FEAT, dtype=torch.float32, device=self.dev)
-        gemm(B * HW, FEAT, [(kmajor(dcur, B * HW, C), mnmajor(ps.B("P"), FEAT, C, ld=FEAT))],
+        gemm(B * HW, FEAT, [(mnmajor(dcur, B * HW, C, ld=HW, fold=HW, fold_stride=C * HW),
+                             mnmajor(ps.B("P"), FEAT, C, ld=FEAT))],
              dfeat, OutMap.rowmajor(FEAT), status=st)
         deps = torch.empty(B, c.H, c.W, dtype=torch.float32, device=self.dev)
         _lib.check("dn_fno_features_bwd", L.dn_fno_features_bwd(

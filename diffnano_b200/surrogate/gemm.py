@@ -98,6 +98,7 @@ def gemm(M: int, N: int, segs: Sequence[Tuple[Operand, Operand]], out: torch.Ten
          omap: OutMap, *, batch: int = 1, accumulate: bool = False, alpha: float = 1.0,
          act: int = ACT_NONE, bias: Optional[torch.Tensor] = None,
          row_scale: Optional[torch.Tensor] = None, batch_scale: Optional[torch.Tensor] = None,
+         col_scale: Optional[torch.Tensor] = None, row_bias: Optional[torch.Tensor] = None,
          addend: Optional[torch.Tensor] = None, aux: Optional[torch.Tensor] = None,
          pre: Optional[torch.Tensor] = None, block_n: int = 0, max_ctas: int = 0,
          status: Optional[torch.Tensor] = None) -> torch.Tensor:
@@ -109,7 +110,7 @@ def gemm(M: int, N: int, segs: Sequence[Tuple[Operand, Operand]], out: torch.Ten
     for i, (a, b) in enumerate(segs):
         g.a[i] = a.c()
         g.b[i] = b.c()
-    for t in (bias, row_scale, batch_scale):
+    for t in (bias, row_scale, batch_scale, col_scale, row_bias):
         if t is not None and (t.dtype != torch.float32 or not t.is_contiguous()):
             raise TypeError("bias / row_scale / batch_scale are contiguous float32")
     g.out = _ptr(out)
@@ -121,6 +122,7 @@ def gemm(M: int, N: int, segs: Sequence[Tuple[Operand, Operand]], out: torch.Ten
     g.alpha = float(alpha)
     g.act = int(act)
     g.bias, g.row_scale, g.batch_scale = _ptr(bias), _ptr(row_scale), _ptr(batch_scale)
+    g.col_scale, g.row_bias = _ptr(col_scale), _ptr(row_bias)
     g.addend, g.addend_dtype = _ptr(addend), _dtype_code(addend)
     g.aux, g.aux_dtype = _ptr(aux), _dtype_code(aux)
     g.pre, g.pre_dtype = _ptr(pre), _dtype_code(pre)

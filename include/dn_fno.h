@@ -53,7 +53,8 @@ typedef struct dn_gemm_operand {
 
 /* C[z] (M x N) = sum over segments s of A_s[z] * B_s[z]^T  (K_s = a[s].k =
  * b[s].k), then the epilogue, per element (z, r, c):
- *   v = alpha * acc * row_scale[r] * batch_scale[z] + bias[c] + addend[z,r,c]
+ *   v = alpha * acc * row_scale[r] * col_scale[c] * batch_scale[z] + bias[c]
+ *       + row_bias[r] + addend[z,r,c]
  *   y = v | gelu(v) | v * gelu'(aux[z,r,c])          (act)
  *   out[z,r,c] = y   (or += y when accumulate, FP32 output only)
  * with every optional pointer NULL to skip it.  out, addend, aux and pre
@@ -92,6 +93,8 @@ typedef struct dn_gemm {
   int32_t pre_dtype;
   int32_t block_n;  /* 0 = choose; else 64, 128 or 256 */
   int32_t max_ctas; /* 0 = one per SM */
+  const float* col_scale;
+  const float* row_bias;
 } dn_gemm;
 
 /* Persistent warp-specialised kernel: a TMA producer warp (128-byte swizzled
@@ -102,7 +105,7 @@ typedef struct dn_gemm {
 int32_t dn_gemm_run(const dn_gemm* g, int32_t* status, void* stream);
 
 /* ---- memory-bound helpers of the operator's passes ----------------------
- * Channel-last BF16 activations (sample, row, column, channel). */
+ * BF16 activations are channel-first (sample, channel, row, column). */
 
 /* feat[i, 0..7] = ((eps - lo) / (hi - lo), column / (W-1), row / (H-1), 0 x 5)
  * as BF16 for every pixel of n_img (H, W) FP32 maps; feat 16-byte aligned.
@@ -114,11 +117,11 @@ int32_t dn_fno_features(const float* eps, int64_t n_img, int32_t H, int32_t W, f
 int32_t dn_fno_features_bwd(const float* dfeat, int64_t n_pix, float eps_lo, float eps_hi,
                             float* deps, void* stream);
 
-/* out[b, w, c] = sum_h r[h, c] * x[b, h, w, c]   (x, out BF16; r FP32 (H, C)) */
+/* out[b, w, c] = sum_h r[h, c] * x[b, c, h, w]   (x, out BF16; r FP32 (H, C)) */
 int32_t dn_fno_readout(const void* x, const float* r, int64_t nb, int32_t H, int32_t W,
                        int32_t C, void* out, void* stream);
-/* dx[b, h, w, c] = r[h, c] * dR[b, w, c] (BF16; NULL skips) and
- * dr_part[b, h, c] = sum_w dR[b, w, c] * x[b, h, w, c] (FP32; NULL skips) */
+/* dx[b, c, h, w] = r[h, c] * dR[b, w, c] (BF16; NULL skips) and
+ * dr_part[b, h, c] = sum_w dR[b, w, c] * x[b, c, h, w] (FP32; NULL skips) */
 int32_t dn_fno_readout_bwd(const void* x, const float* r, const void* dR, int64_t nb, int32_t H,
                            int32_t W, int32_t C, void* dx, float* dr_part, void* stream);
 
@@ -152,6 +155,18 @@ int32_t dn_fno_pack_modes(const float* wre, const float* wim, int64_t n_modes, i
                           int32_t c_in, void* blk, void* stream);
 int32_t dn_fno_unpack_mode_grads(const float* dblk, int64_t n_modes, int32_t c_out, int32_t c_in,
                                  float* dwre, float* dwim, void* stream);
+
+/* Kept Fourier modes between the per-mode layout the mixing GEMM reads and
+ * writes, (n_modes, nb, 2, C), and the per-channel layout of the transform
+ * GEMMs, (nb, C, 2, n_modes) (2 = real, imaginary); to_rows != 0 converts the
+ * first to the second.  BF16, src != dst. */
+int32_t dn_fno_modes_rows(const void* src, void* dst, int32_t n_modes, int64_t nb, int32_t C,
+                          int32_t to_rows, void* stream);
+
+/* out[c] = sum over samples b and pixels p of x[b, c, p] (BF16, channel-first
+ * (nb, C, n_pix)), FP32, deterministic; scratch: 256 * C floats. */
+int32_t dn_fno_channel_sums(const void* x, int64_t nb, int32_t C, int64_t n_pix, float* out,
+                            float* scratch, void* stream);
 
 /* out[i] = bf16(in[i]) */
 int32_t dn_f32_to_bf16(const float* in, int64_t n, void* out, void* stream);
