@@ -165,6 +165,8 @@ SIGNATURES = {
     "dn_f32_to_bf16": (c_int32, [c_void_p, c_int64, c_void_p, c_void_p]),
     "dn_fno_channel_sums": (c_int32, [c_void_p, c_int64, c_int32, c_int64, c_void_p, c_void_p,
                                       c_void_p]),
+    "dn_fno_pack_pointwise": (c_int32, [c_void_p, c_void_p, c_int32, c_void_p, c_void_p,
+                                        c_void_p, c_void_p]),
     "dn_fno_modes_rows": (c_int32, [c_void_p, c_void_p, c_int32, c_int64, c_int32, c_int32,
                                     c_void_p]),
     "dn_density_forward": (c_int32, [ctypes.POINTER(DnDensity), c_void_p, c_void_p, c_void_p,

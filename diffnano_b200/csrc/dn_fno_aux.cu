@@ -70,35 +70,64 @@ __global__ void k_readout(const unsigned short* __restrict__ x, const float* __r
   }
 }
 
-// dx[b, c, h, w] = r[h, c] * dR[b, w, c]            (one thread per element)
+// dx[b, c, h, w] = r[h, c] * dR[b, w, c]; one thread per 8 consecutive w
 __global__ void k_readout_bwd_x(const float* __restrict__ r, const unsigned short* __restrict__ dR,
                                 long long nb, int H, int W, int C, unsigned short* __restrict__ dx) {
-  const long long n = nb * C * H * W;
+  const int W8 = W / 8;
+  const long long n = nb * C * H * W8;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
-    const int w = (int)(i % W);
-    const int h = (int)((i / W) % H);
-    const int c = (int)((i / ((long long)W * H)) % C);
-    const long long b = i / ((long long)C * H * W);
-    dx[i] = f2bf(r[h * C + c] * bf2f(dR[(b * W + w) * C + c]));
+    const int w0 = (int)(i % W8) * 8;
+    const long long row = i / W8;  // (b, c, h)
+    const int h = (int)(row % H);
+    const long long bc = row / H;
+    const int c = (int)(bc % C);
+    const long long b = bc / C;
+    const float rv = r[h * C + c];
+    const unsigned short* d = dR + (b * W + w0) * C + c;
+    uint32_t o[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e)
+      o[e] = (uint32_t)f2bf(rv * bf2f(d[(2 * e) * C])) |
+             ((uint32_t)f2bf(rv * bf2f(d[(2 * e + 1) * C])) << 16);
+    reinterpret_cast<uint4*>(dx + row * W + w0)[0] = make_uint4(o[0], o[1], o[2], o[3]);
   }
 }
 
-// dr_part[b, h, c] = sum_w dR[b, w, c] * x[b, c, h, w]   (one thread per (b, c, h))
+// dr_part[b, h, c] = sum_w dR[b, w, c] * x[b, c, h, w]; one warp per (b, c, h)
 __global__ void k_readout_bwd_r(const unsigned short* __restrict__ x,
                                 const unsigned short* __restrict__ dR, long long nb, int H, int W,
                                 int C, float* __restrict__ dr_part) {
   const long long n = nb * C * H;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long i = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); i < n;
+       i += warps) {
     const int h = (int)(i % H);
     const int c = (int)((i / H) % C);
     const long long b = i / ((long long)H * C);
     const unsigned short* xr = x + ((b * C + c) * H + h) * (long long)W;
     const unsigned short* dr = dR + b * W * (long long)C + c;
     float s = 0.0f;
-    for (int w = 0; w < W; ++w) s = fmaf(bf2f(dr[(long long)w * C]), bf2f(xr[w]), s);
-    dr_part[(b * H + h) * C + c] = s;
+    for (int w = lane; w < W; w += 32) s = fmaf(bf2f(dr[(long long)w * C]), bf2f(xr[w]), s);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) dr_part[(b * H + h) * C + c] = s;
+  }
+}
+
+// blockdiag(W, W) and blockdiag(W^T, W^T) (2C x 2C, BF16) and [b, b]
+__global__ void k_pack_pointwise(const float* __restrict__ Wm, const float* __restrict__ bias,
+                                 int C, unsigned short* __restrict__ blk,
+                                 unsigned short* __restrict__ blkT, float* __restrict__ bias2) {
+  const int n = 4 * C * C;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int r = i / (2 * C), q = i % (2 * C);
+    const bool diag = (r < C) == (q < C);
+    const int rr = r % C, qq = q % C;
+    blk[i] = f2bf(diag ? Wm[rr * C + qq] : 0.0f);
+    blkT[i] = f2bf(diag ? Wm[qq * C + rr] : 0.0f);
+    if (i < 2 * C) bias2[i] = bias[i % C];
   }
 }
 
@@ -334,12 +363,13 @@ extern "C" int32_t dn_fno_readout_bwd(const void* x, const float* r, const void*
     return DN_EINVAL;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (dx) {
-    k_readout_bwd_x<<<grid_for(nb * C * H * W), 256, 0, s>>>(
+    if (W % 8) return DN_EINVAL;
+    k_readout_bwd_x<<<grid_for(nb * C * H * (W / 8)), 256, 0, s>>>(
         r, static_cast<const unsigned short*>(dR), nb, H, W, C, static_cast<unsigned short*>(dx));
     DN_CUDA_CHECK(cudaGetLastError());
   }
   if (dr_part) {
-    k_readout_bwd_r<<<grid_for(nb * C * H), 256, 0, s>>>(
+    k_readout_bwd_r<<<grid_for(nb * C * H * 32), 256, 0, s>>>(
         static_cast<const unsigned short*>(x), static_cast<const unsigned short*>(dR), nb, H, W, C,
         dr_part);
     DN_CUDA_CHECK(cudaGetLastError());
@@ -449,6 +479,15 @@ extern "C" int32_t dn_fno_channel_sums(const void* x, int64_t nb, int32_t C, int
       static_cast<const unsigned short*>(x), nb, C, n_pix, scratch);
   DN_CUDA_CHECK(cudaGetLastError());
   k_colsum_final<<<(unsigned)((C + 255) / 256), 256, 0, s>>>(scratch, parts, C, out, 0);
+  DN_CUDA_CHECK(cudaGetLastError());
+  return DN_OK;
+}
+
+extern "C" int32_t dn_fno_pack_pointwise(const float* Wm, const float* bias, int32_t C, void* blk,
+                                         void* blkT, float* bias2, void* stream) {
+  if (!Wm || !bias || !blk || !blkT || !bias2 || C < 1) return DN_EINVAL;
+  k_pack_pointwise<<<grid_for(4LL * C * C), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      Wm, bias, C, static_cast<unsigned short*>(blk), static_cast<unsigned short*>(blkT), bias2);
   DN_CUDA_CHECK(cudaGetLastError());
   return DN_OK;
 }

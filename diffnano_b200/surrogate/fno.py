@@ -155,6 +155,11 @@ class FNO2d:
         self.Gm = torch.from_numpy(G).to(torch.bfloat16).to(self.dev).contiguous()
         self.blk = [torch.empty(c.n_modes, 2 * c.width, 2 * c.width, dtype=torch.bfloat16,
                                 device=self.dev) for _ in range(c.layers)]
+        # 1x1 mixes of a sample pair: blockdiag(W, W), blockdiag(W^T, W^T), [b, b]
+        pw = dict(dtype=torch.bfloat16, device=self.dev)
+        self.pw = [torch.empty(2 * c.width, 2 * c.width, **pw) for _ in range(c.layers)]
+        self.pwT = [torch.empty(2 * c.width, 2 * c.width, **pw) for _ in range(c.layers)]
+        self.pw_bias = [torch.empty(2 * c.width, device=self.dev) for _ in range(c.layers)]
         # G = F2^T diag(cw): cw = c_kw / (H W) per mode row (c = 1 for kw = 0, else 2)
         _, kw = mode_table(c)
         cw = torch.from_numpy(np.where(kw == 0, 1.0, 2.0) / (c.H * c.W)).to(torch.float32)
@@ -215,6 +220,9 @@ class FNO2d:
             _lib.check("dn_fno_pack_modes", L.dn_fno_pack_modes(
                 _c(self.ps.P(f"wre{l}")), _c(self.ps.P(f"wim{l}")), c.n_modes, c.width,
                 c.width, _c(self.blk[l]), s))
+            _lib.check("dn_fno_pack_pointwise", L.dn_fno_pack_pointwise(
+                _c(self.ps.P(f"W{l}")), _c(self.ps.P(f"b{l}")), c.width, _c(self.pw[l]),
+                _c(self.pwT[l]), _c(self.pw_bias[l]), s))
 
     @staticmethod
     def _stream() -> int:
@@ -226,15 +234,15 @@ class FNO2d:
             return self._ws[B]
         c, d = self.cfg, self.dev
         HW, C, NM, NR = c.H * c.W, c.width, c.n_modes, c.n_mode_rows
+        Bp = B + (B & 1)  # pair tensors: an even number of samples, the spare one zero
         bf = dict(dtype=torch.bfloat16, device=d)
         ws = {
             "feat": torch.zeros(B, HW, FEAT, **bf),
-            "X": [torch.empty(B, C, HW, **bf) for _ in range(c.layers + 1)],
-            "pre": [torch.empty(B, C, HW, **bf) for _ in range(c.layers - 1)],
+            "X": [torch.zeros(Bp, C, HW, **bf) for _ in range(c.layers + 1)],
+            "pre": [torch.zeros(Bp, C, HW, **bf) for _ in range(c.layers - 1)],
             "Zm": [torch.empty(NM, B, 2 * C, **bf) for _ in range(c.layers)],
             "Ym": torch.empty(NM, B, 2 * C, **bf),
-            "Yt": torch.empty(B, C, NR, **bf),
-            "S": torch.empty(B, C, HW, **bf),
+            "Yt": torch.zeros(Bp, C, NR, **bf),
             "R": torch.empty(B, c.W, C, **bf),
             "U": torch.empty(B * c.W, c.hidden, **bf),
             "preU": torch.empty(B * c.W, c.hidden, **bf),
@@ -249,19 +257,19 @@ class FNO2d:
             return ws
         c, d = self.cfg, self.dev
         HW, C, NM, NR = c.H * c.W, c.width, c.n_modes, c.n_mode_rows
+        Bp = B + (B & 1)
         bf = dict(dtype=torch.bfloat16, device=d)
         f32 = dict(dtype=torch.float32, device=d)
         ws.update({
             "gout": torch.zeros(B * c.W, OUT_LD, **bf),
             "dpreU": torch.empty(B * c.W, c.hidden, **bf),
             "dR": torch.empty(B * c.W, C, **bf),
-            "dA": torch.empty(B, C, HW, **bf),
-            "dB": torch.empty(B, C, HW, **bf),
-            "dXs": torch.empty(B, C, HW, **bf),
+            "dA": torch.zeros(Bp, C, HW, **bf),
+            "dB": torch.zeros(Bp, C, HW, **bf),
             "dYt": torch.empty(B, C, NR, **bf),
             "dYm": torch.empty(NM, B, 2 * C, **bf),
             "dZm": torch.empty(NM, B, 2 * C, **bf),
-            "dZt": torch.empty(B, C, NR, **bf),
+            "dZt": torch.zeros(Bp, C, NR, **bf),
             "dblk": torch.empty(NM, 2 * C, 2 * C, **f32),
             "part": torch.empty(B * max(c.H, c.hidden, OUT_LD) * max(C, c.hidden), **f32),
             "scratch": torch.empty(int(self.L.dn_colsum_scratch_elems(max(B * c.W, B),
@@ -290,6 +298,7 @@ class FNO2d:
     def _forward(self, eps, ws, B):
         c, ps, L, s = self.cfg, self.ps, self.L, self._stream()
         HW, C, NM, NR = c.H * c.W, c.width, c.n_modes, c.n_mode_rows
+        Bp = B + (B & 1)
         st = self.status
         _lib.check("dn_fno_features", L.dn_fno_features(
             _c(eps), B, c.H, c.W, c.eps_lo, c.eps_hi, _c(ws["feat"]), s))
@@ -308,15 +317,16 @@ class FNO2d:
                              kmajor(self.blk[l], 2 * C, 2 * C, batch_stride=4 * C * C))],
                  ws["Ym"], OutMap.rowmajor(2 * C, batch=B * 2 * C), batch=NM, status=st)
             self._modes_rows(ws["Ym"], ws["Yt"], B, True)
-            # inverse DFT: S[(b, o), hw]
-            gemm(B * C, HW, [(kmajor(ws["Yt"], B * C, NR), kmajor(self.Gm, HW, NR))],
-                 ws["S"], OutMap.rowmajor(HW), status=st)
-            # 1x1 mix + S + bias (+ GELU), per sample X'[o, hw] = W X[:, hw]
+            # inverse DFT + 1x1 mix + bias (+ GELU) in one GEMM per sample pair:
+            # rows (b, o) of the pair; K = the kept modes, then the pair's 2C
+            # channels against blockdiag(W, W)
             last = l == c.layers - 1
-            gemm(C, HW, [(kmajor(ps.B(f"W{l}"), C, C),
-                          mnmajor(X[l], HW, C, ld=HW, batch_stride=C * HW))],
-                 X[l + 1], OutMap.rowmajor(HW, batch=C * HW), batch=B, row_bias=ps.P(f"b{l}"),
-                 addend=ws["S"], act=0 if last else ACT_GELU,
+            gemm(2 * C, HW, [(kmajor(ws["Yt"], 2 * C, NR, batch_stride=2 * C * NR),
+                              kmajor(self.Gm, HW, NR)),
+                             (kmajor(self.pw[l], 2 * C, 2 * C),
+                              mnmajor(X[l], HW, 2 * C, ld=HW, batch_stride=2 * C * HW))],
+                 X[l + 1], OutMap.rowmajor(HW, batch=2 * C * HW), batch=Bp // 2,
+                 row_bias=self.pw_bias[l], act=0 if last else ACT_GELU,
                  pre=None if last else ws["pre"][l], status=st)
         _lib.check("dn_fno_readout", L.dn_fno_readout(
             _c(X[c.layers]), _c(ps.P("r")), B, c.H, c.W, C, _c(ws["R"]), s))
@@ -351,6 +361,7 @@ class FNO2d:
         if gout_bf16 is not None:
             ws["gout"].copy_(gout_bf16.view(B * c.W, OUT_LD))
         HW, C, NM, NR = c.H * c.W, c.width, c.n_modes, c.n_mode_rows
+        Bp = B + (B & 1)
         st, X, part = self.status, ws["X"], ws["part"]
         F32, BF16 = 0, 2
         BW = B * c.W
@@ -398,21 +409,21 @@ class FNO2d:
                  ws["dZm"], OutMap.rowmajor(2 * C, batch=B * 2 * C), batch=NM,
                  batch_scale=self.bscale, status=st)
             self._modes_rows(ws["dZm"], ws["dZt"], B, True)
-            # through the DFT: dXs = dZ F2 = (dZ diag(HW/c)) G^T
-            gemm(B * C, HW, [(kmajor(ws["dZt"], B * C, NR), kmajor(self.Gm, HW, NR))],
-                 ws["dXs"], OutMap.rowmajor(HW), status=st)
             # 1x1 weights and bias
             gemm(C, C, [(kmajor(dcur, C, HW, batch_stride=C * HW),
                          kmajor(X[l], C, HW, batch_stride=C * HW))],
                  part, OutMap.rowmajor(C, batch=C * C), batch=B, status=st)
             self._colsum(part, F32, B, C * C, ps.G(f"W{l}"), ws)
             self._channel_sums(dcur, B, ps.G(f"b{l}"), ws)
-            # dX_l = dXs + W^T dpre_l, through GELU of layer l-1
+            # dX_l = dZ F2 + W^T dpre_l (dZ F2 = (dZ diag(HW/c)) G^T), through
+            # GELU of layer l-1; one GEMM per sample pair as in the forward pass
             act = ACT_GELU_GRAD if l > 0 else 0
-            gemm(C, HW, [(mnmajor(ps.B(f"W{l}"), C, C, ld=C),
-                          mnmajor(dcur, HW, C, ld=HW, batch_stride=C * HW))],
-                 dnext, OutMap.rowmajor(HW, batch=C * HW), batch=B, addend=ws["dXs"],
-                 act=act, aux=ws["pre"][l - 1] if l > 0 else None, status=st)
+            gemm(2 * C, HW, [(kmajor(ws["dZt"], 2 * C, NR, batch_stride=2 * C * NR),
+                              kmajor(self.Gm, HW, NR)),
+                             (kmajor(self.pwT[l], 2 * C, 2 * C),
+                              mnmajor(dcur, HW, 2 * C, ld=HW, batch_stride=2 * C * HW))],
+                 dnext, OutMap.rowmajor(HW, batch=2 * C * HW), batch=Bp // 2, act=act,
+                 aux=ws["pre"][l - 1] if l > 0 else None, status=st)
             dcur, dnext = dnext, dcur
         # lift (dcur = dX0)
         gemm(C, FEAT, [(kmajor(dcur, C, HW, batch_stride=C * HW),

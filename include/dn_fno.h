@@ -120,7 +120,7 @@ int32_t dn_fno_features_bwd(const float* dfeat, int64_t n_pix, float eps_lo, flo
 /* out[b, w, c] = sum_h r[h, c] * x[b, c, h, w]   (x, out BF16; r FP32 (H, C)) */
 int32_t dn_fno_readout(const void* x, const float* r, int64_t nb, int32_t H, int32_t W,
                        int32_t C, void* out, void* stream);
-/* dx[b, c, h, w] = r[h, c] * dR[b, w, c] (BF16; NULL skips) and
+/* dx[b, c, h, w] = r[h, c] * dR[b, w, c] (BF16; NULL skips; W a multiple of 8) and
  * dr_part[b, h, c] = sum_w dR[b, w, c] * x[b, c, h, w] (FP32; NULL skips) */
 int32_t dn_fno_readout_bwd(const void* x, const float* r, const void* dR, int64_t nb, int32_t H,
                            int32_t W, int32_t C, void* dx, float* dr_part, void* stream);
@@ -167,6 +167,12 @@ int32_t dn_fno_modes_rows(const void* src, void* dst, int32_t n_modes, int64_t n
  * (nb, C, n_pix)), FP32, deterministic; scratch: 256 * C floats. */
 int32_t dn_fno_channel_sums(const void* x, int64_t nb, int32_t C, int64_t n_pix, float* out,
                             float* scratch, void* stream);
+
+/* The 1x1 channel mix of two samples at once: blk = blockdiag(W, W), blkT =
+ * blockdiag(W^T, W^T) ((2C, 2C) BF16) and bias2 = [bias, bias] (FP32), from
+ * W (C, C) and bias (C) FP32. */
+int32_t dn_fno_pack_pointwise(const float* W, const float* bias, int32_t C, void* blk, void* blkT,
+                              float* bias2, void* stream);
 
 /* out[i] = bf16(in[i]) */
 int32_t dn_f32_to_bf16(const float* in, int64_t n, void* out, void* stream);

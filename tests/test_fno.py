@@ -109,3 +109,19 @@ def test_fno_adam_step_decreases_loss(cuda):
     torch.cuda.synchronize()
     net.check_status()
     assert losses[-1] < 0.5 * losses[0], losses
+
+
+@pytest.mark.gpu
+def test_fno_odd_batch_matches_even(cuda):
+    """Samples are processed in pairs; an odd batch pads with a zero sample
+    that must not leak into the real ones."""
+    from diffnano_b200.surrogate.fno import FNO2d
+    net = FNO2d(FNOConfig(), cuda, seed=7)
+    eps = _design_batch(4, 31).to(cuda)
+    full = net.forward(eps).clone()
+    odd = net.forward(eps[:3]).clone()
+    one = net.forward(eps[2:3]).clone()
+    torch.cuda.synchronize()
+    net.check_status()
+    assert torch.equal(odd, full[:3])
+    assert torch.equal(one[0], full[2])
