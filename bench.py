@@ -396,7 +396,7 @@ def run_ours(args):
 BATCH_SIDES = (128, 192, 256, 384, 512, 768, 1024)
 
 
-def batch2d_workload(n_inst=64, seed=7):
+def batch2d_workload(n_inst=64, seed=7, tscale=1.0):
     from diffnano_b200.solvers.batch2d import BatchInstance
     from diffnano_b200.workloads import blob_eps_2d, gaussian_pulse_for_band
 
@@ -405,7 +405,7 @@ def batch2d_workload(n_inst=64, seed=7):
     wls = torch.linspace(1450.0, 1650.0, 8).tolist()
     specs, eps = [], []
     for b, side in enumerate(sides):
-        T = int(round(1500 + (side - 128) * 4500 / 896))
+        T = max(16, int(round(tscale * (1500 + (side - 128) * 4500 / 896))))
         wl = wls[b % 8]
         src = gaussian_pulse_for_band(wl, 200.0)
         src.update(row=30)
@@ -420,7 +420,7 @@ def run_batch2d(args):
     from diffnano_b200.solvers.batch2d import FDTDBatch2D
 
     dev = torch.device("cuda", 0)
-    specs, eps = batch2d_workload()
+    specs, eps = batch2d_workload(args.batch2d_n, tscale=args.batch2d_tscale)
     cells_steps = sum(s.grid_shape[0] * s.grid_shape[1] * s.n_steps for s in specs)
     batch = FDTDBatch2D(specs, "TM", torch.float32, dev)
     e_dev = [e.to(dev).requires_grad_(True) for e in eps]
@@ -439,7 +439,10 @@ def run_batch2d(args):
     line = {"metric": METRIC, "value": cells_steps / f_s / 1e9, "unit": UNIT, "n_gpus": 1,
             "steps": 1, "warmup": 1, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "batched_2d_tm_64_instances", "instances": len(specs),
+            "config": {"workload": f"batched_2d_tm_{len(specs)}_instances"
+                                   + ("" if args.batch2d_tscale == 1.0
+                                      else f"_steps_x{args.batch2d_tscale:g}"),
+                       "instances": len(specs),
                        "sides": sorted({s.grid_shape[0] for s in specs}),
                        "cell_steps": cells_steps, "tile_rows": batch.tile_rows,
                        "checkpoint_interval": batch.K},
@@ -578,6 +581,90 @@ def run_design(args):
     return 0
 
 
+def run_gemm(args):
+    """tcgen05 BF16 GEMM alone: a square GEMM and the operator's transform shape."""
+    from diffnano_b200.surrogate.gemm import OutMap, gemm, kmajor
+
+    dev = torch.device("cuda", 0)
+    n = args.gemm_n
+    a = torch.randn(n, n, device=dev).to(torch.bfloat16)
+    b = torch.randn(n, n, device=dev).to(torch.bfloat16)
+    o = torch.empty(n, n, device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn, reps):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize(dev)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / reps
+
+    ms = timed(lambda: gemm(n, n, [(kmajor(a, n, n), kmajor(b, n, n))], o, OutMap.rowmajor(n)),
+               args.steps)
+    ref = a[:128].float() @ b.float().T
+    err = float((o[:128] - ref).norm() / ref.norm())
+    mt = torch.matmul(a, b.T)
+    ms_ref = timed(lambda: torch.matmul(a, b.T, out=mt), args.steps)
+    peak, peak_sus, kind = measured_peak_bf16()
+    tf = 2 * n ** 3 / ms / 1e9
+    line = {"metric": "BF16 GEMM TFLOP/s (tcgen05, FP32 accumulate)", "value": tf,
+            "unit": "TFLOP/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16",
+            "data": "synthetic", "config": {"workload": f"gemm_{n}x{n}x{n}_bf16"},
+            "rel_err_vs_fp32": err, "torch_matmul_tflops": 2 * n ** 3 / ms_ref / 1e9,
+            "roofline": {"bound": "tensor", "achieved": tf, "peak": peak, "unit": "TFLOP/s",
+                         "frac": tf / peak, "peak_kind": f"{kind} burst bf16"}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_fno_step(args):
+    """Operator training steps (forward, MSE, backward, Adam) on synthetic inputs."""
+    from diffnano_b200.surrogate.fno import FNO2d, FNOConfig
+
+    dev = torch.device("cuda", 0)
+    B = args.fno_batch
+    net = FNO2d(FNOConfig(), dev, seed=0)
+    g = torch.Generator(device=dev).manual_seed(0)
+    eps = 2.085 + 10.0 * torch.rand(B, 128, 128, device=dev, generator=g)
+    tgt = 0.1 * torch.randn(B, 128, 6, device=dev, generator=g)
+
+    def step():
+        net.forward(eps)
+        net.loss(tgt)
+        net.ps.g.zero_()
+        net.backward(B=B)
+        net.adam_step()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    net.check_status()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / args.steps
+    peak, peak_sus, kind = measured_peak_bf16()
+    tf = net.gemm_flops(B) / ms / 1e9
+    line = {"metric": "FNO training step throughput", "value": B / ms * 1e3,
+            "unit": "samples/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16", "data": "synthetic",
+            "config": {"workload": f"fno_4layer_w64_m16_128x128_b{B}"},
+            "roofline": {"bound": "tensor", "achieved": tf, "peak": peak_sus, "unit": "TFLOP/s",
+                         "frac": tf / peak_sus, "peak_kind": f"{kind} sustained bf16",
+                         "flops": "useful GEMM FLOPs of forward + backward"}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -590,11 +677,18 @@ def main():
     ap.add_argument("--adjoint-steps", type=int, default=256)
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-grad-e2e", action="store_true")
-    ap.add_argument("--workload", choices=["fdtd3d", "batch2d", "fno", "design"],
+    ap.add_argument("--workload", choices=["fdtd3d", "batch2d", "fno", "design", "gemm",
+                                           "fno-step"],
                     default="fdtd3d",
                     help="fdtd3d: the benchmark (3-D 256^3); batch2d: 64 ragged 2-D instances; "
                          "fno: surrogate data generation + training; design: 3-D inverse "
                          "design, plain vs surrogate-assisted")
+    ap.add_argument("--gemm-n", type=int, default=8192)
+    ap.add_argument("--batch2d-n", type=int, default=64,
+                    help="instances of the batched 2-D workload (64 is the workload)")
+    ap.add_argument("--batch2d-tscale", type=float, default=1.0,
+                    help="scale the step counts (1 is the workload; smaller for profiling)")
+    ap.add_argument("--fno-batch", type=int, default=256)
     ap.add_argument("--design-iters", type=int, default=100)
     ap.add_argument("--design-max-verify", type=int, default=40)
     ap.add_argument("--design-scale", type=int, default=1,
@@ -617,6 +711,10 @@ def main():
         return run_fno(args)
     if args.workload == "design":
         return run_design(args)
+    if args.workload == "gemm":
+        return run_gemm(args)
+    if args.workload == "fno-step":
+        return run_fno_step(args)
     return run_ours(args)
 
 
