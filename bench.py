@@ -417,10 +417,16 @@ def batch2d_workload(n_inst=64, seed=7, tscale=1.0):
 
 
 def run_batch2d(args):
+    from diffnano_b200.shard import rank_share, sum_over_ranks
     from diffnano_b200.solvers.batch2d import FDTDBatch2D
 
-    dev = torch.device("cuda", 0)
+    ws, rank, local = dist_setup()
+    dev = torch.device("cuda", local)
     specs, eps = batch2d_workload(args.batch2d_n, tscale=args.batch2d_tscale)
+    if ws > 1:  # independent instances: each rank takes a cost-balanced share
+        mine = rank_share([s.grid_shape[0] * s.grid_shape[1] * s.n_steps for s in specs], ws,
+                          rank)
+        specs, eps = [specs[i] for i in mine], [eps[i] for i in mine]
     cells_steps = sum(s.grid_shape[0] * s.grid_shape[1] * s.n_steps for s in specs)
     batch = FDTDBatch2D(specs, "TM", torch.float32, dev)
     e_dev = [e.to(dev).requires_grad_(True) for e in eps]
@@ -429,6 +435,8 @@ def run_batch2d(args):
     torch.cuda.synchronize(dev)
     e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
     e_dev = [e.to(dev).requires_grad_(True) for e in eps]
+    barrier(ws)
+    torch.cuda.synchronize(dev)
     e0.record()
     fields, dfts = batch.forward(e_dev)
     e1.record()
@@ -436,13 +444,22 @@ def run_batch2d(args):
     e2.record()
     torch.cuda.synchronize(dev)
     f_s, b_s = e0.elapsed_time(e1) / 1e3, e1.elapsed_time(e2) / 1e3
-    line = {"metric": METRIC, "value": cells_steps / f_s / 1e9, "unit": UNIT, "n_gpus": 1,
+    f_s, b_s = max_over_ranks(f_s, ws, dev), max_over_ranks(b_s, ws, dev)
+    cells_steps = int(sum_over_ranks(float(cells_steps), ws, dev))
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+        if rank != 0:
+            return 0
+    line = {"metric": METRIC, "value": cells_steps / f_s / 1e9, "unit": UNIT, "n_gpus": ws,
             "steps": 1, "warmup": 1, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"batched_2d_tm_{len(specs)}_instances"
                                    + ("" if args.batch2d_tscale == 1.0
                                       else f"_steps_x{args.batch2d_tscale:g}"),
-                       "instances": len(specs),
+                       "instances": args.batch2d_n,
+                       "parallelism": f"instances split over {ws} GPU(s) by cost",
                        "sides": sorted({s.grid_shape[0] for s in specs}),
                        "cell_steps": cells_steps, "tile_rows": batch.tile_rows,
                        "checkpoint_interval": batch.K},
