@@ -598,6 +598,94 @@ def run_design(args):
     return 0
 
 
+def run_fdtd2d(args):
+    """Config 0: the 256^2 TMz solve (2000 steps) through FDTDSolver2D, and 1024^2."""
+    from diffnano_b200.solvers import FDTDSolver2D
+    from diffnano_b200.surrogate.data import TMzSetup, blob_designs, design_eps
+
+    dev = torch.device("cuda", 0)
+    st = TMzSetup()
+    mask, _ = blob_designs(1, 0, (3.0, 3.0))
+    eps = torch.full((st.side, st.side), 2.085, dtype=torch.float64)
+    o = st.offset
+    eps[o:o + st.design, o:o + st.design] = design_eps(mask[0]).to(torch.float64)
+    src = st.instance().source
+    mon = [{"component": "Ez", "row": st.mon_row, "wavelengths_nm": list(st.wavelengths_nm)}]
+    out = {}
+    for side, T, key in ((st.side, st.n_steps, "cfg0"), (1024, 1000, "1024")):
+        e = eps if side == st.side else torch.nn.functional.pad(eps, ((1024 - 256) // 2,) * 4,
+                                                                value=2.085)
+        solver = FDTDSolver2D(grid_shape=(side, side), dl=st.dl, wavelength_nm=st.center_nm,
+                              pml_layers=st.pml, n_steps=T, courant=st.courant, device=dev,
+                              dtype=torch.float32, monitors=mon)
+        ed = e.to(dev)
+        for _ in range(args.warmup):
+            solver.forward(ed, source=dict(src))
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 5
+        e0.record()
+        for _ in range(reps):
+            r = solver.forward(ed, source=dict(src))
+        e1.record()
+        torch.cuda.synchronize(dev)
+        s_solve = e0.elapsed_time(e1) / 1e3 / reps
+        out[key] = {"grid": side, "steps": T, "s_per_solve": s_solve,
+                    "gcells": side * side * T / s_solve / 1e9,
+                    "gbs": 28 * side * side * T / s_solve / 1e9}
+        if key == "cfg0":
+            host = FDTDSolver2D(grid_shape=(side, side), dl=st.dl, wavelength_nm=st.center_nm,
+                                pml_layers=st.pml, n_steps=T, courant=st.courant, device="cpu",
+                                dtype=torch.float32, monitors=mon)
+            ep = e.to(torch.float32).pin_memory()
+            host.forward(ep, source=dict(src))
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                rh = host.forward(ep, source=dict(src))
+            e2e_s = (time.perf_counter() - t0) / reps
+            out["e2e"] = {"value": side * side * T / e2e_s / 1e9, "unit": UNIT,
+                          "h2d_bytes_per_step": 4 * side * side,
+                          "d2h_bytes_per_step": 4 * side * side + 16 * 3 * side,
+                          "step": "FDTDSolver2D(device='cpu').forward of the 2000-step solve"}
+            del rh
+    cpu = None
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, ROOT)
+        from oracle import fdtd_ref
+
+        torch.set_num_threads(os.cpu_count() or 1)
+        dt = st.courant * st.dl / math.sqrt(2.0)
+        t0 = time.perf_counter()
+        fdtd_ref.run_2d(eps, dl=st.dl, dt=dt, omega=2 * math.pi / st.center_nm,
+                        pml_layers=st.pml, n_steps=st.n_steps, source=dict(src),
+                        monitors=[{"component": "Ez", "box": ((st.mon_row, st.mon_row + 1),
+                                                                (0, st.side)),
+                                   "wavelengths_nm": list(st.wavelengths_nm)}])
+        cpu_s = time.perf_counter() - t0
+        cpu = {"value": st.side * st.side * st.n_steps / cpu_s / 1e9, "unit": UNIT,
+               "cores": torch.get_num_threads(), "kind": "port",
+               "sample": "the full 256^2 x 2000-step solve, FP64 torch-CPU restatement of "
+                         "fdtd2d.py:_time_step_tm (oracle/fdtd_ref.py)"}
+    peak, _ = measured_peak_hbm()
+    c0 = out["cfg0"]
+    line = {"metric": METRIC, "value": c0["gcells"], "unit": UNIT, "n_gpus": 1,
+            "steps": c0["steps"], "warmup": args.warmup,
+            "ms_per_step": c0["s_per_solve"] / c0["steps"] * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "2d_tmz_256x256_cpml20_2000steps (state L2-resident)",
+                       "source": "Gaussian line source row 30, 1550 nm, 200 nm band",
+                       "monitor": "Ez row 226 at 1500/1550/1600 nm"},
+            "grid_1024": out["1024"],
+            "roofline": {"bound": "hbm", "achieved": out["1024"]["gbs"], "peak": peak,
+                         "unit": "GB/s", "frac": out["1024"]["gbs"] / peak,
+                         "note": "1024^2 grid (28 B/cell-step); 256^2 is L2-resident"},
+            "e2e": out["e2e"], "cpu_baseline": cpu,
+            "gpu_launches": c0["steps"], "kernels": "k_fdtd2d_step (one launch per step)"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_gemm(args):
     """tcgen05 BF16 GEMM alone: a square GEMM and the operator's transform shape."""
     from diffnano_b200.surrogate.gemm import OutMap, gemm, kmajor
@@ -694,8 +782,8 @@ def main():
     ap.add_argument("--adjoint-steps", type=int, default=256)
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-grad-e2e", action="store_true")
-    ap.add_argument("--workload", choices=["fdtd3d", "batch2d", "fno", "design", "gemm",
-                                           "fno-step"],
+    ap.add_argument("--workload", choices=["fdtd3d", "fdtd2d", "batch2d", "fno", "design",
+                                           "gemm", "fno-step"],
                     default="fdtd3d",
                     help="fdtd3d: the benchmark (3-D 256^3); batch2d: 64 ragged 2-D instances; "
                          "fno: surrogate data generation + training; design: 3-D inverse "
@@ -730,6 +818,8 @@ def main():
         return run_design(args)
     if args.workload == "gemm":
         return run_gemm(args)
+    if args.workload == "fdtd2d":
+        return run_fdtd2d(args)
     if args.workload == "fno-step":
         return run_fno_step(args)
     return run_ours(args)

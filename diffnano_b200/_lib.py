@@ -139,6 +139,10 @@ SIGNATURES = {
                                   c_void_p, c_int64]),
     "dn_batch2d_forward": (c_int32, [ctypes.POINTER(DnBatch2d), c_void_p, c_void_p, c_void_p]),
     "dn_batch2d_backward": (c_int32, [ctypes.POINTER(DnBatch2d), c_void_p, c_void_p, c_void_p]),
+    "dn_batch2d_cluster_size": (c_int32, [ctypes.POINTER(DnBatch2d), ctypes.POINTER(DnBatch2dInst),
+                                          ctypes.POINTER(c_int64)]),
+    "dn_batch2d_forward_cluster": (c_int32, [ctypes.POINTER(DnBatch2d), c_void_p, c_int32,
+                                             c_int64, c_void_p]),
     "dn_fom_abs2_scratch_bytes": (c_int64, [c_int64]),
     "dn_fom_abs2": (c_int32, [c_void_p, c_int64, c_void_p, c_void_p, c_int64, c_void_p]),
     "dn_gemm_run": (c_int32, [ctypes.POINTER(DnGemm), c_void_p, c_void_p]),

@@ -27,6 +27,8 @@
 #include <numeric>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "dn_host.cuh"
 
 namespace dn {
@@ -503,7 +505,7 @@ __device__ __forceinline__ Sets<T> slot_set(void* base, long long slot, long lon
 }
 
 template <typename T, int POL, int TI>
-__global__ void __launch_bounds__(NTB) k_batch2d_fwd(unsigned char* table, int* status) {
+__global__ void __launch_bounds__(NTB, 8) k_batch2d_fwd(unsigned char* table, int* status) {
   __shared__ TileSmem<T, TI> s;
   const TableView v = view(table);
   __shared__ unsigned int s_gen;
@@ -530,7 +532,7 @@ __global__ void __launch_bounds__(NTB) k_batch2d_fwd(unsigned char* table, int* 
 }
 
 template <typename T, int POL, int TI>
-__global__ void __launch_bounds__(NTB) k_batch2d_bwd(unsigned char* table, int* status) {
+__global__ void __launch_bounds__(NTB, 8) k_batch2d_bwd(unsigned char* table, int* status) {
   __shared__ TileSmem<T, TI> s;
   const TableView v = view(table);
   __shared__ unsigned int s_gen;
@@ -575,6 +577,208 @@ __global__ void __launch_bounds__(NTB) k_batch2d_bwd(unsigned char* table, int* 
       }
       if (!grid_sync(v.h->bar, gen, status)) return;
     }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// forward-only solve with every grid held in one thread-block cluster
+// ---------------------------------------------------------------------------
+// Cluster c (CL CTAs) solves instance c of the table.  CTA r of the cluster
+// owns rows [r*rows, r*rows + rows) of the grid (rows = ceil(H/CL)) and keeps
+// the three fields and dt/eps of its band in shared memory for the whole run;
+// the one neighbouring row each half-step needs is read from the next or
+// previous CTA's shared memory (distributed shared memory), and two cluster
+// barriers per step order the half-steps.  Every CTA of a cluster runs the same
+// instance's step count, so the barrier sequence is identical on all of them.
+// The arithmetic is fwd_tile's, expression for expression.
+namespace cg = cooperative_groups;
+
+template <typename T>
+struct Band {
+  T* f;   // injected field (Ez / Hz)   rows x W
+  T* a;   // Hx / Ex
+  T* b;   // Hy / Ey
+  T* ce;  // dt / eps
+  T* bx;  // W
+  T* gx;  // W
+  T* by;  // rows
+  T* gy;  // rows
+};
+
+__host__ __device__ inline long long band_elems(long long rows, long long W) {
+  return 4 * rows * W + 2 * W + 2 * rows;
+}
+
+template <typename T>
+__device__ __forceinline__ Band<T> band_layout(unsigned char* smem, int rows, int W) {
+  Band<T> s;
+  T* p = reinterpret_cast<T*>(smem);
+  const long long n = (long long)rows * W;
+  s.f = p;
+  s.a = p + n;
+  s.b = p + 2 * n;
+  s.ce = p + 3 * n;
+  s.bx = p + 4 * n;
+  s.gx = s.bx + W;
+  s.by = s.gx + W;
+  s.gy = s.by + rows;
+  return s;
+}
+
+template <typename T, int POL, int CL>
+__global__ void __launch_bounds__(512, 1) k_batch2d_cluster(unsigned char* table) {
+  extern __shared__ __align__(16) unsigned char c_smem[];
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank();
+  const TableView v = view(table);
+  // the instance's fields in registers: the monitor stores below go to global
+  // memory and would otherwise force re-reads of the descriptor
+  const dn_batch2d_inst* Ip = v.inst + blockIdx.x / CL;
+  const int H = Ip->H, W = Ip->W, T_steps = Ip->n_steps;
+  const long long py = Ip->pitch;
+  const T dt = static_cast<T>(Ip->dt), idl = static_cast<T>(1.0 / Ip->dl);
+  const bool src = Ip->src_comp >= 0, mon = Ip->mon_comp >= 0;
+  const dn_box sb = Ip->src_box, mb = Ip->mon_box;
+  const int nfq = Ip->n_freq;
+  const double* __restrict__ phase = Ip->phase;
+  double* __restrict__ accb = Ip->acc;
+  const T* __restrict__ wave = static_cast<const T*>(Ip->wave);
+  const double* pb0 = Ip->b[0];
+  const double* pb1 = Ip->b[1];
+  const double* pc0 = Ip->c[0];
+  const double* pc1 = Ip->c[1];
+  const T* __restrict__ ceg = static_cast<const T*>(Ip->ce);
+  T* const* outp = reinterpret_cast<T* const*>(Ip->f[T_steps & 1]);
+  T* const o0 = outp[0];
+  T* const o1 = outp[1];
+  T* const o2 = outp[2];
+  const int rows = (H + CL - 1) / CL;
+  const int r0 = rank * rows;
+  const int nr = max(0, min(rows, H - r0));
+  Band<T> s = band_layout<T>(c_smem, rows, W);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  // this band's monitor accumulators (FP64, in shared memory for the whole run)
+  const int mw = mb.hi[2] - mb.lo[2];
+  const int mr0 = mon ? max(mb.lo[1], r0) : 0;
+  const int mr1 = mon ? min(mb.hi[1], r0 + nr) : 0;
+  const int mrows = max(0, mr1 - mr0);
+  const long long ncell = mon ? (long long)(mb.hi[1] - mb.lo[1]) * mw : 0;
+  double* macc = reinterpret_cast<double*>(
+      c_smem + ((band_elems(rows, W) * sizeof(T) + 15) / 16) * 16);
+  const long long mcells = (long long)mrows * mw;
+  for (long long q = threadIdx.x; q < mcells * nfq; q += blockDim.x) {
+    const long long fq = q / mcells, c = q % mcells;
+    const long long cell = (long long)(mr0 - mb.lo[1]) * mw + c;
+    macc[2 * q] = accb[(fq * ncell + cell) * 2];
+    macc[2 * q + 1] = accb[(fq * ncell + cell) * 2 + 1];
+  }
+
+  for (int j = threadIdx.x; j < W; j += blockDim.x) {
+    s.bx[j] = static_cast<T>(pb1[j]);
+    s.gx[j] = static_cast<T>(1.0 + pc1[j]);
+  }
+  for (int r = threadIdx.x; r < nr; r += blockDim.x) {
+    s.by[r] = static_cast<T>(pb0[r0 + r]);
+    s.gy[r] = static_cast<T>(1.0 + pc0[r0 + r]);
+  }
+  for (int r = warp; r < nr; r += nw)
+    for (int j = lane; j < W; j += 32) {
+      const long long o = (long long)r * W + j;
+      s.f[o] = T(0);
+      s.a[o] = T(0);
+      s.b[o] = T(0);
+      s.ce[o] = ceg[(long long)(r0 + r) * py + j];
+    }
+  cl.sync();  // every band initialised before any neighbour reads it
+
+  // neighbour bands (distributed shared memory); unused when out of range
+  const int up = rank + 1 < CL ? rank + 1 : rank, dn_ = rank > 0 ? rank - 1 : rank;
+  const Band<T> nxt = band_layout<T>(cl.map_shared_rank(c_smem, up), rows, W);
+  const Band<T> prv = band_layout<T>(cl.map_shared_rank(c_smem, dn_), rows, W);
+
+  for (int n = 0; n < T_steps; ++n) {
+    // half-step 1: H (TM) / E (TE) from the injected field
+    for (int r = warp; r < nr; r += nw) {
+      const int i = r0 + r;
+      const T byr = s.by[r], gyr = s.gy[r];
+      const bool last = i == H - 1, first = i == 0;
+      const T* below = (r + 1 < nr) ? s.f + (long long)(r + 1) * W : nxt.f;
+      const T* above = (r > 0) ? s.f + (long long)(r - 1) * W : prv.f + (long long)(rows - 1) * W;
+      for (int j = lane; j < W; j += 32) {
+        const long long o = (long long)r * W + j;
+        if (POL == DN_TM) {
+          const T ez = s.f[o];
+          const T dj = (j < W - 1) ? s.f[o + 1] - ez : T(0);
+          const T di = !last ? below[j] - ez : T(0);
+          s.a[o] = byr * s.a[o] - dt * gyr * (dj * idl);
+          s.b[o] = s.bx[j] * s.b[o] + dt * s.gx[j] * (di * idl);
+        } else {
+          const T hz = s.f[o];
+          const T dj = (j > 0) ? hz - s.f[o - 1] : T(0);
+          const T di = !first ? hz - above[j] : T(0);
+          const T cx = s.gx[j] * (dj * idl);
+          const T cy = -(gyr * (di * idl));
+          const T c = s.ce[o];
+          s.a[o] = s.bx[j] * s.a[o] + c * cx;
+          s.b[o] = byr * s.b[o] + c * cy;
+        }
+      }
+    }
+    cl.sync();
+    // half-step 2: the injected field from the new pair, source, monitors
+    const T wv = src ? wave[n] : T(0);
+    const double* ph = mon ? phase + (long long)n * nfq * 2 : nullptr;
+    for (int r = warp; r < nr; r += nw) {
+      const int i = r0 + r;
+      const T byr = s.by[r], gyr = s.gy[r];
+      const bool last = i == H - 1, first = i == 0;
+      const T* bup = (r > 0) ? s.b + (long long)(r - 1) * W : prv.b + (long long)(rows - 1) * W;
+      const T* bdn = (r + 1 < nr) ? s.b + (long long)(r + 1) * W : nxt.b;
+      const bool src_row = src && i >= sb.lo[1] && i < sb.hi[1];
+      const bool mon_row = mon && i >= mb.lo[1] && i < mb.hi[1];
+      for (int j = lane; j < W; j += 32) {
+        const long long o = (long long)r * W + j;
+        const T fo = s.f[o];
+        const T bb = s.bx[j] * byr;
+        T v0;
+        if (POL == DN_TM) {
+          const T dHy = !first ? s.b[o] - bup[j] : T(0);
+          const T dHx = (j > 0) ? s.a[o] - s.a[o - 1] : T(0);
+          const T cz = s.gx[j] * (dHy * idl) - gyr * (dHx * idl);
+          v0 = bb * fo + s.ce[o] * cz;
+        } else {
+          const T dEy = !last ? bdn[j] - s.b[o] : T(0);
+          const T dEx = (j < W - 1) ? s.a[o + 1] - s.a[o] : T(0);
+          v0 = bb * fo + dt * (s.gx[j] * (dEy * idl) - gyr * (dEx * idl));
+        }
+        if (src_row && j >= sb.lo[2] && j < sb.hi[2]) v0 += wv;
+        if (mon_row && j >= mb.lo[2] && j < mb.hi[2]) {
+          const long long c = (long long)(i - mr0) * mw + (j - mb.lo[2]);
+          const double x = static_cast<double>(v0);
+          for (int fq = 0; fq < nfq; ++fq) {
+            double* acc = macc + (fq * mcells + c) * 2;
+            acc[0] = fma(x, ph[2 * fq], acc[0]);
+            acc[1] = fma(x, ph[2 * fq + 1], acc[1]);
+          }
+        }
+        s.f[o] = v0;
+      }
+    }
+    cl.sync();
+  }
+  // final state into the set a step-by-step run would end in; monitor sums out
+  for (int r = warp; r < nr; r += nw)
+    for (int j = lane; j < W; j += 32) {
+      const long long o = (long long)r * W + j, g = (long long)(r0 + r) * py + j;
+      o0[g] = s.f[o];
+      o1[g] = s.a[o];
+      o2[g] = s.b[o];
+    }
+  for (long long q = threadIdx.x; q < mcells * nfq; q += blockDim.x) {
+    const long long fq = q / mcells, c = q % mcells;
+    const long long cell = (long long)(mr0 - mb.lo[1]) * mw + c;
+    accb[(fq * ncell + cell) * 2] = macc[2 * q];
+    accb[(fq * ncell + cell) * 2 + 1] = macc[2 * q + 1];
   }
 }
 
@@ -652,8 +856,93 @@ int run(bool fwd, const dn_batch2d* cfg, void* dev_table, int32_t* status, void*
             : dispatch_rows<double, DN_TE>(fwd, cfg->tile_rows, dev_table, status, s, max_tiles);
 }
 
+constexpr long long CLUSTER_SMEM_MAX = 227 * 1024;
+
+// bytes of shared memory per CTA for a cluster of cl CTAs, -1 if too large
+long long cluster_bytes(const dn_batch2d* cfg, const dn_batch2d_inst* insts, int cl) {
+  const long long es = cfg->dtype == DN_F32 ? 4 : 8;
+  long long need = 0;
+  for (int b = 0; b < cfg->n_inst; ++b) {
+    const dn_batch2d_inst& I = insts[b];
+    const long long rows = (I.H + cl - 1) / cl;
+    long long bytes = (band_elems(rows, I.W) * es + 15) / 16 * 16;
+    if (I.mon_comp != DN_NONE) {  // the band's share of the monitor box, FP64 complex
+      const long long bh = I.mon_box.hi[1] - I.mon_box.lo[1];
+      const long long bw = I.mon_box.hi[2] - I.mon_box.lo[2];
+      bytes += std::min(rows, bh) * bw * I.n_freq * 16;
+    }
+    need = std::max(need, bytes);
+  }
+  return need <= CLUSTER_SMEM_MAX ? need : -1;
+}
+
+template <typename T, int POL, int CL>
+int launch_cluster(void* table, int n_inst, long long smem, cudaStream_t s) {
+  auto kern = k_batch2d_cluster<T, POL, CL>;
+  DN_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  if (CL > 8)
+    DN_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  cudaLaunchConfig_t lc = {};
+  lc.gridDim = dim3((unsigned)(n_inst * CL));
+  lc.blockDim = dim3(512);
+  lc.dynamicSmemBytes = (size_t)smem;
+  lc.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = CL;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  lc.attrs = attr;
+  lc.numAttrs = 1;
+  int clusters = 0;
+  DN_CUDA_CHECK(cudaOccupancyMaxActiveClusters(&clusters, kern, &lc));
+  if (clusters < 1) return DN_EUNSUPPORTED;
+  DN_CUDA_CHECK(cudaLaunchKernelEx(&lc, kern, static_cast<unsigned char*>(table)));
+  DN_CUDA_CHECK(cudaGetLastError());
+  return DN_OK;
+}
+
+template <typename T, int POL>
+int dispatch_cluster(int cl, void* table, int n_inst, long long smem, cudaStream_t s) {
+  return cl == 8 ? launch_cluster<T, POL, 8>(table, n_inst, smem, s)
+                 : launch_cluster<T, POL, 16>(table, n_inst, smem, s);
+}
+
 }  // namespace
 }  // namespace dn
+
+extern "C" int32_t dn_batch2d_cluster_size(const dn_batch2d* cfg, const dn_batch2d_inst* insts,
+                                           int64_t* smem_bytes) {
+  if (dn::validate(cfg, insts) != DN_OK || !smem_bytes) return -1;
+  // 16 CTAs per grid (half the band of 8 each, twice the SMs per grid) is the
+  // faster of the two on B200; any grid that fits 8 CTAs also fits 16
+  for (int cl : {16, 8}) {
+    const long long b = dn::cluster_bytes(cfg, insts, cl);
+    if (b > 0) {
+      *smem_bytes = b;
+      return cl;
+    }
+  }
+  return 0;
+}
+
+extern "C" int32_t dn_batch2d_forward_cluster(const dn_batch2d* cfg, void* dev_table,
+                                              int32_t cluster, int64_t smem_bytes,
+                                              void* stream) {
+  if (!cfg || !dev_table || (reinterpret_cast<uintptr_t>(dev_table) & 15)) return DN_EINVAL;
+  if (cfg->pol != DN_TM && cfg->pol != DN_TE) return DN_EINVAL;
+  if (cfg->dtype != DN_F32 && cfg->dtype != DN_F64) return DN_EINVAL;
+  if ((cluster != 8 && cluster != 16) || smem_bytes < 1 || smem_bytes > dn::CLUSTER_SMEM_MAX ||
+      cfg->n_inst < 1 || (long long)cfg->n_inst * cluster > 0x7fffffffLL)
+    return DN_EINVAL;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const bool tm = cfg->pol == DN_TM;
+  if (cfg->dtype == DN_F32)
+    return tm ? dn::dispatch_cluster<float, DN_TM>(cluster, dev_table, cfg->n_inst, smem_bytes, s)
+              : dn::dispatch_cluster<float, DN_TE>(cluster, dev_table, cfg->n_inst, smem_bytes, s);
+  return tm ? dn::dispatch_cluster<double, DN_TM>(cluster, dev_table, cfg->n_inst, smem_bytes, s)
+            : dn::dispatch_cluster<double, DN_TE>(cluster, dev_table, cfg->n_inst, smem_bytes, s);
+}
 
 extern "C" int64_t dn_batch2d_table_bytes(const dn_batch2d* cfg, const dn_batch2d_inst* insts) {
   if (dn::validate(cfg, insts) != DN_OK) return -1;

@@ -39,7 +39,7 @@ struct CurlRec2 {
 };
 
 template <typename T, int POL, bool REC>
-__global__ void __launch_bounds__(NT2) k_fdtd2d_step(const StepParams<T> p, const CurlRec2<T> rec) {
+__global__ void __launch_bounds__(NT2, 8) k_fdtd2d_step(const StepParams<T> p, const CurlRec2<T> rec) {
   __shared__ T s_f[TI2 + 2][TJ2 + 2];
   __shared__ T s_a[TI2 + 1][TJ2 + 1];
   __shared__ T s_b[TI2 + 1][TJ2 + 1];

@@ -155,10 +155,14 @@ class FDTDBatch2D:
     checkpoint_interval : steps between stored states for the adjoint
         (default sqrt of the longest step count)
     tile_rows : 8, 16 or 32; None lets ``autotune_tile_rows`` choose
+    cluster : gradient-free solves with each grid in one 16-CTA thread-block
+        cluster: None = when every grid fits, False = never, True = always
+        (error if a grid does not fit)
     """
 
     def __init__(self, instances, polarization: str = "TM", dtype=torch.float32,
-                 device="cuda", checkpoint_interval: int | None = None, tile_rows: int | None = None):
+                 device="cuda", checkpoint_interval: int | None = None, tile_rows: int | None = None,
+                 cluster: bool | None = None):
         if not instances:
             raise ValueError("empty batch")
         self.specs = list(instances)
@@ -176,6 +180,10 @@ class FDTDBatch2D:
         self._grad_alloc = None
         self._graph = None
         self.status = torch.zeros(1, dtype=torch.int32, device=self.device)
+        # gradient-free solves: whole grids in thread-block clusters when they fit
+        # (None = when possible, False = never)
+        self.cluster = cluster
+        self._cluster = (0, 0)
 
     # ------------------------------------------------------------------
     def _cfg(self, rows: int, n_inst: int, max_ctas: int) -> _lib.DnBatch2d:
@@ -201,6 +209,11 @@ class FDTDBatch2D:
         tiles = sum(((i.W + 31) // 32) * ((i.H + self.tile_rows - 1) // self.tile_rows)
                     for i in self._insts)
         self.cfg = self._cfg(self.tile_rows, len(self._insts), tiles)
+        smem = ctypes.c_int64(0)
+        cl = int(L.dn_batch2d_cluster_size(ctypes.byref(self.cfg), arr, ctypes.byref(smem)))
+        self._cluster = (cl, int(smem.value)) if cl > 0 else (0, 0)
+        if self.cluster and not self._cluster[0]:
+            raise ValueError("an instance is too large for a thread-block cluster")
         nbytes = int(L.dn_batch2d_table_bytes(ctypes.byref(self.cfg), arr))
         if nbytes < 0:
             raise ValueError("invalid batch description")
@@ -208,13 +221,23 @@ class FDTDBatch2D:
         _lib.check("dn_batch2d_pack", L.dn_batch2d_pack(ctypes.byref(self.cfg), arr, host, nbytes))
         self.table = torch.frombuffer(bytearray(host), dtype=torch.uint8).to(self.device)
 
-    def _launch(self, fwd: bool):
+    def uses_cluster(self, grad: bool) -> bool:
+        """Whether a forward with / without gradient runs the cluster kernel."""
+        return (not grad) and self.cluster is not False and self._cluster[0] > 0
+
+    def _launch(self, fwd: bool, grad: bool = True):
         L = _lib.lib()
-        fn = "dn_batch2d_forward" if fwd else "dn_batch2d_backward"
         with torch.cuda.device(self.device):
             stream = torch.cuda.current_stream(self.device).cuda_stream
-            rc = getattr(L, fn)(ctypes.byref(self.cfg), self.table.data_ptr(),
-                                self.status.data_ptr(), ctypes.c_void_p(stream))
+            if fwd and self.uses_cluster(grad):
+                fn = "dn_batch2d_forward_cluster"
+                rc = L.dn_batch2d_forward_cluster(ctypes.byref(self.cfg), self.table.data_ptr(),
+                                                  self._cluster[0], self._cluster[1],
+                                                  ctypes.c_void_p(stream))
+            else:
+                fn = "dn_batch2d_forward" if fwd else "dn_batch2d_backward"
+                rc = getattr(L, fn)(ctypes.byref(self.cfg), self.table.data_ptr(),
+                                    self.status.data_ptr(), ctypes.c_void_p(stream))
         _lib.check(fn, rc)
 
     def _reset(self):
@@ -234,7 +257,7 @@ class FDTDBatch2D:
         self._build(grad)
         self._set_eps(eps_list)
         self._reset()
-        self._launch(True)
+        self._launch(True, grad)
         return self._outputs()
 
     def _outputs(self):
@@ -289,7 +312,7 @@ class FDTDBatch2D:
         for i, e in zip(self._insts, self._static_eps):
             i.ce[:, : i.W] = (i.spec.dt / e).to(self.dtype)
         self._reset()
-        self._launch(True)
+        self._launch(True, False)
 
     def check_status(self):
         s = int(self.status.item())

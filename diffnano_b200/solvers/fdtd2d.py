@@ -10,6 +10,8 @@ validation), and DFT ``monitors``.
 
 from __future__ import annotations
 
+import json
+
 import math
 from collections.abc import Sequence
 
@@ -116,9 +118,15 @@ class FDTDSolver2D:
         mons = monitors if monitors is not None else self.monitors
         probe = src.get("probe", None)
         eng = self._make_engine(self.n_steps, src, mons, probe)
-        from diffnano_b200.solvers._adjoint import run_forward
+        fast = None
+        if probe is None and not (torch.is_grad_enabled() and eps.requires_grad):
+            fast = self._cluster_solve(eps, src, eng)
+        if fast is not None:
+            field, dfts = fast
+        else:
+            from diffnano_b200.solvers._adjoint import run_forward
 
-        field, dfts = run_forward(self, eng, eps, self._fields()[0])
+            field, dfts = run_forward(self, eng, eps, self._fields()[0])
         out_dev = self._device
         snapshots = []
         if probe is not None:
@@ -128,6 +136,43 @@ class FDTDSolver2D:
         if eng.monitors:
             meta["monitors"] = monitor_metadata(eng, [d.to(out_dev) for d in dfts])
         return SimResult(field=field.unsqueeze(0).to(out_dev), wavelengths=wl, metadata=meta)
+
+    def _cluster_solve(self, eps, src, eng):
+        """Gradient-free solve with the whole grid in one thread-block cluster
+        (``dn_batch2d_forward_cluster``) when the grid fits and there is at most
+        one monitor, on the injected field; None otherwise."""
+        if len(eng.monitors) > 1:
+            return None
+        comp = _lib.DN_EZ if self.polarization == "TM" else _lib.DN_HZ
+        mon = None
+        if eng.monitors:
+            m = eng.monitors[0]
+            if m.component != comp:
+                return None
+            mon = {"box": [list(m.box[1]), list(m.box[2])], "wavelengths_nm": list(m.wavelengths)}
+        key = json.dumps([src, mon, str(self.dtype), list(self.grid_shape), self.n_steps,
+                          self.dl, self.wavelength_nm, self.pml_layers, self.courant,
+                          self.polarization, str(self._device)], sort_keys=True, default=str)
+        cache = self.__dict__.setdefault("_cluster_cache", {})
+        if key not in cache:
+            from diffnano_b200.solvers.batch2d import BatchInstance, FDTDBatch2D
+
+            spec = BatchInstance(grid_shape=tuple(self.grid_shape), n_steps=self.n_steps,
+                                 dl=self.dl, wavelength_nm=self.wavelength_nm,
+                                 pml_layers=self.pml_layers, courant=self.courant,
+                                 source={k: v for k, v in src.items() if k != "probe"},
+                                 monitor=mon)
+            b = FDTDBatch2D([spec], self.polarization, self.dtype,
+                            compute_device(self._device), tile_rows=16)
+            b._build(False)
+            cache[key] = b if b.uses_cluster(False) else None
+        b = cache[key]
+        if b is None:
+            return None
+        with torch.no_grad():
+            fields, dfts = b.run_forward([eps], grad=False)
+        b.check_status()
+        return fields[0], [d for d in dfts if d is not None]
 
     def time_series(self, eps_r: torch.Tensor, probe: tuple[int, int], source: dict | None = None,
                     n_steps: int | None = None) -> torch.Tensor:

@@ -256,6 +256,20 @@ int32_t dn_batch2d_forward(const dn_batch2d* cfg, void* dev_table, int32_t* stat
 int32_t dn_batch2d_backward(const dn_batch2d* cfg, void* dev_table, int32_t* status,
                             void* stream);
 
+/* Forward-only solve of every instance of a packed table with each grid held
+ * in the shared memory of one thread-block cluster (CTAs own row bands, the
+ * neighbouring rows come from the next / previous CTA's shared memory, two
+ * cluster barriers per step): no global traffic for the fields between the
+ * first and the last step.  Same results as dn_batch2d_forward (final fields in
+ * f[n_steps % 2], monitor DFTs accumulated), no checkpoints.
+ * dn_batch2d_cluster_size returns the cluster size to use (16 CTAs per grid)
+ * and sets *smem_bytes (per CTA); 0 when some instance is too large for a
+ * cluster, -1 on invalid input.  dn_batch2d_forward_cluster also takes 8. */
+int32_t dn_batch2d_cluster_size(const dn_batch2d* cfg, const dn_batch2d_inst* insts,
+                                int64_t* smem_bytes);
+int32_t dn_batch2d_forward_cluster(const dn_batch2d* cfg, void* dev_table, int32_t cluster,
+                                   int64_t smem_bytes, void* stream);
+
 /* ---- figure of merit ----------------------------------------------------
  * *out = sum_i |dft[i]|^2 over n_complex FP64 (re, im) pairs, reduced in FP64
  * (warp-shuffle trees, per-block partials in `scratch`, deterministic final

@@ -92,3 +92,39 @@ def test_autotuner_picks_a_candidate_and_caches(cuda, tmp_path, monkeypatch):
     assert rows in (8, 16, 32)
     assert (tmp_path / "diffnano_b200" / "autotune.json").exists()
     assert autotune_tile_rows(b) == rows
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+@pytest.mark.parametrize("pol", ["TM", "TE"])
+def test_cluster_forward_matches_persistent_kernel(cuda, pol, dtype):
+    """Gradient-free solves keep each grid in one thread-block cluster's shared
+    memory; same fields and DFTs as the tile-by-tile persistent kernel.  The
+    large instances (400 x 320 FP32, 386 x 97 FP64) fill most of a cluster's
+    shared memory and have row bands that do not divide the height."""
+    big = (400, 320) if dtype == torch.float32 else (386, 97)
+    shapes = SHAPES + [big]
+    specs = _specs(pol) + [BatchInstance(grid_shape=big, n_steps=50, dl=20.0,
+                                         pml_layers=6, courant=0.5,
+                                         source={"type": "gaussian_pulse", "row": 9,
+                                                 "spread": 300.0, "t0": 900.0},
+                                         monitor={"col": 40, "wavelengths_nm": [1550.0]})]
+    g = torch.Generator().manual_seed(3)
+    eps = [(1.5 + 2.0 * torch.rand(*s, dtype=torch.float64, generator=g)).to(cuda)
+           for s in shapes]
+    a = FDTDBatch2D(specs, pol, dtype, cuda, tile_rows=16, cluster=True)
+    b = FDTDBatch2D(specs, pol, dtype, cuda, tile_rows=16, cluster=False)
+    fa, da = a.forward(eps)
+    fb, db = b.forward(eps)
+    a.check_status()
+    b.check_status()
+    assert a.uses_cluster(False) and not b.uses_cluster(False) and not a.uses_cluster(True)
+    assert a._cluster[0] == 16
+    tol = 1e-6 if dtype == torch.float32 else 1e-13
+    for x, y in zip(fa, fb):
+        assert rel_l2(x, y) < tol
+    for x, y in zip(da, db):
+        assert rel_l2(torch.view_as_real(x), torch.view_as_real(y)) < tol
+    # graph replay uses the cluster kernel too
+    fg, dg = a.forward_graphed(eps)
+    for x, y in zip(fg, fa):
+        assert torch.equal(x, y)
