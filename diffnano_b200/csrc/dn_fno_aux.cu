@@ -70,49 +70,34 @@ __global__ void k_readout(const unsigned short* __restrict__ x, const float* __r
   }
 }
 
-// dx[b, c, h, w] = r[h, c] * dR[b, w, c]; one thread per 8 consecutive w
-__global__ void k_readout_bwd_x(const float* __restrict__ r, const unsigned short* __restrict__ dR,
-                                long long nb, int H, int W, int C, unsigned short* __restrict__ dx) {
-  const int W8 = W / 8;
-  const long long n = nb * C * H * W8;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    const int w0 = (int)(i % W8) * 8;
-    const long long row = i / W8;  // (b, c, h)
-    const int h = (int)(row % H);
-    const long long bc = row / H;
-    const int c = (int)(bc % C);
-    const long long b = bc / C;
+// readout backward, one block per (b, c): dR[b, :, c] staged in shared memory,
+//   dx[b, c, h, w] = r[h, c] * dR[b, w, c]                       (dx != NULL)
+//   dr_part[b, h, c] = sum_w dR[b, w, c] * x[b, c, h, w]         (dr_part != NULL)
+// warps over rows h, lanes over w (x and dx rows are contiguous)
+__global__ void k_readout_bwd(const unsigned short* __restrict__ x, const float* __restrict__ r,
+                              const unsigned short* __restrict__ dR, int nb, int H, int W, int C,
+                              unsigned short* __restrict__ dx, float* __restrict__ dr_part) {
+  extern __shared__ float s_dr[];  // W
+  const int c = blockIdx.x % C;
+  const long long b = blockIdx.x / C;
+  for (int w = threadIdx.x; w < W; w += blockDim.x) s_dr[w] = bf2f(dR[(b * W + w) * C + c]);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const long long base = (b * C + c) * (long long)H * W;
+  for (int h = warp; h < H; h += nw) {
     const float rv = r[h * C + c];
-    const unsigned short* d = dR + (b * W + w0) * C + c;
-    uint32_t o[4];
+    const unsigned short* xr = x + base + (long long)h * W;
+    float acc = 0.0f;
+    for (int w = lane; w < W; w += 32) {
+      const float d = s_dr[w];
+      if (dr_part) acc = fmaf(d, bf2f(xr[w]), acc);
+      if (dx) dx[base + (long long)h * W + w] = f2bf(rv * d);
+    }
+    if (dr_part) {
 #pragma unroll
-    for (int e = 0; e < 4; ++e)
-      o[e] = (uint32_t)f2bf(rv * bf2f(d[(2 * e) * C])) |
-             ((uint32_t)f2bf(rv * bf2f(d[(2 * e + 1) * C])) << 16);
-    reinterpret_cast<uint4*>(dx + row * W + w0)[0] = make_uint4(o[0], o[1], o[2], o[3]);
-  }
-}
-
-// dr_part[b, h, c] = sum_w dR[b, w, c] * x[b, c, h, w]; one warp per (b, c, h)
-__global__ void k_readout_bwd_r(const unsigned short* __restrict__ x,
-                                const unsigned short* __restrict__ dR, long long nb, int H, int W,
-                                int C, float* __restrict__ dr_part) {
-  const long long n = nb * C * H;
-  const int lane = threadIdx.x & 31;
-  const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
-  for (long long i = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); i < n;
-       i += warps) {
-    const int h = (int)(i % H);
-    const int c = (int)((i / H) % C);
-    const long long b = i / ((long long)H * C);
-    const unsigned short* xr = x + ((b * C + c) * H + h) * (long long)W;
-    const unsigned short* dr = dR + b * W * (long long)C + c;
-    float s = 0.0f;
-    for (int w = lane; w < W; w += 32) s = fmaf(bf2f(dr[(long long)w * C]), bf2f(xr[w]), s);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    if (lane == 0) dr_part[(b * H + h) * C + c] = s;
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+      if (lane == 0) dr_part[(b * H + h) * C + c] = acc;
+    }
   }
 }
 
@@ -361,19 +346,12 @@ extern "C" int32_t dn_fno_readout_bwd(const void* x, const float* r, const void*
                                       void* stream) {
   if (!x || !r || !dR || nb < 1 || H < 1 || W < 1 || C < 1 || (!dx && !dr_part))
     return DN_EINVAL;
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if (dx) {
-    if (W % 8) return DN_EINVAL;
-    k_readout_bwd_x<<<grid_for(nb * C * H * (W / 8)), 256, 0, s>>>(
-        r, static_cast<const unsigned short*>(dR), nb, H, W, C, static_cast<unsigned short*>(dx));
-    DN_CUDA_CHECK(cudaGetLastError());
-  }
-  if (dr_part) {
-    k_readout_bwd_r<<<grid_for(nb * C * H * 32), 256, 0, s>>>(
-        static_cast<const unsigned short*>(x), static_cast<const unsigned short*>(dR), nb, H, W, C,
-        dr_part);
-    DN_CUDA_CHECK(cudaGetLastError());
-  }
+  if (nb * C > 0x7fffffffLL || W > 12 * 1024) return DN_EUNSUPPORTED;
+  k_readout_bwd<<<(unsigned)(nb * C), 256, W * sizeof(float),
+                  static_cast<cudaStream_t>(stream)>>>(
+      static_cast<const unsigned short*>(x), r, static_cast<const unsigned short*>(dR), (int)nb, H,
+      W, C, static_cast<unsigned short*>(dx), dr_part);
+  DN_CUDA_CHECK(cudaGetLastError());
   return DN_OK;
 }
 

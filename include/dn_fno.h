@@ -120,7 +120,7 @@ int32_t dn_fno_features_bwd(const float* dfeat, int64_t n_pix, float eps_lo, flo
 /* out[b, w, c] = sum_h r[h, c] * x[b, c, h, w]   (x, out BF16; r FP32 (H, C)) */
 int32_t dn_fno_readout(const void* x, const float* r, int64_t nb, int32_t H, int32_t W,
                        int32_t C, void* out, void* stream);
-/* dx[b, c, h, w] = r[h, c] * dR[b, w, c] (BF16; NULL skips; W a multiple of 8) and
+/* dx[b, c, h, w] = r[h, c] * dR[b, w, c] (BF16; NULL skips) and
  * dr_part[b, h, c] = sum_w dR[b, w, c] * x[b, c, h, w] (FP32; NULL skips) */
 int32_t dn_fno_readout_bwd(const void* x, const float* r, const void* dR, int64_t nb, int32_t H,
                            int32_t W, int32_t C, void* dx, float* dr_part, void* stream);
