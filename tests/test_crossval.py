@@ -1,0 +1,66 @@
+"""Cross-validation file format (the reference's ExternalCrossValidator JSON):
+round trip, the comparisons, the seeded test case; and, where the reference
+checkout is present, its own loader reads what save_results writes."""
+
+from __future__ import annotations
+
+import importlib.util
+import os
+import sys
+
+import pytest
+import torch
+
+from diffnano_b200.crossval import ExternalCrossValidator, save_results
+
+
+def test_round_trip_and_comparisons(tmp_path):
+    g = torch.Generator().manual_seed(0)
+    field = torch.randn(3, 4, 5, generator=g, dtype=torch.float64)
+    grad = torch.randn(4, 5, generator=g, dtype=torch.float64)
+    p = tmp_path / "r.json"
+    save_results(str(p), field=field, gradient=grad, solver="diffnano_b200", n_steps=7)
+    r = ExternalCrossValidator.load_external_results(str(p))
+    assert torch.equal(r["field"], field) and torch.equal(r["gradient"], grad)
+    assert r["solver"] == "diffnano_b200" and r["n_steps"] == 7
+    v = ExternalCrossValidator()
+    ok = v.validate_forward(field * (1 + 1e-5), field)
+    assert ok["passed"] and ok["relative_error"] < 2e-5
+    bad = v.validate_forward(field + 1.0, field)
+    assert not bad["passed"]
+    gr = v.validate_gradient(grad, 2.0 * grad)
+    assert gr["passed"] and abs(gr["cosine_similarity"] - 1.0) < 1e-12
+    assert not v.validate_gradient(grad, -grad)["passed"]
+    with pytest.raises(ValueError):
+        save_results(str(p), field=torch.zeros(2, dtype=torch.complex128))
+
+
+def test_seeded_case_matches_reference_recipe():
+    tc = ExternalCrossValidator().generate_test_case((4, 5, 6))
+    torch_state = torch.get_rng_state()
+    torch.manual_seed(42)
+    ref = 1.5 + 1.0 * torch.rand(4, 5, 6, dtype=torch.float64)
+    torch.set_rng_state(torch_state)
+    assert torch.equal(tc["eps"], ref)
+    assert tc["source_pos"] == (2, 2, 3) and tc["seed"] == 42
+
+
+REF = os.path.join("/root", "reference", "diffnano", "solvers", "fdtd_benchmark.py")
+
+
+@pytest.mark.skipif(not os.path.exists(REF), reason="reference checkout not present")
+def test_reference_loader_reads_our_files(tmp_path):
+    spec = importlib.util.spec_from_file_location("_ref_fdtd_benchmark", REF)
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[spec.name] = mod
+    try:
+        spec.loader.exec_module(mod)
+    except ImportError as e:  # its package imports something absent here
+        pytest.skip(f"reference module not importable: {e}")
+    finally:
+        sys.modules.pop(spec.name, None)
+    field = torch.arange(24, dtype=torch.float64).reshape(2, 3, 4)
+    p = tmp_path / "ours.json"
+    save_results(str(p), field=field, solver="diffnano_b200")
+    r = mod.ExternalCrossValidator.load_external_results(str(p))
+    assert torch.equal(r["field"], field) and r["solver"] == "diffnano_b200"
