@@ -708,8 +708,8 @@ def run_gemm(args):
         torch.cuda.synchronize(dev)
         return e0.elapsed_time(e1) / reps
 
-    ms = timed(lambda: gemm(n, n, [(kmajor(a, n, n), kmajor(b, n, n))], o, OutMap.rowmajor(n)),
-               args.steps)
+    ms = timed(lambda: gemm(n, n, [(kmajor(a, n, n), kmajor(b, n, n))], o, OutMap.rowmajor(n),
+                            pair=args.gemm_pair), args.steps)
     ref = a[:128].float() @ b.float().T
     err = float((o[:128] - ref).norm() / ref.norm())
     mt = torch.matmul(a, b.T)
@@ -719,7 +719,10 @@ def run_gemm(args):
     line = {"metric": "BF16 GEMM TFLOP/s (tcgen05, FP32 accumulate)", "value": tf,
             "unit": "TFLOP/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16",
-            "data": "synthetic", "config": {"workload": f"gemm_{n}x{n}x{n}_bf16"},
+            "data": "synthetic",
+            "config": {"workload": f"gemm_{n}x{n}x{n}_bf16",
+                       "tiles": {0: "one-CTA 128x256", 1: "one-CTA 128x256",
+                                 2: "two-CTA 256x256"}[args.gemm_pair]},
             "rel_err_vs_fp32": err, "torch_matmul_tflops": 2 * n ** 3 / ms_ref / 1e9,
             "roofline": {"bound": "tensor", "achieved": tf, "peak": peak, "unit": "TFLOP/s",
                          "frac": tf / peak, "peak_kind": f"{kind} burst bf16"}}
@@ -789,6 +792,8 @@ def main():
                          "fno: surrogate data generation + training; design: 3-D inverse "
                          "design, plain vs surrogate-assisted")
     ap.add_argument("--gemm-n", type=int, default=8192)
+    ap.add_argument("--gemm-pair", type=int, default=0, choices=[0, 1, 2],
+                    help="GEMM tiles: 0 or 1 one-CTA, 2 two-CTA pairs")
     ap.add_argument("--batch2d-n", type=int, default=64,
                     help="instances of the batched 2-D workload (64 is the workload)")
     ap.add_argument("--batch2d-tscale", type=float, default=1.0,

@@ -92,7 +92,8 @@ class DnGemm(ctypes.Structure):
                 ("row_scale", c_void_p), ("batch_scale", c_void_p), ("addend", c_void_p),
                 ("addend_dtype", c_int32), ("aux_dtype", c_int32), ("aux", c_void_p),
                 ("pre", c_void_p), ("pre_dtype", c_int32), ("block_n", c_int32),
-                ("max_ctas", c_int32), ("col_scale", c_void_p), ("row_bias", c_void_p)]
+                ("max_ctas", c_int32), ("col_scale", c_void_p), ("row_bias", c_void_p),
+                ("pair", c_int32)]
 
 
 class DnDensity(ctypes.Structure):

@@ -6,7 +6,7 @@
 //   two-digit index map (so one GEMM can write a transposed or re-blocked
 //   layout that the next GEMM reads directly).
 //
-// Persistent CTAs (one per SM, 192 threads) walk the tile list: per batch,
+// Persistent CTAs (one per SM, 320 threads) walk the tile list: per batch,
 // groups of 16 m tiles, n tiles inside a group, m fastest (neighbouring CTAs
 // share A rows and B columns in L2):
 //   warp 0, lane 0  TMA producer.  Per 64-wide k block it loads the 128 x 64
@@ -19,9 +19,21 @@
 //                   last k block signals the accumulator buffer (two TMEM
 //                   buffers of BN columns, so the epilogue of one tile runs
 //                   under the MMAs of the next);
-//   warps 2..5      epilogue.  Warp w reads TMEM lanes 32*(w%4) .. +31 (its
-//                   rows) with tcgen05.ld.32x32b.x32, applies the epilogue
-//                   and stores 32 consecutive columns per thread.
+//   warps 2..9      epilogue.  Warp w reads TMEM lanes 32*(w%4) .. +31 (its
+//                   rows) of one half of the tile's columns ((w-2)/4) with
+//                   tcgen05.ld.32x32b.x32, applies the epilogue and stores 32
+//                   consecutive columns per thread.  Two warps per lane
+//                   quadrant: the operator's transform GEMMs (K ~ 1 000, a
+//                   GELU per element) are bound by epilogue instructions.
+// Pair mode (two-CTA clusters, tcgen05 cta_group::2): the tile is 256 x BN;
+// each CTA of the pair loads its own 128 rows of A and half (BN / 2 rows) of
+// B, both loads completing on the leading CTA's ring barrier, and the leading
+// CTA's MMA thread issues M = 256 MMAs that read both CTAs' shared memory and
+// write 128 accumulator rows into each CTA's tensor memory.  Per SM that is
+// 32 KB of operands per 64-wide k block instead of 48 KB, so 6 ring stages
+// fit.  Stage and accumulator releases are two plain commits (one per CTA's
+// barrier); the epilogue warps of both CTAs release an accumulator buffer on
+// the leading CTA's barrier.  No multicast anywhere.
 // Descriptor encodings follow the PTX ISA's tcgen05 shared-memory matrix
 // descriptor (start >> 4, leading byte offset >> 4, stride byte offset >> 4,
 // version 1, swizzle mode 2 = 128 B) and instruction descriptor (F32
@@ -41,21 +53,29 @@ namespace gm {
 
 constexpr int BM = 128;
 constexpr int BK = 64;
-constexpr int NT = 192;
+constexpr int NEPI = 8;  // epilogue warps: two per tensor-memory lane quadrant
+constexpr int NT = 64 + 32 * NEPI;
 constexpr int ATOM = 64;                   // MN extent of one 128-byte swizzle atom
 constexpr int ATOM_BYTES = ATOM * BK * 2;  // 8 KB
 constexpr int RING_BYTES = 192 * 1024;
+constexpr int RING_BYTES_PAIR = 192 * 1024;
 constexpr unsigned long long WAIT_NS = 4000000000ull;  // 4 s per wait
 constexpr uint32_t SLEEP_NS = 20000;
 
-template <int BN>
+template <int BN, bool PAIR>
 struct Cfg {
+  static constexpr int TILE_M = PAIR ? 2 * BM : BM;  // rows of one tile
+  static constexpr int B_ROWS = PAIR ? BN / 2 : BN;  // B rows this CTA loads
   static constexpr int A_BYTES = BM * BK * 2;
-  static constexpr int B_BYTES = BN * BK * 2;
+  static constexpr int B_BYTES = B_ROWS * BK * 2;
   static constexpr int STAGE = A_BYTES + B_BYTES;
-  static constexpr int S = RING_BYTES / STAGE;  // 8, 6, 4 stages for BN 64, 128, 256
-  static constexpr int TMEM_COLS = 2 * BN;      // two accumulator buffers
+  // 8, 6, 4 stages for BN 64, 128, 256; 6 in pair mode at BN 256
+  static constexpr int S = (PAIR ? RING_BYTES_PAIR : RING_BYTES) / STAGE;
+  static constexpr int TMEM_COLS = 2 * BN;  // two accumulator buffers
+  static constexpr int TEMPTY_ARRIVALS = PAIR ? 2 * NEPI : NEPI;  // one per epilogue warp
   static constexpr size_t SMEM = (size_t)S * STAGE + 1024 + 256;
+  static_assert(SMEM <= 232448, "dynamic shared memory above the per-CTA limit");
+  static_assert(B_ROWS % ATOM == 0, "B tile in whole swizzle atoms");
 };
 
 struct OpDev {
@@ -88,6 +108,7 @@ struct Params {
   char* pre;
   int pre_bf16;
   int vec;
+  int vec32;  // 32-byte aligned chunk rows: 256-bit stores
   int* status;
 };
 
@@ -120,8 +141,45 @@ __device__ __forceinline__ bool gwait(uint64_t* bar, uint32_t parity, volatile i
   }
 }
 
-__device__ __forceinline__ void fail(volatile int* abort, int* status) {
+// ---- cluster (CTA pair) helpers ---------------------------------------------
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ uint32_t cluster_id() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%clusterid.x;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ uint32_t cluster_count() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%nclusterid.x;" : "=r"(r));
+  return r;
+}
+// shared::cluster address of the same shared-memory offset in CTA `rank`
+__device__ __forceinline__ uint32_t map_rank(const void* p, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(p)), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t caddr) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(caddr)
+               : "memory");
+}
+__device__ __forceinline__ void st_cluster_u32(uint32_t caddr, uint32_t v) {
+  asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(caddr), "r"(v) : "memory");
+}
+// every thread of both CTAs (no convergence requirement)
+__device__ __forceinline__ void cluster_barrier() {
+  asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;" ::: "memory");
+}
+
+// raise the abort flag of this CTA and (pair mode, peer_abort != 0) of the
+// other CTA of the pair, and report the timeout
+__device__ __forceinline__ void fail(volatile int* abort, int* status, uint32_t peer_abort = 0) {
   *abort = 1;
+  if (peer_abort) st_cluster_u32(peer_abort, 1u);
   report_status(status, DN_ETIMEOUT);
 }
 
@@ -138,19 +196,47 @@ __device__ __forceinline__ void tma_load_4d_g(void* dst, const CUtensorMap* m, u
       : "memory");
 }
 
-// one operand tile (`rows_tile` rows from r0, k block from k0) into `dst`
+// pair-mode TMA loads: the data lands in this CTA's shared memory, the
+// completion is counted on the barrier at cluster address `bar` (the leading
+// CTA's).  No multicast.
+__device__ __forceinline__ void tma_load_3d_pair(void* dst, const CUtensorMap* m, uint32_t bar,
+                                                 int x, int y, int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(m)), "r"(bar), "r"(x), "r"(y), "r"(z)
+      : "memory");
+}
+__device__ __forceinline__ void tma_load_4d_pair(void* dst, const CUtensorMap* m, uint32_t bar,
+                                                 int x, int y, int z, int w) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4, %5, %6}], [%2];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(m)), "r"(bar), "r"(x), "r"(y), "r"(z), "r"(w)
+      : "memory");
+}
+
+// one operand tile (`rows_tile` rows from r0, k block from k0) into `dst`;
+// pair mode: completion on the barrier at cluster address `cbar`
+template <bool PAIR>
 __device__ __forceinline__ void load_operand(unsigned char* dst, const CUtensorMap* m,
-                                             const OpDev& o, uint64_t* bar, int r0, int k0,
-                                             int bz, int rows_tile) {
+                                             const OpDev& o, uint64_t* bar, uint32_t cbar,
+                                             int r0, int k0, int bz, int rows_tile) {
   const int z = o.batched ? bz : 0;
   if (!o.mn) {
-    tma_load_3d(dst, m, bar, k0, r0, z);
+    if constexpr (PAIR)
+      tma_load_3d_pair(dst, m, cbar, k0, r0, z);
+    else
+      tma_load_3d(dst, m, bar, k0, r0, z);
   } else {
     for (int j = 0; j < rows_tile / ATOM; ++j) {
       const int r = r0 + j * ATOM;
       const int x = o.fold ? r % o.fold : r;
       const int f = o.fold ? r / o.fold : 0;
-      tma_load_4d_g(dst + j * ATOM_BYTES, m, bar, x, k0, f, z);
+      if constexpr (PAIR)
+        tma_load_4d_pair(dst + j * ATOM_BYTES, m, cbar, x, k0, f, z);
+      else
+        tma_load_4d_g(dst + j * ATOM_BYTES, m, bar, x, k0, f, z);
     }
   }
 }
@@ -167,10 +253,10 @@ __device__ __forceinline__ uint64_t desc_mnmajor(uint32_t saddr) {
          (64ull << 32) | (1ull << 46) | (2ull << 61);
 }
 
-template <int BN>
+template <int BN, int TILE_M>
 __device__ __forceinline__ uint32_t idesc(int a_mn, int b_mn) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)a_mn << 15) | ((uint32_t)b_mn << 16) |
-         ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+         ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(TILE_M >> 4) << 24);
 }
 
 __device__ __forceinline__ float gelu_f(float v) {
@@ -230,6 +316,37 @@ __device__ __forceinline__ void load32(const char* base, int bf16, long long off
   }
 }
 
+__device__ __forceinline__ void st256(void* p, uint32_t a, uint32_t b, uint32_t c, uint32_t d,
+                                      uint32_t e, uint32_t f, uint32_t g, uint32_t h) {
+  asm volatile("st.global.v8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "r"(a), "r"(b),
+               "r"(c), "r"(d), "r"(e), "r"(f), "r"(g), "r"(h)
+               : "memory");
+}
+
+// 32 values from element offset `off` with 256-bit stores, so that every
+// lane writes whole 32-byte sectors (the lanes of a warp write 32 different
+// rows); the chunk start is 32-byte aligned
+__device__ __forceinline__ void store32_v8(char* base, int bf16, long long off, const float* v) {
+  if (bf16) {
+    char* p = base + off * 2;
+    uint32_t w[16];
+#pragma unroll
+    for (int e = 0; e < 16; ++e)
+      w[e] = static_cast<uint32_t>(f2bf(v[2 * e])) |
+             (static_cast<uint32_t>(f2bf(v[2 * e + 1])) << 16);
+    st256(p, w[0], w[1], w[2], w[3], w[4], w[5], w[6], w[7]);
+    st256(p + 32, w[8], w[9], w[10], w[11], w[12], w[13], w[14], w[15]);
+  } else {
+    char* p = base + off * 4;
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      st256(p + 32 * q, __float_as_uint(v[8 * q]), __float_as_uint(v[8 * q + 1]),
+            __float_as_uint(v[8 * q + 2]), __float_as_uint(v[8 * q + 3]),
+            __float_as_uint(v[8 * q + 4]), __float_as_uint(v[8 * q + 5]),
+            __float_as_uint(v[8 * q + 6]), __float_as_uint(v[8 * q + 7]));
+  }
+}
+
 __device__ __forceinline__ void store32(char* base, int bf16, long long off, long long cs,
                                         bool vec, int nv, const float* v) {
   if (vec) {
@@ -279,12 +396,12 @@ __device__ __forceinline__ void tile_coords(long long t, const Params& p, int& m
   nt = (int)(r / gm);
 }
 
-template <int BN>
+template <int BN, bool PAIR>
 __global__ void __launch_bounds__(NT, 1)
     k_gemm(const __grid_constant__ CUtensorMap ta0, const __grid_constant__ CUtensorMap tb0,
            const __grid_constant__ CUtensorMap ta1, const __grid_constant__ CUtensorMap tb1,
            const Params p) {
-  using C = Cfg<BN>;
+  using C = Cfg<BN, PAIR>;
   constexpr int S = C::S;
   extern __shared__ __align__(1024) unsigned char g_raw[];
   unsigned char* ring = reinterpret_cast<unsigned char*>(
@@ -298,6 +415,13 @@ __global__ void __launch_bounds__(NT, 1)
   volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // pair mode: rank 0 of the cluster leads (issues the MMAs, owns the ring
+  // and accumulator-release barriers that both CTAs signal)
+  const uint32_t rank = PAIR ? cluster_rank() : 0u;
+  const long long unit0 = PAIR ? (long long)cluster_id() : (long long)blockIdx.x;
+  const long long n_units = PAIR ? (long long)cluster_count() : (long long)gridDim.x;
+  const uint32_t peer_abort = PAIR ? map_rank((const void*)abort, rank ^ 1u) : 0u;
+
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) {
       mbar_init(&full[s], 1);
@@ -305,51 +429,70 @@ __global__ void __launch_bounds__(NT, 1)
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&tfull[b], 1);
-      mbar_init(&tempty[b], 128);
+      mbar_init(&tempty[b], C::TEMPTY_ARRIVALS);
     }
     mbar_init(drain, 1);
     *abort = 0;
     fence_barrier_init();
   }
   if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
-                     smem_u32(tmem_slot)),
-                 "r"((uint32_t)C::TMEM_COLS)
-                 : "memory");
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    if constexpr (PAIR) {
+      asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                       smem_u32(tmem_slot)),
+                   "r"((uint32_t)C::TMEM_COLS)
+                   : "memory");
+      asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+    } else {
+      asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                       smem_u32(tmem_slot)),
+                   "r"((uint32_t)C::TMEM_COLS)
+                   : "memory");
+      asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
+  if constexpr (PAIR) cluster_barrier();  // both CTAs' barriers initialised
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
   const int kb_total = p.kb[0] + (p.n_seg > 1 ? p.kb[1] : 0);
 
   if (warp == 0) {
     if (lane == 0) {
-      // ---- TMA producer ----------------------------------------------------
+      // ---- TMA producer (both CTAs in pair mode) -----------------------------
       long long g = 0;
-      for (long long t = blockIdx.x; t < p.n_tiles && !*abort; t += gridDim.x) {
+      for (long long t = unit0; t < p.n_tiles && !*abort; t += n_units) {
         int mt, nt, bz;
         tile_coords(t, p, mt, nt, bz);
         bool ok = true;
         for (int kb = 0; kb < kb_total; ++kb, ++g) {
           const int s = (int)(g % S);
           if (g >= S && !gwait_spin(&empty[s], (uint32_t)(((g / S) - 1) & 1), abort)) {
-            fail(abort, p.status);
+            fail(abort, p.status, peer_abort);
             ok = false;
             break;
           }
           const int seg = kb < p.kb[0] ? 0 : 1;
           const int k0 = (seg == 0 ? kb : kb - p.kb[0]) * BK;
           unsigned char* st = ring + s * C::STAGE;
-          mbar_arrive_expect_tx(&full[s], C::STAGE);
-          load_operand(st, seg == 0 ? &ta0 : &ta1, p.a[seg], &full[s], mt * BM, k0, bz, BM);
-          load_operand(st + C::A_BYTES, seg == 0 ? &tb0 : &tb1, p.b[seg], &full[s], nt * BN, k0,
-                       bz, BN);
+          uint32_t cbar = 0;
+          if constexpr (PAIR) {
+            // the leading CTA's barrier counts both CTAs' bytes
+            cbar = map_rank(&full[s], 0u);
+            if (rank == 0) mbar_arrive_expect_tx(&full[s], 2 * C::STAGE);
+          } else {
+            mbar_arrive_expect_tx(&full[s], C::STAGE);
+          }
+          const int ar0 = mt * C::TILE_M + (int)rank * BM;
+          const int br0 = nt * BN + (int)rank * C::B_ROWS;
+          load_operand<PAIR>(st, seg == 0 ? &ta0 : &ta1, p.a[seg], &full[s], cbar, ar0, k0, bz,
+                             BM);
+          load_operand<PAIR>(st + C::A_BYTES, seg == 0 ? &tb0 : &tb1, p.b[seg], &full[s], cbar,
+                             br0, k0, bz, C::B_ROWS);
         }
         if (!ok) break;
       }
-      if (*abort) {
+      if (*abort && rank == 0) {
         // let the copies already issued land before the CTA goes away
         for (long long q = (g > S ? g - S : 0); q < g; ++q) {
           const int s = (int)(q % S);
@@ -361,16 +504,16 @@ __global__ void __launch_bounds__(NT, 1)
       }
     }
   } else if (warp == 1) {
-    if (lane == 0) {
-      // ---- MMA issuer ------------------------------------------------------
-      const uint32_t id0 = idesc<BN>(p.a[0].mn, p.b[0].mn);
-      const uint32_t id1 = idesc<BN>(p.a[1].mn, p.b[1].mn);
+    if (lane == 0 && rank == 0) {
+      // ---- MMA issuer (the leading CTA only in pair mode) ---------------------
+      const uint32_t id0 = idesc<BN, C::TILE_M>(p.a[0].mn, p.b[0].mn);
+      const uint32_t id1 = idesc<BN, C::TILE_M>(p.a[1].mn, p.b[1].mn);
       long long g = 0;
       int it = 0;
-      for (long long t = blockIdx.x; t < p.n_tiles && !*abort; t += gridDim.x, ++it) {
+      for (long long t = unit0; t < p.n_tiles && !*abort; t += n_units, ++it) {
         const int buf = it & 1;
         if (it >= 2 && !gwait_spin(&tempty[buf], (uint32_t)(((it >> 1) - 1) & 1), abort)) {
-          fail(abort, p.status);
+          fail(abort, p.status, peer_abort);
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -379,7 +522,7 @@ __global__ void __launch_bounds__(NT, 1)
         for (int kb = 0; kb < kb_total; ++kb, ++g) {
           const int s = (int)(g % S);
           if (!gwait_spin(&full[s], (uint32_t)((g / S) & 1), abort)) {
-            fail(abort, p.status);
+            fail(abort, p.status, peer_abort);
             ok = false;
             break;
           }
@@ -395,48 +538,87 @@ __global__ void __launch_bounds__(NT, 1)
             const uint64_t db =
                 bmn ? desc_mnmajor(sbb + k16 * 2048) : desc_kmajor(sbb + k16 * 32);
             const uint32_t accum = (kb > 0 || k16 > 0) ? 1u : 0u;
+            if constexpr (PAIR) {
+              asm volatile(
+                  "{\n\t.reg .pred p;\n\t"
+                  "setp.ne.b32 p, %4, 0;\n\t"
+                  "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(acc_addr),
+                  "l"(da), "l"(db), "r"(id), "r"(accum)
+                  : "memory");
+            } else {
+              asm volatile(
+                  "{\n\t.reg .pred p;\n\t"
+                  "setp.ne.b32 p, %4, 0;\n\t"
+                  "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(acc_addr),
+                  "l"(da), "l"(db), "r"(id), "r"(accum)
+                  : "memory");
+            }
+          }
+          if constexpr (PAIR) {
             asm volatile(
-                "{\n\t.reg .pred p;\n\t"
-                "setp.ne.b32 p, %4, 0;\n\t"
-                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(acc_addr),
-                "l"(da), "l"(db), "r"(id), "r"(accum)
+                "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                    smem_u32(&empty[s]))
+                : "memory");
+            asm volatile(
+                "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                    map_rank(&empty[s], 1u))
+                : "memory");
+          } else {
+            asm volatile(
+                "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                    smem_u32(&empty[s]))
                 : "memory");
           }
-          asm volatile(
-              "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                  smem_u32(&empty[s]))
-              : "memory");
         }
         if (!ok) break;
-        asm volatile(
-            "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                smem_u32(&tfull[buf]))
-            : "memory");
+        if constexpr (PAIR) {
+          asm volatile(
+              "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                  smem_u32(&tfull[buf]))
+              : "memory");
+          asm volatile(
+              "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                  map_rank(&tfull[buf], 1u))
+              : "memory");
+        } else {
+          asm volatile(
+              "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                  smem_u32(&tfull[buf]))
+              : "memory");
+        }
       }
       // every MMA issued by this thread completes before TMEM is freed
-      asm volatile(
-          "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-              smem_u32(drain))
-          : "memory");
+      if constexpr (PAIR) {
+        asm volatile(
+            "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                smem_u32(drain))
+            : "memory");
+      } else {
+        asm volatile(
+            "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                smem_u32(drain))
+            : "memory");
+      }
       const unsigned long long t0 = gtimer();
       while (!mbar_try_wait_sleep(drain, 0, SLEEP_NS) && gtimer() - t0 < WAIT_NS) {
       }
     }
   } else {
-    // ---- epilogue: warps 2..5 ----------------------------------------------
+    // ---- epilogue: warps 2..9 ----------------------------------------------
     const int quad = warp & 3;  // TMEM lanes 32*quad .. 32*quad+31
+    const int c_beg = ((warp - 2) >> 2) * (BN / 2);  // this warp's half of the columns
     int it = 0;
-    for (long long t = blockIdx.x; t < p.n_tiles; t += gridDim.x, ++it) {
+    for (long long t = unit0; t < p.n_tiles; t += n_units, ++it) {
       const int buf = it & 1;
       const bool ready = gwait(&tfull[buf], (uint32_t)((it >> 1) & 1), abort);
       if (!__all_sync(0xffffffffu, ready)) {
-        if (lane == 0) fail(abort, p.status);
+        if (lane == 0) fail(abort, p.status, peer_abort);
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       int mt, nt, bz;
       tile_coords(t, p, mt, nt, bz);
-      const long long row = (long long)mt * BM + quad * 32 + lane;
+      const long long row = (long long)mt * C::TILE_M + (long long)rank * BM + quad * 32 + lane;
       const bool row_ok = row < p.M;
       float scale = p.alpha;
       if (row_ok && p.row_scale) scale *= p.row_scale[row];
@@ -444,7 +626,7 @@ __global__ void __launch_bounds__(NT, 1)
       if (p.batch_scale) scale *= p.batch_scale[bz];
       const long long roff = (long long)bz * p.sb + (row % p.R0) * p.r0 + (row / p.R0) * p.r1;
 #pragma unroll 1
-      for (int c = 0; c < BN; c += 32) {
+      for (int c = c_beg; c < c_beg + BN / 2; c += 32) {
         uint32_t r[32];
         const uint32_t taddr = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(buf * BN + c);
         asm volatile(
@@ -488,7 +670,12 @@ __global__ void __launch_bounds__(NT, 1)
             for (int j = 0; j < 32; ++j) v[j] += w[j];
           }
           if (p.act == DN_ACT_GELU) {
-            if (p.pre) store32(p.pre, p.pre_bf16, off, p.c0, vec, nv, v);
+            if (p.pre) {
+              if (vec && p.vec32)
+                store32_v8(p.pre, p.pre_bf16, off, v);
+              else
+                store32(p.pre, p.pre_bf16, off, p.c0, vec, nv, v);
+            }
 #pragma unroll
             for (int j = 0; j < 32; ++j) v[j] = gelu_f(v[j]);
           } else if (p.act == DN_ACT_GELU_GRAD) {
@@ -501,23 +688,43 @@ __global__ void __launch_bounds__(NT, 1)
 #pragma unroll
             for (int j = 0; j < 32; ++j) v[j] += w[j];
           }
-          store32(p.out, p.out_bf16, off, p.c0, vec, nv, v);
+          if (vec && p.vec32)
+            store32_v8(p.out, p.out_bf16, off, v);
+          else
+            store32(p.out, p.out_bf16, off, p.c0, vec, nv, v);
         }
         __syncwarp();  // reconverge before the next warp-wide tcgen05.ld
       }
+      // release the accumulator buffer: one arrival per warp, on the leading
+      // CTA's barrier in pair mode
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-      mbar_arrive(&tempty[buf]);
+      __syncwarp();
+      if (lane == 0) {
+        if constexpr (PAIR)
+          mbar_arrive_cluster(map_rank(&tempty[buf], 0u));
+        else
+          mbar_arrive(&tempty[buf]);
+      }
     }
   }
 
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
+  // pair mode: neither CTA leaves (or frees its tensor memory) while the
+  // other may still signal its barriers or the MMAs read its shared memory
+  if constexpr (PAIR) cluster_barrier();
   if (warp == 0) {
     __syncwarp();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
-                 "r"((uint32_t)C::TMEM_COLS)
-                 : "memory");
+    if constexpr (PAIR) {
+      asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                   "r"((uint32_t)C::TMEM_COLS)
+                   : "memory");
+    } else {
+      asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                   "r"((uint32_t)C::TMEM_COLS)
+                   : "memory");
+    }
   }
 }
 
@@ -581,25 +788,74 @@ int sm_count() {
   return n > 0 ? n : 148;
 }
 
+// co-resident two-CTA clusters of the pair kernel (0 when none fit)
 template <int BN>
+int pair_clusters() {
+  static int cached = -1;
+  if (cached >= 0) return cached;
+  using C = Cfg<BN, true>;
+  auto kern = k_gemm<BN, true>;
+  int n = 0;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM) ==
+      cudaSuccess) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(2 * (unsigned)sm_count(), 1, 1);
+    cfg.blockDim = dim3(NT, 1, 1);
+    cfg.dynamicSmemBytes = C::SMEM;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (cudaOccupancyMaxActiveClusters(&n, kern, &cfg) != cudaSuccess) n = 0;
+  }
+  (void)cudaGetLastError();
+  cached = n;
+  return n;
+}
+
+template <int BN, bool PAIR>
 int launch(const dn_gemm& g, Params p, int* status, cudaStream_t s) {
+  using C = Cfg<BN, PAIR>;
   CUtensorMap m[4];
   int rc;
   for (int seg = 0; seg < 2; ++seg) {
     const int src = seg < g.n_seg ? seg : 0;  // unused segment: a valid copy of segment 0
     if ((rc = encode_operand(&m[2 * seg], g.a[src], g.batch, BM)) != DN_OK) return rc;
-    if ((rc = encode_operand(&m[2 * seg + 1], g.b[src], g.batch, BN)) != DN_OK) return rc;
+    if ((rc = encode_operand(&m[2 * seg + 1], g.b[src], g.batch, C::B_ROWS)) != DN_OK) return rc;
   }
-  p.tiles_m = (int)((g.M + BM - 1) / BM);
+  p.tiles_m = (int)((g.M + C::TILE_M - 1) / C::TILE_M);
   p.tiles_n = (int)((g.N + BN - 1) / BN);
   p.n_tiles = (long long)p.tiles_m * p.tiles_n * g.batch;
   p.status = status;
-  long long ctas = g.max_ctas > 0 ? g.max_ctas : sm_count();
-  if (ctas > p.n_tiles) ctas = p.n_tiles;
-  auto kern = k_gemm<BN>;
+  auto kern = k_gemm<BN, PAIR>;
   DN_CUDA_CHECK(
-      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg<BN>::SMEM));
-  kern<<<(unsigned)ctas, NT, Cfg<BN>::SMEM, s>>>(m[0], m[1], m[2], m[3], p);
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM));
+  if constexpr (!PAIR) {
+    long long ctas = g.max_ctas > 0 ? g.max_ctas : sm_count();
+    if (ctas > p.n_tiles) ctas = p.n_tiles;
+    kern<<<(unsigned)ctas, NT, C::SMEM, s>>>(m[0], m[1], m[2], m[3], p);
+  } else {
+    long long pairs = pair_clusters<BN>();
+    if (g.max_ctas > 0 && g.max_ctas / 2 < pairs) pairs = g.max_ctas / 2;
+    if (pairs > p.n_tiles) pairs = p.n_tiles;
+    if (pairs < 1) return DN_EUNSUPPORTED;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(2 * pairs), 1, 1);
+    cfg.blockDim = dim3(NT, 1, 1);
+    cfg.dynamicSmemBytes = C::SMEM;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    DN_CUDA_CHECK(cudaLaunchKernelEx(&cfg, kern, m[0], m[1], m[2], m[3], p));
+  }
   DN_CUDA_CHECK(cudaGetLastError());
   return DN_OK;
 }
@@ -607,11 +863,11 @@ int launch(const dn_gemm& g, Params p, int* status, cudaStream_t s) {
 bool dtype_ok(int32_t d) { return d == DN_F32 || d == DN_BF16; }
 int esize(int32_t d) { return d == DN_BF16 ? 2 : 4; }
 
-// 16-byte vector access to a 32-column chunk is valid for this pointer
-bool vec_ok(const dn_gemm& g, const void* ptr, int es) {
+// `bytes`-wide vector access to a 32-column chunk is valid for this pointer
+bool vec_ok(const dn_gemm& g, const void* ptr, int es, int bytes = 16) {
   if (!ptr) return true;
-  if (!aligned16(ptr)) return false;
-  const long long q = 16 / es;
+  if (reinterpret_cast<uintptr_t>(ptr) % bytes) return false;
+  const long long q = bytes / es;
   const long long strides[4] = {g.c_batch_stride, g.c_row_stride0, g.c_row_stride1,
                                 g.c_col_stride1};
   for (long long st : strides)
@@ -651,6 +907,8 @@ extern "C" int32_t dn_gemm_run(const dn_gemm* g, int32_t* status, void* stream) 
   if (g->c_row_radix < 0 || g->c_col_radix < 0 || (g->c_col_radix % 32)) return DN_EINVAL;
   if (g->block_n != 0 && g->block_n != 64 && g->block_n != 128 && g->block_n != 256)
     return DN_EINVAL;
+  if (g->pair < 0 || g->pair > 2 || (g->pair == 2 && g->block_n != 0 && g->block_n != 256))
+    return DN_EINVAL;
 
   p.M = g->M;
   p.N = g->N;
@@ -681,6 +939,10 @@ extern "C" int32_t dn_gemm_run(const dn_gemm* g, int32_t* status, void* stream) 
   p.vec = g->c_col_stride0 == 1 && vec_ok(*g, g->out, esize(g->out_dtype)) &&
           vec_ok(*g, g->addend, esize(g->addend_dtype)) &&
           vec_ok(*g, g->aux, esize(g->aux_dtype)) && vec_ok(*g, g->pre, esize(g->pre_dtype));
+  // a chunk starts at a multiple of 32 columns (and of the column radix), so
+  // 32-byte aligned bases and strides keep every chunk start 32-byte aligned
+  p.vec32 = p.vec && vec_ok(*g, g->out, esize(g->out_dtype), 32) &&
+            vec_ok(*g, g->pre, esize(g->pre_dtype), 32);
 
   int bn = g->block_n;
   if (bn == 0) {
@@ -697,7 +959,14 @@ extern "C" int32_t dn_gemm_run(const dn_gemm* g, int32_t* status, void* stream) 
     }
   }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if (bn == 64) return launch<64>(*g, p, status, s);
-  if (bn == 128) return launch<128>(*g, p, status, s);
-  return launch<256>(*g, p, status, s);
+  // two-CTA 256 x 256 tiles only when asked for: on B200 they measured
+  // 2-5 % slower than one-CTA tiles at 4096^3 / 8192^3 and on the operator's
+  // transform GEMMs (the one-CTA kernel is not operand-bandwidth bound)
+  if (g->pair == 2) {
+    if (pair_clusters<256>() < 1) return DN_EUNSUPPORTED;
+    return launch<256, true>(*g, p, status, s);
+  }
+  if (bn == 64) return launch<64, false>(*g, p, status, s);
+  if (bn == 128) return launch<128, false>(*g, p, status, s);
+  return launch<256, false>(*g, p, status, s);
 }

@@ -101,8 +101,10 @@ def gemm(M: int, N: int, segs: Sequence[Tuple[Operand, Operand]], out: torch.Ten
          col_scale: Optional[torch.Tensor] = None, row_bias: Optional[torch.Tensor] = None,
          addend: Optional[torch.Tensor] = None, aux: Optional[torch.Tensor] = None,
          pre: Optional[torch.Tensor] = None, block_n: int = 0, max_ctas: int = 0,
-         status: Optional[torch.Tensor] = None) -> torch.Tensor:
-    """Launch one ``dn_gemm_run`` on the current stream; returns ``out``."""
+         pair: int = 0, status: Optional[torch.Tensor] = None) -> torch.Tensor:
+    """Launch one ``dn_gemm_run`` on the current stream; returns ``out``.
+    ``pair``: 0 or 1 one-CTA tiles, 2 two-CTA 256 x 256 tiles (tcgen05
+    cta_group::2; correct, but measured slower than one-CTA tiles on B200)."""
     if not 1 <= len(segs) <= 2:
         raise ValueError("one or two K segments")
     g = _lib.DnGemm()
@@ -126,7 +128,7 @@ def gemm(M: int, N: int, segs: Sequence[Tuple[Operand, Operand]], out: torch.Ten
     g.addend, g.addend_dtype = _ptr(addend), _dtype_code(addend)
     g.aux, g.aux_dtype = _ptr(aux), _dtype_code(aux)
     g.pre, g.pre_dtype = _ptr(pre), _dtype_code(pre)
-    g.block_n, g.max_ctas = int(block_n), int(max_ctas)
+    g.block_n, g.max_ctas, g.pair = int(block_n), int(max_ctas), int(pair)
     stream = torch.cuda.current_stream().cuda_stream
     st = None if status is None else status.data_ptr()
     _lib.check("dn_gemm_run", _lib.lib().dn_gemm_run(ctypes.byref(g), st, stream))

@@ -95,13 +95,16 @@ typedef struct dn_gemm {
   int32_t max_ctas; /* 0 = one per SM */
   const float* col_scale;
   const float* row_bias;
+  int32_t pair; /* 0 or 1 = one-CTA tiles; 2 = two-CTA 256 x 256 tiles */
 } dn_gemm;
 
 /* Persistent warp-specialised kernel: a TMA producer warp (128-byte swizzled
  * 128x64 / block_n x64 tiles), one thread issuing tcgen05.mma (M = 128, K =
- * 16 each) into double-buffered tensor-memory accumulators, four epilogue
- * warps.  Bounded waits; a wait that gives up stores DN_ETIMEOUT in *status
- * (status may be NULL). */
+ * 16 each) into double-buffered tensor-memory accumulators, eight epilogue
+ * warps.  Pair mode (pair = 2) runs two-CTA clusters on 256 x 256 tiles
+ * (tcgen05 cta_group::2, M = 256; each CTA loads half the operand bytes).
+ * Bounded waits; a wait that gives up stores DN_ETIMEOUT in *status (status
+ * may be NULL). */
 int32_t dn_gemm_run(const dn_gemm* g, int32_t* status, void* stream);
 
 /* ---- memory-bound helpers of the operator's passes ----------------------

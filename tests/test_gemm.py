@@ -1,8 +1,9 @@
 """The tcgen05 BF16 GEMM against a float64 torch product of the same BF16
 inputs: operand layouts (K-major, MN-major, folded MN-major, shared and
-batched), two K segments, K/M/N tails, every tile width, and the fused
-epilogue (scales, bias, addend, GELU, GELU gradient, accumulate, BF16
-output, index maps)."""
+batched), two K segments, K/M/N tails, every tile width, one-CTA and
+two-CTA (256 x 256 pair) tiles, and the fused epilogue (scales, bias,
+addend, GELU, GELU gradient, accumulate, BF16 output with 32- and 16-byte
+aligned rows, index maps)."""
 
 from __future__ import annotations
 
@@ -176,6 +177,92 @@ def test_scalar_epilogue_path(cuda):
     assert float(out[:, 1:, :].abs().max()) == 0.0
 
 
+@pytest.mark.gpu
+def test_bf16_rows_16_byte_aligned(cuda):
+    # BF16 output rows 272 bytes apart: 16-byte but not 32-byte aligned, so
+    # the epilogue takes its 16-byte store path
+    M, N, K, LD = 200, 128, 96, 136
+    a, b = _bf(M, K, seed=42), _bf(N, K, seed=43)
+    out = torch.zeros(M, LD, dtype=torch.bfloat16, device=cuda)
+    st = _status(cuda)
+    gemm(M, N, [(kmajor(a, M, K), kmajor(b, N, K))], out, OutMap.rowmajor(LD), status=st)
+    torch.cuda.synchronize()
+    _check_status(st)
+    assert _rel(out[:, :N], a.double() @ b.double().T) < TOL_BF16
+    assert float(out[:, N:].abs().max()) == 0.0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("M,N,K,max_ctas", [
+    (300, 200, 200, 0),    # ragged pair tile: the second CTA's rows partly past M
+    (100, 256, 64, 0),     # the second CTA's rows entirely past M
+    (130, 520, 1000, 0),   # N tail inside the second half of B; long K
+    (1100, 700, 576, 4),   # two pairs walk many tiles: both accumulator buffers, ring wraps
+])
+def test_pair_tiles_kmajor(cuda, M, N, K, max_ctas):
+    a, b = _bf(M, K, seed=31), _bf(N, K, seed=32)
+    ref = a.double() @ b.double().T
+    for pair in (1, 2):
+        out = torch.full((M, N), float("nan"), device=cuda)
+        st = _status(cuda)
+        gemm(M, N, [(kmajor(a, M, K), kmajor(b, N, K))], out, OutMap.rowmajor(N), pair=pair,
+             max_ctas=max_ctas, status=st)
+        torch.cuda.synchronize()
+        _check_status(st)
+        assert _rel(out, ref) < TOL_F32, f"pair={pair}"
+
+
+@pytest.mark.gpu
+def test_pair_tiles_mnmajor_and_fold(cuda):
+    M, N, K = 384, 640, 130
+    at, bt = _bf(K, M, seed=33), _bf(K, N, seed=34)
+    out = torch.zeros(M, N, device=cuda)
+    st = _status(cuda)
+    gemm(M, N, [(mnmajor(at, M, K, ld=M), mnmajor(bt, N, K, ld=N))], out, OutMap.rowmajor(N),
+         pair=2, status=st)
+    torch.cuda.synchronize()
+    _check_status(st)
+    assert _rel(out, at.double().T @ bt.double()) < TOL_F32
+    # B[(b, c), hw] = X[b, hw, c] folded by C = 64 channels
+    nb, HW, C, M2 = 7, 200, 64, 300
+    x, a = _bf(nb, HW, C, seed=35), _bf(M2, HW, seed=36)
+    N2 = nb * C
+    out = torch.zeros(M2, N2, device=cuda)
+    gemm(M2, N2, [(kmajor(a, M2, HW), mnmajor(x, N2, HW, ld=C, fold=C, fold_stride=HW * C))],
+         out, OutMap.rowmajor(N2), pair=2, status=st)
+    torch.cuda.synchronize()
+    _check_status(st)
+    B = x.double().permute(0, 2, 1).reshape(N2, HW)
+    assert _rel(out, a.double() @ B.T) < TOL_F32
+
+
+@pytest.mark.gpu
+def test_pair_tiles_segments_batch_epilogue(cuda):
+    # two K segments (K-major A0, MN-major A1), batched A and shared B, the
+    # full epilogue into BF16 with a transposed store
+    Z, M, N, K0, K1 = 3, 320, 288, 192, 64
+    a0, b0 = _bf(Z, M, K0, seed=37), _bf(N, K0, seed=38)
+    a1t, b1 = _bf(Z, K1, M, seed=39), _bf(N, K1, seed=40)
+    g = torch.Generator().manual_seed(41)
+    bias = torch.randn(N, generator=g).to(cuda)
+    rb = torch.randn(M, generator=g).to(cuda)
+    cs = (torch.rand(N, generator=g) + 0.5).to(cuda)
+    bs = (torch.rand(Z, generator=g) + 0.5).to(cuda)
+    acc = torch.einsum("zmk,nk->zmn", a0.double(), b0.double()) \
+        + torch.einsum("zkm,nk->zmn", a1t.double(), b1.double())
+    v = acc * cs.double() * bs.double()[:, None, None] + bias.double() + rb.double()[:, None]
+    y = torch.zeros(Z, N, M, dtype=torch.bfloat16, device=cuda)
+    om = OutMap(batch=N * M, row0=1, col0=M)
+    st = _status(cuda)
+    gemm(M, N, [(kmajor(a0, M, K0, batch_stride=M * K0), kmajor(b0, N, K0)),
+                (mnmajor(a1t, M, K1, ld=M, batch_stride=K1 * M), kmajor(b1, N, K1))],
+         y, om, batch=Z, act=ACT_GELU, bias=bias, row_bias=rb, col_scale=cs, batch_scale=bs,
+         pair=2, status=st)
+    torch.cuda.synchronize()
+    _check_status(st)
+    assert _rel(y.transpose(1, 2), torch.nn.functional.gelu(v)) < TOL_BF16
+
+
 def test_gemm_rejects_bad_arguments():
     """Host-side validation (no GPU work): misaligned strides and mismatched K."""
     L = _lib.lib()
@@ -195,4 +282,9 @@ def test_gemm_rejects_bad_arguments():
     assert L.dn_gemm_run(ctypes.byref(g), None, None) == 1
     g.block_n = 0
     g.accumulate, g.out_dtype = 1, 2  # accumulate into BF16
+    assert L.dn_gemm_run(ctypes.byref(g), None, None) == 1
+    g.accumulate, g.out_dtype = 0, 0
+    g.pair = 3  # not a tile mode
+    assert L.dn_gemm_run(ctypes.byref(g), None, None) == 1
+    g.pair, g.block_n = 2, 64  # pair tiles are 256 wide
     assert L.dn_gemm_run(ctypes.byref(g), None, None) == 1
