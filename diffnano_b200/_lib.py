@@ -149,6 +149,8 @@ SIGNATURES = {
     "dn_gemm_run": (c_int32, [ctypes.POINTER(DnGemm), c_void_p, c_void_p]),
     "dn_fno_features": (c_int32, [c_void_p, c_int64, c_int32, c_int32, ctypes.c_float,
                                   ctypes.c_float, c_void_p, c_void_p]),
+    "dn_fno_lift": (c_int32, [c_void_p, c_void_p, c_void_p, c_int64, c_int64, c_int32,
+                              c_void_p, c_void_p]),
     "dn_fno_features_bwd": (c_int32, [c_void_p, c_int64, ctypes.c_float, ctypes.c_float,
                                       c_void_p, c_void_p]),
     "dn_fno_readout": (c_int32, [c_void_p, c_void_p, c_int64, c_int32, c_int32, c_int32,

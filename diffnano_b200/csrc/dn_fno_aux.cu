@@ -53,6 +53,68 @@ __global__ void k_features_bwd(const float* __restrict__ dfeat, long long n, flo
     deps[i] = dfeat[i * FEAT] * inv_span;
 }
 
+// x0[b, c, p] = bf16(sum_k P[c, k] * feat[b, p, k] + bias[c]) (the lifting
+// layer; K = FEAT = 8).  One thread per 8 consecutive pixels of one sample:
+// the 8 feature rows are read once (128 bytes), then every channel's 8
+// outputs go out as one 16-byte store, so a warp writes 512 contiguous bytes
+// per channel.  The BF16 products are exact in FP32 and are summed in FP32,
+// as the tensor-core path does.  `vec`: n_pix is a multiple of 8.
+template <bool VEC>
+__global__ void k_lift(const unsigned short* __restrict__ feat,
+                       const unsigned short* __restrict__ P, const float* __restrict__ bias,
+                       long long nb, long long n_pix, int C, unsigned short* __restrict__ x0) {
+  extern __shared__ float s_lift[];  // P as FP32 (C x FEAT), then bias (C)
+  for (int e = threadIdx.x; e < C * FEAT; e += blockDim.x) s_lift[e] = bf2f(P[e]);
+  for (int e = threadIdx.x; e < C; e += blockDim.x) s_lift[C * FEAT + e] = bias[e];
+  __syncthreads();
+  const long long groups = (n_pix + 7) / 8;
+  const long long n = nb * groups;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long b = i / groups;
+    const long long p0 = (i % groups) * 8;
+    const int np = (int)(n_pix - p0 < 8 ? n_pix - p0 : 8);
+    float f[8][FEAT];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      uint4 u = make_uint4(0u, 0u, 0u, 0u);
+      if (q < np) u = reinterpret_cast<const uint4*>(feat)[b * n_pix + p0 + q];
+      const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        f[q][2 * e] = __uint_as_float(w[e] << 16);
+        f[q][2 * e + 1] = __uint_as_float(w[e] & 0xFFFF0000u);
+      }
+    }
+    unsigned short* out = x0 + b * (long long)C * n_pix + p0;
+    for (int c = 0; c < C; ++c) {
+      const float* pc = s_lift + c * FEAT;
+      const float bc = s_lift[C * FEAT + c];
+      float v[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        float acc = 0.0f;
+#pragma unroll
+        for (int k = 0; k < FEAT; ++k) acc = fmaf(pc[k], f[q][k], acc);
+        v[q] = acc + bc;
+      }
+      unsigned short* o = out + (long long)c * n_pix;
+      if (VEC) {
+        uint4 u;
+        u.x = (uint32_t)f2bf(v[0]) | ((uint32_t)f2bf(v[1]) << 16);
+        u.y = (uint32_t)f2bf(v[2]) | ((uint32_t)f2bf(v[3]) << 16);
+        u.z = (uint32_t)f2bf(v[4]) | ((uint32_t)f2bf(v[5]) << 16);
+        u.w = (uint32_t)f2bf(v[6]) | ((uint32_t)f2bf(v[7]) << 16);
+        *reinterpret_cast<uint4*>(o) = u;
+      } else {
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+          if (q < np) o[q] = f2bf(v[q]);
+      }
+    }
+  }
+}
+
 // out[b, w, c] = sum_h r[h, c] * x[b, c, h, w]; one thread per (b, c, w)
 // (x channel-first, out channel-last)
 __global__ void k_readout(const unsigned short* __restrict__ x, const float* __restrict__ r,
@@ -328,6 +390,25 @@ extern "C" int32_t dn_fno_features_bwd(const float* dfeat, int64_t n_pix, float 
   if (!dfeat || !deps || n_pix < 1 || !(eps_hi > eps_lo)) return DN_EINVAL;
   k_features_bwd<<<grid_for(n_pix), 256, 0, static_cast<cudaStream_t>(stream)>>>(
       dfeat, n_pix, 1.0f / (eps_hi - eps_lo), deps);
+  DN_CUDA_CHECK(cudaGetLastError());
+  return DN_OK;
+}
+
+extern "C" int32_t dn_fno_lift(const void* feat, const void* P, const float* bias, int64_t nb,
+                               int64_t n_pix, int32_t C, void* x0, void* stream) {
+  if (!feat || !P || !bias || !x0 || nb < 1 || n_pix < 1 || C < 1 || C > 1024 || !al16(feat) ||
+      !al16(x0))
+    return DN_EINVAL;
+  const long long n = nb * ((n_pix + 7) / 8);
+  const size_t smem = (size_t)C * (FEAT + 1) * sizeof(float);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const auto* fp = static_cast<const unsigned short*>(feat);
+  const auto* pp = static_cast<const unsigned short*>(P);
+  auto* xp = static_cast<unsigned short*>(x0);
+  if (n_pix % 8 == 0)
+    k_lift<true><<<grid_for(n), 256, smem, s>>>(fp, pp, bias, nb, n_pix, C, xp);
+  else
+    k_lift<false><<<grid_for(n), 256, smem, s>>>(fp, pp, bias, nb, n_pix, C, xp);
   DN_CUDA_CHECK(cudaGetLastError());
   return DN_OK;
 }

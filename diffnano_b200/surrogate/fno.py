@@ -303,10 +303,10 @@ class FNO2d:
         _lib.check("dn_fno_features", L.dn_fno_features(
             _c(eps), B, c.H, c.W, c.eps_lo, c.eps_hi, _c(ws["feat"]), s))
         X = ws["X"]
-        # lift, per sample X0[c, hw] = P feat^T + p (channel-first rows)
-        gemm(C, HW, [(kmajor(ps.B("P"), C, FEAT),
-                      kmajor(ws["feat"], HW, FEAT, batch_stride=HW * FEAT))],
-             X[0], OutMap.rowmajor(HW, batch=C * HW), batch=B, row_bias=ps.P("p"), status=st)
+        # lift, per sample X0[c, hw] = P feat^T + p (channel-first rows): a
+        # K = 8 contraction, so a memory-bound kernel rather than a GEMM
+        _lib.check("dn_fno_lift", L.dn_fno_lift(
+            _c(ws["feat"]), _c(ps.B("P")), _c(ps.P("p")), B, HW, C, _c(X[0]), s))
         zmap = OutMap(row_radix=NM, row0=B * 2 * C, row1=C, col_radix=C, col0=1, col1=2 * C)
         for l in range(c.layers):
             # truncated DFT of every (sample, channel) row: Zm[m, b, (ri, c)]

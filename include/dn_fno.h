@@ -120,6 +120,15 @@ int32_t dn_fno_features(const float* eps, int64_t n_img, int32_t H, int32_t W, f
 int32_t dn_fno_features_bwd(const float* dfeat, int64_t n_pix, float eps_lo, float eps_hi,
                             float* deps, void* stream);
 
+/* The lifting layer: x0[b, c, p] = sum_k P[c, k] * feat[b, p, k] + bias[c]
+ * (feat (nb, n_pix, 8) and P (C, 8) BF16, bias FP32, x0 (nb, C, n_pix) BF16;
+ * FP32 sums of the exact BF16 products, as the tensor-core GEMM forms them).
+ * A memory-bound kernel in place of a K = 8 GEMM.  feat, x0 16-byte aligned;
+ * C <= 1024.  Replaces the input layer of the reference network
+ * (diffnano/solvers/surrogate.py:62-72, _SurrogateNet.forward). */
+int32_t dn_fno_lift(const void* feat, const void* P, const float* bias, int64_t nb,
+                    int64_t n_pix, int32_t C, void* x0, void* stream);
+
 /* out[b, w, c] = sum_h r[h, c] * x[b, c, h, w]   (x, out BF16; r FP32 (H, C)) */
 int32_t dn_fno_readout(const void* x, const float* r, int64_t nb, int32_t H, int32_t W,
                        int32_t C, void* out, void* stream);

@@ -125,3 +125,38 @@ def test_fno_odd_batch_matches_even(cuda):
     net.check_status()
     assert torch.equal(odd, full[:3])
     assert torch.equal(one[0], full[2])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n_pix", [16384, 1003])
+def test_lift_kernel_matches_lift_gemm(cuda, n_pix):
+    """dn_fno_lift (the lifting layer as a memory-bound kernel) against the
+    same contraction run as a K = 8 tensor-core GEMM with a row bias: equal up
+    to one BF16 rounding step (the FP32 sums may be formed in another order);
+    n_pix = 1003 takes the per-element store path."""
+    from diffnano_b200 import _lib
+    from diffnano_b200.surrogate.gemm import OutMap, gemm, kmajor
+
+    nb, C, FEAT = 5, 64, 8
+    g = torch.Generator().manual_seed(7)
+    feat = torch.randn(nb, n_pix, FEAT, generator=g).to(torch.bfloat16).to(cuda)
+    P = torch.randn(C, FEAT, generator=g).to(torch.bfloat16).to(cuda)
+    bias = torch.randn(C, generator=g).to(cuda)
+    x_kernel = torch.full((nb, C, n_pix), float("nan"), dtype=torch.bfloat16, device=cuda)
+    x_gemm = torch.empty_like(x_kernel)
+    s = torch.cuda.current_stream().cuda_stream
+    _lib.check("dn_fno_lift", _lib.lib().dn_fno_lift(
+        feat.data_ptr(), P.data_ptr(), bias.data_ptr(), nb, n_pix, C, x_kernel.data_ptr(), s))
+    gemm(C, n_pix, [(kmajor(P, C, FEAT), kmajor(feat, n_pix, FEAT, batch_stride=n_pix * FEAT))],
+         x_gemm, OutMap.rowmajor(n_pix, batch=C * n_pix), batch=nb, row_bias=bias)
+    torch.cuda.synchronize()
+    ref = torch.einsum("ck,bpk->bcp", P.double(), feat.double()) + bias.double()[None, :, None]
+    mag = torch.einsum("ck,bpk->bcp", P.double().abs(), feat.double().abs()) \
+        + bias.double().abs()[None, :, None]
+    # half a BF16 step of the result (2^-8 relative) plus FP32 summation
+    # error of 9 terms, with a margin
+    bound = 1.01 * 2.0 ** -8 * ref.abs() + 2.0 ** -18 * mag
+    for name, x in (("kernel", x_kernel), ("gemm", x_gemm)):
+        d = (x.double() - ref).abs()
+        assert bool((d <= bound).all()), (name, float((d / bound).max()))
+    assert rel_l2(x_kernel.double(), x_gemm.double()) < 1e-3
