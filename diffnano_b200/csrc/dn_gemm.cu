@@ -259,12 +259,29 @@ __device__ __forceinline__ uint32_t idesc(int a_mn, int b_mn) {
          ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(TILE_M >> 4) << 24);
 }
 
+// GELU in its tanh form (Hendrycks & Gimpel 2016):
+//   gelu(v) = v/2 (1 + tanh(u)),  u = sqrt(2/pi) (v + 0.044715 v^3)
+//   gelu'(v) = (1 + t)/2 + v/2 (1 - t^2) sqrt(2/pi) (1 + 3 * 0.044715 v^2),  t = tanh(u)
+// with the hardware tanh (tanh.approx.f32, ~2^-11 relative error, far below
+// the BF16 rounding of the activations).  The transform GEMMs of the
+// operator are bound by epilogue instructions; this form costs a few FMAs
+// and one special-function op per element.
+constexpr float GELU_K0 = 0.7978845608028654f;  // sqrt(2/pi)
+constexpr float GELU_K1 = 0.044715f;
+__device__ __forceinline__ float tanh_hw(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
 __device__ __forceinline__ float gelu_f(float v) {
-  return 0.5f * v * (1.0f + erff(v * 0.70710678118654752f));
+  const float t = tanh_hw(GELU_K0 * fmaf(GELU_K1 * v * v, v, v));
+  return 0.5f * fmaf(v, t, v);
 }
 __device__ __forceinline__ float gelu_grad_f(float v) {
-  return 0.5f * (1.0f + erff(v * 0.70710678118654752f)) +
-         v * 0.39894228040143268f * expf(-0.5f * v * v);
+  const float v2 = v * v;
+  const float t = tanh_hw(GELU_K0 * fmaf(GELU_K1 * v2, v, v));
+  const float du = GELU_K0 * fmaf(3.0f * GELU_K1, v2, 1.0f);
+  return 0.5f * fmaf(v * fmaf(-t, t, 1.0f), du, 1.0f + t);
 }
 
 __device__ __forceinline__ float bf2f(unsigned short h) {

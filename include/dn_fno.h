@@ -29,7 +29,7 @@ extern "C" {
 #define DN_BF16 2 /* element type code next to DN_F32 / DN_F64 */
 
 #define DN_ACT_NONE 0
-#define DN_ACT_GELU 1      /* y = gelu(v) (erf form); `pre` (optional) receives v */
+#define DN_ACT_GELU 1      /* y = gelu(v) (tanh form); `pre` (optional) receives v */
 #define DN_ACT_GELU_GRAD 2 /* y = v * gelu'(aux), aux = the pre-activation       */
 
 /* One BF16 operand of C = A * B^T.  Element (r, k), r the row index (M for A,

@@ -10,7 +10,7 @@ with mse_loss and Adam, ``:128, 193-197``), so there is no reference output to
 pin.  This module restates the published 2-D Fourier neural operator (Li et
 al., "Fourier Neural Operator for Parametric Partial Differential Equations",
 ICLR 2021: lift, spectral convolution over the low rfft2 modes with complex
-per-mode channel weights plus a pointwise linear path, GELU, projection) with
+per-mode channel weights plus a pointwise linear path, GELU (tanh form), projection) with
 the parameter layout of ``diffnano_b200.surrogate.fno`` and this project's
 row readout, in FP32 with ``torch.fft.rfft2`` / ``irfft2`` on the CPU;
 gradients come from torch autograd.  It shares no code with the GPU path: the
@@ -58,9 +58,9 @@ def forward(params: Dict[str, torch.Tensor], eps: torch.Tensor, *, layers: int, 
     for l in range(layers):
         pre = spectral(X, params[f"wre{l}"], params[f"wim{l}"], modes) \
             + X @ params[f"W{l}"].T + params[f"b{l}"]
-        X = F.gelu(pre) if l < layers - 1 else pre
+        X = F.gelu(pre, approximate="tanh") if l < layers - 1 else pre
     R = torch.einsum("bhwc,hc->bwc", X, params["r"])
-    U = F.gelu(R @ params["Q1"].T + params["q1"])
+    U = F.gelu(R @ params["Q1"].T + params["q1"], approximate="tanh")
     return U @ params["Q2"][:n_out].T + params["q2"][:n_out]
 
 

@@ -153,14 +153,14 @@ def test_epilogue_chain(cuda):
          batch_scale=bs, addend=addend, pre=pre)
     torch.cuda.synchronize()
     assert _rel(pre, v) < TOL_BF16
-    assert _rel(y, torch.nn.functional.gelu(v)) < TOL_BF16
+    assert _rel(y, torch.nn.functional.gelu(v, approximate="tanh")) < TOL_BF16
     # gradient form, accumulated onto an FP32 output
     base = torch.randn(Z, M, N, generator=g).to(cuda)
     out = base.clone()
     gemm(M, N, ops, out, om, batch=Z, act=ACT_GELU_GRAD, aux=pre, accumulate=True)
     torch.cuda.synchronize()
     x = pre.double().requires_grad_(True)
-    gp, = torch.autograd.grad(torch.nn.functional.gelu(x).sum(), x)
+    gp, = torch.autograd.grad(torch.nn.functional.gelu(x, approximate="tanh").sum(), x)
     assert _rel(out, base.double() + acc * gp) < 1e-5
 
 
@@ -260,7 +260,7 @@ def test_pair_tiles_segments_batch_epilogue(cuda):
          pair=2, status=st)
     torch.cuda.synchronize()
     _check_status(st)
-    assert _rel(y.transpose(1, 2), torch.nn.functional.gelu(v)) < TOL_BF16
+    assert _rel(y.transpose(1, 2), torch.nn.functional.gelu(v, approximate="tanh")) < TOL_BF16
 
 
 def test_gemm_rejects_bad_arguments():
