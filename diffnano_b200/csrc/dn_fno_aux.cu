@@ -240,6 +240,47 @@ __global__ void k_modes_rows(const unsigned short* __restrict__ src, unsigned sh
   }
 }
 
+// The same permutation on 64 x 64 tiles with two elements (4 bytes) per lane
+// on both sides, so a warp moves 128 contiguous bytes per instruction (the
+// 32 x 32 kernel above moves 64).  nm and C even, pointers 4-byte aligned.
+// Shared tile rows of 66 elements: the 4-byte stores of the read side are
+// aligned and conflict-free; the 2-byte loads of the write side conflict at
+// most 2-way.
+__global__ void k_modes_rows64(const unsigned short* __restrict__ src,
+                               unsigned short* __restrict__ dst, int nm, long long nb, int C,
+                               int to_rows) {
+  __shared__ __align__(16) unsigned short tile[64][66];
+  const long long br = blockIdx.z;
+  const long long b = br >> 1;
+  const int r = (int)(br & 1);
+  const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+  // tile rows are the source's rows (m when to_rows, else c; grid x), tile
+  // columns the other index (grid y)
+  const int a0 = blockIdx.x * 64;  // source row index base
+  const int e0 = blockIdx.y * 64;  // source column index base
+  const int na = to_rows ? nm : C, ne = to_rows ? C : nm;
+  for (int k = ty; k < 64; k += 8) {
+    const int a = a0 + k, e = e0 + 2 * tx;
+    uint32_t u = 0u;
+    if (a < na && e < ne) {
+      const long long off = to_rows ? ((a * nb + b) * 2 + r) * (long long)C + e
+                                    : ((b * C + a) * 2 + r) * (long long)nm + e;
+      u = *reinterpret_cast<const uint32_t*>(src + off);
+    }
+    *reinterpret_cast<uint32_t*>(&tile[k][2 * tx]) = u;
+  }
+  __syncthreads();
+  for (int k = ty; k < 64; k += 8) {
+    const int e = e0 + k, a = a0 + 2 * tx;  // destination row e, columns a, a+1
+    if (e < ne && a < na) {
+      const uint32_t u = (uint32_t)tile[2 * tx][k] | ((uint32_t)tile[2 * tx + 1][k] << 16);
+      const long long off = to_rows ? ((b * C + e) * 2 + r) * (long long)nm + a
+                                    : ((e * nb + b) * 2 + r) * (long long)C + a;
+      *reinterpret_cast<uint32_t*>(dst + off) = u;
+    }
+  }
+}
+
 // column sums, pass 1: block (bx, by) sums rows [by*rpb, (by+1)*rpb) of
 // columns bx*256 + threadIdx.x into part[by, col]
 __global__ void k_colsum_part(const void* __restrict__ in, int bf16, long long rows,
@@ -261,13 +302,25 @@ __global__ void k_colsum_part(const void* __restrict__ in, int bf16, long long r
 }
 
 // pass 2: out[col] (+)= sum over the parts, in order
+// pass 2: block (32 x 8) per 32 columns; warp w sums partial rows w, w+8,
+// w+16, ... of its lane's column, then the 8 warp sums are added in warp
+// order (fixed partition and order: deterministic)
 __global__ void k_colsum_final(const float* __restrict__ part, long long nparts, long long cols,
                                float* __restrict__ out, int accumulate) {
-  const long long col = blockIdx.x * 256LL + threadIdx.x;
-  if (col >= cols) return;
+  __shared__ float s_w[8][33];
+  const long long col = blockIdx.x * 32LL + threadIdx.x;
+  const int w = threadIdx.y;
   float s = 0.0f;
-  for (long long q = 0; q < nparts; ++q) s += part[q * cols + col];
-  out[col] = accumulate ? out[col] + s : s;
+  if (col < cols)
+    for (long long q = w; q < nparts; q += 8) s += part[q * cols + col];
+  s_w[w][threadIdx.x] = s;
+  __syncthreads();
+  if (w == 0 && col < cols) {
+    float t = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) t += s_w[k][threadIdx.x];
+    out[col] = accumulate ? out[col] + t : t;
+  }
 }
 
 // MSE over the first `used` of `ld` columns; grad = scale * 2 (pred - target)
@@ -455,8 +508,8 @@ extern "C" int32_t dn_colsum(const void* in, int32_t dtype, int64_t rows, int64_
   const dim3 g1((unsigned)((cols + 255) / 256), (unsigned)nparts);
   k_colsum_part<<<g1, 256, 0, s>>>(in, dtype == DN_BF16, rows, cols, ld, rpb, scratch);
   DN_CUDA_CHECK(cudaGetLastError());
-  k_colsum_final<<<(unsigned)((cols + 255) / 256), 256, 0, s>>>(scratch, nparts, cols, out,
-                                                                  accumulate);
+  k_colsum_final<<<(unsigned)((cols + 31) / 32), dim3(32, 8), 0, s>>>(scratch, nparts, cols, out,
+                                                                        accumulate);
   DN_CUDA_CHECK(cudaGetLastError());
   return DN_OK;
 }
@@ -519,6 +572,17 @@ extern "C" int32_t dn_fno_modes_rows(const void* src, void* dst, int32_t n_modes
                                      int32_t C, int32_t to_rows, void* stream) {
   if (!src || !dst || src == dst || n_modes < 1 || nb < 1 || C < 1) return DN_EINVAL;
   if (nb * 2 > 65535) return DN_EUNSUPPORTED;
+  if (n_modes % 2 == 0 && C % 2 == 0 && (reinterpret_cast<uintptr_t>(src) & 3) == 0 &&
+      (reinterpret_cast<uintptr_t>(dst) & 3) == 0) {
+    // grid x covers the source rows, y the source columns
+    const int na = to_rows ? n_modes : C, ne = to_rows ? C : n_modes;
+    const dim3 g64((unsigned)((na + 63) / 64), (unsigned)((ne + 63) / 64), (unsigned)(nb * 2));
+    k_modes_rows64<<<g64, dim3(32, 8), 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const unsigned short*>(src), static_cast<unsigned short*>(dst), n_modes, nb,
+        C, to_rows != 0);
+    DN_CUDA_CHECK(cudaGetLastError());
+    return DN_OK;
+  }
   const dim3 grid((unsigned)((n_modes + 31) / 32), (unsigned)((C + 31) / 32), (unsigned)(nb * 2));
   k_modes_rows<<<grid, dim3(32, 8), 0, static_cast<cudaStream_t>(stream)>>>(
       static_cast<const unsigned short*>(src), static_cast<unsigned short*>(dst), n_modes, nb, C,
@@ -537,7 +601,7 @@ extern "C" int32_t dn_fno_channel_sums(const void* x, int64_t nb, int32_t C, int
   k_channel_part<<<dim3((unsigned)C, (unsigned)parts), 256, 0, s>>>(
       static_cast<const unsigned short*>(x), nb, C, n_pix, scratch);
   DN_CUDA_CHECK(cudaGetLastError());
-  k_colsum_final<<<(unsigned)((C + 255) / 256), 256, 0, s>>>(scratch, parts, C, out, 0);
+  k_colsum_final<<<(unsigned)((C + 31) / 32), dim3(32, 8), 0, s>>>(scratch, parts, C, out, 0);
   DN_CUDA_CHECK(cudaGetLastError());
   return DN_OK;
 }

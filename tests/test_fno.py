@@ -160,3 +160,60 @@ def test_lift_kernel_matches_lift_gemm(cuda, n_pix):
         d = (x.double() - ref).abs()
         assert bool((d <= bound).all()), (name, float((d / bound).max()))
     assert rel_l2(x_kernel.double(), x_gemm.double()) < 1e-3
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nm,nb,C", [(512, 4, 64), (130, 3, 70), (7, 2, 5)])
+def test_modes_rows_permutation(cuda, nm, nb, C):
+    """dn_fno_modes_rows both ways against torch's permute, bit for bit: the
+    64 x 64 two-element kernel (even sizes, ragged tiles) and the 32 x 32 one
+    (odd sizes)."""
+    from diffnano_b200 import _lib
+
+    g = torch.Generator().manual_seed(3)
+    modes = torch.randn(nm, nb, 2, C, generator=g).to(torch.bfloat16).to(cuda)
+    rows = torch.empty(nb, C, 2, nm, dtype=torch.bfloat16, device=cuda)
+    back = torch.empty_like(modes)
+    s = torch.cuda.current_stream().cuda_stream
+    L = _lib.lib()
+    _lib.check("dn_fno_modes_rows", L.dn_fno_modes_rows(
+        modes.data_ptr(), rows.data_ptr(), nm, nb, C, 1, s))
+    _lib.check("dn_fno_modes_rows", L.dn_fno_modes_rows(
+        rows.data_ptr(), back.data_ptr(), nm, nb, C, 0, s))
+    torch.cuda.synchronize()
+    assert torch.equal(rows, modes.permute(1, 3, 2, 0))
+    assert torch.equal(back, modes)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rows,cols,bf16", [(32768, 6, True), (256, 4096, False), (1000, 37, False)])
+def test_colsum_matches_torch(cuda, rows, cols, bf16):
+    """dn_colsum (two-pass deterministic column sums) against an FP64 sum,
+    overwrite and accumulate, and bit-identical on a repeat."""
+    from diffnano_b200 import _lib
+
+    L = _lib.lib()
+    g = torch.Generator().manual_seed(11)
+    x = torch.randn(rows, cols + 3, generator=g)
+    x = x.to(torch.bfloat16) if bf16 else x
+    x = x.to(cuda)
+    n_scr = int(L.dn_colsum_scratch_elems(rows, cols))
+    scratch = torch.empty(n_scr, device=cuda)
+    out = torch.full((cols,), 5.0, device=cuda)
+    s = torch.cuda.current_stream().cuda_stream
+    dt = 2 if bf16 else 0
+
+    def run(acc):
+        _lib.check("dn_colsum", L.dn_colsum(x.data_ptr(), dt, rows, cols, cols + 3, out.data_ptr(),
+                                            acc, scratch.data_ptr(), n_scr, s))
+
+    run(0)
+    first = out.clone()
+    run(0)
+    torch.cuda.synchronize()
+    ref = x[:, :cols].double().sum(0)
+    assert torch.equal(first, out)
+    assert rel_l2(out.double(), ref) < 1e-6
+    run(1)
+    torch.cuda.synchronize()
+    assert rel_l2(out.double(), 2 * ref) < 1e-6
