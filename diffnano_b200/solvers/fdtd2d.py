@@ -25,7 +25,7 @@ from diffnano_b200.solvers._common import (
     monitor_metadata,
     parse_monitors,
 )
-from diffnano_b200.solvers._engine import Engine, compute_device
+from diffnano_b200.solvers._engine import Engine, compute_device, to_result_device
 from diffnano_b200.solvers._result import SimResult
 
 __all__ = ["FDTDSolver2D"]
@@ -134,8 +134,9 @@ class FDTDSolver2D:
         meta = {"polarization": self.polarization, "n_steps": self.n_steps, "dt": self.dt,
                 "courant": self.courant, "snapshots": snapshots}
         if eng.monitors:
-            meta["monitors"] = monitor_metadata(eng, [d.to(out_dev) for d in dfts])
-        return SimResult(field=field.unsqueeze(0).to(out_dev), wavelengths=wl, metadata=meta)
+            meta["monitors"] = monitor_metadata(eng, [to_result_device(d, out_dev) for d in dfts])
+        return SimResult(field=to_result_device(field.unsqueeze(0), out_dev), wavelengths=wl,
+                         metadata=meta)
 
     def _cluster_solve(self, eps, src, eng):
         """Gradient-free solve with the whole grid in one thread-block cluster

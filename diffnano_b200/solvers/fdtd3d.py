@@ -25,7 +25,7 @@ from diffnano_b200.solvers._common import (
     monitor_metadata,
     parse_monitors,
 )
-from diffnano_b200.solvers._engine import Engine, compute_device
+from diffnano_b200.solvers._engine import Engine, compute_device, to_result_device
 from diffnano_b200.solvers._result import SimResult
 
 __all__ = ["FDTDSolver3D"]
@@ -135,8 +135,10 @@ class FDTDSolver3D:
         if self.backward == "time_reversal":
             meta["backward"] = "time_reversal"
         if eng.monitors:
-            meta["monitors"] = monitor_metadata(eng, [d.to(self._device) for d in dfts])
-        return SimResult(field=field.to(self._device), wavelengths=wl, metadata=meta)
+            meta["monitors"] = monitor_metadata(
+                eng, [to_result_device(d, self._device) for d in dfts])
+        return SimResult(field=to_result_device(field, self._device), wavelengths=wl,
+                         metadata=meta)
 
     def time_series(self, eps_r: torch.Tensor, probe: tuple[int, int, int],
                     source: dict | None = None, n_steps: int | None = None) -> torch.Tensor:
