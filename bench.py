@@ -261,12 +261,17 @@ def run_ours(args):
     D, H, W = SHAPE
     cells = D * H * W
     K, Wm = args.steps, args.warmup
-    n_total = max(T_SOLVE, K + Wm)
+    # The timed window sits in the middle of a T_SOLVE-step solve: once the pulse
+    # fills the grid the board draws ~950 W and the power cap lowers the clocks,
+    # so steps on a still mostly zero field are a few percent faster than the
+    # solve's average.  Untimed pre-roll steps bring the state there first.
+    preroll = max(0, (T_SOLVE - K) // 2 - Wm)
+    n_total = max(T_SOLVE, preroll + Wm + K)
     solver = dn.FDTDSolver3D(grid_shape=SHAPE, dl=DL, wavelength_nm=1550.0, pml_layers=PML,
                              n_steps=n_total, courant=COURANT, device=dev, dtype=torch.float32)
     eng = solver._make_engine(n_total, src, mons)
     eng.set_eps(eps.to(dev))
-    eng.run(0, Wm)
+    eng.run(0, preroll + Wm)
     torch.cuda.synchronize(dev)
     stream = torch.cuda.current_stream(dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -274,7 +279,7 @@ def run_ours(args):
     torch.cuda.synchronize(dev)
     with ClockSampler(local) as cs:
         e0.record(stream)
-        eng.run(Wm, K)
+        eng.run(preroll + Wm, K)
         e1.record(stream)
         torch.cuda.synchronize(dev)
     barrier(ws)
@@ -373,7 +378,7 @@ def run_ours(args):
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K,
                 "warmup": Wm, "ms_per_step": el_max / K * 1e3, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": config_dict(),
+                "config": config_dict({"timed_steps": [preroll + Wm, preroll + Wm + K]}),
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic,
                              "peak_source": f"hbm_gbs of {peak_kind}",
