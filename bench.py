@@ -691,6 +691,70 @@ def run_fdtd2d(args):
     return 0
 
 
+def run_fdtd3d_phases(args):
+    """Diagnostics of the 3-D workload (no bench line): per-step time over 500-step
+    segments of a 4000-step solve, continuing vs restarting each segment from the
+    zero state, and the phases of one host-in / host-out FDTDSolver3D solve."""
+    import diffnano_b200 as dn
+    from diffnano_b200.solvers._adjoint import run_forward
+
+    dev = torch.device("cuda", 0)
+    eps, src, mons = workload()
+    solver = dn.FDTDSolver3D(grid_shape=SHAPE, dl=DL, wavelength_nm=1550.0, pml_layers=PML,
+                             n_steps=T_SOLVE, courant=COURANT, device=dev, dtype=torch.float32)
+    eng = solver._make_engine(T_SOLVE, dict(src), mons)
+    eng.set_eps(eps.to(dev))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    seg = 500
+    out = {"segment_steps": seg}
+    for mode in ("continue", "restart_each"):
+        eng.reset()
+        t, times = 0, []
+        for _ in range(T_SOLVE // seg):
+            if mode == "restart_each":
+                eng.reset()
+                t = 0
+            torch.cuda.synchronize(dev)
+            e0.record()
+            eng.run(t, seg)
+            e1.record()
+            torch.cuda.synchronize(dev)
+            times.append(round(e0.elapsed_time(e1) / seg, 4))
+            t += seg
+        out[f"ms_per_step_{mode}"] = times
+    eng.check_status()
+    del eng
+    torch.cuda.empty_cache()
+
+    def tick():
+        torch.cuda.synchronize(dev)
+        return time.perf_counter()
+
+    host = dn.FDTDSolver3D(grid_shape=SHAPE, dl=DL, wavelength_nm=1550.0, pml_layers=PML,
+                           n_steps=T_SOLVE, courant=COURANT, device="cpu", dtype=torch.float32)
+    ep = eps.to(torch.float32).pin_memory()
+    host.forward(ep, source=dict(src), monitors=mons)  # warm-up
+    t0 = tick()
+    host.forward(ep, source=dict(src), monitors=mons)
+    out["host_forward_s"] = round(tick() - t0, 4)
+    t0 = tick()
+    eng = host._make_engine(T_SOLVE, dict(src), mons)
+    out["engine_setup_s"] = round(tick() - t0, 4)
+    t0 = tick()
+    field, _ = run_forward(host, eng, host._prep_eps(ep), ("Ez", "Ex", "Ey"))
+    out["solve_s"] = round(tick() - t0, 4)
+    t0 = tick()
+    field.to("cpu")
+    out["field_to_pageable_host_s"] = round(tick() - t0, 4)
+    pinned = torch.empty(field.shape, dtype=field.dtype, pin_memory=True)
+    t0 = tick()
+    pinned.copy_(field, non_blocking=True)
+    out["field_to_pinned_host_s"] = round(tick() - t0, 4)
+    out["field_bytes"] = field.numel() * field.element_size()
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def run_gemm(args):
     """tcgen05 BF16 GEMM alone: a square GEMM and the operator's transform shape."""
     from diffnano_b200.surrogate.gemm import OutMap, gemm, kmajor
@@ -791,7 +855,7 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-grad-e2e", action="store_true")
     ap.add_argument("--workload", choices=["fdtd3d", "fdtd2d", "batch2d", "fno", "design",
-                                           "gemm", "fno-step"],
+                                           "gemm", "fno-step", "fdtd3d-phases"],
                     default="fdtd3d",
                     help="fdtd3d: the benchmark (3-D 256^3); batch2d: 64 ragged 2-D instances; "
                          "fno: surrogate data generation + training; design: 3-D inverse "
@@ -826,6 +890,8 @@ def main():
         return run_fno(args)
     if args.workload == "design":
         return run_design(args)
+    if args.workload == "fdtd3d-phases":
+        return run_fdtd3d_phases(args)
     if args.workload == "gemm":
         return run_gemm(args)
     if args.workload == "fdtd2d":
