@@ -19,6 +19,7 @@ DN_F32, DN_F64 = 0, 1
 DN_EX, DN_EY, DN_EZ, DN_HX, DN_HY, DN_HZ = range(6)
 DN_NONE = -1
 DN_TM, DN_TE = 0, 1
+DN_CLUSTER_DOUBLE_BUFFERED = 0x100  # flag in dn_batch2d_cluster_size's result
 DN_AXES_REFERENCE, DN_AXES_PHYSICAL = 0, 1
 DN_MAX_MONITORS = 4
 DN_MAX_FREQS = 16

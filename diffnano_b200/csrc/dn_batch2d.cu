@@ -783,6 +783,256 @@ __global__ void __launch_bounds__(512, 1) k_batch2d_cluster(unsigned char* table
 }
 
 // ---------------------------------------------------------------------------
+// Double-buffered cluster solve: every field has two band buffers; step n
+// reads buffer n & 1 and writes the other.  The one row of the other
+// half-step's field that comes from a neighbouring band (TM: Hy of the row
+// above the band; TE: Ey of the row below it) is recomputed here from the
+// neighbour's unchanged input buffers with the neighbour's own arithmetic, so
+// the two half-steps need only a CTA barrier between them and each step one
+// cluster barrier (the in-place kernel above needs two).  Twice the field
+// shared memory: used when the grid fits, else the in-place kernel.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct BandDB {
+  // buffer k of the fields at fld + (3k + {0, 1, 2}) * n: the injected field
+  // (Ez / Hz), Hx / Ex, Hy / Ey, rows x W each (pointer arithmetic, not an
+  // array indexed by the step parity, keeps the view in registers)
+  T* fld;
+  long long n;
+  __device__ __forceinline__ T* f(int k) const { return fld + (3 * k) * n; }
+  __device__ __forceinline__ T* a(int k) const { return fld + (3 * k + 1) * n; }
+  __device__ __forceinline__ T* b(int k) const { return fld + (3 * k + 2) * n; }
+  T* ce;    // dt / eps
+  T* bx;    // W
+  T* gx;    // W
+  T* by;    // rows
+  T* gy;    // rows
+  T* halo;  // W: the neighbour-row value of the second half-step
+};
+
+__host__ __device__ inline long long band_elems_db(long long rows, long long W) {
+  return 7 * rows * W + 3 * W + 2 * rows;
+}
+
+template <typename T>
+__device__ __forceinline__ BandDB<T> band_layout_db(unsigned char* smem, int rows, int W) {
+  BandDB<T> s;
+  T* p = reinterpret_cast<T*>(smem);
+  const long long n = (long long)rows * W;
+  s.fld = p;
+  s.n = n;
+  s.ce = p + 6 * n;
+  s.bx = p + 7 * n;
+  s.gx = s.bx + W;
+  s.by = s.gx + W;
+  s.gy = s.by + rows;
+  s.halo = s.gy + rows;
+  return s;
+}
+
+template <typename T, int POL, int CL>
+__global__ void __launch_bounds__(512, 1) k_batch2d_cluster_db(unsigned char* table) {
+  extern __shared__ __align__(16) unsigned char c_smem[];
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank();
+  const TableView v = view(table);
+  const dn_batch2d_inst* Ip = v.inst + blockIdx.x / CL;
+  const int H = Ip->H, W = Ip->W, T_steps = Ip->n_steps;
+  const long long py = Ip->pitch;
+  const T dt = static_cast<T>(Ip->dt), idl = static_cast<T>(1.0 / Ip->dl);
+  const bool src = Ip->src_comp >= 0, mon = Ip->mon_comp >= 0;
+  const dn_box sb = Ip->src_box, mb = Ip->mon_box;
+  const int nfq = Ip->n_freq;
+  const double* __restrict__ phase = Ip->phase;
+  double* __restrict__ accb = Ip->acc;
+  const T* __restrict__ wave = static_cast<const T*>(Ip->wave);
+  const double* pb0 = Ip->b[0];
+  const double* pb1 = Ip->b[1];
+  const double* pc0 = Ip->c[0];
+  const double* pc1 = Ip->c[1];
+  const T* __restrict__ ceg = static_cast<const T*>(Ip->ce);
+  T* const* outp = reinterpret_cast<T* const*>(Ip->f[T_steps & 1]);
+  T* const o0 = outp[0];
+  T* const o1 = outp[1];
+  T* const o2 = outp[2];
+  const int rows = (H + CL - 1) / CL;
+  const int r0 = rank * rows;
+  const int nr = max(0, min(rows, H - r0));
+  BandDB<T> s = band_layout_db<T>(c_smem, rows, W);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int mw = mb.hi[2] - mb.lo[2];
+  const int mr0 = mon ? max(mb.lo[1], r0) : 0;
+  const int mr1 = mon ? min(mb.hi[1], r0 + nr) : 0;
+  const int mrows = max(0, mr1 - mr0);
+  const long long ncell = mon ? (long long)(mb.hi[1] - mb.lo[1]) * mw : 0;
+  double* macc = reinterpret_cast<double*>(
+      c_smem + ((band_elems_db(rows, W) * sizeof(T) + 15) / 16) * 16);
+  const long long mcells = (long long)mrows * mw;
+  for (long long q = threadIdx.x; q < mcells * nfq; q += blockDim.x) {
+    const long long fq = q / mcells, c = q % mcells;
+    const long long cell = (long long)(mr0 - mb.lo[1]) * mw + c;
+    macc[2 * q] = accb[(fq * ncell + cell) * 2];
+    macc[2 * q + 1] = accb[(fq * ncell + cell) * 2 + 1];
+  }
+  for (int j = threadIdx.x; j < W; j += blockDim.x) {
+    s.bx[j] = static_cast<T>(pb1[j]);
+    s.gx[j] = static_cast<T>(1.0 + pc1[j]);
+  }
+  for (int r = threadIdx.x; r < nr; r += blockDim.x) {
+    s.by[r] = static_cast<T>(pb0[r0 + r]);
+    s.gy[r] = static_cast<T>(1.0 + pc0[r0 + r]);
+  }
+  for (int r = warp; r < nr; r += nw)
+    for (int j = lane; j < W; j += 32) {
+      const long long o = (long long)r * W + j;
+      s.f(0)[o] = T(0);
+      s.a(0)[o] = T(0);
+      s.b(0)[o] = T(0);
+      s.ce[o] = ceg[(long long)(r0 + r) * py + j];
+    }
+  cl.sync();  // every band initialised before any neighbour reads it
+
+  const int up = rank + 1 < CL ? rank + 1 : rank, dn_ = rank > 0 ? rank - 1 : rank;
+  const BandDB<T> nxt = band_layout_db<T>(cl.map_shared_rank(c_smem, up), rows, W);
+  const BandDB<T> prv = band_layout_db<T>(cl.map_shared_rank(c_smem, dn_), rows, W);
+  // the neighbour row of the second half-step exists (TM: a band above; TE: a
+  // band below that holds rows)
+  const bool halo_tm = r0 > 0 && nr > 0;
+  const bool halo_te = nr > 0 && r0 + nr < H;
+
+  for (int n = 0; n < T_steps; ++n) {
+    const int p = n & 1, q = p ^ 1;
+    const T* fp = s.f(p);
+    const T* ap = s.a(p);
+    const T* bp = s.b(p);
+    T* aq = s.a(q);
+    T* bq = s.b(q);
+    // the neighbour row is spread over all threads, one column each (more
+    // columns than threads: the rest after the own rows); the remote loads of
+    // the first column are issued here and used after the own rows
+    const bool hal = POL == DN_TM ? halo_tm : halo_te;
+    const int hj = threadIdx.x;
+    const long long hrow = POL == DN_TM ? (long long)(rows - 1) * W : 0;  // neighbour's row
+    const long long orow = POL == DN_TM ? 0 : (long long)(nr - 1) * W;   // own boundary row
+    const T* hf = POL == DN_TM ? prv.f(p) : nxt.f(p);
+    const T* hb = POL == DN_TM ? prv.b(p) : nxt.b(p);
+    T pf = T(0), pb = T(0), pc = T(0);
+    if (hal && hj < W) {
+      pf = hf[hrow + hj];
+      pb = hb[hrow + hj];
+      if (POL == DN_TE) pc = nxt.ce[hj];
+    }
+    // half-step 1: H (TM) / E (TE) from the injected field of buffer p
+    for (int r = warp; r < nr; r += nw) {
+      const int i = r0 + r;
+      const T byr = s.by[r], gyr = s.gy[r];
+      const bool last = i == H - 1, first = i == 0;
+      const T* below = (r + 1 < nr) ? fp + (long long)(r + 1) * W : nxt.f(p);
+      const T* above = (r > 0) ? fp + (long long)(r - 1) * W : prv.f(p) + (long long)(rows - 1) * W;
+#pragma unroll 4
+      for (int j = lane; j < W; j += 32) {
+        const long long o = (long long)r * W + j;
+        if (POL == DN_TM) {
+          const T ez = fp[o];
+          const T dj = (j < W - 1) ? fp[o + 1] - ez : T(0);
+          const T di = !last ? below[j] - ez : T(0);
+          aq[o] = byr * ap[o] - dt * gyr * (dj * idl);
+          bq[o] = s.bx[j] * bp[o] + dt * s.gx[j] * (di * idl);
+        } else {
+          const T hz = fp[o];
+          const T dj = (j > 0) ? hz - fp[o - 1] : T(0);
+          const T di = !first ? hz - above[j] : T(0);
+          const T cx = s.gx[j] * (dj * idl);
+          const T cy = -(gyr * (di * idl));
+          const T c = s.ce[o];
+          aq[o] = s.bx[j] * ap[o] + c * cx;
+          bq[o] = byr * bp[o] + c * cy;
+        }
+      }
+    }
+    // the neighbour row, with the neighbour's own arithmetic
+    if (hal) {
+      const T nby = POL == DN_TE ? nxt.by[0] : T(0), ngy = POL == DN_TE ? nxt.gy[0] : T(0);
+      for (int j = hj; j < W; j += blockDim.x) {
+        T vf = pf, vb = pb, vc = pc;
+        if (j != hj) {
+          vf = hf[hrow + j];
+          vb = hb[hrow + j];
+          if (POL == DN_TE) vc = nxt.ce[j];
+        }
+        if (POL == DN_TM) {
+          // Hy of row r0-1 (the band above's last row; r0-1 < H-1)
+          const T di = fp[orow + j] - vf;
+          s.halo[j] = s.bx[j] * vb + dt * s.gx[j] * (di * idl);
+        } else {
+          // Ey of row r0+nr (the band below's first row; r0+nr > 0)
+          const T di = vf - fp[orow + j];
+          const T cy = -(ngy * (di * idl));
+          s.halo[j] = nby * vb + vc * cy;
+        }
+      }
+    }
+    __syncthreads();
+    // half-step 2: the injected field from the new pair, source, monitors
+    const T wv = src ? wave[n] : T(0);
+    const double* ph = mon ? phase + (long long)n * nfq * 2 : nullptr;
+    T* fq = s.f(q);
+    for (int r = warp; r < nr; r += nw) {
+      const int i = r0 + r;
+      const T byr = s.by[r], gyr = s.gy[r];
+      const bool last = i == H - 1, first = i == 0;
+      const T* bup = (r > 0) ? bq + (long long)(r - 1) * W : s.halo;
+      const T* bdn = (r + 1 < nr) ? bq + (long long)(r + 1) * W : s.halo;
+      const bool src_row = src && i >= sb.lo[1] && i < sb.hi[1];
+      const bool mon_row = mon && i >= mb.lo[1] && i < mb.hi[1];
+#pragma unroll 4
+      for (int j = lane; j < W; j += 32) {
+        const long long o = (long long)r * W + j;
+        const T fo = fp[o];
+        const T bb = s.bx[j] * byr;
+        T v0;
+        if (POL == DN_TM) {
+          const T dHy = !first ? bq[o] - bup[j] : T(0);
+          const T dHx = (j > 0) ? aq[o] - aq[o - 1] : T(0);
+          const T cz = s.gx[j] * (dHy * idl) - gyr * (dHx * idl);
+          v0 = bb * fo + s.ce[o] * cz;
+        } else {
+          const T dEy = !last ? bdn[j] - bq[o] : T(0);
+          const T dEx = (j < W - 1) ? aq[o + 1] - aq[o] : T(0);
+          v0 = bb * fo + dt * (s.gx[j] * (dEy * idl) - gyr * (dEx * idl));
+        }
+        if (src_row && j >= sb.lo[2] && j < sb.hi[2]) v0 += wv;
+        if (mon_row && j >= mb.lo[2] && j < mb.hi[2]) {
+          const long long c = (long long)(i - mr0) * mw + (j - mb.lo[2]);
+          const double x = static_cast<double>(v0);
+          for (int f = 0; f < nfq; ++f) {
+            double* acc = macc + (f * mcells + c) * 2;
+            acc[0] = fma(x, ph[2 * f], acc[0]);
+            acc[1] = fma(x, ph[2 * f + 1], acc[1]);
+          }
+        }
+        fq[o] = v0;
+      }
+    }
+    cl.sync();  // buffer q complete everywhere before step n+1 reads it
+  }
+  const int fin = T_steps & 1;  // the buffer the last step wrote
+  for (int r = warp; r < nr; r += nw)
+    for (int j = lane; j < W; j += 32) {
+      const long long o = (long long)r * W + j, g = (long long)(r0 + r) * py + j;
+      o0[g] = s.f(fin)[o];
+      o1[g] = s.a(fin)[o];
+      o2[g] = s.b(fin)[o];
+    }
+  for (long long q = threadIdx.x; q < mcells * nfq; q += blockDim.x) {
+    const long long fq = q / mcells, c = q % mcells;
+    const long long cell = (long long)(mr0 - mb.lo[1]) * mw + c;
+    accb[(fq * ncell + cell) * 2] = macc[2 * q];
+    accb[(fq * ncell + cell) * 2 + 1] = macc[2 * q + 1];
+  }
+}
+
+// ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
 int validate(const dn_batch2d* cfg, const dn_batch2d_inst* insts) {
@@ -858,14 +1108,16 @@ int run(bool fwd, const dn_batch2d* cfg, void* dev_table, int32_t* status, void*
 
 constexpr long long CLUSTER_SMEM_MAX = 227 * 1024;
 
-// bytes of shared memory per CTA for a cluster of cl CTAs, -1 if too large
-long long cluster_bytes(const dn_batch2d* cfg, const dn_batch2d_inst* insts, int cl) {
+// bytes of shared memory per CTA for a cluster of cl CTAs (db: the
+// double-buffered kernel), -1 if too large
+long long cluster_bytes(const dn_batch2d* cfg, const dn_batch2d_inst* insts, int cl, bool db) {
   const long long es = cfg->dtype == DN_F32 ? 4 : 8;
   long long need = 0;
   for (int b = 0; b < cfg->n_inst; ++b) {
     const dn_batch2d_inst& I = insts[b];
     const long long rows = (I.H + cl - 1) / cl;
-    long long bytes = (band_elems(rows, I.W) * es + 15) / 16 * 16;
+    const long long elems = db ? band_elems_db(rows, I.W) : band_elems(rows, I.W);
+    long long bytes = (elems * es + 15) / 16 * 16;
     if (I.mon_comp != DN_NONE) {  // the band's share of the monitor box, FP64 complex
       const long long bh = I.mon_box.hi[1] - I.mon_box.lo[1];
       const long long bw = I.mon_box.hi[2] - I.mon_box.lo[2];
@@ -876,9 +1128,9 @@ long long cluster_bytes(const dn_batch2d* cfg, const dn_batch2d_inst* insts, int
   return need <= CLUSTER_SMEM_MAX ? need : -1;
 }
 
-template <typename T, int POL, int CL>
+template <typename T, int POL, int CL, bool DB>
 int launch_cluster(void* table, int n_inst, long long smem, cudaStream_t s) {
-  auto kern = k_batch2d_cluster<T, POL, CL>;
+  auto kern = DB ? k_batch2d_cluster_db<T, POL, CL> : k_batch2d_cluster<T, POL, CL>;
   DN_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   if (CL > 8)
     DN_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
@@ -903,9 +1155,12 @@ int launch_cluster(void* table, int n_inst, long long smem, cudaStream_t s) {
 }
 
 template <typename T, int POL>
-int dispatch_cluster(int cl, void* table, int n_inst, long long smem, cudaStream_t s) {
-  return cl == 8 ? launch_cluster<T, POL, 8>(table, n_inst, smem, s)
-                 : launch_cluster<T, POL, 16>(table, n_inst, smem, s);
+int dispatch_cluster(int cl, bool db, void* table, int n_inst, long long smem, cudaStream_t s) {
+  if (db)
+    return cl == 8 ? launch_cluster<T, POL, 8, true>(table, n_inst, smem, s)
+                   : launch_cluster<T, POL, 16, true>(table, n_inst, smem, s);
+  return cl == 8 ? launch_cluster<T, POL, 8, false>(table, n_inst, smem, s)
+                 : launch_cluster<T, POL, 16, false>(table, n_inst, smem, s);
 }
 
 }  // namespace
@@ -915,14 +1170,16 @@ extern "C" int32_t dn_batch2d_cluster_size(const dn_batch2d* cfg, const dn_batch
                                            int64_t* smem_bytes) {
   if (dn::validate(cfg, insts) != DN_OK || !smem_bytes) return -1;
   // 16 CTAs per grid (half the band of 8 each, twice the SMs per grid) is the
-  // faster of the two on B200; any grid that fits 8 CTAs also fits 16
-  for (int cl : {16, 8}) {
-    const long long b = dn::cluster_bytes(cfg, insts, cl);
-    if (b > 0) {
-      *smem_bytes = b;
-      return cl;
+  // faster size on B200; the double-buffered kernel (one cluster barrier per
+  // step) where its twice-as-large bands fit, else the in-place one
+  for (int cl : {16, 8})
+    for (bool db : {true, false}) {
+      const long long b = dn::cluster_bytes(cfg, insts, cl, db);
+      if (b > 0) {
+        *smem_bytes = b;
+        return cl | (db ? DN_CLUSTER_DOUBLE_BUFFERED : 0);
+      }
     }
-  }
   return 0;
 }
 
@@ -932,16 +1189,19 @@ extern "C" int32_t dn_batch2d_forward_cluster(const dn_batch2d* cfg, void* dev_t
   if (!cfg || !dev_table || (reinterpret_cast<uintptr_t>(dev_table) & 15)) return DN_EINVAL;
   if (cfg->pol != DN_TM && cfg->pol != DN_TE) return DN_EINVAL;
   if (cfg->dtype != DN_F32 && cfg->dtype != DN_F64) return DN_EINVAL;
-  if ((cluster != 8 && cluster != 16) || smem_bytes < 1 || smem_bytes > dn::CLUSTER_SMEM_MAX ||
-      cfg->n_inst < 1 || (long long)cfg->n_inst * cluster > 0x7fffffffLL)
+  const bool db = (cluster & DN_CLUSTER_DOUBLE_BUFFERED) != 0;
+  const int csize = cluster & ~DN_CLUSTER_DOUBLE_BUFFERED;
+  if ((csize != 8 && csize != 16) || smem_bytes < 1 || smem_bytes > dn::CLUSTER_SMEM_MAX ||
+      cfg->n_inst < 1 || (long long)cfg->n_inst * csize > 0x7fffffffLL)
     return DN_EINVAL;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const bool tm = cfg->pol == DN_TM;
+  const int n = cfg->n_inst;
   if (cfg->dtype == DN_F32)
-    return tm ? dn::dispatch_cluster<float, DN_TM>(cluster, dev_table, cfg->n_inst, smem_bytes, s)
-              : dn::dispatch_cluster<float, DN_TE>(cluster, dev_table, cfg->n_inst, smem_bytes, s);
-  return tm ? dn::dispatch_cluster<double, DN_TM>(cluster, dev_table, cfg->n_inst, smem_bytes, s)
-            : dn::dispatch_cluster<double, DN_TE>(cluster, dev_table, cfg->n_inst, smem_bytes, s);
+    return tm ? dn::dispatch_cluster<float, DN_TM>(csize, db, dev_table, n, smem_bytes, s)
+              : dn::dispatch_cluster<float, DN_TE>(csize, db, dev_table, n, smem_bytes, s);
+  return tm ? dn::dispatch_cluster<double, DN_TM>(csize, db, dev_table, n, smem_bytes, s)
+            : dn::dispatch_cluster<double, DN_TE>(csize, db, dev_table, n, smem_bytes, s);
 }
 
 extern "C" int64_t dn_batch2d_table_bytes(const dn_batch2d* cfg, const dn_batch2d_inst* insts) {

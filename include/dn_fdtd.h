@@ -258,13 +258,18 @@ int32_t dn_batch2d_backward(const dn_batch2d* cfg, void* dev_table, int32_t* sta
 
 /* Forward-only solve of every instance of a packed table with each grid held
  * in the shared memory of one thread-block cluster (CTAs own row bands, the
- * neighbouring rows come from the next / previous CTA's shared memory, two
- * cluster barriers per step): no global traffic for the fields between the
- * first and the last step.  Same results as dn_batch2d_forward (final fields in
- * f[n_steps % 2], monitor DFTs accumulated), no checkpoints.
- * dn_batch2d_cluster_size returns the cluster size to use (16 CTAs per grid)
- * and sets *smem_bytes (per CTA); 0 when some instance is too large for a
- * cluster, -1 on invalid input.  dn_batch2d_forward_cluster also takes 8. */
+ * neighbouring rows come from the next / previous CTA's shared memory): no
+ * global traffic for the fields between the first and the last step.  Same
+ * results as dn_batch2d_forward (final fields in f[n_steps % 2], monitor DFTs
+ * accumulated), no checkpoints.  Where the grid fits twice, the fields are
+ * double-buffered and each step takes one cluster barrier (the neighbour row
+ * of the second half-step is recomputed locally); otherwise they are updated
+ * in place with two barriers per step.
+ * dn_batch2d_cluster_size returns the value to pass as `cluster`: the cluster
+ * size (16, else 8 CTAs per grid), with DN_CLUSTER_DOUBLE_BUFFERED set for the
+ * double-buffered kernel, and sets *smem_bytes (per CTA); 0 when some instance
+ * is too large for a cluster, -1 on invalid input. */
+#define DN_CLUSTER_DOUBLE_BUFFERED 0x100
 int32_t dn_batch2d_cluster_size(const dn_batch2d* cfg, const dn_batch2d_inst* insts,
                                 int64_t* smem_bytes);
 int32_t dn_batch2d_forward_cluster(const dn_batch2d* cfg, void* dev_table, int32_t cluster,

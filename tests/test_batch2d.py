@@ -10,6 +10,7 @@ import torch
 from conftest import rel_l2
 
 import diffnano_b200 as dn
+from diffnano_b200 import _lib
 from diffnano_b200.solvers.batch2d import BatchInstance, FDTDBatch2D, autotune_tile_rows
 
 pytestmark = pytest.mark.gpu
@@ -118,7 +119,8 @@ def test_cluster_forward_matches_persistent_kernel(cuda, pol, dtype):
     a.check_status()
     b.check_status()
     assert a.uses_cluster(False) and not b.uses_cluster(False) and not a.uses_cluster(True)
-    assert a._cluster[0] == 16
+    # both large grids fit twice: the double-buffered kernel, one barrier per step
+    assert a._cluster[0] == 16 | _lib.DN_CLUSTER_DOUBLE_BUFFERED
     tol = 1e-6 if dtype == torch.float32 else 1e-13
     for x, y in zip(fa, fb):
         assert rel_l2(x, y) < tol
@@ -128,3 +130,28 @@ def test_cluster_forward_matches_persistent_kernel(cuda, pol, dtype):
     fg, dg = a.forward_graphed(eps)
     for x, y in zip(fg, fa):
         assert torch.equal(x, y)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("pol", ["TM", "TE"])
+def test_cluster_in_place_kernel_for_grids_that_fit_once(cuda, pol):
+    """A 460 x 400 FP32 grid fits a 16-CTA cluster's shared memory once but not
+    twice: the in-place cluster kernel (two barriers per step) runs it, with the
+    tile kernel's fields and DFTs."""
+    spec = BatchInstance(grid_shape=(460, 400), n_steps=40, dl=20.0, pml_layers=6, courant=0.5,
+                         source={"type": "gaussian_pulse", "row": 9, "spread": 300.0,
+                                 "t0": 900.0},
+                         monitor={"col": 40, "wavelengths_nm": [1550.0]})
+    g = torch.Generator().manual_seed(5)
+    eps = [(1.5 + 2.0 * torch.rand(460, 400, dtype=torch.float64, generator=g)).to(cuda)]
+    a = FDTDBatch2D([spec], pol, torch.float32, cuda, tile_rows=16, cluster=True)
+    b = FDTDBatch2D([spec], pol, torch.float32, cuda, tile_rows=16, cluster=False)
+    fa, da = a.forward(eps)
+    fb, db = b.forward(eps)
+    a.check_status()
+    b.check_status()
+    assert a.uses_cluster(False) and a._cluster[0] == 16  # packed on the first forward
+    for x, y in zip(fa, fb):
+        assert rel_l2(x, y) < 1e-6
+    for x, y in zip(da, db):
+        assert rel_l2(torch.view_as_real(x), torch.view_as_real(y)) < 1e-6
