@@ -132,6 +132,36 @@ __global__ void k_readout(const unsigned short* __restrict__ x, const float* __r
   }
 }
 
+// the same with four consecutive columns w per thread (W % 4 == 0, x 8-byte
+// aligned): 8-byte loads, a warp reads 256 contiguous bytes per row h
+__global__ void k_readout4(const unsigned short* __restrict__ x, const float* __restrict__ r,
+                           long long nb, int H, int W, int C, unsigned short* __restrict__ out) {
+  const int W4 = W / 4;
+  const long long n = nb * C * W4;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int w0 = (int)(i % W4) * 4;
+    const int c = (int)((i / W4) % C);
+    const long long b = i / ((long long)W4 * C);
+    const unsigned short* xp = x + (b * C + c) * (long long)H * W + w0;
+    float s0 = 0.0f, s1 = 0.0f, s2 = 0.0f, s3 = 0.0f;
+#pragma unroll 4
+    for (int h = 0; h < H; ++h) {
+      const uint2 u = *reinterpret_cast<const uint2*>(xp + (long long)h * W);
+      const float rv = r[h * C + c];
+      s0 = fmaf(rv, __uint_as_float(u.x << 16), s0);
+      s1 = fmaf(rv, __uint_as_float(u.x & 0xFFFF0000u), s1);
+      s2 = fmaf(rv, __uint_as_float(u.y << 16), s2);
+      s3 = fmaf(rv, __uint_as_float(u.y & 0xFFFF0000u), s3);
+    }
+    unsigned short* o = out + (b * W + w0) * C + c;
+    o[0] = f2bf(s0);
+    o[C] = f2bf(s1);
+    o[2 * C] = f2bf(s2);
+    o[3 * C] = f2bf(s3);
+  }
+}
+
 // readout backward, one block per (b, c): dR[b, :, c] staged in shared memory,
 //   dx[b, c, h, w] = r[h, c] * dR[b, w, c]                       (dx != NULL)
 //   dr_part[b, h, c] = sum_w dR[b, w, c] * x[b, c, h, w]         (dr_part != NULL)
@@ -371,6 +401,34 @@ __global__ void k_adam(float* __restrict__ p, const float* __restrict__ g, float
 
 // blk[m, (ro, o), (ri, i)] for ro, ri in {0, 1} (real, imaginary):
 //   [[wre, -wim], [wim, wre]] so that [yre; yim] = blk [zre; zim]
+// one thread per two consecutive inputs i of one (m, o): reads the two complex
+// weights once and writes the four 2x2-block entries of both as BF16 pairs
+// (ci even; the odd-ci kernel below writes element by element)
+__global__ void k_pack_modes2(const float* __restrict__ wre, const float* __restrict__ wim,
+                              long long nm, int co, int ci, unsigned int* __restrict__ blk2) {
+  const int hc = ci / 2;
+  const long long n = nm * co * hc;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const int i2 = (int)(idx % hc);
+    const long long mo = idx / hc;  // m * co + o
+    const int o = (int)(mo % co);
+    const long long m = mo / co;
+    const long long w = mo * ci + 2 * i2;
+    const float re0 = wre[w], re1 = wre[w + 1], im0 = wim[w], im1 = wim[w + 1];
+    const uint32_t pre = (uint32_t)f2bf(re0) | ((uint32_t)f2bf(re1) << 16);
+    const uint32_t pim = (uint32_t)f2bf(im0) | ((uint32_t)f2bf(im1) << 16);
+    const uint32_t nim = (uint32_t)f2bf(-im0) | ((uint32_t)f2bf(-im1) << 16);
+    // rows o (real out) and co + o (imaginary out) of mode m, in pairs of columns
+    const long long top = ((m * 2 * co + o) * 2 * ci) / 2;
+    const long long bot = ((m * 2 * co + co + o) * 2 * ci) / 2;
+    blk2[top + i2] = pre;       // [wre, ...
+    blk2[top + hc + i2] = nim;  //  ..., -wim]
+    blk2[bot + i2] = pim;       // [wim, ...
+    blk2[bot + hc + i2] = pre;  //  ..., wre]
+  }
+}
+
 __global__ void k_pack_modes(const float* __restrict__ wre, const float* __restrict__ wim,
                              long long nm, int co, int ci, unsigned short* __restrict__ blk) {
   const long long n = nm * 2 * co * 2 * ci;
@@ -469,6 +527,12 @@ extern "C" int32_t dn_fno_lift(const void* feat, const void* P, const float* bia
 extern "C" int32_t dn_fno_readout(const void* x, const float* r, int64_t nb, int32_t H,
                                   int32_t W, int32_t C, void* out, void* stream) {
   if (!x || !r || !out || nb < 1 || H < 1 || W < 1 || C < 1) return DN_EINVAL;
+  if (W % 4 == 0 && (reinterpret_cast<uintptr_t>(x) & 7) == 0) {
+    k_readout4<<<grid_for(nb * C * (W / 4)), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const unsigned short*>(x), r, nb, H, W, C, static_cast<unsigned short*>(out));
+    DN_CUDA_CHECK(cudaGetLastError());
+    return DN_OK;
+  }
   k_readout<<<grid_for(nb * C * W), 256, 0, static_cast<cudaStream_t>(stream)>>>(
       static_cast<const unsigned short*>(x), r, nb, H, W, C, static_cast<unsigned short*>(out));
   DN_CUDA_CHECK(cudaGetLastError());
@@ -542,6 +606,13 @@ extern "C" int32_t dn_adam(float* p, const float* g, float* m, float* v, int64_t
 extern "C" int32_t dn_fno_pack_modes(const float* wre, const float* wim, int64_t n_modes,
                                      int32_t c_out, int32_t c_in, void* blk, void* stream) {
   if (!wre || !wim || !blk || n_modes < 1 || c_out < 1 || c_in < 1) return DN_EINVAL;
+  if (c_in % 2 == 0 && (reinterpret_cast<uintptr_t>(blk) & 3) == 0) {
+    k_pack_modes2<<<grid_for(n_modes * (long long)c_out * (c_in / 2)), 256, 0,
+                    static_cast<cudaStream_t>(stream)>>>(wre, wim, n_modes, c_out, c_in,
+                                                         static_cast<unsigned int*>(blk));
+    DN_CUDA_CHECK(cudaGetLastError());
+    return DN_OK;
+  }
   k_pack_modes<<<grid_for(n_modes * 4LL * c_out * c_in), 256, 0,
                  static_cast<cudaStream_t>(stream)>>>(wre, wim, n_modes, c_out, c_in,
                                                       static_cast<unsigned short*>(blk));

@@ -217,3 +217,41 @@ def test_colsum_matches_torch(cuda, rows, cols, bf16):
     run(1)
     torch.cuda.synchronize()
     assert rel_l2(out.double(), 2 * ref) < 1e-6
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nm,co,ci", [(512, 64, 64), (9, 5, 7)])
+def test_pack_modes_block_form(cuda, nm, co, ci):
+    """dn_fno_pack_modes against [[wre, -wim], [wim, wre]] built by torch, bit
+    for bit (even c_in: two entries per thread; odd: one)."""
+    from diffnano_b200 import _lib
+
+    g = torch.Generator().manual_seed(9)
+    wre = torch.randn(nm, co, ci, generator=g).to(cuda)
+    wim = torch.randn(nm, co, ci, generator=g).to(cuda)
+    blk = torch.empty(nm, 2 * co, 2 * ci, dtype=torch.bfloat16, device=cuda)
+    s = torch.cuda.current_stream().cuda_stream
+    _lib.check("dn_fno_pack_modes", _lib.lib().dn_fno_pack_modes(
+        wre.data_ptr(), wim.data_ptr(), nm, co, ci, blk.data_ptr(), s))
+    torch.cuda.synchronize()
+    ref = torch.cat([torch.cat([wre, -wim], 2), torch.cat([wim, wre], 2)], 1).to(torch.bfloat16)
+    assert torch.equal(blk, ref)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nb,H,W,C", [(3, 128, 128, 64), (2, 9, 13, 5)])
+def test_readout_matches_einsum(cuda, nb, H, W, C):
+    """dn_fno_readout (four columns per thread when W % 4 == 0, else one)
+    against an FP64 einsum of the same BF16 inputs, to one BF16 rounding."""
+    from diffnano_b200 import _lib
+
+    g = torch.Generator().manual_seed(13)
+    x = torch.randn(nb, C, H, W, generator=g).to(torch.bfloat16).to(cuda)
+    r = torch.randn(H, C, generator=g).to(cuda)
+    out = torch.empty(nb, W, C, dtype=torch.bfloat16, device=cuda)
+    s = torch.cuda.current_stream().cuda_stream
+    _lib.check("dn_fno_readout", _lib.lib().dn_fno_readout(
+        x.data_ptr(), r.data_ptr(), nb, H, W, C, out.data_ptr(), s))
+    torch.cuda.synchronize()
+    ref = torch.einsum("hc,bchw->bwc", r.double(), x.double())
+    assert rel_l2(out.double(), ref) < 4e-3
