@@ -109,6 +109,7 @@ struct Params {
   int pre_bf16;
   int vec;
   int vec32;  // 32-byte aligned chunk rows: 256-bit stores
+  int csub;   // column radix dividing 32 (else 0): per-element column offsets
   int* status;
 };
 
@@ -705,10 +706,24 @@ __global__ void __launch_bounds__(NT, 1)
 #pragma unroll
             for (int j = 0; j < 32; ++j) v[j] += w[j];
           }
-          if (vec && p.vec32)
+          if (p.csub) {
+            // column radix dividing 32: a chunk holds 32 / csub whole radix
+            // groups; plain stores only (checked on the host)
+            const long long ob = roff + (col / p.csub) * p.c1;
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+              if (j >= nv) continue;
+              const long long o = ob + (j % p.csub) * p.c0 + (j / p.csub) * p.c1;
+              if (p.out_bf16)
+                reinterpret_cast<unsigned short*>(p.out)[o] = f2bf(v[j]);
+              else
+                reinterpret_cast<float*>(p.out)[o] = v[j];
+            }
+          } else if (vec && p.vec32) {
             store32_v8(p.out, p.out_bf16, off, v);
-          else
+          } else {
             store32(p.out, p.out_bf16, off, p.c0, vec, nv, v);
+          }
         }
         __syncwarp();  // reconverge before the next warp-wide tcgen05.ld
       }
@@ -921,7 +936,12 @@ extern "C" int32_t dn_gemm_run(const dn_gemm* g, int32_t* status, void* stream) 
   if (g->act == DN_ACT_GELU_GRAD && (!g->aux || !dtype_ok(g->aux_dtype))) return DN_EINVAL;
   if (g->pre && (g->act != DN_ACT_GELU || !dtype_ok(g->pre_dtype))) return DN_EINVAL;
   if (g->addend && !dtype_ok(g->addend_dtype)) return DN_EINVAL;
-  if (g->c_row_radix < 0 || g->c_col_radix < 0 || (g->c_col_radix % 32)) return DN_EINVAL;
+  if (g->c_row_radix < 0 || g->c_col_radix < 0) return DN_EINVAL;
+  // a column radix is a multiple of 32, or a divisor of 32 for plain stores
+  const bool small_radix = g->c_col_radix > 0 && g->c_col_radix < 32;
+  if (small_radix && (32 % g->c_col_radix || g->addend || g->aux || g->pre || g->accumulate))
+    return DN_EINVAL;
+  if (!small_radix && (g->c_col_radix % 32)) return DN_EINVAL;
   if (g->block_n != 0 && g->block_n != 64 && g->block_n != 128 && g->block_n != 256)
     return DN_EINVAL;
   if (g->pair < 0 || g->pair > 2 || (g->pair == 2 && g->block_n != 0 && g->block_n != 256))
@@ -937,7 +957,8 @@ extern "C" int32_t dn_gemm_run(const dn_gemm* g, int32_t* status, void* stream) 
   p.R0 = g->c_row_radix > 0 ? g->c_row_radix : (1LL << 62);
   p.r0 = g->c_row_stride0;
   p.r1 = g->c_row_stride1;
-  p.C0 = g->c_col_radix > 0 ? g->c_col_radix : (1LL << 62);
+  p.C0 = g->c_col_radix >= 32 ? g->c_col_radix : (1LL << 62);
+  p.csub = small_radix ? (int)g->c_col_radix : 0;
   p.c0 = g->c_col_stride0;
   p.c1 = g->c_col_stride1;
   p.alpha = g->alpha;

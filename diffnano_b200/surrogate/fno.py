@@ -93,6 +93,46 @@ def dft_matrices(cfg: FNOConfig) -> Tuple[np.ndarray, np.ndarray]:
     return F2, G
 
 
+def separable_dft_matrices(cfg: FNOConfig) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """The truncated rfft2 of dft_matrices as a pass along W then one along H,
+    in float64:
+
+    Fw (2*modes, W): Fw[ri*modes + kw, w] = cos / -sin(2 pi kw w / W), so the
+    W pass gives T = sum_w x e^{-i th_w} as (Re, Im) pairs;
+    FwS: Fw with row (ri, kw) scaled by c_kw / (H W) (c = 1 for kw = 0, else 2),
+    the analysis of the adjoint of the synthesis G;
+    Fh (4*modes, 2*H): Z = sum_h T e^{-i th_h} as a real map from (Re T, Im T)
+    over h to (Re Z, Im Z) over khi: [[cos, sin], [-sin, cos]] of
+    th_h = 2 pi kh h / H, kh as in mode_table."""
+    M = cfg.modes
+    kw = np.arange(M)
+    tw = 2 * np.pi * np.outer(kw, np.arange(cfg.W)) / cfg.W
+    Fw = np.concatenate([np.cos(tw), -np.sin(tw)], axis=0)
+    c = np.where(kw == 0, 1.0, 2.0) / (cfg.H * cfg.W)
+    FwS = Fw * np.concatenate([c, c])[:, None]
+    khi = np.arange(2 * M)
+    kh = np.where(khi < M, khi, khi - 2 * M + cfg.H)
+    th = 2 * np.pi * np.outer(kh, np.arange(cfg.H)) / cfg.H
+    Ch, Sh = np.cos(th), np.sin(th)
+    Fh = np.block([[Ch, Sh], [-Sh, Ch]])
+    return Fw, FwS, Fh
+
+
+def t1_half(H: int) -> int:
+    """Length of each (Re, Im) half of a T1 row: H rounded up to a multiple of
+    4, so that rows of 2 * t1_half(H) elements are valid GEMM operands."""
+    return (H + 3) // 4 * 4
+
+
+def padded_h_pass(Fh: np.ndarray, H: int) -> np.ndarray:
+    """Fh (4*modes, 2*H) with each half of its columns zero-padded to t1_half(H)."""
+    Hp = t1_half(H)
+    out = np.zeros((Fh.shape[0], 2 * Hp))
+    out[:, :H] = Fh[:, :H]
+    out[:, Hp:Hp + H] = Fh[:, H:]
+    return out
+
+
 class ParamSet:
     """FP32 master parameters in one flat buffer (each tensor 8-element
     aligned so that its BF16 mirror is a valid GEMM operand), with the
@@ -150,9 +190,16 @@ class FNO2d:
                        "Q2": (OUT_LD, c.hidden), "q2": (OUT_LD,)})
         self.ps = ParamSet(shapes, self.dev)
         self._init_params(seed)
-        F2, G = dft_matrices(c)
-        self.F2 = torch.from_numpy(F2).to(torch.bfloat16).to(self.dev).contiguous()
+        if 32 % c.modes and c.modes % 32:
+            raise ValueError("modes must divide 32 or be a multiple of 32 (the transform "
+                             "passes' output maps)")
+        _, G = dft_matrices(c)
         self.Gm = torch.from_numpy(G).to(torch.bfloat16).to(self.dev).contiguous()
+        Fw, FwS, Fh = separable_dft_matrices(c)
+        bfd = dict(dtype=torch.bfloat16, device=self.dev)
+        self.Fw = torch.from_numpy(Fw).to(**bfd).contiguous()
+        self.FwS = torch.from_numpy(FwS).to(**bfd).contiguous()
+        self.Fh = torch.from_numpy(padded_h_pass(Fh, c.H)).to(**bfd).contiguous()
         self.blk = [torch.empty(c.n_modes, 2 * c.width, 2 * c.width, dtype=torch.bfloat16,
                                 device=self.dev) for _ in range(c.layers)]
         # 1x1 mixes of a sample pair: blockdiag(W, W), blockdiag(W^T, W^T), [b, b]
@@ -160,10 +207,10 @@ class FNO2d:
         self.pw = [torch.empty(2 * c.width, 2 * c.width, **pw) for _ in range(c.layers)]
         self.pwT = [torch.empty(2 * c.width, 2 * c.width, **pw) for _ in range(c.layers)]
         self.pw_bias = [torch.empty(2 * c.width, device=self.dev) for _ in range(c.layers)]
-        # G = F2^T diag(cw): cw = c_kw / (H W) per mode row (c = 1 for kw = 0, else 2)
+        # cw = c_kw / (H W) per mode (c = 1 for kw = 0, else 2); the mixing
+        # backward's HW/c per mode turns the synthesis G into the analysis F2^T
         _, kw = mode_table(c)
         cw = torch.from_numpy(np.where(kw == 0, 1.0, 2.0) / (c.H * c.W)).to(torch.float32)
-        self.cscale = torch.cat([cw, cw]).to(self.dev)
         self.bscale = (1.0 / cw).to(self.dev)
         self.status = torch.zeros(1, dtype=torch.int32, device=self.dev)
         self._ws: Dict[int, Dict[str, torch.Tensor]] = {}
@@ -240,7 +287,11 @@ class FNO2d:
             "feat": torch.zeros(B, HW, FEAT, **bf),
             "X": [torch.zeros(Bp, C, HW, **bf) for _ in range(c.layers + 1)],
             "pre": [torch.zeros(Bp, C, HW, **bf) for _ in range(c.layers - 1)],
-            "Zm": [torch.empty(NM, B, 2 * C, **bf) for _ in range(c.layers)],
+            # kept modes of each layer's input, (mode, re/im, sample, channel)
+            "Zm": [torch.empty(NM, 2, B, C, **bf) for _ in range(c.layers)],
+            # W-pass output of the transform, ((kw, sample, channel), (re/im, h)),
+            # each half padded to t1_half(H); zeroed once, the pad stays zero
+            "T1": torch.zeros(c.modes * B * C, 2 * t1_half(c.H), **bf),
             "Ym": torch.empty(NM, B, 2 * C, **bf),
             "Yt": torch.zeros(Bp, C, NR, **bf),
             "R": torch.empty(B, c.W, C, **bf),
@@ -266,8 +317,7 @@ class FNO2d:
             "dR": torch.empty(B * c.W, C, **bf),
             "dA": torch.zeros(Bp, C, HW, **bf),
             "dB": torch.zeros(Bp, C, HW, **bf),
-            "dYt": torch.empty(B, C, NR, **bf),
-            "dYm": torch.empty(NM, B, 2 * C, **bf),
+            "dYm": torch.empty(NM, 2, B, C, **bf),
             "dZm": torch.empty(NM, B, 2 * C, **bf),
             "dZt": torch.zeros(Bp, C, NR, **bf),
             "dblk": torch.empty(NM, 2 * C, 2 * C, **f32),
@@ -277,6 +327,32 @@ class FNO2d:
             "loss_part": torch.zeros(256, dtype=torch.float64, device=d),
         })
         return ws
+
+    def _analysis(self, src, Fw, dst, ws, B):
+        """dst (modes, re/im, B, C) = the kept rfft2 modes of every (sample,
+        channel) image of src (B, C, H, W) channel-first, in two GEMMs: along W
+        (K = W, rows (sample, channel, h), into T1 ordered ((kw, sample,
+        channel), (re/im, h))), then along H (K = 2H, rows (kw, sample,
+        channel), columns (re/im, khi)), written straight into the
+        per-mode layout.  Fw: self.Fw, or self.FwS for the adjoint of the
+        synthesis.  ~30x fewer FLOPs than one dense (2 n_modes x H W) GEMM."""
+        c, st = self.cfg, self.status
+        M, H, W, R = c.modes, c.H, c.W, B * c.width
+        Hp = t1_half(H)
+        T1 = ws["T1"]
+        if H % 32 == 0:
+            # as T1^T = Fw X^T: rows (re/im, kw), columns (sample, channel, h)
+            # with h contiguous in T1, so the epilogue stores whole 32-column runs
+            gemm(2 * M, R * H, [(kmajor(Fw, 2 * M, W), kmajor(src, R * H, W))], T1,
+                 OutMap(row_radix=M, row0=R * 2 * Hp, row1=Hp, col_radix=H, col0=1,
+                        col1=2 * Hp), status=st)
+        else:
+            gemm(R * H, 2 * M, [(kmajor(src, R * H, W), kmajor(Fw, 2 * M, W))], T1,
+                 OutMap(row_radix=H, row0=1, row1=2 * Hp, col_radix=M, col0=R * 2 * Hp,
+                        col1=Hp), status=st)
+        gemm(M * R, 4 * M, [(kmajor(T1, M * R, 2 * Hp), kmajor(self.Fh, 4 * M, 2 * Hp))], dst,
+             OutMap(row_radix=R, row0=1, row1=2 * R, col_radix=2 * M, col0=2 * M * R, col1=R),
+             status=st)
 
     def _modes_rows(self, src, dst, B, to_rows):
         c = self.cfg
@@ -307,14 +383,18 @@ class FNO2d:
         # K = 8 contraction, so a memory-bound kernel rather than a GEMM
         _lib.check("dn_fno_lift", L.dn_fno_lift(
             _c(ws["feat"]), _c(ps.B("P")), _c(ps.P("p")), B, HW, C, _c(X[0]), s))
-        zmap = OutMap(row_radix=NM, row0=B * 2 * C, row1=C, col_radix=C, col0=1, col1=2 * C)
         for l in range(c.layers):
-            # truncated DFT of every (sample, channel) row: Zm[m, b, (ri, c)]
-            gemm(NR, B * C, [(kmajor(self.F2, NR, HW), kmajor(X[l], B * C, HW))],
-                 ws["Zm"][l], zmap, status=st)
-            # per-mode complex channel mixing: Ym[m, b, (ri, o)]
-            gemm(B, 2 * C, [(kmajor(ws["Zm"][l], B, 2 * C, batch_stride=B * 2 * C),
-                             kmajor(self.blk[l], 2 * C, 2 * C, batch_stride=4 * C * C))],
+            # truncated DFT of every (sample, channel) image: Zm[m, ri, b, c]
+            Zl = ws["Zm"][l]
+            self._analysis(X[l], self.Fw, Zl, ws, B)
+            # per-mode complex channel mixing: Ym[m, b, (ri, o)]; K = (ri, c) as
+            # two segments (the re and im halves of Zm and of blk's columns)
+            blk = self.blk[l]
+            gemm(B, 2 * C, [(kmajor(Zl, B, C, batch_stride=2 * B * C),
+                             kmajor(blk, 2 * C, C, ld=2 * C, batch_stride=4 * C * C)),
+                            (kmajor(Zl.view(-1)[B * C:], B, C, batch_stride=2 * B * C),
+                             kmajor(blk.view(-1)[C:], 2 * C, C, ld=2 * C,
+                                    batch_stride=4 * C * C))],
                  ws["Ym"], OutMap.rowmajor(2 * C, batch=B * 2 * C), batch=NM, status=st)
             self._modes_rows(ws["Ym"], ws["Yt"], B, True)
             # inverse DFT + 1x1 mix + bias (+ GELU) in one GEMM per sample pair:
@@ -391,20 +471,23 @@ class FNO2d:
         self._colsum(part, F32, B, c.H * C, ps.G("r"), ws)
         for l in reversed(range(c.layers)):
             # dcur = d loss / d pre_l, channel-first
-            # through the inverse DFT: dYt = dpre G = (dpre F2^T) diag(c/HW)
-            gemm(B * C, NR, [(kmajor(dcur, B * C, HW), kmajor(self.F2, NR, HW))],
-                 ws["dYt"], OutMap.rowmajor(NR), col_scale=self.cscale, status=st)
-            self._modes_rows(ws["dYt"], ws["dYm"], B, False)
-            # mode weights
-            gemm(2 * C, 2 * C, [(mnmajor(ws["dYm"], 2 * C, B, ld=2 * C, batch_stride=B * 2 * C),
-                                 mnmajor(ws["Zm"][l], 2 * C, B, ld=2 * C,
-                                         batch_stride=B * 2 * C))],
+            # through the inverse DFT: dY = dpre G = the analysis of dpre with
+            # c/HW per kw (FwS), straight into dYm[m, ri, b, c]
+            dYm = ws["dYm"]
+            self._analysis(dcur, self.FwS, dYm, ws, B)
+            # mode weights: rows (ri, o) of a mode are C-long runs B*C apart
+            fold = dict(fold=C, fold_stride=B * C, batch_stride=2 * B * C)
+            gemm(2 * C, 2 * C, [(mnmajor(dYm, 2 * C, B, ld=C, **fold),
+                                 mnmajor(ws["Zm"][l], 2 * C, B, ld=C, **fold))],
                  ws["dblk"], OutMap.rowmajor(2 * C, batch=4 * C * C), batch=NM, status=st)
             _lib.check("dn_fno_unpack_mode_grads", L.dn_fno_unpack_mode_grads(
                 _c(ws["dblk"]), NM, C, C, _c(ps.G(f"wre{l}")), _c(ps.G(f"wim{l}")), s))
             # back through the mixing; HW/c per mode turns G into F2^T below
-            gemm(B, 2 * C, [(kmajor(ws["dYm"], B, 2 * C, batch_stride=B * 2 * C),
-                             mnmajor(self.blk[l], 2 * C, 2 * C, ld=2 * C,
+            blk = self.blk[l]
+            gemm(B, 2 * C, [(kmajor(dYm, B, C, batch_stride=2 * B * C),
+                             mnmajor(blk, 2 * C, C, ld=2 * C, batch_stride=4 * C * C)),
+                            (kmajor(dYm.view(-1)[B * C:], B, C, batch_stride=2 * B * C),
+                             mnmajor(blk.view(-1)[2 * C * C:], 2 * C, C, ld=2 * C,
                                      batch_stride=4 * C * C))],
                  ws["dZm"], OutMap.rowmajor(2 * C, batch=B * 2 * C), batch=NM,
                  batch_scale=self.bscale, status=st)
@@ -477,13 +560,16 @@ class FNO2d:
         """Tensor-core FLOPs the GEMMs of one forward (+ backward) execute."""
         c = self.cfg
         HW, C, NR, NM = c.H * c.W, c.width, c.n_mode_rows, c.n_modes
-        fwd = 2 * B * HW * FEAT * C
-        layer = 2 * NR * HW * B * C + 2 * NM * B * (2 * C) ** 2 + 2 * B * HW * C * (NR + C)
+        M = c.modes
+        # the analysis transform's two passes (W, then H)
+        dft = 2 * B * C * c.H * (2 * M) * c.W + 2 * M * B * C * (4 * M) * (2 * c.H)
+        fwd = 0  # the lift is a memory-bound kernel, not a GEMM
+        layer = dft + 2 * NM * B * (2 * C) ** 2 + 2 * B * HW * C * (NR + C)
         fwd += c.layers * layer + 2 * B * c.W * (C * c.hidden + c.hidden * OUT_LD)
         if not backward:
             return float(fwd)
         bwd = 2 * B * c.W * (OUT_LD * c.hidden * 2 + c.hidden * C * 2)
-        bwd += c.layers * (2 * NR * HW * B * C + 2 * 2 * NM * B * (2 * C) ** 2
+        bwd += c.layers * (dft + 2 * 2 * NM * B * (2 * C) ** 2
                            + 2 * B * HW * C * C + 2 * B * HW * C * (NR + C))
         bwd += 2 * B * HW * C * FEAT
         return float(fwd + bwd)

@@ -62,7 +62,8 @@ typedef struct dn_gemm_operand {
  *   off(z, r, c) = z*c_batch_stride + (r % c_row_radix)*c_row_stride0
  *                + (r / c_row_radix)*c_row_stride1
  *                + (c % c_col_radix)*c_col_stride0 + (c / c_col_radix)*c_col_stride1
- * (radix 0 = no split).  c_col_radix, when set, is a multiple of 32. */
+ * (radix 0 = no split).  c_col_radix, when set, is a multiple of 32, or a
+ * divisor of 32 (2 .. 16) for plain stores (no addend, aux, pre, accumulate). */
 typedef struct dn_gemm {
   int64_t M;
   int64_t N;

@@ -8,7 +8,8 @@ import numpy as np
 import pytest
 import torch
 
-from diffnano_b200.surrogate.fno import FNOConfig, dft_matrices, mode_table
+from diffnano_b200.surrogate.fno import (FNOConfig, dft_matrices, mode_table, padded_h_pass,
+                                          separable_dft_matrices, t1_half)
 from oracle import fno_ref
 
 from conftest import rel_l2
@@ -36,6 +37,45 @@ def test_dft_matrices_match_rfft2_irfft2():
     Yc = np.einsum("moi,bmi->bmo", (wre + 1j * wim).numpy(), ref)
     xs = np.einsum("pm,bmc->bpc", G, np.concatenate([Yc.real, Yc.imag], axis=1))
     assert np.abs(s - xs.reshape(s.shape)).max() < 1e-10
+
+
+def _place(vals, out, row_radix, row0, row1, col_radix, col0, col1):
+    """Store a (rows x cols) result through a GEMM output map (FP64 emulation)."""
+    rows, cols = vals.shape
+    r = np.arange(rows)[:, None]
+    cc = np.arange(cols)[None, :]
+    off = (r % row_radix) * row0 + (r // row_radix) * row1 \
+        + (cc % col_radix) * col0 + (cc // col_radix) * col1
+    out[off.reshape(-1)] = vals.reshape(-1)
+
+
+@pytest.mark.parametrize("H,W,modes,B,C", [(32, 24, 4, 2, 8), (40, 64, 16, 1, 4),
+                                           (10, 64, 4, 3, 4), (64, 32, 16, 2, 4)])
+def test_separable_analysis_layout_matches_rfft2(H, W, modes, B, C):
+    """The two transform passes of FNO2d._analysis, emulated in FP64 with the
+    same output maps: the kept rfft2 modes land at dst[(m, re/im, b, c)]; the
+    scaled W-pass matrix applies c_kw / (H W) per mode."""
+    cfg = FNOConfig(H=H, W=W, width=C, modes=modes)
+    Fw, FwS, Fh = separable_dft_matrices(cfg)
+    M, R, NM = modes, B * C, cfg.n_modes
+    Hp = t1_half(H)
+    Fhp = padded_h_pass(Fh, H)
+    rng = np.random.default_rng(1)
+    x = rng.standard_normal((B, C, H, W))
+    kh, kw = mode_table(cfg)
+    ref = np.fft.rfft2(x, axes=(2, 3))[:, :, kh, kw]          # (B, C, NM)
+    for F, scale in ((Fw, np.ones(NM)), (FwS, np.where(kw == 0, 1.0, 2.0) / (H * W))):
+        T1 = np.zeros(M * R * 2 * Hp)
+        if H % 32 == 0:  # the transposed first pass
+            _place(F @ x.reshape(R * H, W).T, T1, M, R * 2 * Hp, Hp, H, 1, 2 * Hp)
+        else:
+            _place(x.reshape(R * H, W) @ F.T, T1, H, 1, 2 * Hp, M, R * 2 * Hp, Hp)
+        dst = np.zeros(NM * 2 * R)
+        _place(T1.reshape(M * R, 2 * Hp) @ Fhp.T, dst, R, 1, 2 * R, 2 * M, 2 * M * R, R)
+        got = dst.reshape(NM, 2, B, C)
+        want = ref.transpose(2, 0, 1) * scale[:, None, None]    # (NM, B, C)
+        assert np.abs(got[:, 0] - want.real).max() < 1e-9
+        assert np.abs(got[:, 1] - want.imag).max() < 1e-9
 
 
 def _bf16_round(params):
