@@ -89,22 +89,42 @@ struct StepParams {
 
 // ---------------------------------------------------------------------------
 // source injection and monitor accumulation for one cell's stored values
-// v[6] holds the new values of all six components for the cell (components
-// the solver does not carry hold zero).
+// A 2-D cell carries three components, F, A and B (TM: Ez, Hx, Hy; TE: Hz,
+// Ex, Ey); the others are zero.  They are three named scalars, never an array
+// indexed by a run-time component id, which would put them in a per-thread
+// stack frame.
 // ---------------------------------------------------------------------------
-template <typename T>
+template <typename T, int F, int A, int B>
+struct Cell3 {
+  T f, a, b;
+  __device__ __forceinline__ T get(int c) const {
+    return c == F ? f : c == A ? a : c == B ? b : T(0);
+  }
+  __device__ __forceinline__ void add(int c, T w) {
+    if (c == F)
+      f += w;
+    else if (c == A)
+      a += w;
+    else if (c == B)
+      b += w;
+  }
+};
+
+template <typename T, class Cell>
 __device__ __forceinline__ void inject_source(const StepParams<T>& p, int i, int j, int k,
-                                              T* v) {
-  if (p.src.comp >= 0 && p.src.box.contains(i, j, k)) v[p.src.comp] += p.src.wave[p.t];
+                                              Cell& v) {
+  if (p.src.comp >= 0 && p.src.box.contains(i, j, k)) v.add(p.src.comp, p.src.wave[p.t]);
 }
 
-template <typename T>
+template <typename T, class Cell>
 __device__ __forceinline__ void accumulate_monitors(const StepParams<T>& p, int i, int j, int k,
-                                                    const T* v) {
-  for (int m = 0; m < p.n_mon; ++m) {
+                                                    const Cell& v) {
+#pragma unroll
+  for (int m = 0; m < DN_MAX_MONITORS; ++m) {
+    if (m >= p.n_mon) break;
     const MonDev& M = p.mon[m];
     if (!M.box.contains(i, j, k)) continue;
-    const double x = static_cast<double>(v[M.comp]);
+    const double x = static_cast<double>(v.get(M.comp));
     const long long cell = M.box.offset(i, j, k);
     const double* ph = M.phase + (long long)p.t * M.nf * 2;
     for (int f = 0; f < M.nf; ++f) {
@@ -115,11 +135,11 @@ __device__ __forceinline__ void accumulate_monitors(const StepParams<T>& p, int 
   }
 }
 
-template <typename T>
+template <typename T, class Cell>
 __device__ __forceinline__ void record_probe(const StepParams<T>& p, int i, int j, int k,
-                                             const T* v) {
+                                             const Cell& v) {
   if (p.probe.comp >= 0 && i == p.probe.pos[0] && j == p.probe.pos[1] && k == p.probe.pos[2])
-    p.probe.out[p.t] = v[p.probe.comp];
+    p.probe.out[p.t] = v.get(p.probe.comp);
 }
 
 // Does plane i hold a source, monitor or probe cell?  (Unrolled over the

@@ -14,21 +14,32 @@
 //       Ey <- b_y[i] Ey - (dt/eps) (1+c_y[i]) dHz/di
 //       Hz <- b_x[j] b_y[i] Hz + dt [(1+c_x[j]) dEy/di - (1+c_y[i]) dEx/dj]
 //
-// One CTA owns a 16 x 32 tile.  The field differenced first (Ez for TM, Hz
-// for TE) is staged in shared memory with a one-cell ring; the tile's two
-// intermediate fields are computed for the tile plus the one-cell halo that
-// the second update needs (recomputed, never exchanged), so a step reads
-// each array once and writes each once (28 B per cell in FP32).  Ping-pong
-// buffers keep neighbouring CTAs from seeing this step's writes.
+// Work layout: a warp owns a strip of 32*VEC columns, VEC adjacent columns
+// per lane (16-byte loads and stores: VEC = 4 in FP32, 2 in FP64, when the
+// rows and arrays are 16-byte aligned; VEC = 1 otherwise), and R consecutive
+// rows, which it marches down.  The row neighbours of a cell are carried in
+// registers from one row to the next; column neighbours are in the lane's
+// own registers or, across a lane boundary, come from the adjacent lane by
+// shuffle; the two values a strip needs from outside its columns (TM: Hx at
+// column j0-1 and Ez at j0+32*VEC; TE: Hz at j0-1 and Ex at j0+32*VEC) are
+// loaded or recomputed by the edge lane with the owner's own arithmetic.
+// The intermediate field of the row just above (TM: Hy) or below (TE: Ey,
+// Ex) the warp's rows is recomputed the same way, so warps never exchange
+// data: no shared memory, no barrier.  A step reads each array once and
+// writes each once (28 B per cell in FP32); ping-pong buffers keep other
+// warps from seeing this step's writes.  R is chosen by the host so that the
+// grid fits one wave of resident CTAs.
+#include <algorithm>
+#include <type_traits>
+
 #include "dn_host.cuh"
 
 namespace dn {
 namespace {
 
-constexpr int TJ2 = 32;  // tile columns (x, contiguous)
-constexpr int TI2 = 16;  // tile rows (y)
-constexpr int NT2 = 256;
-constexpr int R2 = TI2 / (NT2 / 32);  // rows per thread
+constexpr int NT2 = 256;  // threads per CTA: 8 warps stacked along the rows
+constexpr int WARPS2 = NT2 / 32;
+constexpr unsigned FULL = 0xffffffffu;
 
 // curl record for the adjoint replay (see dn_curl_record)
 template <typename T>
@@ -38,173 +49,367 @@ struct CurlRec2 {
   int t0;
 };
 
-template <typename T, int POL, bool REC>
-__global__ void __launch_bounds__(NT2, 8) k_fdtd2d_step(const StepParams<T> p, const CurlRec2<T> rec) {
-  __shared__ T s_f[TI2 + 2][TJ2 + 2];
-  __shared__ T s_a[TI2 + 1][TJ2 + 1];
-  __shared__ T s_b[TI2 + 1][TJ2 + 1];
-  __shared__ T s_bx[TJ2 + 2], s_gx[TJ2 + 2];
-  __shared__ T s_by[TI2 + 2], s_gy[TI2 + 2];
-  __shared__ int s_skip;
-  // a previous launch that recorded an error turns this one into a no-op
-  if (threadIdx.x == 0)
-    s_skip = p.status != nullptr && *reinterpret_cast<volatile int*>(p.status) != 0;
-  __syncthreads();
-  if (s_skip) return;
+template <typename T>
+__device__ __forceinline__ T ld(const T* a, long long o, bool ok) {
+  return ok ? __ldg(a + o) : T(0);
+}
 
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int i0 = blockIdx.y * TI2, j0 = blockIdx.x * TJ2;
+// VEC adjacent values of one row, from column jv
+template <typename T, int VEC>
+struct Vec {
+  T v[VEC];
+  __device__ __forceinline__ T& operator[](int q) { return v[q]; }
+  __device__ __forceinline__ const T& operator[](int q) const { return v[q]; }
+};
+
+// Columns jv .. jv+VEC-1 at offset o; columns at or past W (and all of them
+// when !ok) read as 0.  One 16-byte load when all VEC columns are in the
+// grid (`full`), else one load per column in the grid.
+template <typename T, int VEC>
+__device__ __forceinline__ Vec<T, VEC> ldv(const T* a, long long o, bool ok, bool full, int jv,
+                                           int W) {
+  Vec<T, VEC> r;
+  if (VEC > 1 && ok && full) {
+    if constexpr (VEC == 4 && std::is_same<T, float>::value) {
+      const float4 x = __ldg(reinterpret_cast<const float4*>(a + o));
+      r[0] = x.x, r[1] = x.y, r[2] = x.z, r[3] = x.w;
+      return r;
+    } else if constexpr (VEC == 2 && std::is_same<T, double>::value) {
+      const double2 x = __ldg(reinterpret_cast<const double2*>(a + o));
+      r[0] = x.x, r[1] = x.y;
+      return r;
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < VEC; ++q) r[q] = ld(a, o + q, ok && jv + q < W);
+  return r;
+}
+
+// Store the columns of v that are in the grid (one 16-byte store when all are).
+template <typename T, int VEC>
+__device__ __forceinline__ void stv(T* a, long long o, const Vec<T, VEC>& v, bool full, int jv,
+                                    int W) {
+  if (VEC > 1 && full) {
+    if constexpr (VEC == 4 && std::is_same<T, float>::value) {
+      *reinterpret_cast<float4*>(a + o) = make_float4(v[0], v[1], v[2], v[3]);
+      return;
+    } else if constexpr (VEC == 2 && std::is_same<T, double>::value) {
+      *reinterpret_cast<double2*>(a + o) = make_double2(v[0], v[1]);
+      return;
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < VEC; ++q)
+    if (jv + q < W) a[o + q] = v[q];
+}
+
+// Does row i hold a source, monitor or probe cell?  (A superset test per
+// row; the per-cell tests in the helpers decide.  Unrolled over the fixed
+// monitor capacity so the parameter array is never indexed at run time.)
+template <typename T>
+__device__ __forceinline__ bool row_special(const StepParams<T>& p, int i) {
+  bool any = p.src.comp >= 0 && i >= p.src.box.lo[1] && i < p.src.box.hi[1];
+  any |= p.probe.comp >= 0 && p.probe.pos[1] == i;
+#pragma unroll
+  for (int m = 0; m < DN_MAX_MONITORS; ++m)
+    any |= m < p.n_mon && i >= p.mon[m].box.lo[1] && i < p.mon[m].box.hi[1];
+  return any;
+}
+
+// Store row i's new values for the lane's columns: f = Ez (TM) / Hz (TE),
+// a = Hx / Ex, b = Hy / Ey.  On rows with a source, monitor or probe the soft
+// source is added per cell and the monitors and probe see the stored values.
+template <typename T, int POL, int VEC>
+__device__ __forceinline__ void store_row(const StepParams<T>& p, bool special, int i, int jv,
+                                          long long o, bool full, Vec<T, VEC> f, Vec<T, VEC> a,
+                                          Vec<T, VEC> b) {
+  constexpr int F = (POL == DN_TM) ? DN_EZ : DN_HZ;
+  constexpr int A = (POL == DN_TM) ? DN_HX : DN_EX;
+  constexpr int B = (POL == DN_TM) ? DN_HY : DN_EY;
+  const int W = p.W;
+  if (special) {
+#pragma unroll
+    for (int q = 0; q < VEC; ++q) {
+      if (jv + q >= W) continue;
+      Cell3<T, F, A, B> v{f[q], a[q], b[q]};
+      inject_source(p, 0, i, jv + q, v);
+      if (p.n_mon) accumulate_monitors(p, 0, i, jv + q, v);
+      record_probe(p, 0, i, jv + q, v);
+      f[q] = v.f;
+      a[q] = v.a;
+      b[q] = v.b;
+    }
+  }
+  stv(p.out[F], o, f, full, jv, W);
+  stv(p.out[A], o, a, full, jv, W);
+  stv(p.out[B], o, b, full, jv, W);
+}
+
+// Column profile of the lane's columns (1 outside the grid).
+template <typename T, int VEC>
+__device__ __forceinline__ void column_profile(const StepParams<T>& p, int jv, Vec<T, VEC>& bx,
+                                               Vec<T, VEC>& gx) {
+#pragma unroll
+  for (int q = 0; q < VEC; ++q) {
+    const int j = jv + q;
+    bx[q] = j < p.W ? static_cast<T>(p.b[2][j]) : T(1);
+    gx[q] = j < p.W ? static_cast<T>(1.0 + p.c[2][j]) : T(1);
+  }
+}
+
+// TM: rows [ia, ib) of the strip of columns from j0.
+template <typename T, int VEC, bool REC>
+__device__ __forceinline__ void march_tm(const StepParams<T>& p, const CurlRec2<T>& rec, int j0,
+                                         int ia, int ib) {
+  using V = Vec<T, VEC>;
+  const int lane = threadIdx.x & 31;
   const int H = p.H, W = p.W;
   const long long py = p.py;
-  constexpr int F = (POL == DN_TM) ? DN_EZ : DN_HZ;
+  const int jv = j0 + lane * VEC;
+  const bool any = jv < W, full = jv + VEC <= W;
   const T dt = p.dt, idl = p.inv_dl;
+  const T* Ez = p.in[DN_EZ];
+  const T* Hx = p.in[DN_HX];
+  const T* Hy = p.in[DN_HY];
+  V bx, gx;
+  column_profile(p, jv, bx, gx);
+  const bool edge_l = lane == 0 && j0 > 0;         // recomputes Hx at column j0-1
+  const bool edge_r = lane == 31 && jv + VEC < W;  // loads Ez at column j0+32*VEC
 
-  // profile tables: entry t <-> position origin - 1 + t
-  for (int t = threadIdx.x; t < TJ2 + 2; t += NT2) {
-    const int j = j0 - 1 + t;
-    const bool ok = j >= 0 && j < W;
-    s_bx[t] = ok ? static_cast<T>(p.b[2][j]) : T(1);
-    s_gx[t] = ok ? static_cast<T>(1.0 + p.c[2][j]) : T(1);
-  }
-  for (int t = threadIdx.x; t < TI2 + 2; t += NT2) {
-    const int i = i0 - 1 + t;
-    const bool ok = i >= 0 && i < H;
-    s_by[t] = ok ? static_cast<T>(p.b[1][i]) : T(1);
-    s_gy[t] = ok ? static_cast<T>(1.0 + p.c[1][i]) : T(1);
-  }
-  for (int t = threadIdx.x; t < (TI2 + 2) * (TJ2 + 2); t += NT2) {
-    const int r = t / (TJ2 + 2), c = t % (TJ2 + 2);
-    const int i = i0 - 1 + r, j = j0 - 1 + c;
-    s_f[r][c] = (i >= 0 && i < H && j >= 0 && j < W) ? p.in[F][i * py + j] : T(0);
-  }
-  __syncthreads();
-
-  const int jj = lane;
-  const int j = j0 + jj;
-  T a_own[R2], b_own[R2];  // TM: Hx, Hy   TE: Ex, Ey  (new values of owned cells)
-
-  if (POL == DN_TM) {
-    // ---- H from old Ez: owned cells ------------------------------------
+  long long o = (long long)ia * py + jv;
+  V ez_c = ldv<T, VEC>(Ez, o, any, full, jv, W);
+  // Hy of row ia-1, recomputed with its owner's arithmetic
+  V hy_up;
 #pragma unroll
-    for (int r = 0; r < R2; ++r) {
-      const int ii = warp + 8 * r, i = i0 + ii;
-      a_own[r] = b_own[r] = T(0);
-      if (i < H && j < W) {
-        const long long o = i * py + j;
-        const T ez = s_f[ii + 1][jj + 1];
-        const T dj = (j < W - 1) ? s_f[ii + 1][jj + 2] - ez : T(0);
-        const T di = (i < H - 1) ? s_f[ii + 2][jj + 1] - ez : T(0);
-        a_own[r] = s_by[ii + 1] * p.in[DN_HX][o] - dt * s_gy[ii + 1] * (dj * idl);
-        b_own[r] = s_bx[jj + 1] * p.in[DN_HY][o] + dt * s_gx[jj + 1] * (di * idl);
-      }
-      s_a[ii][jj + 1] = a_own[r];
-      s_b[ii + 1][jj] = b_own[r];
-    }
-    // ---- halos: Hx at column j0-1, Hy at row i0-1 ------------------------
-    if (warp == 0 && lane < TI2) {
-      const int ii = lane, i = i0 + ii, jh = j0 - 1;
-      T v = T(0);
-      if (jh >= 0 && i < H) {
-        const T dj = s_f[ii + 1][1] - s_f[ii + 1][0];
-        v = s_by[ii + 1] * p.in[DN_HX][i * py + jh] - dt * s_gy[ii + 1] * (dj * idl);
-      }
-      s_a[ii][0] = v;
-    } else if (warp == 1) {
-      const int ih = i0 - 1;
-      T v = T(0);
-      if (ih >= 0 && j < W) {
-        const T di = s_f[1][jj + 1] - s_f[0][jj + 1];
-        v = s_bx[jj + 1] * p.in[DN_HY][ih * py + j] + dt * s_gx[jj + 1] * (di * idl);
-      }
-      s_b[0][jj] = v;
-    }
-  } else {
-    // ---- E from old Hz: owned cells ------------------------------------
+  for (int q = 0; q < VEC; ++q) hy_up[q] = T(0);
+  if (ia > 0) {
+    const V ez_u = ldv<T, VEC>(Ez, o - py, any, full, jv, W);
+    const V hy_o = ldv<T, VEC>(Hy, o - py, any, full, jv, W);
 #pragma unroll
-    for (int r = 0; r < R2; ++r) {
-      const int ii = warp + 8 * r, i = i0 + ii;
-      a_own[r] = b_own[r] = T(0);
-      if (i < H && j < W) {
-        const long long o = i * py + j;
-        const T ce = p.ce[o];
-        const T hz = s_f[ii + 1][jj + 1];
-        const T dj = (j > 0) ? hz - s_f[ii + 1][jj] : T(0);
-        const T di = (i > 0) ? hz - s_f[ii][jj + 1] : T(0);
-        const T curl_x = s_gx[jj + 1] * (dj * idl);
-        const T curl_y = -(s_gy[ii + 1] * (di * idl));
-        a_own[r] = s_bx[jj + 1] * p.in[DN_EX][o] + ce * curl_x;
-        b_own[r] = s_by[ii + 1] * p.in[DN_EY][o] + ce * curl_y;
-        if (REC) {
-          const long long oc = (long long)(p.t - rec.t0) * rec.stride + o;
-          rec.curl[0][oc] = curl_x;
-          rec.curl[1][oc] = curl_y;
-        }
-      }
-      s_a[ii][jj] = a_own[r];
-      s_b[ii][jj] = b_own[r];
-    }
-    // ---- halos: Ex at column j0+TJ, Ey at row i0+TI ----------------------
-    if (warp == 0 && lane < TI2) {
-      const int ii = lane, i = i0 + ii, jh = j0 + TJ2;
-      T v = T(0);
-      if (jh < W && i < H) {
-        const long long o = i * py + jh;
-        const T dj = s_f[ii + 1][TJ2 + 1] - s_f[ii + 1][TJ2];
-        v = s_bx[TJ2 + 1] * p.in[DN_EX][o] + p.ce[o] * s_gx[TJ2 + 1] * (dj * idl);
-      }
-      s_a[ii][TJ2] = v;
-    } else if (warp == 1) {
-      const int ih = i0 + TI2;
-      T v = T(0);
-      if (ih < H && j < W) {
-        const long long o = ih * py + j;
-        const T di = s_f[TI2 + 1][jj + 1] - s_f[TI2][jj + 1];
-        v = s_by[TI2 + 1] * p.in[DN_EY][o] - p.ce[o] * s_gy[TI2 + 1] * (di * idl);
-      }
-      s_b[TI2][jj] = v;
-    }
+    for (int q = 0; q < VEC; ++q) hy_up[q] = bx[q] * hy_o[q] + dt * gx[q] * ((ez_c[q] - ez_u[q]) * idl);
   }
-  __syncthreads();
+  for (int i = ia; i < ib; ++i, o += py) {
+    const V ez_n = ldv<T, VEC>(Ez, o + py, any && i + 1 < H, full, jv, W);
+    const V hx_o = ldv<T, VEC>(Hx, o, any, full, jv, W);
+    const V hy_o = ldv<T, VEC>(Hy, o, any, full, jv, W);
+    const V c_e = ldv<T, VEC>(p.ce, o, any, full, jv, W);
+    const T ez_r31 = ld(Ez, o + VEC, edge_r);
+    const T ez_l0 = ld(Ez, o - 1, edge_l);
+    const T hx_l0 = ld(Hx, o - 1, edge_l);
+    const T by = static_cast<T>(p.b[1][i]);
+    const T gy = static_cast<T>(1.0 + p.c[1][i]);
 
-  // ---- second update, source, monitors, stores ----------------------------
+    T ez_rl = __shfl_down_sync(FULL, ez_c[0], 1);
+    if (lane == 31) ez_rl = ez_r31;
+    V hx, hy;
 #pragma unroll
-  for (int r = 0; r < R2; ++r) {
-    const int ii = warp + 8 * r, i = i0 + ii;
-    if (i >= H || j >= W) continue;
-    const long long o = i * py + j;
-    T v[6];
-    const T fo = s_f[ii + 1][jj + 1];
-    const T bb = s_bx[jj + 1] * s_by[ii + 1];
-    if (POL == DN_TM) {
-      const T dHy = (i > 0) ? s_b[ii + 1][jj] - s_b[ii][jj] : T(0);
-      const T dHx = (j > 0) ? s_a[ii][jj + 1] - s_a[ii][jj] : T(0);
-      const T curl_z = s_gx[jj + 1] * (dHy * idl) - s_gy[ii + 1] * (dHx * idl);
-      v[DN_EZ] = bb * fo + p.ce[o] * curl_z;
-      if (REC) rec.curl[2][(long long)(p.t - rec.t0) * rec.stride + o] = curl_z;
-      v[DN_HX] = a_own[r];
-      v[DN_HY] = b_own[r];
-      v[DN_HZ] = v[DN_EX] = v[DN_EY] = T(0);
-    } else {
-      const T dEy = (i < H - 1) ? s_b[ii + 1][jj] - s_b[ii][jj] : T(0);
-      const T dEx = (j < W - 1) ? s_a[ii][jj + 1] - s_a[ii][jj] : T(0);
-      v[DN_HZ] = bb * fo + dt * (s_gx[jj + 1] * (dEy * idl) - s_gy[ii + 1] * (dEx * idl));
-      v[DN_EX] = a_own[r];
-      v[DN_EY] = b_own[r];
-      v[DN_EZ] = v[DN_HX] = v[DN_HY] = T(0);
+    for (int q = 0; q < VEC; ++q) {
+      const int j = jv + q;
+      const T ez_r = (q < VEC - 1) ? ez_c[q < VEC - 1 ? q + 1 : q] : ez_rl;
+      const T dj = (j < W - 1) ? ez_r - ez_c[q] : T(0);
+      const T di = (i < H - 1) ? ez_n[q] - ez_c[q] : T(0);
+      hx[q] = by * hx_o[q] - dt * gy * (dj * idl);
+      hy[q] = bx[q] * hy_o[q] + dt * gx[q] * (di * idl);
     }
-    inject_source(p, 0, i, j, v);
-    if (p.n_mon) accumulate_monitors(p, 0, i, j, v);
-    record_probe(p, 0, i, j, v);
-    if (POL == DN_TM) {
-      p.out[DN_EZ][o] = v[DN_EZ];
-      p.out[DN_HX][o] = v[DN_HX];
-      p.out[DN_HY][o] = v[DN_HY];
-    } else {
-      p.out[DN_HZ][o] = v[DN_HZ];
-      p.out[DN_EX][o] = v[DN_EX];
-      p.out[DN_EY][o] = v[DN_EY];
+    T hx_ll = __shfl_up_sync(FULL, hx[VEC - 1], 1);
+    if (lane == 0) hx_ll = edge_l ? by * hx_l0 - dt * gy * ((ez_c[0] - ez_l0) * idl) : T(0);
+    V ez, cz;
+#pragma unroll
+    for (int q = 0; q < VEC; ++q) {
+      const int j = jv + q;
+      const T hx_l = (q > 0) ? hx[q > 0 ? q - 1 : 0] : hx_ll;
+      const T dHy = (i > 0) ? hy[q] - hy_up[q] : T(0);
+      const T dHx = (j > 0) ? hx[q] - hx_l : T(0);
+      cz[q] = gx[q] * (dHy * idl) - gy * (dHx * idl);
+      ez[q] = (bx[q] * by) * ez_c[q] + c_e[q] * cz[q];
     }
+    const bool sp = row_special(p, i);
+    if (any) {
+      if (REC) stv(rec.curl[2], (long long)(p.t - rec.t0) * rec.stride + o, cz, full, jv, W);
+      store_row<T, DN_TM, VEC>(p, sp, i, jv, o, full, ez, hx, hy);
+    }
+    hy_up = hy;
+    ez_c = ez_n;
   }
+}
+
+// TE: rows [ia, ib) of the strip of columns from j0.  E of row i+1 is
+// computed in iteration i (Hz of row i needs Ey of row i+1) and carried to
+// iteration i+1.
+template <typename T, int VEC, bool REC>
+__device__ __forceinline__ void march_te(const StepParams<T>& p, const CurlRec2<T>& rec, int j0,
+                                         int ia, int ib) {
+  using V = Vec<T, VEC>;
+  const int lane = threadIdx.x & 31;
+  const int H = p.H, W = p.W;
+  const long long py = p.py;
+  const int jv = j0 + lane * VEC;
+  const bool any = jv < W, full = jv + VEC <= W;
+  const T dt = p.dt, idl = p.inv_dl;
+  const T* Hz = p.in[DN_HZ];
+  const T* Ex = p.in[DN_EX];
+  const T* Ey = p.in[DN_EY];
+  V bx, gx;
+  column_profile(p, jv, bx, gx);
+  const bool edge_l = lane == 0 && j0 > 0;         // loads Hz at column j0-1
+  const bool edge_r = lane == 31 && jv + VEC < W;  // recomputes Ex at column j0+32*VEC
+  const T bx_r = edge_r ? static_cast<T>(p.b[2][jv + VEC]) : T(1);
+  const T gx_r = edge_r ? static_cast<T>(1.0 + p.c[2][jv + VEC]) : T(1);
+
+  // new Ex, Ey of row r (offset oo) from old Hz of rows r (hz) and r-1
+  // (hz_u), with the curl terms the adjoint replays; all 32 lanes call it
+  auto e_row = [&](int r, long long oo, const V& hz, const V& hz_u, V& ex, V& ey, V& cx, V& cy) {
+    const V ex_o = ldv<T, VEC>(Ex, oo, any, full, jv, W);
+    const V ey_o = ldv<T, VEC>(Ey, oo, any, full, jv, W);
+    const V c_e = ldv<T, VEC>(p.ce, oo, any, full, jv, W);
+    const T hz_l0 = ld(Hz, oo - 1, edge_l);
+    const T by = static_cast<T>(p.b[1][r]);
+    const T gy = static_cast<T>(1.0 + p.c[1][r]);
+    T hz_ll = __shfl_up_sync(FULL, hz[VEC - 1], 1);
+    if (lane == 0) hz_ll = hz_l0;
+#pragma unroll
+    for (int q = 0; q < VEC; ++q) {
+      const int j = jv + q;
+      const T hz_l = (q > 0) ? hz[q > 0 ? q - 1 : 0] : hz_ll;
+      const T dj = (j > 0) ? hz[q] - hz_l : T(0);
+      const T di = (r > 0) ? hz[q] - hz_u[q] : T(0);
+      cx[q] = gx[q] * (dj * idl);
+      cy[q] = -(gy * (di * idl));
+      ex[q] = bx[q] * ex_o[q] + c_e[q] * cx[q];
+      ey[q] = by * ey_o[q] + c_e[q] * cy[q];
+    }
+  };
+
+  long long o = (long long)ia * py + jv;
+  V hz_c = ldv<T, VEC>(Hz, o, any, full, jv, W);
+  const V hz_u = ldv<T, VEC>(Hz, o - py, any && ia > 0, full, jv, W);
+  V ex_c, ey_c, cx_c, cy_c;
+  e_row(ia, o, hz_c, hz_u, ex_c, ey_c, cx_c, cy_c);
+  for (int i = ia; i < ib; ++i, o += py) {
+    const bool nxt = i + 1 < H;
+    const V hz_n = ldv<T, VEC>(Hz, o + py, any && nxt, full, jv, W);
+    const T ex_o31 = ld(Ex, o + VEC, edge_r);
+    const T ce31 = ld(p.ce, o + VEC, edge_r);
+    const T hz31 = ld(Hz, o + VEC, edge_r);
+    const T by = static_cast<T>(p.b[1][i]);
+    const T gy = static_cast<T>(1.0 + p.c[1][i]);
+    V ex_n, ey_n, cx_n, cy_n;
+#pragma unroll
+    for (int q = 0; q < VEC; ++q) ex_n[q] = ey_n[q] = cx_n[q] = cy_n[q] = T(0);
+    if (nxt) e_row(i + 1, o + py, hz_n, hz_c, ex_n, ey_n, cx_n, cy_n);
+
+    T ex_rl = __shfl_down_sync(FULL, ex_c[0], 1);
+    if (lane == 31)
+      ex_rl = edge_r ? bx_r * ex_o31 + ce31 * (gx_r * ((hz31 - hz_c[VEC - 1]) * idl)) : T(0);
+    V hz;
+#pragma unroll
+    for (int q = 0; q < VEC; ++q) {
+      const int j = jv + q;
+      const T ex_r = (q < VEC - 1) ? ex_c[q < VEC - 1 ? q + 1 : q] : ex_rl;
+      const T dEy = (i < H - 1) ? ey_n[q] - ey_c[q] : T(0);
+      const T dEx = (j < W - 1) ? ex_r - ex_c[q] : T(0);
+      hz[q] = (bx[q] * by) * hz_c[q] + dt * (gx[q] * (dEy * idl) - gy * (dEx * idl));
+    }
+    const bool sp = row_special(p, i);
+    if (any) {
+      if (REC) {
+        const long long oc = (long long)(p.t - rec.t0) * rec.stride + o;
+        stv(rec.curl[0], oc, cx_c, full, jv, W);
+        stv(rec.curl[1], oc, cy_c, full, jv, W);
+      }
+      store_row<T, DN_TE, VEC>(p, sp, i, jv, o, full, hz, ex_c, ey_c);
+    }
+    hz_c = hz_n;
+    ex_c = ex_n;
+    ey_c = ey_n;
+    cx_c = cx_n;
+    cy_c = cy_n;
+  }
+}
+
+template <typename T, int POL, bool REC, int VEC>
+__global__ void __launch_bounds__(NT2) k_fdtd2d_step(const StepParams<T> p, const CurlRec2<T> rec,
+                                                     int R) {
+  // a previous launch that recorded an error turns this one into a no-op
+  if (p.status != nullptr && *reinterpret_cast<volatile int*>(p.status) != 0) return;
+  const int warp = threadIdx.x >> 5;
+  const int j0 = blockIdx.x * 32 * VEC;
+  const long long ia = ((long long)blockIdx.y * WARPS2 + warp) * R;
+  if (ia >= p.H) return;  // whole warp: the shuffles below see all 32 lanes
+  const int ib = static_cast<int>(std::min<long long>(ia + R, p.H));
+  if (POL == DN_TM)
+    march_tm<T, VEC, REC>(p, rec, j0, static_cast<int>(ia), ib);
+  else
+    march_te<T, VEC, REC>(p, rec, j0, static_cast<int>(ia), ib);
+}
+
+// Rows per warp: the smallest R (at least 2) for which the grid of CTAs fits
+// one wave of resident CTAs, so that no SM runs a second, partial wave.
+template <typename T, int POL, bool REC, int VEC>
+int rows_per_warp(int H, int strips, int* R) {
+  static int per_sm = 0, nsm = 0;  // per kernel instance; identical on every B200
+  if (per_sm == 0) {
+    int dev = 0, n = 0, b = 0;
+    DN_CUDA_CHECK(cudaGetDevice(&dev));
+    DN_CUDA_CHECK(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+    DN_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &b, k_fdtd2d_step<T, POL, REC, VEC>, NT2, 0));
+    nsm = n;
+    per_sm = std::max(b, 1);
+  }
+  const long long slots = (long long)nsm * per_sm;
+  const long long row_ctas = std::max<long long>(1, slots / strips);
+  const long long r = (H + WARPS2 * row_ctas - 1) / (WARPS2 * row_ctas);
+  *R = static_cast<int>(std::max<long long>(2, r));
+  return DN_OK;
+}
+
+template <typename T, int POL, bool REC, int VEC>
+int launch_steps(StepParams<T>& p, const CurlRec2<T>& rec, void* const fa[6], void* const fb[6],
+                 int32_t t0, int32_t nsteps, cudaStream_t s) {
+  const int strips = (p.W + 32 * VEC - 1) / (32 * VEC);
+  int R = 2;
+  const int rc = rows_per_warp<T, POL, REC, VEC>(p.H, strips, &R);
+  if (rc != DN_OK) return rc;
+  const long long rows_per_cta = (long long)WARPS2 * R;
+  const dim3 grid(strips, static_cast<unsigned>((p.H + rows_per_cta - 1) / rows_per_cta));
+  for (int n = 0; n < nsteps; ++n) {
+    const bool even = (n % 2) == 0;
+    set_io(&p, even ? fa : fb, even ? fb : fa);
+    p.t = t0 + n;
+    k_fdtd2d_step<T, POL, REC, VEC><<<grid, NT2, 0, s>>>(p, rec, R);
+  }
+  DN_CUDA_CHECK(cudaGetLastError());
+  return DN_OK;
+}
+
+bool aligned16(const void* a) { return (reinterpret_cast<uintptr_t>(a) & 15) == 0; }
+
+// 16-byte row access needs the pitch, every array the polarisation uses and
+// (when recording) the curl slots and their step stride on 16-byte boundaries.
+template <typename T>
+bool vector_rows_ok(const dn_grid* g, void* const fa[6], void* const fb[6], const void* ce,
+                    const CurlRec2<T>* rec) {
+  if ((g->pitch_y * (int64_t)sizeof(T)) % 16 != 0 || !aligned16(ce)) return false;
+  const int comps[2][3] = {{DN_EZ, DN_HX, DN_HY}, {DN_HZ, DN_EX, DN_EY}};
+  for (int c : comps[g->pol == DN_TM ? 0 : 1])
+    if (!aligned16(fa[c]) || !aligned16(fb[c])) return false;
+  if (rec) {
+    if ((rec->stride * (long long)sizeof(T)) % 16 != 0) return false;
+    const int slots[2][2] = {{2, 2}, {0, 1}};
+    for (int c : slots[g->pol == DN_TM ? 0 : 1])
+      if (!aligned16(rec->curl[c])) return false;
+  }
+  return true;
+}
+
+template <typename T, int POL, bool REC>
+int launch_pol(const dn_grid* g, StepParams<T>& p, const CurlRec2<T>& rec, void* const fa[6],
+               void* const fb[6], const void* ce, int32_t t0, int32_t nsteps, cudaStream_t s) {
+  constexpr int VEC = 16 / static_cast<int>(sizeof(T));
+  if (vector_rows_ok<T>(g, fa, fb, ce, REC ? &rec : nullptr))
+    return launch_steps<T, POL, REC, VEC>(p, rec, fa, fb, t0, nsteps, s);
+  return launch_steps<T, POL, REC, 1>(p, rec, fa, fb, t0, nsteps, s);
 }
 
 template <typename T>
@@ -229,24 +434,15 @@ int run2d(const dn_grid* g, void* const fa[6], void* const fb[6], const void* ce
     rec.t0 = crec->t0;
   }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const dim3 grid((g->W + TJ2 - 1) / TJ2, (g->H + TI2 - 1) / TI2);
-  for (int n = 0; n < nsteps; ++n) {
-    const bool even = (n % 2) == 0;
-    set_io(&p, even ? fa : fb, even ? fb : fa);
-    p.t = t0 + n;
-    if (g->pol == DN_TM) {
-      if (record)
-        k_fdtd2d_step<T, DN_TM, true><<<grid, NT2, 0, s>>>(p, rec);
-      else
-        k_fdtd2d_step<T, DN_TM, false><<<grid, NT2, 0, s>>>(p, rec);
-    } else {
-      if (record)
-        k_fdtd2d_step<T, DN_TE, true><<<grid, NT2, 0, s>>>(p, rec);
-      else
-        k_fdtd2d_step<T, DN_TE, false><<<grid, NT2, 0, s>>>(p, rec);
-    }
+  if (nsteps > 0) {
+    if (g->pol == DN_TM)
+      rc = record ? launch_pol<T, DN_TM, true>(g, p, rec, fa, fb, ce, t0, nsteps, s)
+                  : launch_pol<T, DN_TM, false>(g, p, rec, fa, fb, ce, t0, nsteps, s);
+    else
+      rc = record ? launch_pol<T, DN_TE, true>(g, p, rec, fa, fb, ce, t0, nsteps, s)
+                  : launch_pol<T, DN_TE, false>(g, p, rec, fa, fb, ce, t0, nsteps, s);
+    if (rc != DN_OK) return rc;
   }
-  DN_CUDA_CHECK(cudaGetLastError());
   *final_in_b = nsteps % 2;
   return DN_OK;
 }

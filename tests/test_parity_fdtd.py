@@ -169,6 +169,59 @@ def test_2d_monitors_vs_oracle(cuda, pol):
     assert rel_l2(torch.view_as_real(got), torch.view_as_real(ref)) < 1e-11
 
 
+@pytest.mark.parametrize("pol,dtype", [("TM", torch.float32), ("TE", torch.float32),
+                                       ("TM", torch.float64), ("TE", torch.float64)])
+def test_2d_unaligned_rows_match_padded_rows(cuda, pol, dtype):
+    """The 2-D step through the C ABI with tight rows (pitch = W = 45: rows
+    not on 16-byte boundaries, one value per lane) against the engine's
+    padded rows (16-byte row access, with a partly filled last lane)."""
+    import ctypes
+
+    from diffnano_b200 import _lib
+    from diffnano_b200.solvers import _setup
+    from diffnano_b200.solvers._engine import Engine
+
+    H, W, T = 70, 45, 40
+    dl, courant = 20.0, 0.5
+    dt = courant * dl / 2 ** 0.5
+    src = {"type": "gaussian_pulse", "row": 9, "spread": 500.0, "t0": 800.0}
+    p = _lib.DN_TM if pol == "TM" else _lib.DN_TE
+    comp = _lib.DN_EZ if pol == "TM" else _lib.DN_HZ
+    eng = Engine(is3d=False, shape=(H, W), dl=dl, dt=dt, pml_layers=6, dtype=dtype, device=cuda,
+                 n_steps=T, wave=_setup.waveform_table(T, dt, OMEGA, src),
+                 src_box=_setup.source_box_2d((H, W), src), src_comp=comp, pol=p)
+    g = torch.Generator().manual_seed(11)
+    eng.set_eps(1.5 + 2.0 * torch.rand(H, W, dtype=torch.float64, generator=g))
+    assert eng.Wp != W and (eng.Wp * eng.A.element_size()) % 16 == 0
+    eng.run(0, T)
+
+    grid = type(eng.grid).from_buffer_copy(eng.grid)
+    grid.pitch_y, grid.pitch_z = W, H * W
+    fa = torch.zeros((6, H, W), dtype=dtype, device=cuda)
+    fb = torch.zeros_like(fa)
+    ce = eng.ce[0, :, :W].contiguous()
+    assert (W * fa.element_size()) % 16 != 0
+    out = ctypes.c_int32(0)
+    with torch.cuda.device(cuda):
+        stream = torch.cuda.current_stream(cuda).cuda_stream
+        rc = _lib.lib().dn_fdtd2d_run(
+            ctypes.byref(grid), _lib.PTR6(*[fa[c].data_ptr() for c in range(6)]),
+            _lib.PTR6(*[fb[c].data_ptr() for c in range(6)]), ce.data_ptr(),
+            ctypes.byref(eng.cpml), ctypes.byref(eng.src), None, 0,
+            ctypes.byref(_lib.DnProbe(component=_lib.DN_NONE)), None, 0, T,
+            eng.status.data_ptr(), ctypes.c_void_p(stream), ctypes.byref(out))
+    assert rc == _lib.DN_OK
+    eng.check_status()
+    res = fb if out.value else fa
+    tol = 1e-6 if dtype == torch.float32 else 1e-13
+    comps = (_lib.DN_EZ, _lib.DN_HX, _lib.DN_HY) if pol == "TM" else \
+        (_lib.DN_HZ, _lib.DN_EX, _lib.DN_EY)
+    for c in comps:
+        ref = eng.field(c)[0]
+        assert float(ref.abs().max()) > 0
+        assert rel_l2(res[c], ref) < tol
+
+
 def test_deterministic(cuda):
     shape = (32, 32, 32)
     eps = _seeded(shape, 6).to(cuda)
