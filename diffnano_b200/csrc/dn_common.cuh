@@ -87,61 +87,6 @@ struct StepParams {
   int* status;
 };
 
-// ---------------------------------------------------------------------------
-// source injection and monitor accumulation for one cell's stored values
-// A 2-D cell carries three components, F, A and B (TM: Ez, Hx, Hy; TE: Hz,
-// Ex, Ey); the others are zero.  They are three named scalars, never an array
-// indexed by a run-time component id, which would put them in a per-thread
-// stack frame.
-// ---------------------------------------------------------------------------
-template <typename T, int F, int A, int B>
-struct Cell3 {
-  T f, a, b;
-  __device__ __forceinline__ T get(int c) const {
-    return c == F ? f : c == A ? a : c == B ? b : T(0);
-  }
-  __device__ __forceinline__ void add(int c, T w) {
-    if (c == F)
-      f += w;
-    else if (c == A)
-      a += w;
-    else if (c == B)
-      b += w;
-  }
-};
-
-template <typename T, class Cell>
-__device__ __forceinline__ void inject_source(const StepParams<T>& p, int i, int j, int k,
-                                              Cell& v) {
-  if (p.src.comp >= 0 && p.src.box.contains(i, j, k)) v.add(p.src.comp, p.src.wave[p.t]);
-}
-
-template <typename T, class Cell>
-__device__ __forceinline__ void accumulate_monitors(const StepParams<T>& p, int i, int j, int k,
-                                                    const Cell& v) {
-#pragma unroll
-  for (int m = 0; m < DN_MAX_MONITORS; ++m) {
-    if (m >= p.n_mon) break;
-    const MonDev& M = p.mon[m];
-    if (!M.box.contains(i, j, k)) continue;
-    const double x = static_cast<double>(v.get(M.comp));
-    const long long cell = M.box.offset(i, j, k);
-    const double* ph = M.phase + (long long)p.t * M.nf * 2;
-    for (int f = 0; f < M.nf; ++f) {
-      double* a = M.acc + ((long long)f * M.ncell + cell) * 2;
-      a[0] = fma(x, ph[2 * f + 0], a[0]);
-      a[1] = fma(x, ph[2 * f + 1], a[1]);
-    }
-  }
-}
-
-template <typename T, class Cell>
-__device__ __forceinline__ void record_probe(const StepParams<T>& p, int i, int j, int k,
-                                             const Cell& v) {
-  if (p.probe.comp >= 0 && i == p.probe.pos[0] && j == p.probe.pos[1] && k == p.probe.pos[2])
-    p.probe.out[p.t] = v.get(p.probe.comp);
-}
-
 // Does plane i hold a source, monitor or probe cell?  (Unrolled over the
 // fixed monitor capacity so the parameter array is never indexed at run time,
 // which would move it to local memory.)

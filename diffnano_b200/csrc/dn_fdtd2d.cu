@@ -28,7 +28,8 @@
 // data: no shared memory, no barrier.  A step reads each array once and
 // writes each once (28 B per cell in FP32); ping-pong buffers keep other
 // warps from seeing this step's writes.  R is chosen by the host so that the
-// grid fits one wave of resident CTAs.
+// grid fits one wave of resident CTAs (3 per SM), with a floor that keeps the
+// recomputed rows a small share of a warp's loads.
 #include <algorithm>
 #include <type_traits>
 
@@ -116,9 +117,86 @@ __device__ __forceinline__ bool row_special(const StepParams<T>& p, int i) {
   return any;
 }
 
+// Component c of the lane's cell q.  A 2-D cell carries three components
+// (TM: Ez, Hx, Hy; TE: Hz, Ex, Ey) held as three named values, never as an
+// array indexed by a run-time component id, which would move it to a
+// per-thread stack frame.
+template <int F, int A, int B, typename T, int VEC>
+__device__ __forceinline__ T pick(int c, const Vec<T, VEC>& f, const Vec<T, VEC>& a,
+                                  const Vec<T, VEC>& b, int q) {
+  return c == F ? f[q] : c == A ? a[q] : c == B ? b[q] : T(0);
+}
+
+// Row i holds a source, monitor or probe cell: add the soft source to the
+// values about to be stored, accumulate the monitors' running DFTs of those
+// values and record the probe.  The monitor accumulators of one frequency are
+// all loaded before any is stored, so a lane waits for one memory round trip
+// per frequency, not one per cell and frequency.
+template <typename T, int POL, int VEC>
+__device__ __forceinline__ void special_row(const StepParams<T>& p, int i, int jv,
+                                            Vec<T, VEC>& f, Vec<T, VEC>& a, Vec<T, VEC>& b) {
+  constexpr int F = (POL == DN_TM) ? DN_EZ : DN_HZ;
+  constexpr int A = (POL == DN_TM) ? DN_HX : DN_EX;
+  constexpr int B = (POL == DN_TM) ? DN_HY : DN_EY;
+  const int W = p.W;
+  if (p.src.comp >= 0 && i >= p.src.box.lo[1] && i < p.src.box.hi[1]) {
+    const int c = p.src.comp;
+    const T w = p.src.wave[p.t];
+#pragma unroll
+    for (int q = 0; q < VEC; ++q) {
+      if (jv + q >= W || !p.src.box.contains(0, i, jv + q)) continue;
+      if (c == F)
+        f[q] += w;
+      else if (c == A)
+        a[q] += w;
+      else if (c == B)
+        b[q] += w;
+    }
+  }
+#pragma unroll
+  for (int m = 0; m < DN_MAX_MONITORS; ++m) {
+    if (m >= p.n_mon) break;
+    const MonDev& M = p.mon[m];
+    bool in[VEC], any = false;
+    long long cell[VEC];
+    double x[VEC];
+#pragma unroll
+    for (int q = 0; q < VEC; ++q) {
+      in[q] = jv + q < W && M.box.contains(0, i, jv + q);
+      cell[q] = in[q] ? M.box.offset(0, i, jv + q) : 0;
+      x[q] = static_cast<double>(pick<F, A, B>(M.comp, f, a, b, q));
+      any |= in[q];
+    }
+    if (!any) continue;
+    const double* ph = M.phase + (long long)p.t * M.nf * 2;
+    for (int fr = 0; fr < M.nf; ++fr) {
+      const double c = ph[2 * fr + 0], s = ph[2 * fr + 1];
+      double* base = M.acc + (long long)fr * M.ncell * 2;
+      double re[VEC], im[VEC];
+#pragma unroll
+      for (int q = 0; q < VEC; ++q) {
+        re[q] = in[q] ? base[cell[q] * 2 + 0] : 0.0;
+        im[q] = in[q] ? base[cell[q] * 2 + 1] : 0.0;
+      }
+#pragma unroll
+      for (int q = 0; q < VEC; ++q) {
+        if (!in[q]) continue;
+        base[cell[q] * 2 + 0] = fma(x[q], c, re[q]);
+        base[cell[q] * 2 + 1] = fma(x[q], s, im[q]);
+      }
+    }
+  }
+  if (p.probe.comp >= 0 && p.probe.pos[0] == 0 && p.probe.pos[1] == i) {
+#pragma unroll
+    for (int q = 0; q < VEC; ++q)
+      if (jv + q == p.probe.pos[2] && jv + q < W)
+        p.probe.out[p.t] = pick<F, A, B>(p.probe.comp, f, a, b, q);
+  }
+}
+
 // Store row i's new values for the lane's columns: f = Ez (TM) / Hz (TE),
-// a = Hx / Ex, b = Hy / Ey.  On rows with a source, monitor or probe the soft
-// source is added per cell and the monitors and probe see the stored values.
+// a = Hx / Ex, b = Hy / Ey; rows with a source, monitor or probe go through
+// special_row first.
 template <typename T, int POL, int VEC>
 __device__ __forceinline__ void store_row(const StepParams<T>& p, bool special, int i, int jv,
                                           long long o, bool full, Vec<T, VEC> f, Vec<T, VEC> a,
@@ -127,19 +205,7 @@ __device__ __forceinline__ void store_row(const StepParams<T>& p, bool special, 
   constexpr int A = (POL == DN_TM) ? DN_HX : DN_EX;
   constexpr int B = (POL == DN_TM) ? DN_HY : DN_EY;
   const int W = p.W;
-  if (special) {
-#pragma unroll
-    for (int q = 0; q < VEC; ++q) {
-      if (jv + q >= W) continue;
-      Cell3<T, F, A, B> v{f[q], a[q], b[q]};
-      inject_source(p, 0, i, jv + q, v);
-      if (p.n_mon) accumulate_monitors(p, 0, i, jv + q, v);
-      record_probe(p, 0, i, jv + q, v);
-      f[q] = v.f;
-      a[q] = v.a;
-      b[q] = v.b;
-    }
-  }
+  if (special) special_row<T, POL, VEC>(p, i, jv, f, a, b);
   stv(p.out[F], o, f, full, jv, W);
   stv(p.out[A], o, a, full, jv, W);
   stv(p.out[B], o, b, full, jv, W);
@@ -328,7 +394,7 @@ __device__ __forceinline__ void march_te(const StepParams<T>& p, const CurlRec2<
 }
 
 template <typename T, int POL, bool REC, int VEC>
-__global__ void __launch_bounds__(NT2) k_fdtd2d_step(const StepParams<T> p, const CurlRec2<T> rec,
+__global__ void __launch_bounds__(NT2, 3) k_fdtd2d_step(const StepParams<T> p, const CurlRec2<T> rec,
                                                      int R) {
   // a previous launch that recorded an error turns this one into a no-op
   if (p.status != nullptr && *reinterpret_cast<volatile int*>(p.status) != 0) return;
@@ -343,8 +409,11 @@ __global__ void __launch_bounds__(NT2) k_fdtd2d_step(const StepParams<T> p, cons
     march_te<T, VEC, REC>(p, rec, j0, static_cast<int>(ia), ib);
 }
 
-// Rows per warp: the smallest R (at least 2) for which the grid of CTAs fits
-// one wave of resident CTAs, so that no SM runs a second, partial wave.
+// Rows per warp: the smallest R for which the grid of CTAs fits one wave of
+// resident CTAs, so that no SM runs a second, partial wave; at least 4 (a
+// warp recomputes about three rows of loads above or below its own, so short
+// marches spend a large share on them) unless that leaves fewer than 8 warps
+// per SM, then at least 2.
 template <typename T, int POL, bool REC, int VEC>
 int rows_per_warp(int H, int strips, int* R) {
   static int per_sm = 0, nsm = 0;  // per kernel instance; identical on every B200
@@ -360,7 +429,9 @@ int rows_per_warp(int H, int strips, int* R) {
   const long long slots = (long long)nsm * per_sm;
   const long long row_ctas = std::max<long long>(1, slots / strips);
   const long long r = (H + WARPS2 * row_ctas - 1) / (WARPS2 * row_ctas);
-  *R = static_cast<int>(std::max<long long>(2, r));
+  const long long warps4 = (long long)strips * ((H + 3) / 4);
+  const long long r_min = warps4 >= 8LL * nsm ? 4 : 2;
+  *R = static_cast<int>(std::max<long long>(r_min, r));
   return DN_OK;
 }
 
