@@ -19,187 +19,262 @@
 // zero where the forward difference is).  TE is the mirror image: the adjoint
 // of the Hz update comes first, then the E updates.
 //
-// Data flow per launch: TM stages u = ce*lambda_Ez with a one-cell ring, TE
-// stages lambda_Hz with a one-cell ring; the intermediate adjoint fields are
-// computed for the tile plus the halo the second half needs (recomputed, not
-// exchanged) -- the same shape as the forward kernel, so the same 16 x 32
-// tiles and ping-pong buffers.
+// Work layout (the forward step's): a warp owns a strip of 32*VEC columns,
+// VEC adjacent columns per lane with 16-byte loads and stores when rows and
+// arrays are 16-byte aligned, and R consecutive rows, which it marches down
+// with the row neighbours in registers and the column neighbours from its own
+// registers or the adjacent lane (shuffle).  The edge lanes load or recompute
+// the one value outside the strip (TM: vx at column j0-1, u at j0+32*VEC;
+// TE: lambda_Hz at j0-1, ux at j0+32*VEC) and the warp recomputes the
+// intermediate row above (TM: vy) or below (TE: lambda_E', uy) its own, with
+// the owner's arithmetic: no shared memory, no barrier; ping-pong buffers.
+#include <algorithm>
+
 #include "dn_adjoint.cuh"
+#include "dn_strip.cuh"
 
 namespace dn {
 namespace {
 
-constexpr int TJ = 32;
-constexpr int TI = 16;
-constexpr int NTA = 256;
-constexpr int RA = TI / (NTA / 32);
+constexpr int NTA = 256;  // 8 warps stacked along the rows
+constexpr int WARPS_A = NTA / 32;
+constexpr unsigned FULL_A = STRIP_FULL_MASK;
 
-template <typename T, int POL>
-__global__ void __launch_bounds__(NTA) k_adj2d(const AdjParams<T> p) {
-  __shared__ T s_f[TI + 2][TJ + 2];  // TM: u = ce*lambda_Ez ; TE: lambda_Hz  (one-cell ring)
-  __shared__ T s_a[TI + 1][TJ + 1];  // TM: vx (+ col halo j0-1) ; TE: ux (+ col halo j0+TJ)
-  __shared__ T s_b[TI + 1][TJ + 1];  // TM: vy (+ row halo i0-1) ; TE: uy (+ row halo i0+TI)
-  __shared__ T s_bx[TJ + 2], s_gx[TJ + 2];
-  __shared__ T s_by[TI + 2], s_gy[TI + 2];
-  __shared__ int s_skip;
-  if (threadIdx.x == 0)
-    s_skip = p.status != nullptr && *reinterpret_cast<volatile int*>(p.status) != 0;
-  __syncthreads();
-  if (s_skip) return;
-
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int i0 = blockIdx.y * TI, j0 = blockIdx.x * TJ;
+// TM reverse step, rows [ia, ib) of the strip of columns from j0.
+template <typename T, int VEC>
+__device__ __forceinline__ void adj_march_tm(const AdjParams<T>& p, int j0, int ia, int ib) {
+  using V = Vec<T, VEC>;
+  const int lane = threadIdx.x & 31;
   const int H = p.H, W = p.W;
   const long long py = p.py;
+  const int jv = j0 + lane * VEC;
+  const bool any = jv < W, full = jv + VEC <= W;
   const T dt = p.dt, idl = p.inv_dl;
+  const T* lEz = p.in[DN_EZ];
+  const T* lHx = p.in[DN_HX];
+  const T* lHy = p.in[DN_HY];
   const long long cslot = (long long)(p.t - p.curl_t0) * p.curl_stride;
-
-  for (int t = threadIdx.x; t < TJ + 2; t += NTA) {
-    const int j = j0 - 1 + t;
-    const bool ok = j >= 0 && j < W;
-    s_bx[t] = ok ? static_cast<T>(p.b[2][j]) : T(1);
-    s_gx[t] = ok ? static_cast<T>(1.0 + p.c[2][j]) : T(1);
-  }
-  for (int t = threadIdx.x; t < TI + 2; t += NTA) {
-    const int i = i0 - 1 + t;
-    const bool ok = i >= 0 && i < H;
-    s_by[t] = ok ? static_cast<T>(p.b[1][i]) : T(1);
-    s_gy[t] = ok ? static_cast<T>(1.0 + p.c[1][i]) : T(1);
-  }
-  for (int t = threadIdx.x; t < (TI + 2) * (TJ + 2); t += NTA) {
-    const int r = t / (TJ + 2), c = t % (TJ + 2);
-    const int i = i0 - 1 + r, j = j0 - 1 + c;
-    T v = T(0);
-    if (i >= 0 && i < H && j >= 0 && j < W) {
-      const long long o = i * py + j;
-      v = POL == DN_TM ? p.ce[o] * p.in[DN_EZ][o] : p.in[DN_HZ][o];
-    }
-    s_f[r][c] = v;
-  }
-  __syncthreads();
-
-  const int jj = lane, j = j0 + jj;
-  T a_own[RA], b_own[RA];  // TM: lHx', lHy'   TE: lEx', lEy'
-
-  if (POL == DN_TM) {
-    // ---- lH' from u (forward neighbours) ------------------------------------
+  V bx, gx;  // gx = (1 + c_x) / dl
 #pragma unroll
-    for (int r = 0; r < RA; ++r) {
-      const int ii = warp + 8 * r, i = i0 + ii;
-      T vx = T(0), vy = T(0);
-      a_own[r] = b_own[r] = T(0);
-      if (i < H && j < W) {
-        const long long o = i * py + j;
-        const T u = s_f[ii + 1][jj + 1];
-        const T gy = s_gy[ii + 1] * idl, gx = s_gx[jj + 1] * idl;
-        a_own[r] = p.in[DN_HX][o] - gy * ((j > 0 ? u : T(0)) - s_f[ii + 1][jj + 2]);
-        b_own[r] = p.in[DN_HY][o] + gx * ((i > 0 ? u : T(0)) - s_f[ii + 2][jj + 1]);
-        vx = (j < W - 1) ? dt * gy * a_own[r] : T(0);
-        vy = (i < H - 1) ? dt * gx * b_own[r] : T(0);
-      }
-      s_a[ii][jj + 1] = vx;
-      s_b[ii + 1][jj] = vy;
-    }
-    // halos: vx at column j0-1, vy at row i0-1
-    if (warp == 0 && lane < TI) {
-      const int ii = lane, i = i0 + ii, jh = j0 - 1;
-      T v = T(0);
-      if (jh >= 0 && i < H) {
-        const T gy = s_gy[ii + 1] * idl;
-        const T u = s_f[ii + 1][0];
-        const T lh = p.in[DN_HX][i * py + jh] - gy * ((jh > 0 ? u : T(0)) - s_f[ii + 1][1]);
-        v = dt * gy * lh;  // jh < W-1 always
-      }
-      s_a[ii][0] = v;
-    } else if (warp == 1) {
-      const int ih = i0 - 1;
-      T v = T(0);
-      if (ih >= 0 && j < W) {
-        const T gx = s_gx[jj + 1] * idl;
-        const T u = s_f[0][jj + 1];
-        const T lh = p.in[DN_HY][ih * py + j] + gx * ((ih > 0 ? u : T(0)) - s_f[1][jj + 1]);
-        v = dt * gx * lh;  // ih < H-1 always
-      }
-      s_b[0][jj] = v;
-    }
-  } else {
-    // ---- lE' from lambda_Hz (backward neighbours) ------------------------------
-    // lEx' = lEx + wj - wj(j-1), wj = dt cy [j<W-1] lHz
-    // lEy' = lEy - wi + wi(i-1), wi = dt cx [i<H-1] lHz
-#pragma unroll
-    for (int r = 0; r < RA; ++r) {
-      const int ii = warp + 8 * r, i = i0 + ii;
-      T ux = T(0), uy = T(0);
-      a_own[r] = b_own[r] = T(0);
-      if (i < H && j < W) {
-        const long long o = i * py + j;
-        const T lh = s_f[ii + 1][jj + 1];
-        const T cy = dt * s_gy[ii + 1] * idl, cx = dt * s_gx[jj + 1] * idl;
-        const T wj = (j < W - 1) ? cy * lh : T(0);
-        const T wjm = (j > 0) ? cy * s_f[ii + 1][jj] : T(0);
-        const T wi = (i < H - 1) ? cx * lh : T(0);
-        const T wim = (i > 0) ? dt * s_gx[jj + 1] * idl * s_f[ii][jj + 1] : T(0);
-        a_own[r] = p.in[DN_EX][o] + wj - wjm;
-        b_own[r] = p.in[DN_EY][o] - wi + wim;
-        const T ce = p.ce[o];
-        p.grad[o] += static_cast<double>(a_own[r]) * static_cast<double>(p.curl[0][cslot + o]) +
-                     static_cast<double>(b_own[r]) * static_cast<double>(p.curl[1][cslot + o]);
-        ux = (j > 0) ? ce * s_gx[jj + 1] * idl * a_own[r] : T(0);
-        uy = (i > 0) ? ce * s_gy[ii + 1] * idl * b_own[r] : T(0);
-      }
-      s_a[ii][jj] = ux;
-      s_b[ii][jj] = uy;
-    }
-    // halos: ux at column j0+TJ, uy at row i0+TI
-    if (warp == 0 && lane < TI) {
-      const int ii = lane, i = i0 + ii, jh = j0 + TJ;
-      T v = T(0);
-      if (jh < W && i < H) {
-        const long long o = i * py + jh;
-        const T cy = dt * s_gy[ii + 1] * idl;
-        const T wj = (jh < W - 1) ? cy * s_f[ii + 1][TJ + 1] : T(0);
-        const T wjm = cy * s_f[ii + 1][TJ];  // jh > 0
-        const T lex = p.in[DN_EX][o] + wj - wjm;
-        v = p.ce[o] * s_gx[TJ + 1] * idl * lex;  // jh > 0
-      }
-      s_a[ii][TJ] = v;
-    } else if (warp == 1) {
-      const int ih = i0 + TI;
-      T v = T(0);
-      if (ih < H && j < W) {
-        const long long o = ih * py + j;
-        const T cx = dt * s_gx[jj + 1] * idl;
-        const T wi = (ih < H - 1) ? cx * s_f[TI + 1][jj + 1] : T(0);
-        const T wim = cx * s_f[TI][jj + 1];  // ih > 0
-        const T ley = p.in[DN_EY][o] - wi + wim;
-        v = p.ce[o] * s_gy[TI + 1] * idl * ley;  // ih > 0
-      }
-      s_b[TI][jj] = v;
-    }
+  for (int q = 0; q < VEC; ++q) {
+    const int j = jv + q;
+    bx[q] = j < W ? static_cast<T>(p.b[2][j]) : T(1);
+    gx[q] = (j < W ? static_cast<T>(1.0 + p.c[2][j]) : T(1)) * idl;
   }
-  __syncthreads();
+  const bool edge_l = lane == 0 && j0 > 0;         // recomputes vx at column j0-1
+  const bool edge_r = lane == 31 && jv + VEC < W;  // loads u at column j0+32*VEC
 
+  long long o = (long long)ia * py + jv;
+  V lez_c = ldv<T, VEC>(lEz, o, any, full, jv, W);
+  V u_c;
+  {
+    const V ce = ldv<T, VEC>(p.ce, o, any, full, jv, W);
 #pragma unroll
-  for (int r = 0; r < RA; ++r) {
-    const int ii = warp + 8 * r, i = i0 + ii;
-    if (i >= H || j >= W) continue;
-    const long long o = i * py + j;
-    const T bx = s_bx[jj + 1], by = s_by[ii + 1];
-    if (POL == DN_TM) {
-      const T lez = p.in[DN_EZ][o];
-      p.grad[o] += static_cast<double>(lez) * static_cast<double>(p.curl[2][cslot + o]);
-      p.out[DN_EZ][o] = bx * by * lez + (s_a[ii][jj + 1] - s_a[ii][jj]) -
-                        (s_b[ii + 1][jj] - s_b[ii][jj]);
-      p.out[DN_HX][o] = by * a_own[r];
-      p.out[DN_HY][o] = bx * b_own[r];
-    } else {
-      const T lhz = s_f[ii + 1][jj + 1];
-      p.out[DN_HZ][o] = bx * by * lhz + (s_a[ii][jj] - s_a[ii][jj + 1]) -
-                        (s_b[ii][jj] - s_b[ii + 1][jj]);
-      p.out[DN_EX][o] = bx * a_own[r];
-      p.out[DN_EY][o] = by * b_own[r];
+    for (int q = 0; q < VEC; ++q) u_c[q] = ce[q] * lez_c[q];
+  }
+  // vy of row ia-1, recomputed with its owner's arithmetic (row ia-1 < H-1)
+  V vy_up;
+#pragma unroll
+  for (int q = 0; q < VEC; ++q) vy_up[q] = T(0);
+  if (ia > 0) {
+    const V lez_u = ldv<T, VEC>(lEz, o - py, any, full, jv, W);
+    const V ce_u = ldv<T, VEC>(p.ce, o - py, any, full, jv, W);
+    const V lhy_u = ldv<T, VEC>(lHy, o - py, any, full, jv, W);
+#pragma unroll
+    for (int q = 0; q < VEC; ++q) {
+      const T uu = ce_u[q] * lez_u[q];
+      const T lh = lhy_u[q] + gx[q] * ((ia - 1 > 0 ? uu : T(0)) - u_c[q]);
+      vy_up[q] = dt * gx[q] * lh;
     }
   }
+  for (int i = ia; i < ib; ++i, o += py) {
+    const bool nxt = i + 1 < H;
+    const V lez_n = ldv<T, VEC>(lEz, o + py, any && nxt, full, jv, W);
+    const V ce_n = ldv<T, VEC>(p.ce, o + py, any && nxt, full, jv, W);
+    const V lhx = ldv<T, VEC>(lHx, o, any, full, jv, W);
+    const V lhy = ldv<T, VEC>(lHy, o, any, full, jv, W);
+    const V crl = ldv<T, VEC>(p.curl[2], cslot + o, any, full, jv, W);
+    Vec<double, VEC> g = ldv<double, VEC, false>(p.grad, o, any, full, jv, W);
+    const T ce_r31 = ld(p.ce, o + VEC, edge_r), lez_r31 = ld(lEz, o + VEC, edge_r);
+    const T ce_l0 = ld(p.ce, o - 1, edge_l), lez_l0 = ld(lEz, o - 1, edge_l);
+    const T lhx_l0 = ld(lHx, o - 1, edge_l);
+    const T by = static_cast<T>(p.b[1][i]);
+    const T gy = static_cast<T>(1.0 + p.c[1][i]) * idl;
+
+    V u_n;
+#pragma unroll
+    for (int q = 0; q < VEC; ++q) u_n[q] = ce_n[q] * lez_n[q];
+    T u_rl = __shfl_down_sync(FULL_A, u_c[0], 1);
+    if (lane == 31) u_rl = ce_r31 * lez_r31;
+    V a, b, vx, vy;
+#pragma unroll
+    for (int q = 0; q < VEC; ++q) {
+      const int j = jv + q;
+      const T u_r = (q < VEC - 1) ? u_c[q < VEC - 1 ? q + 1 : q] : u_rl;
+      a[q] = lhx[q] - gy * ((j > 0 ? u_c[q] : T(0)) - u_r);
+      b[q] = lhy[q] + gx[q] * ((i > 0 ? u_c[q] : T(0)) - u_n[q]);
+      vx[q] = (j < W - 1) ? dt * gy * a[q] : T(0);
+      vy[q] = (i < H - 1) ? dt * gx[q] * b[q] : T(0);
+    }
+    T vx_ll = __shfl_up_sync(FULL_A, vx[VEC - 1], 1);
+    if (lane == 0) {
+      T v = T(0);
+      if (edge_l) {  // column j0-1 < W-1
+        const T ul = ce_l0 * lez_l0;
+        const T lh = lhx_l0 - gy * ((j0 - 1 > 0 ? ul : T(0)) - u_c[0]);
+        v = dt * gy * lh;
+      }
+      vx_ll = v;
+    }
+    V lez_p, lhx_p, lhy_p;
+#pragma unroll
+    for (int q = 0; q < VEC; ++q) {
+      const T vx_l = (q > 0) ? vx[q > 0 ? q - 1 : 0] : vx_ll;
+      g[q] += static_cast<double>(lez_c[q]) * static_cast<double>(crl[q]);
+      lez_p[q] = bx[q] * by * lez_c[q] + (vx[q] - vx_l) - (vy[q] - vy_up[q]);
+      lhx_p[q] = by * a[q];
+      lhy_p[q] = bx[q] * b[q];
+    }
+    if (any) {
+      stv(p.grad, o, g, full, jv, W);
+      stv(p.out[DN_EZ], o, lez_p, full, jv, W);
+      stv(p.out[DN_HX], o, lhx_p, full, jv, W);
+      stv(p.out[DN_HY], o, lhy_p, full, jv, W);
+    }
+    vy_up = vy;
+    u_c = u_n;
+    lez_c = lez_n;
+  }
+}
+
+// TE reverse step, rows [ia, ib) of the strip of columns from j0.  The
+// E-adjoint half of row i+1 (lambda_E', ux, uy) is computed in iteration i,
+// since the Hz-adjoint of row i needs uy of row i+1, and carried to i+1; each
+// row's gradient is accumulated once, by the warp that owns the row.
+template <typename T, int VEC>
+__device__ __forceinline__ void adj_march_te(const AdjParams<T>& p, int j0, int ia, int ib) {
+  using V = Vec<T, VEC>;
+  const int lane = threadIdx.x & 31;
+  const int H = p.H, W = p.W;
+  const long long py = p.py;
+  const int jv = j0 + lane * VEC;
+  const bool any = jv < W, full = jv + VEC <= W;
+  const T dt = p.dt, idl = p.inv_dl;
+  const T* lHz = p.in[DN_HZ];
+  const T* lEx = p.in[DN_EX];
+  const T* lEy = p.in[DN_EY];
+  const long long cslot = (long long)(p.t - p.curl_t0) * p.curl_stride;
+  V bx, gxr, cx;  // gxr = 1 + c_x, cx = dt (1 + c_x) / dl
+#pragma unroll
+  for (int q = 0; q < VEC; ++q) {
+    const int j = jv + q;
+    bx[q] = j < W ? static_cast<T>(p.b[2][j]) : T(1);
+    gxr[q] = j < W ? static_cast<T>(1.0 + p.c[2][j]) : T(1);
+    cx[q] = dt * gxr[q] * idl;
+  }
+  const bool edge_l = lane == 0 && j0 > 0;         // loads lambda_Hz at column j0-1
+  const bool edge_r = lane == 31 && jv + VEC < W;  // recomputes ux at column j0+32*VEC
+  const T gxr_r = edge_r ? static_cast<T>(1.0 + p.c[2][jv + VEC]) : T(1);
+
+  // E-adjoint half of row r (offset oo) from lambda_Hz of rows r (lh) and
+  // r-1 (lh_u); accumulates the row's gradient when `own`; all 32 lanes call it
+  auto e_row = [&](int r, long long oo, const V& lh, const V& lh_u, bool own, V& a, V& b, V& ux,
+                   V& uy) {
+    const V lex = ldv<T, VEC>(lEx, oo, any, full, jv, W);
+    const V ley = ldv<T, VEC>(lEy, oo, any, full, jv, W);
+    const V ce = ldv<T, VEC>(p.ce, oo, any, full, jv, W);
+    const T lh_l0 = ld(lHz, oo - 1, edge_l);
+    const T gyr = static_cast<T>(1.0 + p.c[1][r]);
+    const T cy = dt * gyr * idl;
+    T lh_ll = __shfl_up_sync(FULL_A, lh[VEC - 1], 1);
+    if (lane == 0) lh_ll = lh_l0;
+#pragma unroll
+    for (int q = 0; q < VEC; ++q) {
+      const int j = jv + q;
+      const T lh_l = (q > 0) ? lh[q > 0 ? q - 1 : 0] : lh_ll;
+      const T wj = (j < W - 1) ? cy * lh[q] : T(0);
+      const T wjm = (j > 0) ? cy * lh_l : T(0);
+      const T wi = (r < H - 1) ? cx[q] * lh[q] : T(0);
+      const T wim = (r > 0) ? cx[q] * lh_u[q] : T(0);
+      a[q] = lex[q] + wj - wjm;
+      b[q] = ley[q] - wi + wim;
+      ux[q] = (j > 0) ? ce[q] * gxr[q] * idl * a[q] : T(0);
+      uy[q] = (r > 0) ? ce[q] * gyr * idl * b[q] : T(0);
+    }
+    if (own && any) {
+      const V c0 = ldv<T, VEC>(p.curl[0], cslot + oo, any, full, jv, W);
+      const V c1 = ldv<T, VEC>(p.curl[1], cslot + oo, any, full, jv, W);
+      Vec<double, VEC> g = ldv<double, VEC, false>(p.grad, oo, any, full, jv, W);
+#pragma unroll
+      for (int q = 0; q < VEC; ++q)
+        g[q] += static_cast<double>(a[q]) * static_cast<double>(c0[q]) +
+                static_cast<double>(b[q]) * static_cast<double>(c1[q]);
+      stv(p.grad, oo, g, full, jv, W);
+    }
+  };
+
+  long long o = (long long)ia * py + jv;
+  V lh_c = ldv<T, VEC>(lHz, o, any, full, jv, W);
+  const V lh_u = ldv<T, VEC>(lHz, o - py, any && ia > 0, full, jv, W);
+  V a_c, b_c, ux_c, uy_c;
+  e_row(ia, o, lh_c, lh_u, true, a_c, b_c, ux_c, uy_c);
+  for (int i = ia; i < ib; ++i, o += py) {
+    const bool nxt = i + 1 < H;
+    const V lh_n = ldv<T, VEC>(lHz, o + py, any && nxt, full, jv, W);
+    const T lex31 = ld(lEx, o + VEC, edge_r), ce31 = ld(p.ce, o + VEC, edge_r);
+    const T lh31 = ld(lHz, o + VEC, edge_r);
+    const T by = static_cast<T>(p.b[1][i]);
+    const T cy = dt * static_cast<T>(1.0 + p.c[1][i]) * idl;
+    V a_n, b_n, ux_n, uy_n;
+#pragma unroll
+    for (int q = 0; q < VEC; ++q) a_n[q] = b_n[q] = ux_n[q] = uy_n[q] = T(0);
+    if (nxt) e_row(i + 1, o + py, lh_n, lh_c, i + 1 < ib, a_n, b_n, ux_n, uy_n);
+
+    T ux_rl = __shfl_down_sync(FULL_A, ux_c[0], 1);
+    if (lane == 31) {
+      T v = T(0);
+      if (edge_r) {  // column jh = j0+32*VEC > 0
+        const T wj = (jv + VEC < W - 1) ? cy * lh31 : T(0);
+        const T wjm = cy * lh_c[VEC - 1];
+        const T lex_p = lex31 + wj - wjm;
+        v = ce31 * gxr_r * idl * lex_p;
+      }
+      ux_rl = v;
+    }
+    V lhz_p, lex_p, ley_p;
+#pragma unroll
+    for (int q = 0; q < VEC; ++q) {
+      const T ux_r = (q < VEC - 1) ? ux_c[q < VEC - 1 ? q + 1 : q] : ux_rl;
+      lhz_p[q] = bx[q] * by * lh_c[q] + (ux_c[q] - ux_r) - (uy_c[q] - uy_n[q]);
+      lex_p[q] = bx[q] * a_c[q];
+      ley_p[q] = by * b_c[q];
+    }
+    if (any) {
+      stv(p.out[DN_HZ], o, lhz_p, full, jv, W);
+      stv(p.out[DN_EX], o, lex_p, full, jv, W);
+      stv(p.out[DN_EY], o, ley_p, full, jv, W);
+    }
+    lh_c = lh_n;
+    a_c = a_n;
+    b_c = b_n;
+    ux_c = ux_n;
+    uy_c = uy_n;
+  }
+}
+
+template <typename T, int POL, int VEC>
+__global__ void __launch_bounds__(NTA, 2) k_adj2d(const AdjParams<T> p, int R) {
+  // a previous launch that recorded an error turns this one into a no-op
+  if (p.status != nullptr && *reinterpret_cast<volatile int*>(p.status) != 0) return;
+  const int warp = threadIdx.x >> 5;
+  const int j0 = blockIdx.x * 32 * VEC;
+  const long long ia = ((long long)blockIdx.y * WARPS_A + warp) * R;
+  if (ia >= p.H) return;  // whole warp: the shuffles see all 32 lanes
+  const int ib = static_cast<int>(std::min<long long>(ia + R, p.H));
+  if (POL == DN_TM)
+    adj_march_tm<T, VEC>(p, j0, static_cast<int>(ia), ib);
+  else
+    adj_march_te<T, VEC>(p, j0, static_cast<int>(ia), ib);
 }
 
 template <typename T>
@@ -311,6 +386,73 @@ template int inject_monitors<double>(const AdjParams<double>&, const dn_monitor*
 
 namespace {
 
+// Rows per warp, as for the forward step: the smallest R for which the grid
+// fits one wave of resident CTAs; at least 4 where that still leaves 8 warps
+// per SM (the recomputed row costs a warp about three rows of loads), else 2.
+template <typename T, int POL, int VEC>
+int adj_rows_per_warp(int H, int strips, int* R) {
+  static int per_sm = 0, nsm = 0;  // per kernel instance; identical on every B200
+  if (per_sm == 0) {
+    int dev = 0, n = 0, b = 0;
+    DN_CUDA_CHECK(cudaGetDevice(&dev));
+    DN_CUDA_CHECK(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+    DN_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_adj2d<T, POL, VEC>, NTA, 0));
+    nsm = n;
+    per_sm = std::max(b, 1);
+  }
+  const long long slots = (long long)nsm * per_sm;
+  const long long row_ctas = std::max<long long>(1, slots / strips);
+  const long long r = (H + WARPS_A * row_ctas - 1) / (WARPS_A * row_ctas);
+  const long long warps4 = (long long)strips * ((H + 3) / 4);
+  const long long r_min = warps4 >= 8LL * nsm ? 4 : 2;
+  *R = static_cast<int>(std::max<long long>(r_min, r));
+  return DN_OK;
+}
+
+template <typename T, int POL, int VEC>
+int adj_launch(const dn_grid* g, AdjParams<T>& p, void* const la[6], void* const lb[6],
+               const dn_monitor* mons, int32_t n_mon, int32_t t_end, int32_t nsteps,
+               cudaStream_t s) {
+  const int strips = (g->W + 32 * VEC - 1) / (32 * VEC);
+  int R = 2;
+  int rc = adj_rows_per_warp<T, POL, VEC>(g->H, strips, &R);
+  if (rc != DN_OK) return rc;
+  const long long rows_per_cta = (long long)WARPS_A * R;
+  const dim3 grid(strips, static_cast<unsigned>((g->H + rows_per_cta - 1) / rows_per_cta));
+  for (int n = 0; n < nsteps; ++n) {
+    const bool even = (n % 2) == 0;
+    for (int c = 0; c < 6; ++c) {
+      p.in[c] = static_cast<const T*>(even ? la[c] : lb[c]);
+      p.out[c] = static_cast<T*>(even ? lb[c] : la[c]);
+    }
+    p.t = t_end - 1 - n;
+    if (n_mon > 0 && (rc = inject_monitors<T>(p, mons, n_mon, false, g->pol, s)) != DN_OK)
+      return rc;
+    k_adj2d<T, POL, VEC><<<grid, NTA, 0, s>>>(p, R);
+  }
+  DN_CUDA_CHECK(cudaGetLastError());
+  return DN_OK;
+}
+
+// 16-byte row access needs the pitch (of the fields and of the FP64
+// gradient), the arrays the polarisation uses, the curl slots and their
+// step stride on 16-byte boundaries.
+template <typename T>
+bool adj_vector_rows_ok(const dn_grid* g, void* const la[6], void* const lb[6], const void* ce,
+                        const dn_curl_record* curl, const double* grad) {
+  if ((g->pitch_y * (int64_t)sizeof(T)) % 16 != 0 || (g->pitch_y * 8) % 16 != 0) return false;
+  if (!aligned16(ce) || !aligned16(grad)) return false;
+  if ((curl->step_stride * (int64_t)sizeof(T)) % 16 != 0) return false;
+  const bool tm = g->pol == DN_TM;
+  const int comps[2][3] = {{DN_EZ, DN_HX, DN_HY}, {DN_HZ, DN_EX, DN_EY}};
+  for (int c : comps[tm ? 0 : 1])
+    if (!aligned16(la[c]) || !aligned16(lb[c])) return false;
+  const int slots[2][2] = {{2, 2}, {0, 1}};
+  for (int c : slots[tm ? 0 : 1])
+    if (!aligned16(curl->curl[c])) return false;
+  return true;
+}
+
 template <typename T>
 int adjoint2d(const dn_grid* g, void* const la[6], void* const lb[6], const void* ce,
               const dn_cpml* cpml, const dn_curl_record* curl, double* grad,
@@ -322,22 +464,17 @@ int adjoint2d(const dn_grid* g, void* const la[6], void* const lb[6], const void
   if (!final_in_b || n_mon < 0 || n_mon > DN_MAX_MONITORS || (n_mon > 0 && !mons))
     return DN_EINVAL;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const dim3 grid((g->W + TJ - 1) / TJ, (g->H + TI - 1) / TI);
-  for (int n = 0; n < nsteps; ++n) {
-    const bool even = (n % 2) == 0;
-    for (int c = 0; c < 6; ++c) {
-      p.in[c] = static_cast<const T*>(even ? la[c] : lb[c]);
-      p.out[c] = static_cast<T*>(even ? lb[c] : la[c]);
-    }
-    p.t = t_end - 1 - n;
-    if (n_mon > 0 && (rc = inject_monitors<T>(p, mons, n_mon, false, g->pol, s)) != DN_OK)
-      return rc;
+  if (nsteps > 0) {
+    constexpr int VEC = 16 / static_cast<int>(sizeof(T));
+    const bool vec = adj_vector_rows_ok<T>(g, la, lb, ce, curl, grad);
     if (g->pol == DN_TM)
-      k_adj2d<T, DN_TM><<<grid, NTA, 0, s>>>(p);
+      rc = vec ? adj_launch<T, DN_TM, VEC>(g, p, la, lb, mons, n_mon, t_end, nsteps, s)
+               : adj_launch<T, DN_TM, 1>(g, p, la, lb, mons, n_mon, t_end, nsteps, s);
     else
-      k_adj2d<T, DN_TE><<<grid, NTA, 0, s>>>(p);
+      rc = vec ? adj_launch<T, DN_TE, VEC>(g, p, la, lb, mons, n_mon, t_end, nsteps, s)
+               : adj_launch<T, DN_TE, 1>(g, p, la, lb, mons, n_mon, t_end, nsteps, s);
+    if (rc != DN_OK) return rc;
   }
-  DN_CUDA_CHECK(cudaGetLastError());
   *final_in_b = nsteps % 2;
   return DN_OK;
 }

@@ -31,16 +31,16 @@
 // grid fits one wave of resident CTAs (3 per SM), with a floor that keeps the
 // recomputed rows a small share of a warp's loads.
 #include <algorithm>
-#include <type_traits>
 
 #include "dn_host.cuh"
+#include "dn_strip.cuh"
 
 namespace dn {
 namespace {
 
 constexpr int NT2 = 256;  // threads per CTA: 8 warps stacked along the rows
 constexpr int WARPS2 = NT2 / 32;
-constexpr unsigned FULL = 0xffffffffu;
+constexpr unsigned FULL = STRIP_FULL_MASK;
 
 // curl record for the adjoint replay (see dn_curl_record)
 template <typename T>
@@ -49,60 +49,6 @@ struct CurlRec2 {
   long long stride;
   int t0;
 };
-
-template <typename T>
-__device__ __forceinline__ T ld(const T* a, long long o, bool ok) {
-  return ok ? __ldg(a + o) : T(0);
-}
-
-// VEC adjacent values of one row, from column jv
-template <typename T, int VEC>
-struct Vec {
-  T v[VEC];
-  __device__ __forceinline__ T& operator[](int q) { return v[q]; }
-  __device__ __forceinline__ const T& operator[](int q) const { return v[q]; }
-};
-
-// Columns jv .. jv+VEC-1 at offset o; columns at or past W (and all of them
-// when !ok) read as 0.  One 16-byte load when all VEC columns are in the
-// grid (`full`), else one load per column in the grid.
-template <typename T, int VEC>
-__device__ __forceinline__ Vec<T, VEC> ldv(const T* a, long long o, bool ok, bool full, int jv,
-                                           int W) {
-  Vec<T, VEC> r;
-  if (VEC > 1 && ok && full) {
-    if constexpr (VEC == 4 && std::is_same<T, float>::value) {
-      const float4 x = __ldg(reinterpret_cast<const float4*>(a + o));
-      r[0] = x.x, r[1] = x.y, r[2] = x.z, r[3] = x.w;
-      return r;
-    } else if constexpr (VEC == 2 && std::is_same<T, double>::value) {
-      const double2 x = __ldg(reinterpret_cast<const double2*>(a + o));
-      r[0] = x.x, r[1] = x.y;
-      return r;
-    }
-  }
-#pragma unroll
-  for (int q = 0; q < VEC; ++q) r[q] = ld(a, o + q, ok && jv + q < W);
-  return r;
-}
-
-// Store the columns of v that are in the grid (one 16-byte store when all are).
-template <typename T, int VEC>
-__device__ __forceinline__ void stv(T* a, long long o, const Vec<T, VEC>& v, bool full, int jv,
-                                    int W) {
-  if (VEC > 1 && full) {
-    if constexpr (VEC == 4 && std::is_same<T, float>::value) {
-      *reinterpret_cast<float4*>(a + o) = make_float4(v[0], v[1], v[2], v[3]);
-      return;
-    } else if constexpr (VEC == 2 && std::is_same<T, double>::value) {
-      *reinterpret_cast<double2*>(a + o) = make_double2(v[0], v[1]);
-      return;
-    }
-  }
-#pragma unroll
-  for (int q = 0; q < VEC; ++q)
-    if (jv + q < W) a[o + q] = v[q];
-}
 
 // Does row i hold a source, monitor or probe cell?  (A superset test per
 // row; the per-cell tests in the helpers decide.  Unrolled over the fixed
@@ -453,8 +399,6 @@ int launch_steps(StepParams<T>& p, const CurlRec2<T>& rec, void* const fa[6], vo
   DN_CUDA_CHECK(cudaGetLastError());
   return DN_OK;
 }
-
-bool aligned16(const void* a) { return (reinterpret_cast<uintptr_t>(a) & 15) == 0; }
 
 // 16-byte row access needs the pitch, every array the polarisation uses and
 // (when recording) the curl slots and their step stride on 16-byte boundaries.

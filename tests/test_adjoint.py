@@ -149,6 +149,72 @@ def test_2d_monitor_gradient_vs_oracle(cuda):
     assert rel_l2(eps.grad, e.grad) < 1e-9
 
 
+@pytest.mark.parametrize("pol,dtype", [("TM", torch.float32), ("TE", torch.float32),
+                                       ("TM", torch.float64), ("TE", torch.float64)])
+def test_adjoint2d_unaligned_rows_match_padded_rows(cuda, pol, dtype):
+    """The 2-D reverse sweep through the C ABI with tight rows (pitch = W = 45:
+    rows not on 16-byte boundaries, one value per lane) against the engine's
+    padded rows (16-byte row access with a partly filled last lane): same
+    adjoint fields and the same FP64 gradient."""
+    import ctypes
+
+    from diffnano_b200 import _lib
+    from diffnano_b200.solvers import _setup
+    from diffnano_b200.solvers._engine import Engine
+
+    H, W, T = 38, 45, 30
+    dl, courant = 20.0, 0.5
+    dt = courant * dl / 2 ** 0.5
+    src = {"type": "gaussian_pulse", "row": 9, "spread": 300.0, "t0": 400.0}
+    p = _lib.DN_TM if pol == "TM" else _lib.DN_TE
+    comp = _lib.DN_EZ if pol == "TM" else _lib.DN_HZ
+    eng = Engine(is3d=False, shape=(H, W), dl=dl, dt=dt, pml_layers=6, dtype=dtype, device=cuda,
+                 n_steps=T, wave=_setup.waveform_table(T, dt, OMEGA, src),
+                 src_box=_setup.source_box_2d((H, W), src), src_comp=comp, pol=p)
+    eng.set_eps(_seeded((H, W), 31))
+    buf = eng.curl_buffer(T)
+    rec = eng.curl_record(buf, 0, T)
+    eng.run(0, T, record=rec)
+    comps = (_lib.DN_EZ, _lib.DN_HX, _lib.DN_HY) if pol == "TM" else \
+        (_lib.DN_HZ, _lib.DN_EX, _lib.DN_EY)
+    g = torch.Generator().manual_seed(32)
+    la = torch.zeros_like(eng.A)
+    for c in comps:
+        la[c, :, :, :W] = torch.randn(1, H, W, dtype=torch.float64, generator=g).to(cuda, dtype)
+    la_t = la[..., :W].contiguous()
+    lb = torch.zeros_like(la)
+    grad = torch.zeros((1, H, eng.Wp), dtype=torch.float64, device=cuda)
+    in_b = eng.adjoint(la, lb, rec, grad, None, 0, T, T)
+    torch.cuda.synchronize(cuda)
+
+    grid = type(eng.grid).from_buffer_copy(eng.grid)
+    grid.pitch_y, grid.pitch_z = W, H * W
+    lb_t = torch.zeros_like(la_t)
+    ce_t = eng.ce[..., :W].contiguous()
+    buf_t = buf[..., :W].contiguous()
+    rec_t = _lib.DnCurlRecord(step_stride=H * W, t0=0, nslots=T)
+    for n, c in enumerate(eng.eps_components()):
+        rec_t.curl[c if c != _lib.DN_EZ else 2] = buf_t[n].data_ptr()
+    grad_t = torch.zeros((1, H, W), dtype=torch.float64, device=cuda)
+    assert (W * la_t.element_size()) % 16 != 0
+    out = ctypes.c_int32(0)
+    with torch.cuda.device(cuda):
+        stream = torch.cuda.current_stream(cuda).cuda_stream
+        rc = _lib.lib().dn_fdtd2d_adjoint(
+            ctypes.byref(grid), _lib.PTR6(*[la_t[c].data_ptr() for c in range(6)]),
+            _lib.PTR6(*[lb_t[c].data_ptr() for c in range(6)]), ce_t.data_ptr(),
+            ctypes.byref(eng.cpml), ctypes.byref(rec_t), grad_t.data_ptr(), None, 0, T, T,
+            eng.status.data_ptr(), ctypes.c_void_p(stream), ctypes.byref(out))
+    assert rc == _lib.DN_OK
+    eng.check_status()
+    tol = 1e-6 if dtype == torch.float32 else 1e-13
+    assert float(grad.abs().max()) > 0
+    assert rel_l2(grad_t[0], grad[0, :, :W]) < tol
+    res, res_t = (lb if in_b else la), (lb_t if out.value else la_t)
+    for c in comps:
+        assert rel_l2(res_t[c], res[c, :, :, :W]) < tol
+
+
 def test_grad3d_central_finite_differences(cuda):
     """dL/deps at 16 seeded voxels vs central differences (h = 1e-3) of the
     FP64 kernels; L = sum |DFT Ey|^2 over a plane."""
