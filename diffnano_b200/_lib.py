@@ -145,6 +145,8 @@ SIGNATURES = {
                                           ctypes.POINTER(c_int64)]),
     "dn_batch2d_forward_cluster": (c_int32, [ctypes.POINTER(DnBatch2d), c_void_p, c_int32,
                                              c_int64, c_void_p]),
+    "dn_batch2d_barrier_selftest": (c_int32, [c_int32, c_int32, c_int64, c_int32, c_void_p,
+                                              c_void_p, c_void_p]),
     "dn_fom_abs2_scratch_bytes": (c_int64, [c_int64]),
     "dn_fom_abs2": (c_int32, [c_void_p, c_int64, c_void_p, c_void_p, c_int64, c_void_p]),
     "dn_gemm_run": (c_int32, [ctypes.POINTER(DnGemm), c_void_p, c_void_p]),

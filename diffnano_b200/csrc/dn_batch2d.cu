@@ -94,17 +94,18 @@ __device__ int active_tiles(const TableView& v, int n) {
   return v.tile_prefix[lo];
 }
 
-// grid barrier over all CTAs of the launch: arrive count + generation word,
-// bounded spin; returns false (and raises the abort word) on expiry or when
-// another CTA aborted
-__device__ bool grid_sync(unsigned int* bar, unsigned int& gen, int* status) {
+// grid barrier over `expected` arrivals (all CTAs of the launch): arrive count
+// + generation word, at most `spin_limit` probes 64 ns apart; returns false
+// (and raises the abort word) on expiry or when another CTA aborted
+__device__ bool grid_sync_n(unsigned int* bar, unsigned int& gen, int* status,
+                            unsigned int expected, unsigned long long spin_limit) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
     __threadfence();
     const unsigned int g = gen;
-    if (atomicAdd(&bar[0], 1u) == gridDim.x - 1) {
+    if (atomicAdd(&bar[0], 1u) == expected - 1) {
       atomicExch(&bar[0], 0u);
       __threadfence();
       atomicExch(&bar[1], g + 1u);
@@ -116,7 +117,7 @@ __device__ bool grid_sync(unsigned int* bar, unsigned int& gen, int* status) {
           break;
         }
         __nanosleep(64);
-        if (++spins > BAR_SPIN_LIMIT) {
+        if (++spins > spin_limit) {
           ok = 0;
           atomicExch(&bar[2], 1u);
           report_status(status, DN_ETIMEOUT);
@@ -130,6 +131,19 @@ __device__ bool grid_sync(unsigned int* bar, unsigned int& gen, int* status) {
   }
   __syncthreads();
   return s_ok != 0;
+}
+
+__device__ __forceinline__ bool grid_sync(unsigned int* bar, unsigned int& gen, int* status) {
+  return grid_sync_n(bar, gen, status, gridDim.x, BAR_SPIN_LIMIT);
+}
+
+// The barrier alone, `rounds` times, for dn_batch2d_barrier_selftest: with
+// `missing` > 0 arrivals that never come, every CTA's wait runs out.
+__global__ void k_barrier_selftest(unsigned int* bar, int* status, unsigned int missing,
+                                   unsigned long long spin_limit, int rounds) {
+  unsigned int gen = 0;
+  for (int r = 0; r < rounds; ++r)
+    if (!grid_sync_n(bar, gen, status, gridDim.x + missing, spin_limit)) return;
 }
 
 template <typename T>
@@ -1269,4 +1283,24 @@ extern "C" int32_t dn_batch2d_backward(const dn_batch2d* cfg, void* dev_table, i
   if (cfg->pol != DN_TM && cfg->pol != DN_TE) return DN_EINVAL;
   if (cfg->dtype != DN_F32 && cfg->dtype != DN_F64) return DN_EINVAL;
   return dn::run(false, cfg, dev_table, status, stream, cfg->max_ctas > 0 ? cfg->max_ctas : 1 << 30);
+}
+
+extern "C" int32_t dn_batch2d_barrier_selftest(int32_t n_ctas, int32_t missing, int64_t spin_limit,
+                                               int32_t rounds, void* dev_bar, int32_t* status,
+                                               void* stream) {
+  if (n_ctas < 1 || missing < 0 || missing > 1024 || rounds < 1 || spin_limit < 1 ||
+      spin_limit > static_cast<int64_t>(dn::BAR_SPIN_LIMIT) || !dev_bar || !status ||
+      (reinterpret_cast<uintptr_t>(dev_bar) & 15))
+    return DN_EINVAL;
+  int dev = 0, nsm = 0;
+  DN_CUDA_CHECK(cudaGetDevice(&dev));
+  DN_CUDA_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  if (n_ctas > nsm) return DN_EINVAL;  // one 32-thread CTA per SM at most: all resident at once
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  DN_CUDA_CHECK(cudaMemsetAsync(dev_bar, 0, 4 * sizeof(unsigned int), s));
+  dn::k_barrier_selftest<<<n_ctas, 32, 0, s>>>(static_cast<unsigned int*>(dev_bar), status,
+                                               static_cast<unsigned int>(missing),
+                                               static_cast<unsigned long long>(spin_limit), rounds);
+  DN_CUDA_CHECK(cudaGetLastError());
+  return DN_OK;
 }

@@ -275,6 +275,18 @@ int32_t dn_batch2d_cluster_size(const dn_batch2d* cfg, const dn_batch2d_inst* in
 int32_t dn_batch2d_forward_cluster(const dn_batch2d* cfg, void* dev_table, int32_t cluster,
                                    int64_t smem_bytes, void* stream);
 
+/* Diagnostic, no reference counterpart: runs the persistent kernels' grid
+ * barrier alone, `rounds` times, on `n_ctas` one-warp CTAs (at most one per
+ * SM), waiting for n_ctas + `missing` arrivals with at most `spin_limit`
+ * probes 64 ns apart (1 .. 2^24, the kernels' own limit).  missing = 0 must
+ * leave *status at DN_OK; missing > 0 arrivals never come, so every CTA's wait
+ * runs out and *status becomes DN_ETIMEOUT (the launch returns, the context
+ * stays usable).  `dev_bar`: 16 bytes of device memory, 16-byte aligned,
+ * cleared by the call; `status`: a device int32 the caller zeroes. */
+int32_t dn_batch2d_barrier_selftest(int32_t n_ctas, int32_t missing, int64_t spin_limit,
+                                    int32_t rounds, void* dev_bar, int32_t* status,
+                                    void* stream);
+
 /* ---- figure of merit ----------------------------------------------------
  * *out = sum_i |dft[i]|^2 over n_complex FP64 (re, im) pairs, reduced in FP64
  * (warp-shuffle trees, per-block partials in `scratch`, deterministic final

@@ -155,3 +155,36 @@ def test_cluster_in_place_kernel_for_grids_that_fit_once(cuda, pol):
         assert rel_l2(x, y) < 1e-6
     for x, y in zip(da, db):
         assert rel_l2(torch.view_as_real(x), torch.view_as_real(y)) < 1e-6
+
+
+def test_grid_barrier_wait_runs_out_and_reports_timeout(cuda):
+    """The persistent kernels' grid barrier (dn_batch2d_barrier_selftest runs it
+    alone): all arrivals -> DN_OK; one arrival that never comes -> every CTA's
+    bounded wait runs out, the status reads DN_ETIMEOUT within milliseconds,
+    and the context stays usable: a persistent batched solve after it gives
+    the same fields as one before it."""
+    import ctypes
+    import time
+
+    L = _lib.lib()
+    specs = _specs("TM")
+    eps = [e.to(cuda) for e in _eps(7)]
+    b = FDTDBatch2D(specs, "TM", torch.float32, cuda, tile_rows=16, cluster=False)
+    before, _ = b.forward(eps)
+    b.check_status()
+    bar = torch.zeros(4, dtype=torch.int32, device=cuda)
+    st = torch.zeros(1, dtype=torch.int32, device=cuda)
+    stream = ctypes.c_void_p(torch.cuda.current_stream(cuda).cuda_stream)
+    rc = L.dn_batch2d_barrier_selftest(8, 0, 1 << 16, 200, bar.data_ptr(), st.data_ptr(), stream)
+    torch.cuda.synchronize(cuda)
+    assert rc == _lib.DN_OK and int(st.item()) == _lib.DN_OK
+    t0 = time.perf_counter()
+    rc = L.dn_batch2d_barrier_selftest(8, 1, 1 << 12, 3, bar.data_ptr(), st.data_ptr(), stream)
+    torch.cuda.synchronize(cuda)
+    elapsed = time.perf_counter() - t0
+    assert rc == _lib.DN_OK and int(st.item()) == _lib.DN_ETIMEOUT
+    assert elapsed < 5.0
+    after, _ = b.forward(eps)
+    b.check_status()
+    for x, y in zip(before, after):
+        assert torch.equal(x, y)

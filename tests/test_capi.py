@@ -148,3 +148,15 @@ def test_batch2d_rejects_bad_configs():
     assert L.dn_batch2d_table_bytes(ctypes.byref(cfg), inst) == -1  # tile rows
     cfg.tile_rows = 16
     assert L.dn_batch2d_table_bytes(ctypes.byref(cfg), inst) == -1  # empty instance
+
+
+@pytest.mark.parametrize("bad", [dict(n_ctas=0), dict(missing=-1), dict(spin_limit=0),
+                                 dict(spin_limit=(1 << 24) + 1), dict(rounds=0),
+                                 dict(bar=None), dict(status=None), dict(bar=8)])
+def test_barrier_selftest_rejects_bad_arguments_before_any_launch(bad):
+    L = _lib.lib()
+    a = dict(n_ctas=4, missing=0, spin_limit=1024, rounds=1, bar=4096, status=8192)
+    a.update(bad)
+    rc = L.dn_batch2d_barrier_selftest(a["n_ctas"], a["missing"], a["spin_limit"], a["rounds"],
+                                       a["bar"], a["status"], None)
+    assert rc == _lib.DN_EINVAL
