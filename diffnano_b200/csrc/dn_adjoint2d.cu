@@ -94,7 +94,7 @@ __device__ __forceinline__ void adj_march_tm(const AdjParams<T>& p, int j0, int 
     const V lhx = ldv<T, VEC>(lHx, o, any, full, jv, W);
     const V lhy = ldv<T, VEC>(lHy, o, any, full, jv, W);
     const V crl = ldv<T, VEC>(p.curl[2], cslot + o, any, full, jv, W);
-    Vec<double, VEC> g = ldv<double, VEC, false>(p.grad, o, any, full, jv, W);
+    Vec<double, VEC> g = ldv<double, VEC, LD_PLAIN>(p.grad, o, any, full, jv, W);
     const T ce_r31 = ld(p.ce, o + VEC, edge_r), lez_r31 = ld(lEz, o + VEC, edge_r);
     const T ce_l0 = ld(p.ce, o - 1, edge_l), lez_l0 = ld(lEz, o - 1, edge_l);
     const T lhx_l0 = ld(lHx, o - 1, edge_l);
@@ -204,7 +204,7 @@ __device__ __forceinline__ void adj_march_te(const AdjParams<T>& p, int j0, int 
     if (own && any) {
       const V c0 = ldv<T, VEC>(p.curl[0], cslot + oo, any, full, jv, W);
       const V c1 = ldv<T, VEC>(p.curl[1], cslot + oo, any, full, jv, W);
-      Vec<double, VEC> g = ldv<double, VEC, false>(p.grad, oo, any, full, jv, W);
+      Vec<double, VEC> g = ldv<double, VEC, LD_PLAIN>(p.grad, oo, any, full, jv, W);
 #pragma unroll
       for (int q = 0; q < VEC; ++q)
         g[q] += static_cast<double>(a[q]) * static_cast<double>(c0[q]) +

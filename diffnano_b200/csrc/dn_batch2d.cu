@@ -19,8 +19,10 @@
 // monitor-DFT gradient added to the adjoint field as it is loaded.  Field
 // loads bypass L1 (other SMs wrote them during the previous step).
 //
-// Tile: `TI` rows x 32 columns, 256 threads; the step arithmetic is that of
-// dn_fdtd2d.cu / dn_adjoint2d.cu (same equations, same boundary rules).
+// Tile: `TI` rows x 32*VEC columns (VEC = 4 in FP32, 2 in FP64), 256 threads:
+// each warp marches TI/8 rows of its 32 lanes x VEC columns with 16-byte
+// loads and stores, no shared memory (the strip march of dn_fdtd2d.cu /
+// dn_adjoint2d.cu: same equations, same boundary rules).
 #include <algorithm>
 #include <cstddef>
 #include <cstring>
@@ -30,11 +32,13 @@
 #include <cooperative_groups.h>
 
 #include "dn_host.cuh"
+#include "dn_strip.cuh"
 
 namespace dn {
 namespace {
 
-constexpr int TJ = 32;
+// tile columns: 32 lanes x VEC values (16 bytes per lane and array)
+inline int tile_cols(int dtype) { return dtype == DN_F32 ? 128 : 64; }
 constexpr int NTB = 256;
 constexpr unsigned long long BAR_SPIN_LIMIT = 1ull << 24;  // x 64 ns ~ 1 s
 
@@ -151,31 +155,6 @@ __device__ __forceinline__ T ld(const T* p) {
   return __ldcg(p);
 }
 
-template <typename T, int TI>
-struct TileSmem {
-  T f[TI + 2][TJ + 2];
-  T a[TI + 1][TJ + 1];
-  T b[TI + 1][TJ + 1];
-  T bx[TJ + 2], gx[TJ + 2];
-  T by[TI + 2], gy[TI + 2];
-};
-
-template <typename T, int TI>
-__device__ void load_tables(TileSmem<T, TI>& s, const dn_batch2d_inst& I, int i0, int j0) {
-  for (int t = threadIdx.x; t < TJ + 2; t += NTB) {
-    const int j = j0 - 1 + t;
-    const bool ok = j >= 0 && j < I.W;
-    s.bx[t] = ok ? static_cast<T>(I.b[1][j]) : T(1);
-    s.gx[t] = ok ? static_cast<T>(1.0 + I.c[1][j]) : T(1);
-  }
-  for (int t = threadIdx.x; t < TI + 2; t += NTB) {
-    const int i = i0 - 1 + t;
-    const bool ok = i >= 0 && i < I.H;
-    s.by[t] = ok ? static_cast<T>(I.b[0][i]) : T(1);
-    s.gy[t] = ok ? static_cast<T>(1.0 + I.c[0][i]) : T(1);
-  }
-}
-
 __device__ __forceinline__ bool in_box(const dn_box& b, int i, int j) {
   return i >= b.lo[1] && i < b.hi[1] && j >= b.lo[2] && j < b.hi[2];
 }
@@ -190,155 +169,210 @@ struct Sets {
 };
 
 // ---------------------------------------------------------------------------
-// forward step of one tile.  zero_in: the input is the all-zero state.
+// forward step of one warp's strip: rows [ia, ib) of the columns j0 ..
+// j0+32*VEC-1 (the single-grid step's march, dn_fdtd2d.cu: row neighbours in
+// registers, column neighbours by shuffle, the edge lanes load or recompute
+// the value outside the strip, the warp recomputes the intermediate row above
+// (TM) or below (TE) its own).  Fields go through L2 only (other CTAs wrote
+// them the step before); zero_in: the input is the all-zero state.
 // ---------------------------------------------------------------------------
-template <typename T, int POL, int TI>
-__device__ void fwd_tile(TileSmem<T, TI>& s, const dn_batch2d_inst& I, int i0, int j0, int n,
-                         const Sets<T> in, bool zero_in, const Sets<T> out, const Sets<T> ckpt,
-                         bool save, const Sets<T> curl, bool record, bool monitors) {
-  constexpr int R = TI / (NTB / 32);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+template <typename T, int POL, int VEC>
+__device__ void fwd_strip(const dn_batch2d_inst& I, int j0, int ia, int ib, int n,
+                          const Sets<T> in, bool zero_in, const Sets<T> out, const Sets<T> ckpt,
+                          bool save, const Sets<T> curl, bool record, bool monitors) {
+  using V = Vec<T, VEC>;
+  const int lane = threadIdx.x & 31;
   const int H = I.H, W = I.W;
   const long long py = I.pitch;
+  const int jv = j0 + lane * VEC;
+  const bool any = jv < W, full = jv + VEC <= W;
   const T dt = static_cast<T>(I.dt), idl = static_cast<T>(1.0 / I.dl);
   const T* ce = static_cast<const T*>(I.ce);
-  auto load = [&](int c, long long o) -> T { return zero_in ? T(0) : ld(in.p[c] + o); };
-
-  load_tables(s, I, i0, j0);
-  for (int t = threadIdx.x; t < (TI + 2) * (TJ + 2); t += NTB) {
-    const int r = t / (TJ + 2), c = t % (TJ + 2);
-    const int i = i0 - 1 + r, j = j0 - 1 + c;
-    s.f[r][c] = (i >= 0 && i < H && j >= 0 && j < W) ? load(0, i * py + j) : T(0);
-  }
-  __syncthreads();
-
-  const int jj = lane, j = j0 + jj;
-  T a_own[R], b_own[R], cx_own[R], cy_own[R];
-  if (POL == DN_TM) {
+  const T* F = in.p[0];
+  const T* A = in.p[1];
+  const T* B = in.p[2];
+  V bx, gx;
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int ii = warp + 8 * r, i = i0 + ii;
-      a_own[r] = b_own[r] = cx_own[r] = cy_own[r] = T(0);
-      if (i < H && j < W) {
-        const long long o = i * py + j;
-        const T ez = s.f[ii + 1][jj + 1];
-        const T dj = (j < W - 1) ? s.f[ii + 1][jj + 2] - ez : T(0);
-        const T di = (i < H - 1) ? s.f[ii + 2][jj + 1] - ez : T(0);
-        a_own[r] = s.by[ii + 1] * load(1, o) - dt * s.gy[ii + 1] * (dj * idl);
-        b_own[r] = s.bx[jj + 1] * load(2, o) + dt * s.gx[jj + 1] * (di * idl);
-      }
-      s.a[ii][jj + 1] = a_own[r];
-      s.b[ii + 1][jj] = b_own[r];
+  for (int q = 0; q < VEC; ++q) {
+    const int j = jv + q;
+    bx[q] = j < W ? static_cast<T>(I.b[1][j]) : T(1);
+    gx[q] = j < W ? static_cast<T>(1.0 + I.c[1][j]) : T(1);
+  }
+  const bool edge_l = lane == 0 && j0 > 0;
+  const bool edge_r = lane == 31 && jv + VEC < W;
+  auto ldf = [&](const T* a, long long o, bool ok) {
+    return ldv<T, VEC, LD_CG>(a, o, ok && !zero_in, full, jv, W);
+  };
+  auto ldf1 = [&](const T* a, long long o, bool ok) {
+    return dn::ld<T, LD_CG>(a, o, ok && !zero_in);
+  };
+  auto ldce = [&](long long o) { return ldv<T, VEC, LD_NC>(ce, o, any, full, jv, W); };
+
+  // source, monitor, stores, checkpoint and curl record of row i
+  auto finish = [&](int i, long long o, V& v, const V& a, const V& b, const V& c0, const V& c1) {
+    if (!any) return;
+    if (I.src_comp >= 0 && i >= I.src_box.lo[1] && i < I.src_box.hi[1]) {
+      const T w = static_cast<const T*>(I.wave)[n];
+#pragma unroll
+      for (int q = 0; q < VEC; ++q)
+        if (jv + q < W && in_box(I.src_box, i, jv + q)) v[q] += w;
     }
-    if (warp == 0 && lane < TI) {
-      const int ii = lane, i = i0 + ii, jh = j0 - 1;
-      T v = T(0);
-      if (jh >= 0 && i < H) {
-        const T dj = s.f[ii + 1][1] - s.f[ii + 1][0];
-        v = s.by[ii + 1] * load(1, i * py + jh) - dt * s.gy[ii + 1] * (dj * idl);
+    if (monitors && I.mon_comp >= 0 && i >= I.mon_box.lo[1] && i < I.mon_box.hi[1]) {
+      // all accumulators of a frequency are loaded before any is stored
+      const long long ncell = (long long)(I.mon_box.hi[1] - I.mon_box.lo[1]) *
+                              (I.mon_box.hi[2] - I.mon_box.lo[2]);
+      bool inq[VEC];
+      long long cell[VEC];
+#pragma unroll
+      for (int q = 0; q < VEC; ++q) {
+        inq[q] = jv + q < W && in_box(I.mon_box, i, jv + q);
+        cell[q] = inq[q] ? box_cell(I.mon_box, i, jv + q) : 0;
       }
-      s.a[ii][0] = v;
-    } else if (warp == 1) {
-      const int ih = i0 - 1;
-      T v = T(0);
-      if (ih >= 0 && j < W) {
-        const T di = s.f[1][jj + 1] - s.f[0][jj + 1];
-        v = s.bx[jj + 1] * load(2, ih * py + j) + dt * s.gx[jj + 1] * (di * idl);
+      const double* ph = I.phase + (long long)n * I.n_freq * 2;
+      for (int f = 0; f < I.n_freq; ++f) {
+        const double cr = ph[2 * f], ci = ph[2 * f + 1];
+        double* base = I.acc + (long long)f * ncell * 2;
+        double re[VEC], im[VEC];
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) {
+          re[q] = inq[q] ? __ldcg(base + cell[q] * 2) : 0.0;
+          im[q] = inq[q] ? __ldcg(base + cell[q] * 2 + 1) : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) {
+          if (!inq[q]) continue;
+          const double x = static_cast<double>(v[q]);
+          base[cell[q] * 2] = fma(x, cr, re[q]);
+          base[cell[q] * 2 + 1] = fma(x, ci, im[q]);
+        }
       }
-      s.b[0][jj] = v;
+    }
+    stv(out.p[0], o, v, full, jv, W);
+    stv(out.p[1], o, a, full, jv, W);
+    stv(out.p[2], o, b, full, jv, W);
+    if (save) {
+      stv(ckpt.p[0], o, v, full, jv, W);
+      stv(ckpt.p[1], o, a, full, jv, W);
+      stv(ckpt.p[2], o, b, full, jv, W);
+    }
+    if (record) {
+      stv(curl.p[0], o, c0, full, jv, W);
+      if (POL == DN_TE) stv(curl.p[1], o, c1, full, jv, W);
+    }
+  };
+
+  long long o = (long long)ia * py + jv;
+  if (POL == DN_TM) {
+    V f_c = ldf(F, o, any);
+    V b_up;  // Hy of row ia-1, recomputed with its owner's arithmetic
+#pragma unroll
+    for (int q = 0; q < VEC; ++q) b_up[q] = T(0);
+    if (ia > 0) {
+      const V f_u = ldf(F, o - py, any);
+      const V b_o = ldf(B, o - py, any);
+#pragma unroll
+      for (int q = 0; q < VEC; ++q) b_up[q] = bx[q] * b_o[q] + dt * gx[q] * ((f_c[q] - f_u[q]) * idl);
+    }
+    for (int i = ia; i < ib; ++i, o += py) {
+      const V f_n = ldf(F, o + py, any && i + 1 < H);
+      const V a_o = ldf(A, o, any);
+      const V b_o = ldf(B, o, any);
+      const V c_e = ldce(o);
+      const T f_r31 = ldf1(F, o + VEC, edge_r);
+      const T f_l0 = ldf1(F, o - 1, edge_l);
+      const T a_l0 = ldf1(A, o - 1, edge_l);
+      const T by = static_cast<T>(I.b[0][i]);
+      const T gy = static_cast<T>(1.0 + I.c[0][i]);
+      T f_rl = __shfl_down_sync(STRIP_FULL_MASK, f_c[0], 1);
+      if (lane == 31) f_rl = f_r31;
+      V a, b;
+#pragma unroll
+      for (int q = 0; q < VEC; ++q) {
+        const int j = jv + q;
+        const T f_r = (q < VEC - 1) ? f_c[q < VEC - 1 ? q + 1 : q] : f_rl;
+        const T dj = (j < W - 1) ? f_r - f_c[q] : T(0);
+        const T di = (i < H - 1) ? f_n[q] - f_c[q] : T(0);
+        a[q] = by * a_o[q] - dt * gy * (dj * idl);
+        b[q] = bx[q] * b_o[q] + dt * gx[q] * (di * idl);
+      }
+      T a_ll = __shfl_up_sync(STRIP_FULL_MASK, a[VEC - 1], 1);
+      if (lane == 0) a_ll = edge_l ? by * a_l0 - dt * gy * ((f_c[0] - f_l0) * idl) : T(0);
+      V v, cz;
+#pragma unroll
+      for (int q = 0; q < VEC; ++q) {
+        const int j = jv + q;
+        const T a_l = (q > 0) ? a[q > 0 ? q - 1 : 0] : a_ll;
+        const T dHy = (i > 0) ? b[q] - b_up[q] : T(0);
+        const T dHx = (j > 0) ? a[q] - a_l : T(0);
+        cz[q] = gx[q] * (dHy * idl) - gy * (dHx * idl);
+        v[q] = (bx[q] * by) * f_c[q] + c_e[q] * cz[q];
+      }
+      finish(i, o, v, a, b, cz, cz);
+      b_up = b;
+      f_c = f_n;
     }
   } else {
+    const T bx_r = edge_r ? static_cast<T>(I.b[1][jv + VEC]) : T(1);
+    const T gx_r = edge_r ? static_cast<T>(1.0 + I.c[1][jv + VEC]) : T(1);
+    // new Ex, Ey of row r from old Hz of rows r (f) and r-1 (f_u), with the
+    // curl terms; all 32 lanes call it
+    auto e_row = [&](int r, long long oo, const V& f, const V& f_u, V& a, V& b, V& cx, V& cy) {
+      const V a_o = ldf(A, oo, any);
+      const V b_o = ldf(B, oo, any);
+      const V c_e = ldce(oo);
+      const T f_l0 = ldf1(F, oo - 1, edge_l);
+      const T by = static_cast<T>(I.b[0][r]);
+      const T gy = static_cast<T>(1.0 + I.c[0][r]);
+      T f_ll = __shfl_up_sync(STRIP_FULL_MASK, f[VEC - 1], 1);
+      if (lane == 0) f_ll = f_l0;
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int ii = warp + 8 * r, i = i0 + ii;
-      a_own[r] = b_own[r] = cx_own[r] = cy_own[r] = T(0);
-      if (i < H && j < W) {
-        const long long o = i * py + j;
-        const T hz = s.f[ii + 1][jj + 1];
-        const T dj = (j > 0) ? hz - s.f[ii + 1][jj] : T(0);
-        const T di = (i > 0) ? hz - s.f[ii][jj + 1] : T(0);
-        cx_own[r] = s.gx[jj + 1] * (dj * idl);
-        cy_own[r] = -(s.gy[ii + 1] * (di * idl));
-        const T c = ld(ce + o);
-        a_own[r] = s.bx[jj + 1] * load(1, o) + c * cx_own[r];
-        b_own[r] = s.by[ii + 1] * load(2, o) + c * cy_own[r];
+      for (int q = 0; q < VEC; ++q) {
+        const int j = jv + q;
+        const T f_l = (q > 0) ? f[q > 0 ? q - 1 : 0] : f_ll;
+        const T dj = (j > 0) ? f[q] - f_l : T(0);
+        const T di = (r > 0) ? f[q] - f_u[q] : T(0);
+        cx[q] = gx[q] * (dj * idl);
+        cy[q] = -(gy * (di * idl));
+        a[q] = bx[q] * a_o[q] + c_e[q] * cx[q];
+        b[q] = by * b_o[q] + c_e[q] * cy[q];
       }
-      s.a[ii][jj] = a_own[r];
-      s.b[ii][jj] = b_own[r];
-    }
-    if (warp == 0 && lane < TI) {
-      const int ii = lane, i = i0 + ii, jh = j0 + TJ;
-      T v = T(0);
-      if (jh < W && i < H) {
-        const long long o = i * py + jh;
-        const T dj = s.f[ii + 1][TJ + 1] - s.f[ii + 1][TJ];
-        v = s.bx[TJ + 1] * load(1, o) + ld(ce + o) * (s.gx[TJ + 1] * (dj * idl));
+    };
+    V f_c = ldf(F, o, any);
+    const V f_u = ldf(F, o - py, any && ia > 0);
+    V a_c, b_c, cx_c, cy_c;
+    e_row(ia, o, f_c, f_u, a_c, b_c, cx_c, cy_c);
+    for (int i = ia; i < ib; ++i, o += py) {
+      const bool nxt = i + 1 < H;
+      const V f_n = ldf(F, o + py, any && nxt);
+      const T a_o31 = ldf1(A, o + VEC, edge_r);
+      const T ce31 = dn::ld<T, LD_NC>(ce, o + VEC, edge_r);
+      const T f31 = ldf1(F, o + VEC, edge_r);
+      const T by = static_cast<T>(I.b[0][i]);
+      const T gy = static_cast<T>(1.0 + I.c[0][i]);
+      V a_n, b_n, cx_n, cy_n;
+#pragma unroll
+      for (int q = 0; q < VEC; ++q) a_n[q] = b_n[q] = cx_n[q] = cy_n[q] = T(0);
+      if (nxt) e_row(i + 1, o + py, f_n, f_c, a_n, b_n, cx_n, cy_n);
+      T a_rl = __shfl_down_sync(STRIP_FULL_MASK, a_c[0], 1);
+      if (lane == 31)
+        a_rl = edge_r ? bx_r * a_o31 + ce31 * (gx_r * ((f31 - f_c[VEC - 1]) * idl)) : T(0);
+      V v;
+#pragma unroll
+      for (int q = 0; q < VEC; ++q) {
+        const int j = jv + q;
+        const T a_r = (q < VEC - 1) ? a_c[q < VEC - 1 ? q + 1 : q] : a_rl;
+        const T dEy = (i < H - 1) ? b_n[q] - b_c[q] : T(0);
+        const T dEx = (j < W - 1) ? a_r - a_c[q] : T(0);
+        v[q] = (bx[q] * by) * f_c[q] + dt * (gx[q] * (dEy * idl) - gy * (dEx * idl));
       }
-      s.a[ii][TJ] = v;
-    } else if (warp == 1) {
-      const int ih = i0 + TI;
-      T v = T(0);
-      if (ih < H && j < W) {
-        const long long o = ih * py + j;
-        const T di = s.f[TI + 1][jj + 1] - s.f[TI][jj + 1];
-        v = s.by[TI + 1] * load(2, o) + ld(ce + o) * (-(s.gy[TI + 1] * (di * idl)));
-      }
-      s.b[TI][jj] = v;
+      finish(i, o, v, a_c, b_c, cx_c, cy_c);
+      f_c = f_n;
+      a_c = a_n;
+      b_c = b_n;
+      cx_c = cx_n;
+      cy_c = cy_n;
     }
   }
-  __syncthreads();
-
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-    const int ii = warp + 8 * r, i = i0 + ii;
-    if (i < H && j < W) {
-      const long long o = i * py + j;
-      const T fo = s.f[ii + 1][jj + 1];
-      const T bb = s.bx[jj + 1] * s.by[ii + 1];
-      T v0, cz = T(0);
-      if (POL == DN_TM) {
-        const T dHy = (i > 0) ? s.b[ii + 1][jj] - s.b[ii][jj] : T(0);
-        const T dHx = (j > 0) ? s.a[ii][jj + 1] - s.a[ii][jj] : T(0);
-        cz = s.gx[jj + 1] * (dHy * idl) - s.gy[ii + 1] * (dHx * idl);
-        v0 = bb * fo + ld(ce + o) * cz;
-      } else {
-        const T dEy = (i < H - 1) ? s.b[ii + 1][jj] - s.b[ii][jj] : T(0);
-        const T dEx = (j < W - 1) ? s.a[ii][jj + 1] - s.a[ii][jj] : T(0);
-        v0 = bb * fo + dt * (s.gx[jj + 1] * (dEy * idl) - s.gy[ii + 1] * (dEx * idl));
-      }
-      if (I.src_comp >= 0 && in_box(I.src_box, i, j))
-        v0 += static_cast<const T*>(I.wave)[n];
-      if (monitors && I.mon_comp >= 0 && in_box(I.mon_box, i, j)) {
-        const long long cell = box_cell(I.mon_box, i, j);
-        const long long ncell = (long long)(I.mon_box.hi[1] - I.mon_box.lo[1]) *
-                                (I.mon_box.hi[2] - I.mon_box.lo[2]);
-        const double x = static_cast<double>(v0);
-        const double* ph = I.phase + (long long)n * I.n_freq * 2;
-        for (int f = 0; f < I.n_freq; ++f) {
-          double* acc = I.acc + ((long long)f * ncell + cell) * 2;
-          acc[0] = fma(x, ph[2 * f], acc[0]);
-          acc[1] = fma(x, ph[2 * f + 1], acc[1]);
-        }
-      }
-      out.p[0][o] = v0;
-      out.p[1][o] = a_own[r];
-      out.p[2][o] = b_own[r];
-      if (save) {
-        ckpt.p[0][o] = v0;
-        ckpt.p[1][o] = a_own[r];
-        ckpt.p[2][o] = b_own[r];
-      }
-      if (record) {
-        if (POL == DN_TM) {
-          curl.p[0][o] = cz;
-        } else {
-          curl.p[0][o] = cx_own[r];
-          curl.p[1][o] = cy_own[r];
-        }
-      }
-    }
-  }
-  __syncthreads();  // shared memory is reused by the next tile
 }
 
 // monitor-DFT gradient added to the adjoint field at (i, j) for step n
@@ -358,151 +392,238 @@ __device__ __forceinline__ T mon_inject(const dn_batch2d_inst& I, int i, int j, 
 }
 
 // ---------------------------------------------------------------------------
-// reverse step of one tile (transpose of fwd_tile; see dn_adjoint2d.cu)
+// reverse step of one warp's strip (transpose of fwd_strip; the single-grid
+// reverse march of dn_adjoint2d.cu).  Every load of lambda_F (TM: Ez, TE: Hz)
+// has the monitor-DFT gradient of step n added.  Adjoint fields and curl
+// records go through L2 only; the FP64 gradient is read the same way.
 // ---------------------------------------------------------------------------
-template <typename T, int POL, int TI>
-__device__ void adj_tile(TileSmem<T, TI>& s, const dn_batch2d_inst& I, int i0, int j0, int n,
-                         const Sets<T> lin_s, const Sets<T> lout_s, const Sets<T> curl_s) {
-  T* const* lin = lin_s.p;
-  T* const* lout = lout_s.p;
-  T* const* curl = curl_s.p;
-  constexpr int R = TI / (NTB / 32);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+template <typename T, int POL, int VEC>
+__device__ void adj_strip(const dn_batch2d_inst& I, int j0, int ia, int ib, int n,
+                          const Sets<T> lin, const Sets<T> lout, const Sets<T> curl) {
+  using V = Vec<T, VEC>;
+  using D = Vec<double, VEC>;
+  const int lane = threadIdx.x & 31;
   const int H = I.H, W = I.W;
   const long long py = I.pitch;
+  const int jv = j0 + lane * VEC;
+  const bool any = jv < W, full = jv + VEC <= W;
   const T dt = static_cast<T>(I.dt), idl = static_cast<T>(1.0 / I.dl);
   const T* ce = static_cast<const T*>(I.ce);
-
-  load_tables(s, I, i0, j0);
-  for (int t = threadIdx.x; t < (TI + 2) * (TJ + 2); t += NTB) {
-    const int r = t / (TJ + 2), c = t % (TJ + 2);
-    const int i = i0 - 1 + r, j = j0 - 1 + c;
-    T v = T(0);
-    if (i >= 0 && i < H && j >= 0 && j < W) {
-      const long long o = i * py + j;
-      const T l0 = ld(lin[0] + o) + mon_inject<T>(I, i, j, n);
-      v = POL == DN_TM ? ld(ce + o) * l0 : l0;
-    }
-    s.f[r][c] = v;
-  }
-  __syncthreads();
-
-  const int jj = lane, j = j0 + jj;
-  T a_own[R], b_own[R];
-  if (POL == DN_TM) {
+  const T* L0 = lin.p[0];
+  const T* L1 = lin.p[1];
+  const T* L2 = lin.p[2];
+  const bool inject = I.gmon != nullptr && I.mon_comp >= 0;
+  auto ldl = [&](const T* a, long long o, bool ok) { return ldv<T, VEC, LD_CG>(a, o, ok, full, jv, W); };
+  auto ldl1 = [&](const T* a, long long o, bool ok) { return dn::ld<T, LD_CG>(a, o, ok); };
+  auto ldce = [&](long long o) { return ldv<T, VEC, LD_NC>(ce, o, any, full, jv, W); };
+  // lambda_F of row r with the monitor gradient of step n added
+  auto ldl0 = [&](int r, long long o, bool ok) {
+    V l = ldl(L0, o, ok);
+    if (inject && ok && r >= I.mon_box.lo[1] && r < I.mon_box.hi[1]) {
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int ii = warp + 8 * r, i = i0 + ii;
-      T vx = T(0), vy = T(0);
-      a_own[r] = b_own[r] = T(0);
-      if (i < H && j < W) {
-        const long long o = i * py + j;
-        const T u = s.f[ii + 1][jj + 1];
-        const T gy = s.gy[ii + 1] * idl, gx = s.gx[jj + 1] * idl;
-        a_own[r] = ld(lin[1] + o) - gy * ((j > 0 ? u : T(0)) - s.f[ii + 1][jj + 2]);
-        b_own[r] = ld(lin[2] + o) + gx * ((i > 0 ? u : T(0)) - s.f[ii + 2][jj + 1]);
-        vx = (j < W - 1) ? dt * gy * a_own[r] : T(0);
-        vy = (i < H - 1) ? dt * gx * b_own[r] : T(0);
-      }
-      s.a[ii][jj + 1] = vx;
-      s.b[ii + 1][jj] = vy;
+      for (int q = 0; q < VEC; ++q)
+        if (jv + q < W) l[q] += mon_inject<T>(I, r, jv + q, n);
     }
-    if (warp == 0 && lane < TI) {
-      const int ii = lane, i = i0 + ii, jh = j0 - 1;
-      T v = T(0);
-      if (jh >= 0 && i < H) {
-        const T gy = s.gy[ii + 1] * idl;
-        const T u = s.f[ii + 1][0];
-        const T lh = ld(lin[1] + i * py + jh) - gy * ((jh > 0 ? u : T(0)) - s.f[ii + 1][1]);
-        v = dt * gy * lh;
+    return l;
+  };
+  auto ldl0_1 = [&](int r, int j, long long o, bool ok) {
+    T l = ldl1(L0, o, ok);
+    if (ok) l += mon_inject<T>(I, r, j, n);
+    return l;
+  };
+  auto add_grad = [&](long long o, const V& x0, const V& c0, const V& x1, const V& c1, bool two) {
+    D g = ldv<double, VEC, LD_CG>(I.grad, o, any, full, jv, W);
+#pragma unroll
+    for (int q = 0; q < VEC; ++q) {
+      if (two)
+        g[q] += static_cast<double>(x0[q]) * static_cast<double>(c0[q]) +
+                static_cast<double>(x1[q]) * static_cast<double>(c1[q]);
+      else
+        g[q] += static_cast<double>(x0[q]) * static_cast<double>(c0[q]);
+    }
+    stv(I.grad, o, g, full, jv, W);
+  };
+
+  long long o = (long long)ia * py + jv;
+  if (POL == DN_TM) {
+    V bx, gx;  // gx = (1 + c_x) / dl
+#pragma unroll
+    for (int q = 0; q < VEC; ++q) {
+      const int j = jv + q;
+      bx[q] = j < W ? static_cast<T>(I.b[1][j]) : T(1);
+      gx[q] = (j < W ? static_cast<T>(1.0 + I.c[1][j]) : T(1)) * idl;
+    }
+    const bool edge_l = lane == 0 && j0 > 0;         // recomputes vx at column j0-1
+    const bool edge_r = lane == 31 && jv + VEC < W;  // loads u at column j0+32*VEC
+    V l_c = ldl0(ia, o, any);
+    V u_c;
+    {
+      const V c_e = ldce(o);
+#pragma unroll
+      for (int q = 0; q < VEC; ++q) u_c[q] = c_e[q] * l_c[q];
+    }
+    V vy_up;  // vy of row ia-1 (row ia-1 < H-1)
+#pragma unroll
+    for (int q = 0; q < VEC; ++q) vy_up[q] = T(0);
+    if (ia > 0) {
+      const V l_u = ldl0(ia - 1, o - py, any);
+      const V c_u = ldce(o - py);
+      const V l2_u = ldl(L2, o - py, any);
+#pragma unroll
+      for (int q = 0; q < VEC; ++q) {
+        const T uu = c_u[q] * l_u[q];
+        const T lh = l2_u[q] + gx[q] * ((ia - 1 > 0 ? uu : T(0)) - u_c[q]);
+        vy_up[q] = dt * gx[q] * lh;
       }
-      s.a[ii][0] = v;
-    } else if (warp == 1) {
-      const int ih = i0 - 1;
-      T v = T(0);
-      if (ih >= 0 && j < W) {
-        const T gx = s.gx[jj + 1] * idl;
-        const T u = s.f[0][jj + 1];
-        const T lh = ld(lin[2] + ih * py + j) + gx * ((ih > 0 ? u : T(0)) - s.f[1][jj + 1]);
-        v = dt * gx * lh;
+    }
+    for (int i = ia; i < ib; ++i, o += py) {
+      const bool nxt = i + 1 < H;
+      const V l_n = ldl0(i + 1, o + py, any && nxt);
+      const V c_n = ldv<T, VEC, LD_NC>(ce, o + py, any && nxt, full, jv, W);
+      const V l1 = ldl(L1, o, any);
+      const V l2 = ldl(L2, o, any);
+      const V crl = ldl(curl.p[0], o, any);
+      const T c_r31 = dn::ld<T, LD_NC>(ce, o + VEC, edge_r);
+      const T l_r31 = ldl0_1(i, jv + VEC, o + VEC, edge_r);
+      const T c_l0 = dn::ld<T, LD_NC>(ce, o - 1, edge_l);
+      const T l_l0 = ldl0_1(i, j0 - 1, o - 1, edge_l);
+      const T l1_l0 = ldl1(L1, o - 1, edge_l);
+      const T by = static_cast<T>(I.b[0][i]);
+      const T gy = static_cast<T>(1.0 + I.c[0][i]) * idl;
+      V u_n;
+#pragma unroll
+      for (int q = 0; q < VEC; ++q) u_n[q] = c_n[q] * l_n[q];
+      T u_rl = __shfl_down_sync(STRIP_FULL_MASK, u_c[0], 1);
+      if (lane == 31) u_rl = c_r31 * l_r31;
+      V a, b, vx, vy;
+#pragma unroll
+      for (int q = 0; q < VEC; ++q) {
+        const int j = jv + q;
+        const T u_r = (q < VEC - 1) ? u_c[q < VEC - 1 ? q + 1 : q] : u_rl;
+        a[q] = l1[q] - gy * ((j > 0 ? u_c[q] : T(0)) - u_r);
+        b[q] = l2[q] + gx[q] * ((i > 0 ? u_c[q] : T(0)) - u_n[q]);
+        vx[q] = (j < W - 1) ? dt * gy * a[q] : T(0);
+        vy[q] = (i < H - 1) ? dt * gx[q] * b[q] : T(0);
       }
-      s.b[0][jj] = v;
+      T vx_ll = __shfl_up_sync(STRIP_FULL_MASK, vx[VEC - 1], 1);
+      if (lane == 0) {
+        T v = T(0);
+        if (edge_l) {  // column j0-1 < W-1
+          const T ul = c_l0 * l_l0;
+          const T lh = l1_l0 - gy * ((j0 - 1 > 0 ? ul : T(0)) - u_c[0]);
+          v = dt * gy * lh;
+        }
+        vx_ll = v;
+      }
+      V o0, o1, o2;
+#pragma unroll
+      for (int q = 0; q < VEC; ++q) {
+        const T vx_l = (q > 0) ? vx[q > 0 ? q - 1 : 0] : vx_ll;
+        o0[q] = bx[q] * by * l_c[q] + (vx[q] - vx_l) - (vy[q] - vy_up[q]);
+        o1[q] = by * a[q];
+        o2[q] = bx[q] * b[q];
+      }
+      if (any) {
+        add_grad(o, l_c, crl, l_c, crl, false);
+        stv(lout.p[0], o, o0, full, jv, W);
+        stv(lout.p[1], o, o1, full, jv, W);
+        stv(lout.p[2], o, o2, full, jv, W);
+      }
+      vy_up = vy;
+      u_c = u_n;
+      l_c = l_n;
     }
   } else {
+    V bx, gxr, cx;  // gxr = 1 + c_x, cx = dt (1 + c_x) / dl
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int ii = warp + 8 * r, i = i0 + ii;
-      T ux = T(0), uy = T(0);
-      a_own[r] = b_own[r] = T(0);
-      if (i < H && j < W) {
-        const long long o = i * py + j;
-        const T lh = s.f[ii + 1][jj + 1];
-        const T cy = dt * s.gy[ii + 1] * idl, cx = dt * s.gx[jj + 1] * idl;
-        const T wj = (j < W - 1) ? cy * lh : T(0);
-        const T wjm = (j > 0) ? cy * s.f[ii + 1][jj] : T(0);
-        const T wi = (i < H - 1) ? cx * lh : T(0);
-        const T wim = (i > 0) ? cx * s.f[ii][jj + 1] : T(0);
-        a_own[r] = ld(lin[1] + o) + wj - wjm;
-        b_own[r] = ld(lin[2] + o) - wi + wim;
-        I.grad[o] += static_cast<double>(a_own[r]) * static_cast<double>(ld(curl[0] + o)) +
-                     static_cast<double>(b_own[r]) * static_cast<double>(ld(curl[1] + o));
-        const T c = ld(ce + o);
-        ux = (j > 0) ? c * s.gx[jj + 1] * idl * a_own[r] : T(0);
-        uy = (i > 0) ? c * s.gy[ii + 1] * idl * b_own[r] : T(0);
-      }
-      s.a[ii][jj] = ux;
-      s.b[ii][jj] = uy;
+    for (int q = 0; q < VEC; ++q) {
+      const int j = jv + q;
+      bx[q] = j < W ? static_cast<T>(I.b[1][j]) : T(1);
+      gxr[q] = j < W ? static_cast<T>(1.0 + I.c[1][j]) : T(1);
+      cx[q] = dt * gxr[q] * idl;
     }
-    if (warp == 0 && lane < TI) {
-      const int ii = lane, i = i0 + ii, jh = j0 + TJ;
-      T v = T(0);
-      if (jh < W && i < H) {
-        const long long o = i * py + jh;
-        const T cy = dt * s.gy[ii + 1] * idl;
-        const T wj = (jh < W - 1) ? cy * s.f[ii + 1][TJ + 1] : T(0);
-        const T wjm = cy * s.f[ii + 1][TJ];
-        const T lex = ld(lin[1] + o) + wj - wjm;
-        v = ld(ce + o) * s.gx[TJ + 1] * idl * lex;
+    const bool edge_l = lane == 0 && j0 > 0;         // loads lambda_Hz at column j0-1
+    const bool edge_r = lane == 31 && jv + VEC < W;  // recomputes ux at column j0+32*VEC
+    const T gxr_r = edge_r ? static_cast<T>(1.0 + I.c[1][jv + VEC]) : T(1);
+    // E-adjoint half of row r from lambda_Hz of rows r (lh) and r-1 (lh_u);
+    // the row's gradient when `own`; all 32 lanes call it
+    auto e_row = [&](int r, long long oo, const V& lh, const V& lh_u, bool own, V& a, V& b, V& ux,
+                     V& uy) {
+      const V l1 = ldl(L1, oo, any);
+      const V l2 = ldl(L2, oo, any);
+      const V c_e = ldce(oo);
+      const T lh_l0 = ldl0_1(r, j0 - 1, oo - 1, edge_l);
+      const T gyr = static_cast<T>(1.0 + I.c[0][r]);
+      const T cy = dt * gyr * idl;
+      T lh_ll = __shfl_up_sync(STRIP_FULL_MASK, lh[VEC - 1], 1);
+      if (lane == 0) lh_ll = lh_l0;
+#pragma unroll
+      for (int q = 0; q < VEC; ++q) {
+        const int j = jv + q;
+        const T lh_l = (q > 0) ? lh[q > 0 ? q - 1 : 0] : lh_ll;
+        const T wj = (j < W - 1) ? cy * lh[q] : T(0);
+        const T wjm = (j > 0) ? cy * lh_l : T(0);
+        const T wi = (r < H - 1) ? cx[q] * lh[q] : T(0);
+        const T wim = (r > 0) ? cx[q] * lh_u[q] : T(0);
+        a[q] = l1[q] + wj - wjm;
+        b[q] = l2[q] - wi + wim;
+        ux[q] = (j > 0) ? c_e[q] * gxr[q] * idl * a[q] : T(0);
+        uy[q] = (r > 0) ? c_e[q] * gyr * idl * b[q] : T(0);
       }
-      s.a[ii][TJ] = v;
-    } else if (warp == 1) {
-      const int ih = i0 + TI;
-      T v = T(0);
-      if (ih < H && j < W) {
-        const long long o = ih * py + j;
-        const T cx = dt * s.gx[jj + 1] * idl;
-        const T wi = (ih < H - 1) ? cx * s.f[TI + 1][jj + 1] : T(0);
-        const T wim = cx * s.f[TI][jj + 1];
-        const T ley = ld(lin[2] + o) - wi + wim;
-        v = ld(ce + o) * s.gy[TI + 1] * idl * ley;
+      if (own && any) {
+        const V c0 = ldl(curl.p[0], oo, any);
+        const V c1 = ldl(curl.p[1], oo, any);
+        add_grad(oo, a, c0, b, c1, true);
       }
-      s.b[TI][jj] = v;
+    };
+    V lh_c = ldl0(ia, o, any);
+    const V lh_u = ldl0(ia - 1, o - py, any && ia > 0);
+    V a_c, b_c, ux_c, uy_c;
+    e_row(ia, o, lh_c, lh_u, true, a_c, b_c, ux_c, uy_c);
+    for (int i = ia; i < ib; ++i, o += py) {
+      const bool nxt = i + 1 < H;
+      const V lh_n = ldl0(i + 1, o + py, any && nxt);
+      const T l1_31 = ldl1(L1, o + VEC, edge_r);
+      const T c31 = dn::ld<T, LD_NC>(ce, o + VEC, edge_r);
+      const T lh31 = ldl0_1(i, jv + VEC, o + VEC, edge_r);
+      const T by = static_cast<T>(I.b[0][i]);
+      const T cy = dt * static_cast<T>(1.0 + I.c[0][i]) * idl;
+      V a_n, b_n, ux_n, uy_n;
+#pragma unroll
+      for (int q = 0; q < VEC; ++q) a_n[q] = b_n[q] = ux_n[q] = uy_n[q] = T(0);
+      if (nxt) e_row(i + 1, o + py, lh_n, lh_c, i + 1 < ib, a_n, b_n, ux_n, uy_n);
+      T ux_rl = __shfl_down_sync(STRIP_FULL_MASK, ux_c[0], 1);
+      if (lane == 31) {
+        T v = T(0);
+        if (edge_r) {  // column jh = j0+32*VEC > 0
+          const T wj = (jv + VEC < W - 1) ? cy * lh31 : T(0);
+          const T wjm = cy * lh_c[VEC - 1];
+          const T lex = l1_31 + wj - wjm;
+          v = c31 * gxr_r * idl * lex;
+        }
+        ux_rl = v;
+      }
+      V o0, o1, o2;
+#pragma unroll
+      for (int q = 0; q < VEC; ++q) {
+        const T ux_r = (q < VEC - 1) ? ux_c[q < VEC - 1 ? q + 1 : q] : ux_rl;
+        o0[q] = bx[q] * by * lh_c[q] + (ux_c[q] - ux_r) - (uy_c[q] - uy_n[q]);
+        o1[q] = bx[q] * a_c[q];
+        o2[q] = by * b_c[q];
+      }
+      if (any) {
+        stv(lout.p[0], o, o0, full, jv, W);
+        stv(lout.p[1], o, o1, full, jv, W);
+        stv(lout.p[2], o, o2, full, jv, W);
+      }
+      lh_c = lh_n;
+      a_c = a_n;
+      b_c = b_n;
+      ux_c = ux_n;
+      uy_c = uy_n;
     }
   }
-  __syncthreads();
-
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-    const int ii = warp + 8 * r, i = i0 + ii;
-    if (i >= H || j >= W) continue;
-    const long long o = i * py + j;
-    const T bx = s.bx[jj + 1], by = s.by[ii + 1];
-    if (POL == DN_TM) {
-      const T lez = ld(lin[0] + o) + mon_inject<T>(I, i, j, n);
-      I.grad[o] += static_cast<double>(lez) * static_cast<double>(ld(curl[0] + o));
-      lout[0][o] = bx * by * lez + (s.a[ii][jj + 1] - s.a[ii][jj]) - (s.b[ii + 1][jj] - s.b[ii][jj]);
-      lout[1][o] = by * a_own[r];
-      lout[2][o] = bx * b_own[r];
-    } else {
-      const T lhz = s.f[ii + 1][jj + 1];
-      lout[0][o] = bx * by * lhz + (s.a[ii][jj] - s.a[ii][jj + 1]) - (s.b[ii][jj] - s.b[ii + 1][jj]);
-      lout[1][o] = bx * a_own[r];
-      lout[2][o] = by * b_own[r];
-    }
-  }
-  __syncthreads();
 }
-
 
 template <typename T>
 __device__ __forceinline__ Sets<T> field_set(void* const f[3]) {
@@ -518,9 +639,27 @@ __device__ __forceinline__ Sets<T> slot_set(void* base, long long slot, long lon
   return s;
 }
 
+// Warp `threadIdx.x / 32`'s share of tile q of instance I: the tile is TI
+// rows x 32*VEC columns, each of the CTA's 8 warps marches TI/8 of its rows.
+struct StripTask {
+  int j0, ia, ib;
+};
+
+template <int VEC, int TI>
+__device__ __forceinline__ StripTask strip_of(const dn_batch2d_inst& I, int q) {
+  const int ntx = (I.W + 32 * VEC - 1) / (32 * VEC);
+  const int ty = q / ntx, tx = q % ntx;
+  constexpr int R = TI / (NTB / 32);
+  StripTask st;
+  st.j0 = tx * 32 * VEC;
+  st.ia = ty * TI + (threadIdx.x >> 5) * R;
+  st.ib = min(st.ia + R, I.H);
+  return st;
+}
+
 template <typename T, int POL, int TI>
-__global__ void __launch_bounds__(NTB, 8) k_batch2d_fwd(unsigned char* table, int* status) {
-  __shared__ TileSmem<T, TI> s;
+__global__ void __launch_bounds__(NTB, 2) k_batch2d_fwd(unsigned char* table, int* status) {
+  constexpr int VEC = 16 / static_cast<int>(sizeof(T));
   const TableView v = view(table);
   __shared__ unsigned int s_gen;
   if (threadIdx.x == 0) s_gen = *reinterpret_cast<volatile unsigned int*>(&v.h->bar[1]);
@@ -532,22 +671,23 @@ __global__ void __launch_bounds__(NTB, 8) k_batch2d_fwd(unsigned char* table, in
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
       const int2 m = v.tile_map[t];
       const dn_batch2d_inst& I = v.inst[m.x];
-      const int ntx = (I.W + TJ - 1) / TJ;
-      const int i0 = (m.y / ntx) * TI, j0 = (m.y % ntx) * TJ;
+      const StripTask st = strip_of<VEC, TI>(I, m.y);
+      if (st.ia >= I.H) continue;  // whole warp: the shuffles see all 32 lanes
       const Sets<T> in = field_set<T>(I.f[n & 1]);
       const Sets<T> out = field_set<T>(I.f[(n + 1) & 1]);
       Sets<T> ck{{nullptr, nullptr, nullptr}};
       const bool save = I.ckpt != nullptr && K > 0 && (n + 1) % K == 0 && (n + 1) < I.n_steps;
       if (save) ck = slot_set<T>(I.ckpt, (n + 1) / K - 1, (long long)I.H * I.pitch, 3);
-      fwd_tile<T, POL, TI>(s, I, i0, j0, n, in, false, out, ck, save, ck, false, true);
+      fwd_strip<T, POL, VEC>(I, st.j0, st.ia, st.ib, n, in, false, out, ck, save, ck, false,
+                             true);
     }
     if (!grid_sync(v.h->bar, gen, status)) return;
   }
 }
 
 template <typename T, int POL, int TI>
-__global__ void __launch_bounds__(NTB, 8) k_batch2d_bwd(unsigned char* table, int* status) {
-  __shared__ TileSmem<T, TI> s;
+__global__ void __launch_bounds__(NTB, 2) k_batch2d_bwd(unsigned char* table, int* status) {
+  constexpr int VEC = 16 / static_cast<int>(sizeof(T));
   const TableView v = view(table);
   __shared__ unsigned int s_gen;
   if (threadIdx.x == 0) s_gen = *reinterpret_cast<volatile unsigned int*>(&v.h->bar[1]);
@@ -563,15 +703,16 @@ __global__ void __launch_bounds__(NTB, 8) k_batch2d_bwd(unsigned char* table, in
       for (int t = blockIdx.x; t < nt; t += gridDim.x) {
         const int2 m = v.tile_map[t];
         const dn_batch2d_inst& I = v.inst[m.x];
-        const int ntx = (I.W + TJ - 1) / TJ;
-        const int i0 = (m.y / ntx) * TI, j0 = (m.y % ntx) * TJ;
+        const StripTask st = strip_of<VEC, TI>(I, m.y);
+        if (st.ia >= I.H) continue;
         const long long fe = (long long)I.H * I.pitch;
         const bool zero_in = n == ta && g == 0;
         const Sets<T> in = n == ta ? (g == 0 ? field_set<T>(I.f[0]) : slot_set<T>(I.ckpt, g - 1, fe, 3))
                                    : field_set<T>(I.f[n & 1]);
         const Sets<T> out = field_set<T>(I.f[(n + 1) & 1]);
         const Sets<T> cr = slot_set<T>(I.curl, n - ta, fe, NCURL);
-        fwd_tile<T, POL, TI>(s, I, i0, j0, n, in, zero_in, out, out, false, cr, true, false);
+        fwd_strip<T, POL, VEC>(I, st.j0, st.ia, st.ib, n, in, zero_in, out, out, false, cr, true,
+                               false);
       }
       if (!grid_sync(v.h->bar, gen, status)) return;
     }
@@ -581,13 +722,13 @@ __global__ void __launch_bounds__(NTB, 8) k_batch2d_bwd(unsigned char* table, in
       for (int t = blockIdx.x; t < nt; t += gridDim.x) {
         const int2 m = v.tile_map[t];
         const dn_batch2d_inst& I = v.inst[m.x];
-        const int ntx = (I.W + TJ - 1) / TJ;
-        const int i0 = (m.y / ntx) * TI, j0 = (m.y % ntx) * TJ;
+        const StripTask st = strip_of<VEC, TI>(I, m.y);
+        if (st.ia >= I.H) continue;
         const long long fe = (long long)I.H * I.pitch;
         const Sets<T> lin = field_set<T>(I.lam[(n + 1) & 1]);
         const Sets<T> lout = field_set<T>(I.lam[n & 1]);
         const Sets<T> cr = slot_set<T>(I.curl, n - ta, fe, NCURL);
-        adj_tile<T, POL, TI>(s, I, i0, j0, n, lin, lout, cr);
+        adj_strip<T, POL, VEC>(I, st.j0, st.ia, st.ib, n, lin, lout, cr);
       }
       if (!grid_sync(v.h->bar, gen, status)) return;
     }
@@ -604,7 +745,7 @@ __global__ void __launch_bounds__(NTB, 8) k_batch2d_bwd(unsigned char* table, in
 // previous CTA's shared memory (distributed shared memory), and two cluster
 // barriers per step order the half-steps.  Every CTA of a cluster runs the same
 // instance's step count, so the barrier sequence is identical on all of them.
-// The arithmetic is fwd_tile's, expression for expression.
+// The arithmetic is fwd_strip's, expression for expression.
 namespace cg = cooperative_groups;
 
 template <typename T>
@@ -1064,6 +1205,16 @@ int validate(const dn_batch2d* cfg, const dn_batch2d_inst* insts) {
     for (int s = 0; s < 2; ++s)
       for (int c = 0; c < 3; ++c)
         if (!I.f[s][c]) return DN_EINVAL;
+    // rows move in 16-byte chunks: 16-byte rows (fields and the FP64
+    // gradient) and 16-byte aligned arrays
+    const int64_t esz = cfg->dtype == DN_F32 ? 4 : 8;
+    if ((I.pitch * esz) % 16 != 0 || (I.pitch * 8) % 16 != 0 || !aligned16(I.ce)) return DN_EINVAL;
+    for (int s = 0; s < 2; ++s)
+      for (int c = 0; c < 3; ++c)
+        if (!aligned16(I.f[s][c]) || (I.lam[s][c] && !aligned16(I.lam[s][c]))) return DN_EINVAL;
+    if ((I.ckpt && !aligned16(I.ckpt)) || (I.curl && !aligned16(I.curl)) ||
+        (I.grad && !aligned16(I.grad)))
+      return DN_EINVAL;
     if (I.src_comp != DN_NONE) {
       if (I.src_comp != first || !I.wave || !box_ok(I.src_box, 1, I.H, I.W)) return DN_EINVAL;
     }
@@ -1079,7 +1230,8 @@ int validate(const dn_batch2d* cfg, const dn_batch2d_inst* insts) {
 int total_tiles_of(const dn_batch2d* cfg, const dn_batch2d_inst* insts) {
   long long t = 0;
   for (int b = 0; b < cfg->n_inst; ++b)
-    t += (long long)((insts[b].W + TJ - 1) / TJ) * ((insts[b].H + cfg->tile_rows - 1) / cfg->tile_rows);
+    t += (long long)((insts[b].W + tile_cols(cfg->dtype) - 1) / tile_cols(cfg->dtype)) *
+         ((insts[b].H + cfg->tile_rows - 1) / cfg->tile_rows);
   return t > 0x7fffffffLL ? -1 : (int)t;
 }
 
@@ -1257,7 +1409,8 @@ extern "C" int32_t dn_batch2d_pack(const dn_batch2d* cfg, const dn_batch2d_inst*
     inst[k] = I;
     steps[k] = I.n_steps;
     prefix[k] = t;
-    const int ntiles = ((I.W + dn::TJ - 1) / dn::TJ) * ((I.H + cfg->tile_rows - 1) / cfg->tile_rows);
+    const int tc = dn::tile_cols(cfg->dtype);
+    const int ntiles = ((I.W + tc - 1) / tc) * ((I.H + cfg->tile_rows - 1) / cfg->tile_rows);
     for (int q = 0; q < ntiles; ++q) map[t++] = make_int2(k, q);
     max_steps = std::max(max_steps, I.n_steps);
   }

@@ -21,15 +21,29 @@ struct Vec {
   __device__ __forceinline__ const T& operator[](int q) const { return v[q]; }
 };
 
-template <typename T>
+// Load paths: LD_NC for arrays no thread writes during the launch
+// (non-coherent read-only path), LD_CG for arrays other CTAs of the same
+// launch write (L2 only, never a stale L1 line), LD_PLAIN otherwise.
+enum { LD_NC = 0, LD_CG = 1, LD_PLAIN = 2 };
+
+template <int LDP, typename P>
+__device__ __forceinline__ P load_as(const P* s) {
+  if constexpr (LDP == LD_NC)
+    return __ldg(s);
+  else if constexpr (LDP == LD_CG)
+    return __ldcg(s);
+  else
+    return *s;
+}
+
+template <typename T, int LDP = LD_NC>
 __device__ __forceinline__ T ld(const T* a, long long o, bool ok) {
-  return ok ? __ldg(a + o) : T(0);
+  return ok ? load_as<LDP>(a + o) : T(0);
 }
 
 // Columns jv .. jv+VEC-1 at offset o; columns at or past W (and all of them
-// when !ok) read as 0.  NC: the array is not written during the launch
-// (read through the non-coherent path); otherwise plain loads.
-template <typename T, int VEC, bool NC = true>
+// when !ok) read as 0.
+template <typename T, int VEC, int LDP = LD_NC>
 __device__ __forceinline__ Vec<T, VEC> ldv(const T* a, long long o, bool ok, bool full, int jv,
                                            int W) {
   Vec<T, VEC> r;
@@ -39,12 +53,10 @@ __device__ __forceinline__ Vec<T, VEC> ldv(const T* a, long long o, bool ok, boo
 #pragma unroll
       for (int c = 0; c < VEC / PER; ++c) {
         if constexpr (std::is_same<T, float>::value) {
-          const float4* s = reinterpret_cast<const float4*>(a + o) + c;
-          const float4 x = NC ? __ldg(s) : *s;
+          const float4 x = load_as<LDP>(reinterpret_cast<const float4*>(a + o) + c);
           r[4 * c + 0] = x.x, r[4 * c + 1] = x.y, r[4 * c + 2] = x.z, r[4 * c + 3] = x.w;
         } else {
-          const double2* s = reinterpret_cast<const double2*>(a + o) + c;
-          const double2 x = NC ? __ldg(s) : *s;
+          const double2 x = load_as<LDP>(reinterpret_cast<const double2*>(a + o) + c);
           r[2 * c + 0] = x.x, r[2 * c + 1] = x.y;
         }
       }
@@ -52,10 +64,7 @@ __device__ __forceinline__ Vec<T, VEC> ldv(const T* a, long long o, bool ok, boo
     }
   }
 #pragma unroll
-  for (int q = 0; q < VEC; ++q) {
-    const bool in = ok && jv + q < W;
-    r[q] = in ? (NC ? __ldg(a + o + q) : a[o + q]) : T(0);
-  }
+  for (int q = 0; q < VEC; ++q) r[q] = ld<T, LDP>(a, o + q, ok && jv + q < W);
   return r;
 }
 
