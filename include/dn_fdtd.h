@@ -208,7 +208,9 @@ int32_t dn_fdtd3d_adjoint(const dn_grid* g, void* const la[6], void* const lb[6]
  * 2K, ... < n_steps) are [slot-1][3][H*pitch]; the curl record of one segment
  * is [K][ncurl][H*pitch] (TM: Ez; TE: Ex, Ey); adjoint sets likewise, the
  * gradient of the final field goes into lam[n_steps % 2] before the backward
- * launch, the result accumulates into grad (FP64 [H*pitch]). */
+ * launch, the result accumulates into grad (FP64 [H*pitch]).  Rows move in
+ * 16-byte chunks: pitch * element size (and pitch * 8, for grad) must be a
+ * multiple of 16 bytes and every array 16-byte aligned (DN_EINVAL otherwise). */
 typedef struct {
   int32_t H, W;
   int64_t pitch;
@@ -238,7 +240,8 @@ typedef struct {
   int32_t dtype;      /* DN_F32 / DN_F64 */
   int32_t n_inst;
   int32_t K;          /* checkpoint interval in steps (>= 1) */
-  int32_t tile_rows;  /* 8, 16 or 32 (tile = tile_rows x 32 cells) */
+  int32_t tile_rows;  /* 8, 16 or 32 (tile = tile_rows x 128 cells in FP32, x 64 in FP64;
+                         each of its 8 warps marches tile_rows / 8 rows) */
   int32_t max_ctas;   /* upper bound on the persistent grid (0: as many as fit) */
 } dn_batch2d;
 
