@@ -176,10 +176,10 @@ struct Sets {
 // (TM) or below (TE) its own).  Fields go through L2 only (other CTAs wrote
 // them the step before); zero_in: the input is the all-zero state.
 // ---------------------------------------------------------------------------
-template <typename T, int POL, int VEC>
+template <typename T, int POL, int VEC, bool RECORD, bool MONITORS>
 __device__ void fwd_strip(const dn_batch2d_inst& I, int j0, int ia, int ib, int n,
                           const Sets<T> in, bool zero_in, const Sets<T> out, const Sets<T> ckpt,
-                          bool save, const Sets<T> curl, bool record, bool monitors) {
+                          bool save, const Sets<T> curl) {
   using V = Vec<T, VEC>;
   const int lane = threadIdx.x & 31;
   const int H = I.H, W = I.W;
@@ -217,7 +217,7 @@ __device__ void fwd_strip(const dn_batch2d_inst& I, int j0, int ia, int ib, int 
       for (int q = 0; q < VEC; ++q)
         if (jv + q < W && in_box(I.src_box, i, jv + q)) v[q] += w;
     }
-    if (monitors && I.mon_comp >= 0 && i >= I.mon_box.lo[1] && i < I.mon_box.hi[1]) {
+    if (MONITORS && I.mon_comp >= 0 && i >= I.mon_box.lo[1] && i < I.mon_box.hi[1]) {
       // all accumulators of a frequency are loaded before any is stored
       const long long ncell = (long long)(I.mon_box.hi[1] - I.mon_box.lo[1]) *
                               (I.mon_box.hi[2] - I.mon_box.lo[2]);
@@ -255,7 +255,7 @@ __device__ void fwd_strip(const dn_batch2d_inst& I, int j0, int ia, int ib, int 
       stv(ckpt.p[1], o, a, full, jv, W);
       stv(ckpt.p[2], o, b, full, jv, W);
     }
-    if (record) {
+    if (RECORD) {
       stv(curl.p[0], o, c0, full, jv, W);
       if (POL == DN_TE) stv(curl.p[1], o, c1, full, jv, W);
     }
@@ -678,8 +678,8 @@ __global__ void __launch_bounds__(NTB, 2) k_batch2d_fwd(unsigned char* table, in
       Sets<T> ck{{nullptr, nullptr, nullptr}};
       const bool save = I.ckpt != nullptr && K > 0 && (n + 1) % K == 0 && (n + 1) < I.n_steps;
       if (save) ck = slot_set<T>(I.ckpt, (n + 1) / K - 1, (long long)I.H * I.pitch, 3);
-      fwd_strip<T, POL, VEC>(I, st.j0, st.ia, st.ib, n, in, false, out, ck, save, ck, false,
-                             true);
+      fwd_strip<T, POL, VEC, false, true>(I, st.j0, st.ia, st.ib, n, in, false, out, ck, save,
+                                          ck);
     }
     if (!grid_sync(v.h->bar, gen, status)) return;
   }
@@ -711,8 +711,8 @@ __global__ void __launch_bounds__(NTB, 2) k_batch2d_bwd(unsigned char* table, in
                                    : field_set<T>(I.f[n & 1]);
         const Sets<T> out = field_set<T>(I.f[(n + 1) & 1]);
         const Sets<T> cr = slot_set<T>(I.curl, n - ta, fe, NCURL);
-        fwd_strip<T, POL, VEC>(I, st.j0, st.ia, st.ib, n, in, zero_in, out, out, false, cr, true,
-                               false);
+        fwd_strip<T, POL, VEC, true, false>(I, st.j0, st.ia, st.ib, n, in, zero_in, out, out,
+                                            false, cr);
       }
       if (!grid_sync(v.h->bar, gen, status)) return;
     }
