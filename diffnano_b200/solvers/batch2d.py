@@ -63,14 +63,18 @@ class _Inst:
     """Device buffers of one instance."""
 
     def __init__(self, spec: BatchInstance, pol: int, dtype, dev, K: int, grad: bool,
-                 shared: dict | None = None):
+                 shared: dict | None = None, views: tuple | None = None):
         H, W = spec.grid_shape
         self.spec, self.H, self.W = spec, H, W
         self.Wp = padded_width(W)
         kw = dict(dtype=dtype, device=dev)
         T = spec.n_steps
-        self.f = torch.zeros((2, 3, H, self.Wp), **kw)
-        self.ce = torch.zeros((H, self.Wp), **kw)
+        # views = (f, ce, acc): slices of batch-wide tensors (uniform batches)
+        if views is not None:
+            self.f, self.ce = views[0], views[1]
+        else:
+            self.f = torch.zeros((2, 3, H, self.Wp), **kw)
+            self.ce = torch.zeros((H, self.Wp), **kw)
         # read-only tables, shared by instances with the same set-up
         key = json.dumps([H, W, T, spec.pml_layers, spec.dl, spec.dt, spec.omega, str(dtype),
                           spec.source, spec.monitor], sort_keys=True, default=str)
@@ -94,7 +98,8 @@ class _Inst:
             self.mon_shape = tuple(b - a for a, b in box[1:])
             cells = self.mon_shape[0] * self.mon_shape[1]
             self.phase = phase
-            self.acc = torch.zeros((self.nf, cells, 2), dtype=F64, device=dev)
+            self.acc = views[2] if views is not None else \
+                torch.zeros((self.nf, cells, 2), dtype=F64, device=dev)
         self.grad_enabled = grad
         nck = max(0, math.ceil(T / K) - 1)
         self.ckpt = torch.zeros((max(1, nck), 3, H, self.Wp), **kw) if grad else None
@@ -177,6 +182,7 @@ class FDTDBatch2D:
         self.K = int(checkpoint_interval or max(1, math.ceil(math.sqrt(T))))
         self.tile_rows = tile_rows
         self._insts = None
+        self._stack = None
         self._grad_alloc = None
         self._graph = None
         self.status = torch.zeros(1, dtype=torch.int32, device=self.device)
@@ -195,18 +201,52 @@ class FDTDBatch2D:
         if self._insts is not None and self._grad_alloc == grad:
             return
         shared: dict = {}
-        self._insts = [_Inst(s, self.pol, self.dtype, self.device, self.K, grad, shared)
-                       for s in self.specs]
+        views = self._stacked_views()
+        self._insts = [_Inst(s, self.pol, self.dtype, self.device, self.K, grad, shared,
+                             None if views is None else views[n])
+                       for n, s in enumerate(self.specs)]
         self._grad_alloc = grad
         self._graph = None
         if self.tile_rows is None:
             self.tile_rows = autotune_tile_rows(self)
         self._pack()
 
+    def _stacked_views(self):
+        """Uniform batches (every instance with the same grid, step count, time
+        step, wavelength and monitor) keep fields, coefficients and monitor
+        sums in three batch-wide tensors, so that eps upload, reset and outputs
+        are one tensor operation each instead of one per instance; returns the
+        per-instance views, or None."""
+        self._stack = None
+        s0 = self.specs[0]
+
+        def key(sp):
+            return json.dumps([list(sp.grid_shape), sp.n_steps, sp.dt, sp.wavelength_nm,
+                               sp.monitor], sort_keys=True, default=str)
+
+        k0 = key(s0)
+        if len(self.specs) < 2 or any(key(sp) != k0 for sp in self.specs[1:]):
+            return None
+        n = len(self.specs)
+        H, W = s0.grid_shape
+        Wp = padded_width(W)
+        kw = dict(dtype=self.dtype, device=self.device)
+        f = torch.zeros((n, 2, 3, H, Wp), **kw)
+        ce = torch.zeros((n, H, Wp), **kw)
+        acc = None
+        if s0.monitor is not None:
+            box = _setup.monitor_box(s0.monitor, (1, H, W), False)
+            nf = len(s0.monitor.get("wavelengths_nm", [s0.wavelength_nm]))
+            cells = (box[1][1] - box[1][0]) * (box[2][1] - box[2][0])
+            acc = torch.zeros((n, nf, cells, 2), dtype=F64, device=self.device)
+        self._stack = (f, ce, acc)
+        return [(f[b], ce[b], None if acc is None else acc[b]) for b in range(n)]
+
     def _pack(self):
         L = _lib.lib()
         arr = (_lib.DnBatch2dInst * len(self._insts))(*[i.struct(self.pol) for i in self._insts])
-        tiles = sum(((i.W + 31) // 32) * ((i.H + self.tile_rows - 1) // self.tile_rows)
+        cols = 128 if self.dtype == torch.float32 else 64  # tile width: 32 lanes x 16 bytes
+        tiles = sum(((i.W + cols - 1) // cols) * ((i.H + self.tile_rows - 1) // self.tile_rows)
                     for i in self._insts)
         self.cfg = self._cfg(self.tile_rows, len(self._insts), tiles)
         smem = ctypes.c_int64(0)
@@ -241,12 +281,26 @@ class FDTDBatch2D:
         _lib.check(fn, rc)
 
     def _reset(self):
+        if self._stack is not None:
+            self._stack[0].zero_()
+            if self._stack[2] is not None:
+                self._stack[2].zero_()
+            return
         for i in self._insts:
             i.f.zero_()
             if i.acc is not None:
                 i.acc.zero_()
 
     def _set_eps(self, eps_list):
+        if self._stack is not None:
+            i0, n = self._insts[0], len(self._insts)
+            eps = eps_list if isinstance(eps_list, torch.Tensor) else \
+                torch.stack([e.detach().to(self.device, F64) for e in eps_list])
+            if eps.shape[0] != n or tuple(eps.shape[-2:]) != (i0.H, i0.W):
+                raise ValueError(f"eps shape {tuple(eps.shape)} != {n} grids {(i0.H, i0.W)}")
+            eps = eps.detach().to(self.device, F64).reshape(n, i0.H, i0.W)
+            self._stack[1][:, :, : i0.W] = (i0.spec.dt / eps).to(self.dtype)
+            return
         for i, e in zip(self._insts, eps_list):
             if tuple(e.shape[-2:]) != (i.H, i.W):
                 raise ValueError(f"eps shape {tuple(e.shape)} != grid {(i.H, i.W)}")
@@ -261,6 +315,14 @@ class FDTDBatch2D:
         return self._outputs()
 
     def _outputs(self):
+        if self._stack is not None:
+            i0, n = self._insts[0], len(self._insts)
+            fields = list(self._stack[0][:, i0.spec.n_steps % 2, 0, :, : i0.W].clone().unbind(0))
+            dfts = [None] * n
+            if self._stack[2] is not None:
+                d = torch.view_as_complex(self._stack[2]).reshape(n, i0.nf, *i0.mon_shape)
+                dfts = list(d.clone().unbind(0))
+            return fields, dfts
         fields, dfts = [], []
         for i in self._insts:
             fields.append(i.f[i.spec.n_steps % 2, 0, :, : i.W].clone())

@@ -188,3 +188,35 @@ def test_grid_barrier_wait_runs_out_and_reports_timeout(cuda):
     b.check_status()
     for x, y in zip(before, after):
         assert torch.equal(x, y)
+
+
+@pytest.mark.parametrize("pol", ["TM", "TE"])
+def test_uniform_batch_keeps_batch_wide_storage_and_matches_single_grids(cuda, pol):
+    """Instances with one grid, step count, time step and monitor share
+    batch-wide field / coefficient / monitor tensors (one-op upload, reset
+    and outputs); fields, DFTs and gradients still match single-grid solves."""
+    shape = (44, 40)
+    spec = BatchInstance(grid_shape=shape, n_steps=50, dl=20.0, wavelength_nm=1550.0,
+                         pml_layers=4, courant=0.5,
+                         source={"type": "gaussian_pulse", "row": 6, "spread": 300.0,
+                                 "t0": 900.0},
+                         monitor={"row": 36, "wavelengths_nm": [1500.0, 1600.0]})
+    specs = [spec] * 4
+    gen = torch.Generator().manual_seed(9)
+    eps0 = [1.5 + 2.0 * torch.rand(*shape, dtype=torch.float64, generator=gen) for _ in specs]
+    G = [torch.randn(*shape, dtype=torch.float64, generator=gen) for _ in specs]
+    b = FDTDBatch2D(specs, pol, torch.float64, cuda, checkpoint_interval=7, tile_rows=16,
+                    cluster=False)
+    eps = [e.clone().to(cuda).requires_grad_(True) for e in eps0]
+    fields, dfts = b.forward(eps)
+    assert b._stack is not None
+    loss = sum((f * g.to(cuda)).sum() + (d.abs() ** 2).sum() for f, g, d in zip(fields, G, dfts))
+    loss.backward()
+    for e0, e, f, d, g in zip(eps0, eps, fields, dfts, G):
+        ref = e0.clone().to(cuda).requires_grad_(True)
+        r = _single(spec, pol, torch.float64, cuda, ref)
+        assert rel_l2(f, r.field[0]) < 1e-12
+        dr = r.metadata["monitors"][0]["dft"]
+        assert rel_l2(torch.view_as_real(d), torch.view_as_real(dr)) < 1e-11
+        ((r.field[0] * g.to(cuda)).sum() + (dr.abs() ** 2).sum()).backward()
+        assert rel_l2(e.grad, ref.grad) < 1e-9
