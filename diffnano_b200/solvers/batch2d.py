@@ -16,7 +16,12 @@ line/point/box monitor on its injected field.
 CUDA graph and replays it when the same batch is solved repeatedly (design
 iterations).  The tile height is
 chosen by ``autotune_tile_rows`` (measured, cached per device and batch
-signature).
+signature).  Gradient-free solves of grids that fit a thread-block cluster's
+shared memory run one cluster per grid (``dn_batch2d_forward_cluster``) unless
+``cluster=False``; large batches stream faster through the persistent kernel.
+Batches of identical grids (same shape, steps, time step, wavelength and
+monitor) keep their fields, coefficients and monitor sums in batch-wide
+tensors, so eps upload, reset and outputs are one tensor operation each.
 """
 
 from __future__ import annotations
