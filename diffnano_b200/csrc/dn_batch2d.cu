@@ -150,11 +150,6 @@ __global__ void k_barrier_selftest(unsigned int* bar, int* status, unsigned int 
     if (!grid_sync_n(bar, gen, status, gridDim.x + missing, spin_limit)) return;
 }
 
-template <typename T>
-__device__ __forceinline__ T ld(const T* p) {
-  return __ldcg(p);
-}
-
 __device__ __forceinline__ bool in_box(const dn_box& b, int i, int j) {
   return i >= b.lo[1] && i < b.hi[1] && j >= b.lo[2] && j < b.hi[2];
 }
