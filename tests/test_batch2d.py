@@ -57,13 +57,16 @@ def test_batched_forward_matches_single_grids(cuda, pol, rows):
         assert rel_l2(torch.view_as_real(d), torch.view_as_real(r.metadata["monitors"][0]["dft"])) < 1e-6
 
 
+@pytest.mark.parametrize("rows", [8, 16, 32])
 @pytest.mark.parametrize("pol", ["TM", "TE"])
-def test_batched_gradients_match_single_grids(cuda, pol):
+def test_batched_gradients_match_single_grids(cuda, pol, rows):
+    """Every tile height: 1, 2 or 4 rows per warp (a one-row warp owns no
+    neighbouring row of its reverse sweep)."""
     specs = _specs(pol)
     eps0 = _eps(2)
     gen = torch.Generator().manual_seed(3)
     G = [torch.randn(*s, dtype=torch.float64, generator=gen) for s in SHAPES]
-    b = FDTDBatch2D(specs, pol, torch.float64, cuda, checkpoint_interval=7, tile_rows=16)
+    b = FDTDBatch2D(specs, pol, torch.float64, cuda, checkpoint_interval=7, tile_rows=rows)
     eps = [e.clone().to(cuda).requires_grad_(True) for e in eps0]
     fields, dfts = b.forward(eps)
     loss = sum((f * g.to(cuda)).sum() + (d.abs() ** 2).sum() for f, g, d in zip(fields, G, dfts))
