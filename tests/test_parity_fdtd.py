@@ -222,6 +222,45 @@ def test_2d_unaligned_rows_match_padded_rows(cuda, pol, dtype):
         assert rel_l2(res[c], ref) < tol
 
 
+@pytest.mark.parametrize("pol", ["TM", "TE"])
+def test_2d_large_grid_vs_oracle(cuda, pol):
+    """1024^2: the per-step kernel marches 4 rows per warp here (the smaller
+    grids of the other tests march 2).  FP32 against the FP64 oracle."""
+    n, T = 1024, 30
+    g = torch.Generator().manual_seed(5)
+    eps = 1.5 + 2.0 * torch.rand(n, n, dtype=torch.float64, generator=g)
+    src = {"type": "gaussian_pulse", "row": 30, "t0": 40.0, "spread": 20.0}
+    o = R.run_2d(eps, dl=20.0, dt=DT2(0.5, 20.0), omega=OMEGA, pml_layers=20, polarization=pol,
+                 n_steps=T, source=dict(src))
+    s = dn.FDTDSolver2D(grid_shape=(n, n), polarization=pol, pml_layers=20, n_steps=T,
+                        dl=20.0, courant=0.5, device=cuda, dtype=torch.float32)
+    # a probe keeps the solve on the per-step kernel (no cluster-resident path)
+    r = s.forward(eps.to(cuda), source=dict(src, probe=[n // 2, n // 2]))
+    comp = "Ez" if pol == "TM" else "Hz"
+    assert float(o[comp].abs().max()) > 0
+    assert rel_l2(r.field[0], o[comp]) < 1e-5
+
+
+def test_2d_large_grid_gradient_vs_oracle(cuda):
+    """1024^2 TM gradient (forward with curl record, 4-row warp marches in both
+    directions) against the oracle's autograd, FP64."""
+    n, T = 1024, 20
+    g = torch.Generator().manual_seed(6)
+    eps0 = 1.5 + 2.0 * torch.rand(n, n, dtype=torch.float64, generator=g)
+    src = {"type": "gaussian_pulse", "row": 30, "t0": 40.0, "spread": 20.0}
+    e = eps0.clone().requires_grad_(True)
+    o = R.run_2d(e, dl=20.0, dt=DT2(0.5, 20.0), omega=OMEGA, pml_layers=20, n_steps=T,
+                 source=dict(src))
+    (o["Ez"] * o["Ez"]).sum().backward()
+    s = dn.FDTDSolver2D(grid_shape=(n, n), pml_layers=20, n_steps=T, dl=20.0, courant=0.5,
+                        device=cuda, dtype=torch.float64)
+    eps = eps0.clone().to(cuda).requires_grad_(True)
+    r = s.forward(eps, source=dict(src))
+    (r.field[0] * r.field[0]).sum().backward()
+    assert float(e.grad.norm()) > 0
+    assert rel_l2(eps.grad, e.grad) < 1e-9
+
+
 def test_deterministic(cuda):
     shape = (32, 32, 32)
     eps = _seeded(shape, 6).to(cuda)
