@@ -11,9 +11,9 @@ validation), and DFT ``monitors``.
 from __future__ import annotations
 
 import json
-
 import math
 from collections.abc import Sequence
+from types import SimpleNamespace
 
 import torch
 
@@ -117,15 +117,21 @@ class FDTDSolver2D:
         eps = self._prep_eps(geometry)
         mons = monitors if monitors is not None else self.monitors
         probe = src.get("probe", None)
-        eng = self._make_engine(self.n_steps, src, mons, probe)
-        fast = None
+        fast, eng, specs = None, None, None
         if probe is None and not (torch.is_grad_enabled() and eps.requires_grad):
-            fast = self._cluster_solve(eps, src, eng)
+            # the cluster-resident path needs only the parsed monitors, not a
+            # per-step engine (field sets, tables and uploads on every call)
+            H, W = self.grid_shape
+            specs = parse_monitors(mons, (1, H, W), False, self.wavelength_nm,
+                                   self._fields()[0], self._fields())
+            fast = self._cluster_solve(eps, src, specs)
         if fast is not None:
             field, dfts = fast
         else:
             from diffnano_b200.solvers._adjoint import run_forward
 
+            eng = self._make_engine(self.n_steps, src, mons, probe)
+            specs = eng.monitors
             field, dfts = run_forward(self, eng, eps, self._fields()[0])
         out_dev = self._device
         snapshots = []
@@ -133,21 +139,23 @@ class FDTDSolver2D:
             snapshots = list(eng.probe_out.to(out_dev).unbind(0))
         meta = {"polarization": self.polarization, "n_steps": self.n_steps, "dt": self.dt,
                 "courant": self.courant, "snapshots": snapshots}
-        if eng.monitors:
-            meta["monitors"] = monitor_metadata(eng, [to_result_device(d, out_dev) for d in dfts])
+        if specs:
+            meta["monitors"] = monitor_metadata(SimpleNamespace(monitors=specs),
+                                                [to_result_device(d, out_dev) for d in dfts])
         return SimResult(field=to_result_device(field.unsqueeze(0), out_dev), wavelengths=wl,
                          metadata=meta)
 
-    def _cluster_solve(self, eps, src, eng):
+    def _cluster_solve(self, eps, src, specs):
         """Gradient-free solve with the whole grid in one thread-block cluster
         (``dn_batch2d_forward_cluster``) when the grid fits and there is at most
-        one monitor, on the injected field; None otherwise."""
-        if len(eng.monitors) > 1:
+        one monitor (``specs``: the parsed monitors), on the injected field;
+        None otherwise."""
+        if len(specs) > 1:
             return None
         comp = _lib.DN_EZ if self.polarization == "TM" else _lib.DN_HZ
         mon = None
-        if eng.monitors:
-            m = eng.monitors[0]
+        if specs:
+            m = specs[0]
             if m.component != comp:
                 return None
             mon = {"box": [list(m.box[1]), list(m.box[2])], "wavelengths_nm": list(m.wavelengths)}
