@@ -130,13 +130,14 @@ class FDTDSolver2D:
         else:
             from diffnano_b200.solvers._adjoint import run_forward
 
-            eng = self._make_engine(self.n_steps, src, mons, probe)
+            needs_grad = torch.is_grad_enabled() and eps.requires_grad
+            eng = self._engine_for(src, mons, probe, reuse=not needs_grad)
             specs = eng.monitors
             field, dfts = run_forward(self, eng, eps, self._fields()[0])
         out_dev = self._device
         snapshots = []
         if probe is not None:
-            snapshots = list(eng.probe_out.to(out_dev).unbind(0))
+            snapshots = list(eng.probe_out.to(out_dev, copy=True).unbind(0))
         meta = {"polarization": self.polarization, "n_steps": self.n_steps, "dt": self.dt,
                 "courant": self.courant, "snapshots": snapshots}
         if specs:
@@ -144,6 +145,30 @@ class FDTDSolver2D:
                                                 [to_result_device(d, out_dev) for d in dfts])
         return SimResult(field=to_result_device(field.unsqueeze(0), out_dev), wavelengths=wl,
                          metadata=meta)
+
+    def _engine_for(self, src: dict, mons, probe, reuse: bool) -> Engine:
+        """The per-step engine of a solve.  Gradient-free calls reuse one per
+        set-up (every run resets its fields and writes eps, and the results
+        are copies), which saves the field allocations and table uploads of a
+        new engine; calls that autograd differentiates get a fresh one, since
+        the backward pass replays from it.  Set-ups that are not plain JSON
+        (tensors in the source or monitor dicts) are not cached."""
+        if not reuse:
+            return self._make_engine(self.n_steps, src, mons, probe)
+        try:
+            key = json.dumps([src, mons, probe, self.n_steps, str(self.dtype),
+                              list(self.grid_shape), self.dl, self.wavelength_nm,
+                              self.pml_layers, self.courant, self.polarization,
+                              str(self._device)], sort_keys=True)
+        except TypeError:
+            return self._make_engine(self.n_steps, src, mons, probe)
+        cache = self.__dict__.setdefault("_engine_cache", {})
+        eng = cache.get(key)
+        if eng is None:
+            if len(cache) >= 4:
+                cache.clear()
+            eng = cache[key] = self._make_engine(self.n_steps, src, mons, probe)
+        return eng
 
     def _cluster_solve(self, eps, src, specs):
         """Gradient-free solve with the whole grid in one thread-block cluster

@@ -261,6 +261,32 @@ def test_2d_large_grid_gradient_vs_oracle(cuda):
     assert rel_l2(eps.grad, e.grad) < 1e-9
 
 
+def test_2d_engine_reuse_keeps_results_independent(cuda):
+    """Gradient-free per-step solves reuse one engine per set-up: results of
+    earlier calls (field, probe snapshots, DFTs) stay as they were, and the
+    same input gives the same output again."""
+    n = 96
+    g = torch.Generator().manual_seed(8)
+    e1 = (1.5 + 2.0 * torch.rand(n, n, dtype=torch.float64, generator=g)).to(cuda)
+    e2 = (1.5 + 2.0 * torch.rand(n, n, dtype=torch.float64, generator=g)).to(cuda)
+    src = {"type": "gaussian_pulse", "row": 10, "probe": [60, 40]}
+    mons = [{"component": "Ez", "row": 70, "wavelengths_nm": [1500.0, 1600.0]}]
+    s = dn.FDTDSolver2D(grid_shape=(n, n), pml_layers=6, n_steps=120, device=cuda,
+                        monitors=mons)
+    r1 = s.forward(e1, source=dict(src))
+    f1 = r1.field.clone()
+    p1 = torch.stack(r1.metadata["snapshots"]).clone()
+    d1 = r1.metadata["monitors"][0]["dft"].clone()
+    r2 = s.forward(e2, source=dict(src))
+    r3 = s.forward(e1, source=dict(src))
+    assert len(s.__dict__.get("_engine_cache", {})) == 1
+    assert not torch.equal(r2.field, f1)
+    assert torch.equal(r1.field, f1) and torch.equal(torch.stack(r1.metadata["snapshots"]), p1)
+    assert torch.equal(r1.metadata["monitors"][0]["dft"], d1)
+    assert torch.equal(r3.field, f1) and torch.equal(torch.stack(r3.metadata["snapshots"]), p1)
+    assert torch.equal(r3.metadata["monitors"][0]["dft"], d1)
+
+
 def test_deterministic(cuda):
     shape = (32, 32, 32)
     eps = _seeded(shape, 6).to(cuda)
