@@ -4,6 +4,7 @@ reference's golden outputs."""
 
 from __future__ import annotations
 
+import json
 import math
 
 import numpy as np
@@ -108,3 +109,32 @@ def test_checkpoint_interval():
     assert checkpoint_interval(4000, False, 4) == 64
     assert checkpoint_interval(10, True, 2) == 5
     assert checkpoint_interval(1, False, 4) == 1
+
+
+def test_2d_engine_reuse_decisions():
+    """FDTDSolver2D._engine_for on the host (engine construction stubbed):
+    one engine per gradient-free set-up, reused; a fresh one per gradient
+    call; no caching of set-ups that are not plain JSON; at most four kept."""
+    s = dn.FDTDSolver2D(grid_shape=(16, 16), n_steps=5)
+    made = []
+
+    def fake(n_steps, src, mons, probe=None):
+        made.append((n_steps, json.dumps(src, default=str), probe))
+        return object()
+
+    s._make_engine = fake
+    src_a = {"type": "gaussian_pulse", "row": 3}
+    src_b = {"type": "gaussian_pulse", "row": 4}
+    e1 = s._engine_for(src_a, None, None, reuse=True)
+    assert s._engine_for(dict(src_a), None, None, reuse=True) is e1
+    assert s._engine_for(src_b, None, None, reuse=True) is not e1
+    assert s._engine_for(src_a, None, None, reuse=False) is not e1  # gradient call
+    assert len(made) == 3
+    # a tensor in the source dict: built every time, never cached
+    src_t = {"type": "gaussian_pulse", "row": 3, "amplitude": torch.tensor(2.0)}
+    assert s._engine_for(src_t, None, None, reuse=True) is not s._engine_for(src_t, None, None,
+                                                                               reuse=True)
+    assert len(s._engine_cache) == 2
+    for r in range(5, 9):
+        s._engine_for({"type": "gaussian_pulse", "row": r}, None, None, reuse=True)
+    assert len(s._engine_cache) <= 4
