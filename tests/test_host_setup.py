@@ -138,3 +138,35 @@ def test_2d_engine_reuse_decisions():
     for r in range(5, 9):
         s._engine_for({"type": "gaussian_pulse", "row": r}, None, None, reuse=True)
     assert len(s._engine_cache) <= 4
+
+
+def test_batch_wide_storage_decision():
+    """FDTDBatch2D._stacked_views on the host (CPU tensors): identical
+    instances get views of one batch-wide tensor per array; any difference
+    in grid, steps or monitor keeps per-instance storage."""
+    from diffnano_b200.solvers.batch2d import BatchInstance, FDTDBatch2D
+
+    def spec(shape=(20, 24), T=30, mon=True):
+        return BatchInstance(grid_shape=shape, n_steps=T, dl=20.0, pml_layers=4, courant=0.5,
+                             source={"type": "gaussian_pulse", "row": 5},
+                             monitor={"row": 12, "wavelengths_nm": [1500.0, 1600.0]} if mon
+                             else None)
+
+    def views(specs):
+        b = FDTDBatch2D.__new__(FDTDBatch2D)
+        b.specs, b.dtype, b.device = specs, torch.float32, torch.device("cpu")
+        return b, b._stacked_views()
+
+    b, v = views([spec()] * 3)
+    assert v is not None and len(v) == 3
+    f, ce, acc = b._stack
+    assert f.shape == (3, 2, 3, 20, 32) and ce.shape == (3, 20, 32) and acc.shape == (3, 2, 24, 2)
+    assert v[1][0].data_ptr() == f.data_ptr() + f[0].numel() * f.element_size()
+    assert v[2][2].shape == (2, 24, 2)
+    for other in (spec(shape=(20, 28)), spec(T=31), spec(mon=False)):
+        b, v = views([spec(), spec(), other])
+        assert v is None and b._stack is None
+    b, v = views([spec(mon=False)] * 2)
+    assert v is not None and b._stack[2] is None and v[0][2] is None
+    b, v = views([spec()])
+    assert v is None
