@@ -160,3 +160,28 @@ def test_barrier_selftest_rejects_bad_arguments_before_any_launch(bad):
     rc = L.dn_batch2d_barrier_selftest(a["n_ctas"], a["missing"], a["spin_limit"], a["rounds"],
                                        a["bar"], a["status"], None)
     assert rc == _lib.DN_EINVAL
+
+
+def test_batch2d_requires_16_byte_rows_and_arrays():
+    """The batched kernels move rows in 16-byte chunks: an instance whose
+    pitch or arrays are not 16-byte aligned is refused before any launch
+    (the pointers are only checked, never dereferenced, here)."""
+    L = _lib.lib()
+    cfg = _lib.DnBatch2d(pol=_lib.DN_TM, dtype=_lib.DN_F32, n_inst=1, K=8, tile_rows=16)
+
+    def inst(pitch=40, ce=0x10000):
+        a = (_lib.DnBatch2dInst * 1)()
+        i = a[0]
+        i.H, i.W, i.pitch, i.n_steps = 20, 37, pitch, 10
+        i.src_comp = i.mon_comp = _lib.DN_NONE
+        i.dt, i.dl = 1.0, 20.0
+        i.ce = ce
+        for k in range(2):
+            i.b[k], i.c[k] = 0x20000 + 0x100 * k, 0x30000 + 0x100 * k
+            for c in range(3):
+                i.f[k][c] = 0x40000 + 0x1000 * (3 * k + c)
+        return a
+
+    assert L.dn_batch2d_table_bytes(ctypes.byref(cfg), inst()) > 0
+    assert L.dn_batch2d_table_bytes(ctypes.byref(cfg), inst(pitch=37)) == -1  # 148-byte rows
+    assert L.dn_batch2d_table_bytes(ctypes.byref(cfg), inst(ce=0x10004)) == -1  # misaligned
