@@ -29,6 +29,7 @@
 // intermediate row above (TM: vy) or below (TE: lambda_E', uy) its own, with
 // the owner's arithmetic: no shared memory, no barrier; ping-pong buffers.
 #include <algorithm>
+#include <atomic>
 
 #include "dn_adjoint.cuh"
 #include "dn_strip.cuh"
@@ -391,20 +392,24 @@ namespace {
 // per SM (the recomputed row costs a warp about three rows of loads), else 2.
 template <typename T, int POL, int VEC>
 int adj_rows_per_warp(int H, int strips, int* R) {
-  static int per_sm = 0, nsm = 0;  // per kernel instance; identical on every B200
-  if (per_sm == 0) {
+  // per kernel instance, identical on every B200; atomics so that concurrent
+  // host threads may fill them (the SM count is published before the
+  // per-SM count that readers test)
+  static std::atomic<int> per_sm{0}, nsm{0};
+  if (per_sm.load(std::memory_order_acquire) == 0) {
     int dev = 0, n = 0, b = 0;
     DN_CUDA_CHECK(cudaGetDevice(&dev));
     DN_CUDA_CHECK(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
     DN_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_adj2d<T, POL, VEC>, NTA, 0));
-    nsm = n;
-    per_sm = std::max(b, 1);
+    nsm.store(n, std::memory_order_relaxed);
+    per_sm.store(std::max(b, 1), std::memory_order_release);
   }
-  const long long slots = (long long)nsm * per_sm;
+  const int q = per_sm.load(std::memory_order_acquire);
+  const long long slots = (long long)nsm.load(std::memory_order_relaxed) * q;
   const long long row_ctas = std::max<long long>(1, slots / strips);
   const long long r = (H + WARPS_A * row_ctas - 1) / (WARPS_A * row_ctas);
   const long long warps4 = (long long)strips * ((H + 3) / 4);
-  const long long r_min = warps4 >= 8LL * nsm ? 4 : 2;
+  const long long r_min = warps4 >= 8LL * nsm.load(std::memory_order_relaxed) ? 4 : 2;
   *R = static_cast<int>(std::max<long long>(r_min, r));
   return DN_OK;
 }

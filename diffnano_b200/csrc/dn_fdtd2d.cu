@@ -31,6 +31,7 @@
 // grid fits one wave of resident CTAs (3 per SM), with a floor that keeps the
 // recomputed rows a small share of a warp's loads.
 #include <algorithm>
+#include <atomic>
 
 #include "dn_host.cuh"
 #include "dn_strip.cuh"
@@ -362,21 +363,25 @@ __global__ void __launch_bounds__(NT2, 3) k_fdtd2d_step(const StepParams<T> p, c
 // per SM, then at least 2.
 template <typename T, int POL, bool REC, int VEC>
 int rows_per_warp(int H, int strips, int* R) {
-  static int per_sm = 0, nsm = 0;  // per kernel instance; identical on every B200
-  if (per_sm == 0) {
+  // per kernel instance, identical on every B200; atomics so that concurrent
+  // host threads may fill them (the SM count is published before the
+  // per-SM count that readers test)
+  static std::atomic<int> per_sm{0}, nsm{0};
+  if (per_sm.load(std::memory_order_acquire) == 0) {
     int dev = 0, n = 0, b = 0;
     DN_CUDA_CHECK(cudaGetDevice(&dev));
     DN_CUDA_CHECK(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
     DN_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
         &b, k_fdtd2d_step<T, POL, REC, VEC>, NT2, 0));
-    nsm = n;
-    per_sm = std::max(b, 1);
+    nsm.store(n, std::memory_order_relaxed);
+    per_sm.store(std::max(b, 1), std::memory_order_release);
   }
-  const long long slots = (long long)nsm * per_sm;
+  const int q = per_sm.load(std::memory_order_acquire);
+  const long long slots = (long long)nsm.load(std::memory_order_relaxed) * q;
   const long long row_ctas = std::max<long long>(1, slots / strips);
   const long long r = (H + WARPS2 * row_ctas - 1) / (WARPS2 * row_ctas);
   const long long warps4 = (long long)strips * ((H + 3) / 4);
-  const long long r_min = warps4 >= 8LL * nsm ? 4 : 2;
+  const long long r_min = warps4 >= 8LL * nsm.load(std::memory_order_relaxed) ? 4 : 2;
   *R = static_cast<int>(std::max<long long>(r_min, r));
   return DN_OK;
 }
