@@ -41,6 +41,7 @@
 // wait is bounded by the global timer; a wait that gives up raises an abort
 // flag that every role polls, reports DN_ETIMEOUT, lets copies and MMAs in
 // flight finish (again bounded) and frees TMEM before the CTA exits.
+#include <atomic>
 #include <cuda.h>
 #include <cuda_bf16.h>
 
@@ -823,8 +824,11 @@ int sm_count() {
 // co-resident two-CTA clusters of the pair kernel (0 when none fit)
 template <int BN>
 int pair_clusters() {
-  static int cached = -1;
-  if (cached >= 0) return cached;
+  // filled once; an atomic so that concurrent host threads may both fill it
+  // (same value, and the shared-memory attribute they set is idempotent)
+  static std::atomic<int> cached{-1};
+  const int c = cached.load(std::memory_order_acquire);
+  if (c >= 0) return c;
   using C = Cfg<BN, true>;
   auto kern = k_gemm<BN, true>;
   int n = 0;
@@ -844,7 +848,7 @@ int pair_clusters() {
     if (cudaOccupancyMaxActiveClusters(&n, kern, &cfg) != cudaSuccess) n = 0;
   }
   (void)cudaGetLastError();
-  cached = n;
+  cached.store(n, std::memory_order_release);
   return n;
 }
 
