@@ -45,16 +45,17 @@ class DnCpml(ctypes.Structure):
 
 
 class DnSource(ctypes.Structure):
-    _fields_ = [("component", c_int32), ("box", DnBox), ("wave", c_void_p)]
+    _fields_ = [("component", c_int32), ("box", DnBox), ("wave", c_void_p), ("n_t", c_int32)]
 
 
 class DnMonitor(ctypes.Structure):
     _fields_ = [("component", c_int32), ("box", DnBox), ("n_freq", c_int32),
-                ("phase", c_void_p), ("acc", c_void_p)]
+                ("phase", c_void_p), ("acc", c_void_p), ("n_t", c_int32)]
 
 
 class DnProbe(ctypes.Structure):
-    _fields_ = [("component", c_int32), ("pos", c_int32 * 3), ("out", c_void_p)]
+    _fields_ = [("component", c_int32), ("pos", c_int32 * 3), ("out", c_void_p),
+                ("n_t", c_int32)]
 
 
 class DnCurlRecord(ctypes.Structure):
@@ -103,11 +104,18 @@ class DnDensity(ctypes.Structure):
                 ("eps_lo", ctypes.c_float), ("eps_hi", ctypes.c_float)]
 
 
+class DnSpan(ctypes.Structure):
+    _fields_ = [("ptr", c_void_p), ("dtype", c_int32), ("rows", c_int64), ("cols", c_int64),
+                ("pitch", c_int64)]
+
+
+DN_MAX_SPANS = 32
+
 STRUCTS = {"dn_box": DnBox, "dn_grid": DnGrid, "dn_cpml": DnCpml, "dn_source": DnSource,
            "dn_monitor": DnMonitor, "dn_probe": DnProbe, "dn_curl_record": DnCurlRecord,
            "dn_batch2d_inst": DnBatch2dInst, "dn_batch2d": DnBatch2d,
            "dn_gemm_operand": DnGemmOperand, "dn_gemm": DnGemm,
-           "dn_density": DnDensity}
+           "dn_density": DnDensity, "dn_span": DnSpan}
 
 PTR6 = c_void_p * 6
 _P6 = ctypes.POINTER(c_void_p)  # a PTR6 instance (or None) is passed here
@@ -187,6 +195,7 @@ SIGNATURES = {
                             c_void_p]),
     "dn_morph3_backward": (c_int32, [c_void_p, c_void_p, c_int32, c_int32, c_int32, c_void_p,
                                      c_void_p]),
+    "dn_check_finite": (c_int32, [ctypes.POINTER(DnSpan), c_int32, c_void_p, c_void_p]),
     "dn_fdtd2d_run_noalloc": (c_int32, [ctypes.POINTER(DnGrid), _P6, c_void_p,
                                         ctypes.POINTER(DnCpml), ctypes.POINTER(DnSource),
                                         ctypes.POINTER(DnMonitor), c_int32,
@@ -237,6 +246,53 @@ def check(fn: str, status: int) -> None:
     if status == DN_EINVAL:
         raise ValueError(f"{fn}: {msg}")
     raise DNError(fn, status, msg)
+
+
+def spans(t) -> list:
+    """:class:`DnSpan` list covering a CUDA float32/float64 tensor.
+
+    A contiguous tensor is cut into rows of 1024 elements (plus one short
+    row for the remainder); any other tensor must have unit inner stride and
+    rows at a constant stride (e.g. a view that narrows the last dimension of
+    a padded field), and its rows are its last dimension."""
+    torch = _torch()
+    if t.dtype not in (torch.float32, torch.float64):
+        raise ValueError("spans: a float32 or float64 tensor is required")
+    dt = DN_F32 if t.dtype == torch.float32 else DN_F64
+    n = t.numel()
+    if t.is_contiguous():
+        out, full = [], n // 1024
+        if full:
+            out.append(DnSpan(ptr=t.data_ptr(), dtype=dt, rows=full, cols=1024, pitch=1024))
+        if n % 1024:
+            out.append(DnSpan(ptr=t.data_ptr() + full * 1024 * t.element_size(), dtype=dt,
+                              rows=1, cols=n % 1024, pitch=n % 1024))
+        return out
+    if t.stride(-1) != 1 or t.dim() < 2:
+        raise ValueError("spans: unit inner stride is required")
+    for d in range(t.dim() - 2):  # leading dimensions must fold into whole rows
+        if t.stride(d) != t.stride(d + 1) * t.shape[d + 1]:
+            raise ValueError("spans: leading dimensions are not a constant row stride")
+    cols = t.shape[-1]
+    return [DnSpan(ptr=t.data_ptr(), dtype=dt, rows=n // cols, cols=cols, pitch=t.stride(-2))]
+
+
+def check_finite(tensors, status, stream) -> None:
+    """Queue the non-finite watchdog (``dn_check_finite``) over CUDA tensors
+    on ``stream``; a NaN or Inf sets DN_ENONFINITE in the device word
+    ``status`` (read later by the caller's status check)."""
+    sp = [x for t in tensors if t is not None and t.numel() > 0 for x in spans(t)]
+    for i in range(0, len(sp), DN_MAX_SPANS):
+        chunk = sp[i:i + DN_MAX_SPANS]
+        arr = (DnSpan * len(chunk))(*chunk)
+        check("dn_check_finite",
+              lib().dn_check_finite(arr, len(chunk), status.data_ptr(), ctypes.c_void_p(stream)))
+
+
+def _torch():
+    import torch
+
+    return torch
 
 
 def box(lo, hi) -> DnBox:

@@ -81,7 +81,9 @@ class ExternalCrossValidator:
         g = torch.Generator().manual_seed(42)
         eps = 1.5 + 1.0 * torch.rand(D, H, W, dtype=torch.float64, generator=g)
         return {"grid_size": grid_size, "source_pos": source_pos, "freq": freq, "eps": eps,
-                "dl": 20.0, "wavelength_nm": 1550.0, "courant": 0.35, "seed": 42}
+                "source_config": {"type": "gaussian_pulse", "pos": list(source_pos),
+                                  "amplitude": 1.0},
+                "n_steps": 50, "dl": 20.0, "wavelength_nm": 1550.0, "courant": 0.35, "seed": 42}
 
     @staticmethod
     def load_external_results(path: str) -> Dict[str, Any]:

@@ -348,6 +348,7 @@ int adjoint3d(const dn_grid* g, void* const la[6], void* const lb[6], const void
   if (rc != DN_OK) return rc;
   if (!final_in_b || n_mon < 0 || n_mon > DN_MAX_MONITORS || (n_mon > 0 && !mons))
     return DN_EINVAL;
+  if (!mons_steps_ok(mons, n_mon, (int64_t)t_end - nsteps, t_end)) return DN_EINVAL;
   const void* ptrs[16];
   for (int c = 0; c < 6; ++c) {
     ptrs[c] = la[c];

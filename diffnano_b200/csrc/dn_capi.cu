@@ -44,6 +44,7 @@ extern "C" int64_t dn_struct_size(const char* name) {
       {"dn_gemm_operand", sizeof(dn_gemm_operand)},
       {"dn_gemm", sizeof(dn_gemm)},
       {"dn_density", sizeof(dn_density)},
+      {"dn_span", sizeof(dn_span)},
   };
   for (const Entry& e : table)
     if (std::strcmp(e.n, name) == 0) return e.s;

@@ -346,6 +346,7 @@ int run3d(const dn_grid* g, void* const fa[6], void* const fb[6], const void* ce
   int rc = build_params<T>(true, g, fa, fb, ce, cpml, src, mons, n_mon, probe, status, &p);
   if (rc != DN_OK) return rc;
   if (t0 < 0 || nsteps < 0 || !final_in_b) return DN_EINVAL;
+  if (!steps_ok(src, mons, n_mon, probe, t0, (int64_t)t0 + nsteps)) return DN_EINVAL;
   const void* ptrs[13];
   for (int c = 0; c < 6; ++c) {
     ptrs[c] = fa[c];

@@ -107,6 +107,26 @@ int build_params(bool is3d, const dn_grid* g, void* const fa[6], void* const fb[
   return DN_OK;
 }
 
+// The source waveform, the monitor phase tables and the probe output are
+// indexed by the absolute step and carry their length (n_t).  A run or a
+// reverse sweep over steps [t_lo, t_hi) may only touch rows below n_t; this is
+// checked before anything is queued, so a too-long call returns DN_EINVAL
+// instead of reading or writing past the caller's arrays.
+inline bool mons_steps_ok(const dn_monitor* mons, int32_t n_mon, int64_t t_lo, int64_t t_hi) {
+  if (t_lo < 0 || t_hi < t_lo) return false;
+  for (int m = 0; m < n_mon; ++m)
+    if (mons[m].n_t < 0 || t_hi > mons[m].n_t) return false;
+  return true;
+}
+
+inline bool steps_ok(const dn_source* src, const dn_monitor* mons, int32_t n_mon,
+                     const dn_probe* probe, int64_t t_lo, int64_t t_hi) {
+  if (!mons_steps_ok(mons, n_mon, t_lo, t_hi)) return false;
+  if (src && src->component != DN_NONE && t_hi > src->n_t) return false;
+  if (probe && probe->component != DN_NONE && t_hi > probe->n_t) return false;
+  return true;
+}
+
 template <typename T>
 void set_io(StepParams<T>* p, void* const from[6], void* const to[6]) {
   for (int c = 0; c < 6; ++c) {

@@ -19,6 +19,9 @@
 //  * The first call on a device looks up the array's device address with
 //    cudaGetSymbolAddress (with that device current) and caches it per
 //    device.  Make that first call before any stream capture on the device.
+//    The cached address belongs to that device's context: after
+//    cudaDeviceReset on the device it is stale, so this entry point must not
+//    be used on that device again in the same process.
 //  * Every call on a device shares the same array and it keeps the previous
 //    call's contents.  Nothing in it has to start at zero: each step writes
 //    every in-domain cell of the set it targets before the next step reads
@@ -81,6 +84,9 @@ extern "C" int32_t dn_fdtd2d_run_noalloc(const dn_grid* g, void* const f[6], con
   if (g->D != 1 || g->H < 1 || g->pitch_y < g->W || (g->pol != DN_TM && g->pol != DN_TE))
     return DN_EINVAL;
   const size_t es = g->dtype == DN_F32 ? 4 : 8;
+  // bound the pitch before multiplying, so that H * pitch_y * es cannot wrap
+  if ((uint64_t)g->pitch_y > (uint64_t)DN_NOALLOC_MAX_BYTES / (3 * es * (size_t)g->H))
+    return DN_ENOMEM;
   // one field of the scratch set, rounded up to keep 256-byte alignment
   const size_t field_bytes = ((size_t)g->H * (size_t)g->pitch_y * es + 255) / 256 * 256;
   if (3 * field_bytes > (size_t)DN_NOALLOC_MAX_BYTES) return DN_ENOMEM;

@@ -91,6 +91,7 @@ class _Runner:
                 M.box = eng.mon_arr[m].box
                 M.n_freq = eng.mon_arr[m].n_freq
                 M.phase = eng.mon_arr[m].phase
+                M.n_t = eng.mon_arr[m].n_t
                 M.acc = gm.data_ptr()
         n_mon = len(eng.monitors) if g_mon is not None else 0
         grad_ce = torch.zeros((D, H, eng.Wp), dtype=F64, device=eng.device)
@@ -112,7 +113,7 @@ class _Runner:
             ended_b = eng.adjoint(la, lb, rec, grad_ce, mon_arr, n_mon, tb, tb - ta)
             if ended_b:
                 la, lb = lb, la
-        eng.check_status()
+        eng.check_status(extra=(grad_ce[..., :W],))
         del grads
         return grad_ce[..., :W]
 

@@ -127,6 +127,7 @@ class Engine:
             self.src.component = src_comp
             self.src.box = _lib.box([a for a, _ in src_box], [b for _, b in src_box])
             self.src.wave = self.wave.data_ptr()
+            self.src.n_t = self.wave.numel()
 
         # monitors
         if len(monitors) > _lib.DN_MAX_MONITORS:
@@ -147,6 +148,7 @@ class Engine:
             M.n_freq = len(spec.wavelengths)
             M.phase = ph.data_ptr()
             M.acc = acc.data_ptr()
+            M.n_t = ph.shape[0]
 
         # probe
         self.probe = _lib.DnProbe(component=_lib.DN_NONE)
@@ -158,6 +160,7 @@ class Engine:
             for a in range(3):
                 self.probe.pos[a] = int(pos[a])
             self.probe.out = self.probe_out.data_ptr()
+            self.probe.n_t = self.probe_out.numel()
 
         self.status = torch.zeros(1, dtype=torch.int32, device=device)
 
@@ -262,8 +265,17 @@ class Engine:
         _lib.check(fn_name, rc)
         return bool(out.value)
 
-    def check_status(self) -> None:
-        """Raise if a kernel recorded a device-side error (synchronises)."""
+    def check_status(self, extra=()) -> None:
+        """Scan the current state of the solver's components, the monitor
+        DFTs, the probe series and the ``extra`` tensors for NaN/Inf with the
+        watchdog kernel, then raise if a kernel or the scan recorded a
+        device-side error (synchronises)."""
+        used = ((_lib.DN_EX, _lib.DN_EY, _lib.DN_EZ, _lib.DN_HX, _lib.DN_HY, _lib.DN_HZ)
+                if self.is3d else (_lib.DN_EZ, _lib.DN_HX, _lib.DN_HY) if self.pol == _lib.DN_TM
+                else (_lib.DN_HZ, _lib.DN_EX, _lib.DN_EY))
+        ts = [self.field(c) for c in used] + list(self.accs) + [self.probe_out, *extra]
+        with torch.cuda.device(self.device):
+            _lib.check_finite(ts, self.status, torch.cuda.current_stream(self.device).cuda_stream)
         s = int(self.status.item())
         if s != _lib.DN_OK:
             _lib.check("device status", s)

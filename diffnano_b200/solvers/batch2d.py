@@ -381,7 +381,22 @@ class FDTDBatch2D:
         self._reset()
         self._launch(True, False)
 
-    def check_status(self):
+    def check_status(self, grads: bool = False):
+        """Scan the final fields and monitor sums (the gradients after a
+        backward sweep) for NaN/Inf with the watchdog kernel, then raise if
+        a kernel or the scan recorded an error (synchronises)."""
+        if self._insts is not None:
+            if grads:
+                ts = [i.grad[:, : i.W] for i in self._insts if i.grad is not None]
+            else:
+                ts = [i.f[i.spec.n_steps % 2, :, :, : i.W] for i in self._insts]
+                if self._stack is not None:  # batch-wide monitor sums: one tensor
+                    ts.append(self._stack[2])
+                else:
+                    ts += [i.acc for i in self._insts if i.acc is not None]
+            with torch.cuda.device(self.device):
+                _lib.check_finite(ts, self.status,
+                                  torch.cuda.current_stream(self.device).cuda_stream)
         s = int(self.status.item())
         if s != _lib.DN_OK:
             self.status.zero_()
@@ -435,7 +450,7 @@ class _BatchFDTD(torch.autograd.Function):
             g_dfts.append(torch.view_as_complex(g.reshape(-1, 2).contiguous())
                           if (g is not None and i.acc is not None) else None)
         gce = batch.run_backward(g_fields, g_dfts)
-        batch.check_status()
+        batch.check_status(grads=True)
         out = []
         for e, gc, i in zip(eps_list, gce, batch._insts):
             ed = e.detach().to(gc.device, F64).reshape(gc.shape)

@@ -90,34 +90,42 @@ typedef struct {
 
 /* soft source: after each full step, field[component][box] += wave[t]
  * (fdtd2d.py:333,351; fdtd3d.py:502).  `wave` is indexed by the absolute
- * step t and has the grid's dtype.  component = DN_NONE disables it. */
+ * step t, has the grid's dtype and holds `n_t` entries: a run of steps
+ * t0 .. t0+nsteps-1 needs t0 + nsteps <= n_t (DN_EINVAL otherwise).
+ * component = DN_NONE disables it. */
 typedef struct {
   int32_t component;
   dn_box box;
   const void* wave;
+  int32_t n_t;
 } dn_source;
 
 /* running-DFT monitor (extension, no reference counterpart):
  * acc[f][cell][0..1] += v_t(cell) * phase[t][f][0..1] on every step t, where
  * v_t is the component's value after step t (source included) and
  * phase[t][f] = (cos(w_f t dt) dt, -sin(w_f t dt) dt).  Cells are the box's
- * cells in (z, y, x) row-major order.  FP64 accumulators. */
+ * cells in (z, y, x) row-major order.  FP64 accumulators.  `phase` has n_t
+ * rows (absolute steps 0 .. n_t-1): every step a forward run or a reverse
+ * sweep touches must be below n_t (DN_EINVAL otherwise). */
 typedef struct {
   int32_t component;
   dn_box box;
   int32_t n_freq;
-  const double* phase; /* [T][n_freq][2] device */
+  const double* phase; /* [n_t][n_freq][2] device */
   double* acc;         /* [n_freq][cells][2] device, caller zeroes it */
+  int32_t n_t;
 } dn_monitor;
 
 /* single-cell probe (fdtd2d.py:335-337 snapshots, fdtd3d.py:698 time_series):
  * out[t] = value of `component` at (pos[0], pos[1], pos[2]) = (z, y, x) after
- * step t (source included).  `out` has the grid dtype and is indexed by the
- * absolute step t.  component = DN_NONE disables it. */
+ * step t (source included).  `out` has the grid dtype, is indexed by the
+ * absolute step t and holds `n_t` entries (t0 + nsteps <= n_t, DN_EINVAL
+ * otherwise).  component = DN_NONE disables it. */
 typedef struct {
   int32_t component;
   int32_t pos[3];
   void* out;
+  int32_t n_t;
 } dn_probe;
 
 /* curl record (forward replay for the adjoint): during step t the bracket
@@ -300,6 +308,25 @@ int64_t dn_fom_abs2_scratch_bytes(int64_t n_complex);
 int32_t dn_fom_abs2(const double* dft, int64_t n_complex, double* out, void* scratch,
                     int64_t scratch_bytes, void* stream);
 
+/* ---- non-finite watchdog -------------------------------------------------
+ * No reference counterpart: the reference returns NaN fields and gradients
+ * without an error (its TE update grows exponentially and overflows FP32
+ * within a few hundred steps, diffnano/solvers/fdtd2d.py:269-303).  Scans
+ * `n_spans` (1 .. DN_MAX_SPANS) strided device arrays and, when any element
+ * is NaN or +-Inf, records DN_ENONFINITE in the device word *status if it
+ * still holds DN_OK.  NaN and Inf are sticky under the leapfrog update, so a
+ * scan of a solve's final fields, monitor DFTs and gradient catches a blow-up
+ * at any step; the solvers do it once per solve and per reverse sweep. */
+typedef struct {
+  const void* ptr;
+  int32_t dtype;  /* DN_F32 / DN_F64 */
+  int64_t rows;   /* rows of `cols` elements ...                    */
+  int64_t cols;
+  int64_t pitch;  /* ... `pitch` elements apart (pitch >= cols)     */
+} dn_span;
+#define DN_MAX_SPANS 32
+int32_t dn_check_finite(const dn_span* spans, int32_t n_spans, int32_t* status, void* stream);
+
 /* ---- stepping without device allocation --------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device
  * memory where they step the solver (a plugin inside an application that owns
@@ -310,9 +337,11 @@ int32_t dn_fom_abs2(const double* dft, int64_t n_complex, double* out, void* scr
  * place; the result is always in `f`.  Grids needing more than
  * DN_NOALLOC_MAX_BYTES for three fields (H * pitch_y * element size each,
  * rounded up to 256 bytes) return DN_ENOMEM.  The first call on a device
- * looks up the array's address; make it before any stream capture.  All
- * calls share the array: calls whose GPU work overlaps race.  Makes no
- * cudaMalloc/cudaFree or other allocating call. */
+ * looks up the array's address; make it before any stream capture.  The
+ * address stays cached for the process: after cudaDeviceReset on a device,
+ * do not call this entry point on that device again.  All calls share the
+ * array: calls whose GPU work overlaps race.  Makes no cudaMalloc/cudaFree
+ * or other allocating call. */
 #define DN_NOALLOC_MAX_BYTES (6 * 1024 * 1024)
 int32_t dn_fdtd2d_run_noalloc(const dn_grid* g, void* const f[6], const void* ce,
                               const dn_cpml* cpml, const dn_source* src, const dn_monitor* mons,

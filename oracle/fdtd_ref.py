@@ -400,23 +400,31 @@ def run_2d(eps, *, dl, dt, omega, pml_layers, polarization="TM", n_steps, source
 
 
 def run_3d(eps, *, dl, dt, omega, pml_layers, n_steps, source, monitors=(), probe=None,
-           axes="reference", component="Ez"):
-    """Run the 3-D solver from zero fields; follows ``fdtd3d.py:471-504``.
+           axes="reference", component="Ez", init=None, t0=0):
+    """Run the 3-D solver; follows ``fdtd3d.py:471-504``.
 
-    The reference injects into Ez (``fdtd3d.py:502``); ``component`` selects
-    Ex/Ey/Ez (extension).  Returns a dict with the six final fields, the probe
-    series of Ez (``fdtd3d.py:698``) and the monitor DFTs.
+    The reference starts from zero fields at step 0 and injects into Ez
+    (``fdtd3d.py:502``); ``component`` selects Ex/Ey/Ez (extension).
+    ``init`` (a dict of the six ``(D, H, W)`` fields) and ``t0`` start the
+    loop from a given state at absolute step ``t0`` instead (extension: it
+    lets a short run touch every cell of a large grid); the waveform and the
+    DFT phases are taken at the absolute step, and monitors accumulate from
+    ``t0``.  Returns a dict with the six final fields, the probe series of Ez
+    (``fdtd3d.py:698``) and the monitor DFTs.
     """
     D, H, W = eps.shape
     prof = (*cpml_profile(W, pml_layers, dl, dt), *cpml_profile(H, pml_layers, dl, dt),
             *cpml_profile(D, pml_layers, dl, dt))
     mask = box_mask((D, H, W), source_box_3d((D, H, W), source))
     names = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
-    f = {k: torch.zeros(D, H, W, dtype=F64) for k in names}
-    phases = [dft_phase(n_steps, dt, m["wavelengths_nm"]) for m in monitors]
+    if init is None:
+        f = {k: torch.zeros(D, H, W, dtype=F64) for k in names}
+    else:
+        f = {k: init[k].to(F64).clone() for k in names}
+    phases = [dft_phase(t0 + n_steps, dt, m["wavelengths_nm"]) for m in monitors]
     acc = [None] * len(monitors)
     series = []
-    for step in range(n_steps):
+    for step in range(t0, t0 + n_steps):
         new = step_3d(*(f[k] for k in names), eps, prof, dt, dl, axes=axes)
         f = dict(zip(names, new))
         w = waveform(step, dt, omega, source)

@@ -185,3 +185,100 @@ def test_batch2d_requires_16_byte_rows_and_arrays():
     assert L.dn_batch2d_table_bytes(ctypes.byref(cfg), inst()) > 0
     assert L.dn_batch2d_table_bytes(ctypes.byref(cfg), inst(pitch=37)) == -1  # 148-byte rows
     assert L.dn_batch2d_table_bytes(ctypes.byref(cfg), inst(ce=0x10004)) == -1  # misaligned
+
+
+def test_step_tables_shorter_than_the_run_are_rejected_before_any_launch():
+    """The waveform, the monitor phase table and the probe output are indexed
+    by the absolute step and carry their length (n_t): a forward run of steps
+    t0 .. t0+nsteps-1 past it, or a reverse sweep past a monitor's table, is
+    refused on the host (the fake pointers are never dereferenced)."""
+    L = _lib.lib()
+    out = ctypes.c_int32(-1)
+    cp = _lib.DnCpml()
+    for a in range(3):
+        cp.b[a] = cp.c[a] = 256
+    cell = _lib.box((0, 0, 0), (1, 1, 1))
+    for fn, D in (("dn_fdtd2d_run", 1), ("dn_fdtd3d_run", 8)):
+        g = _grid(D=D, axes=0, pitch_y=32, pitch_z=256)
+        fake = _lib.PTR6(*([256] * 6))
+        run = getattr(L, fn)
+        src = _lib.DnSource(component=_lib.DN_EZ, box=cell, wave=256, n_t=10)
+        mon = (_lib.DnMonitor * 1)()
+        mon[0] = _lib.DnMonitor(component=_lib.DN_EZ, box=cell, n_freq=1, phase=256, acc=256,
+                                n_t=10)
+        probe = _lib.DnProbe(component=_lib.DN_EZ, out=256, n_t=10)
+        # t0 + nsteps = 11 > 10 for each table in turn
+        assert run(ctypes.byref(g), fake, fake, 256, ctypes.byref(cp), ctypes.byref(src), None, 0,
+                   None, None, 5, 6, None, None, ctypes.byref(out)) == _lib.DN_EINVAL
+        assert run(ctypes.byref(g), fake, fake, 256, ctypes.byref(cp), None, mon, 1, None, None, 5,
+                   6, None, None, ctypes.byref(out)) == _lib.DN_EINVAL
+        assert run(ctypes.byref(g), fake, fake, 256, ctypes.byref(cp), None, None, 0,
+                   ctypes.byref(probe), None, 5, 6, None, None, ctypes.byref(out)) == \
+            _lib.DN_EINVAL
+        # a disabled source / probe carries no table and is not checked
+        off = _lib.DnSource(component=_lib.DN_NONE)
+        assert off.n_t == 0
+    for fn, D in (("dn_fdtd2d_adjoint", 1), ("dn_fdtd3d_adjoint", 8)):
+        g = _grid(D=D, axes=0, pitch_y=32, pitch_z=256)
+        fake = _lib.PTR6(*([256] * 6))
+        rec = _lib.DnCurlRecord(step_stride=8 * 256, t0=0, nslots=16)
+        for c in range(3):
+            rec.curl[c] = 256
+        mon = (_lib.DnMonitor * 1)()
+        mon[0] = _lib.DnMonitor(component=_lib.DN_EZ, box=cell, n_freq=1, phase=256, acc=256,
+                                n_t=10)
+        # reverse steps 10 and 9: step 10 is beyond the 10-row phase table
+        assert getattr(L, fn)(ctypes.byref(g), fake, fake, 256, ctypes.byref(cp),
+                              ctypes.byref(rec), 256, mon, 1, 11, 2, None, None,
+                              ctypes.byref(out)) == _lib.DN_EINVAL
+
+
+@pytest.mark.parametrize("bad", ["n0", "n33", "status", "dtype", "pitch", "ptr"])
+def test_check_finite_rejects_bad_spans_before_any_launch(bad):
+    L = _lib.lib()
+    n = 33 if bad == "n33" else 1
+    arr = (_lib.DnSpan * 33)()
+    for i in range(33):
+        arr[i] = _lib.DnSpan(ptr=4096, dtype=_lib.DN_F32, rows=4, cols=8, pitch=8)
+    if bad == "dtype":
+        arr[0].dtype = 7
+    if bad == "pitch":
+        arr[0].pitch = 4
+    if bad == "ptr":
+        arr[0].ptr = None
+    rc = L.dn_check_finite(arr, 0 if bad == "n0" else n, None if bad == "status" else 8192, None)
+    assert rc == _lib.DN_EINVAL
+
+
+def test_watchdog_spans_cover_tensors_exactly():
+    """Host side of the watchdog: a contiguous tensor becomes 1024-element
+    rows plus a remainder row; a narrowed padded field keeps its pitch."""
+    import torch
+
+    t = torch.zeros(2500, dtype=torch.float64)
+    sp = _lib.spans(t)
+    assert [(s.rows, s.cols, s.pitch) for s in sp] == [(2, 1024, 1024), (1, 452, 452)]
+    assert sp[1].ptr == t.data_ptr() + 2048 * 8 and sp[0].dtype == _lib.DN_F64
+    padded = torch.zeros(2, 5, 7, 32, dtype=torch.float32)
+    v = padded[1, :, :, :20]
+    (s,) = _lib.spans(v)
+    assert (s.rows, s.cols, s.pitch, s.dtype) == (35, 20, 32, _lib.DN_F32)
+    assert s.ptr == v.data_ptr()
+    with pytest.raises(ValueError):
+        _lib.spans(padded[:, 1])  # two set strides that do not fold into rows
+    with pytest.raises(ValueError):
+        _lib.spans(torch.zeros(4, dtype=torch.int32))
+
+
+def test_noalloc_refuses_a_pitch_whose_size_would_wrap():
+    """H * pitch * 4 bytes would wrap 64 bits to a small number; the
+    allocation-free run refuses it as too large before any CUDA call."""
+    L = _lib.lib()
+    g = _grid(H=4, W=8, pitch_y=(1 << 62) + 8)
+    fake = _lib.PTR6(*([256] * 6))
+    cp = _lib.DnCpml()
+    for a in range(3):
+        cp.b[a] = cp.c[a] = 256
+    rc = L.dn_fdtd2d_run_noalloc(ctypes.byref(g), fake, 256, ctypes.byref(cp), None, None, 0,
+                                 None, 0, 1, None, None)
+    assert rc == _lib.DN_ENOMEM

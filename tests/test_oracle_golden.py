@@ -106,3 +106,18 @@ def test_point_monitor_equals_dft_of_reference_series():
         ref = np.sum(g["series"] * np.exp(-1j * w * n * dt)) * dt
         got = o["monitors"][0][li, 0, 0]
         assert abs(complex(got[0], got[1]) - ref) <= 1e-12 * abs(ref)
+
+
+def test_3d_restart_from_state_equals_one_run():
+    """run_3d(init=state at step a, t0=a) continues an uninterrupted run bit
+    for bit: fields exactly, monitor DFT as the remaining steps' share."""
+    g = load_golden("fd3d_plane")
+    kw = dict(dl=25.0, dt=DT3(0.35, 25.0), omega=OMEGA, pml_layers=3, source=g["source"])
+    mon = [{"component": "Ey", "box": ((10, 11), (2, 14), (3, 13)), "wavelengths_nm": [1550.0]}]
+    eps = torch.tensor(g["eps"])
+    full = R.run_3d(eps, n_steps=60, monitors=mon, **kw)
+    head = R.run_3d(eps, n_steps=25, monitors=mon, **kw)
+    tail = R.run_3d(eps, n_steps=35, monitors=mon, init=head, t0=25, **kw)
+    for k in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz"):
+        assert torch.equal(tail[k], full[k]), k
+    assert rel_l2(head["monitors"][0] + tail["monitors"][0], full["monitors"][0]) < 1e-15
