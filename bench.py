@@ -35,9 +35,12 @@ SHAPE = (256, 256, 256)
 DL, COURANT, PML, T_SOLVE = 25.0, 0.4, 12, 4000
 Z_SRC = 40
 BYTES_PER_CELL_STEP = 52  # FP32: read Ex Ey Ez Hx Hy Hz dt/eps, write the six fields
-# reverse step incl. its replay: replay 52 + 12 (curl record); adjoint reads 7
-# fields (28) + curl (12) + FP64 grad (8), writes 6 adjoint fields (24) + grad (8)
-ADJ_BYTES_PER_CELL_STEP = 144
+# reverse step, algorithmic: forward recompute 52 + adjoint update 52 + dL/deps
+# read-modify-write 8 (FP32)
+ADJ_BYTES_PER_CELL_STEP = 112
+# what the reverse step moves on top: the curl record written by the replay and
+# read back by the adjoint (12 + 12) and the FP64 gradient's extra 8 bytes
+ADJ_OVERHEAD_BYTES_PER_CELL_STEP = {"curl_record": 24, "fp64_gradient": 8}
 WORKLOAD = "3d_yee_256cube_cpml12_fp32"
 METRIC = "FDTD Gcell-updates/s"
 UNIT = "Gcell-updates/s"
@@ -89,7 +92,13 @@ def traffic_per_launch():
 
 
 class ClockSampler:
-    """nvidia-smi clock/throttle sampling during the timed region."""
+    """nvidia-smi clock/throttle sampling (query only) in a reader thread.
+
+    The 3-D timed window is only a few milliseconds, shorter than the 100 ms
+    sampling period, so the caller starts the sampler, waits for its first
+    sample (``wait_ready``) and keeps it running over the untimed pre-roll
+    and the timed steps of the same solve: the summary is the clock under
+    that load."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -98,8 +107,12 @@ class ClockSampler:
     def __init__(self, gpu_index: int):
         self.idx = gpu_index
         self.proc = None
+        self.lines = []
+        self._thread = None
 
     def __enter__(self):
+        import threading
+
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
@@ -107,21 +120,33 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
+            return self
+
+        def reader():
+            for ln in self.proc.stdout:
+                if ln.strip():
+                    self.lines.append(ln)
+
+        self._thread = threading.Thread(target=reader, daemon=True)
+        self._thread.start()
         return self
+
+    def wait_ready(self, timeout: float = 5.0) -> None:
+        t = time.perf_counter()
+        while self.proc is not None and not self.lines and time.perf_counter() - t < timeout:
+            time.sleep(0.01)
 
     def __exit__(self, *a):
         if self.proc is not None:
             self.proc.terminate()
             try:
-                out, _ = self.proc.communicate(timeout=5)
+                self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
-                out, _ = self.proc.communicate()
-            self.lines = [ln for ln in out.splitlines() if ln.strip()]
-        else:
-            self.lines = []
+            if self._thread is not None:
+                self._thread.join(timeout=5)
 
-    def summary(self):
+    def summary(self, window: str | None = None):
         if not self.lines:
             return None
         sm, mx, reasons = [], [], set()
@@ -138,8 +163,11 @@ class ClockSampler:
                     reasons.add(n)
         if not sm:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "samples": len(sm),
-                "reasons": sorted(reasons)}
+        out = {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "samples": len(sm),
+               "reasons": sorted(reasons)}
+        if window:
+            out["window"] = window
+        return out
 
 
 def dist_setup():
@@ -174,75 +202,82 @@ def max_over_ranks(x: float, ws: int, dev) -> float:
     return float(t.item())
 
 
+def rel_l2_dev(a, b) -> float:
+    """Relative L2 error of ``a`` against ``b`` (real or complex; any device),
+    computed in FP64 on ``b``'s device."""
+    a = a.detach().to(b.device)
+    if a.is_complex() or b.is_complex():
+        a, b = torch.view_as_real(a.to(torch.complex128)), torch.view_as_real(b.to(torch.complex128))
+    a, b = a.to(torch.float64), b.to(torch.float64)
+    return float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
+
+
 # ---------------------------------------------------------------------------
 # CPU baseline: the oracle (FP64 torch CPU restatement of the reference)
 # ---------------------------------------------------------------------------
-def cpu_baseline(eps, n_steps_hint: int | None = None, budget_s: float = 15.0):
+def timed_window(K: int, Wm: int):
+    """(pre-roll steps, total steps) of the 3-D timing: the K timed steps sit
+    in the middle of a T_SOLVE-step solve, after Wm warm-up steps."""
+    preroll = max(0, (T_SOLVE - K) // 2 - Wm)
+    return preroll, max(T_SOLVE, preroll + Wm + K)
+
+
+def oracle_sample(K: int, Wm: int, t_start: int):
+    """Time K steps (after Wm warm-up steps) of the reference's algorithm on
+    the host cores: the oracle (FP64 torch-CPU restatement of
+    ``fdtd3d.py:_time_step`` + soft source, bit-exact with the reference) on
+    the full 256^3 grid with the Ex plane source and the Ey DFT monitor, at
+    absolute steps t_start .. t_start+K-1.  Returns (Gcell/s, seconds per
+    step, description)."""
     from oracle import fdtd_ref as R
 
     threads = os.cpu_count() or 1
     torch.set_num_threads(threads)
+    eps, src, _ = workload()
     D, H, W = SHAPE
     dt = COURANT * DL / math.sqrt(3.0)
-    prof = (*R.cpml_profile(W, PML, DL, dt), *R.cpml_profile(H, PML, DL, dt),
-            *R.cpml_profile(D, PML, DL, dt))
+    c = D // 2
+    mon = [{"component": "Ey", "box": ((D - 56, D - 55), (c - 32, c + 32), (c - 32, c + 32)),
+            "wavelengths_nm": [1550.0]}]
+    # the zero state at step t_start would need t_start CPU steps first (hours);
+    # a seeded random state costs the same per step
     gen = torch.Generator().manual_seed(0)
-    f = [1e-3 * torch.randn(D, H, W, dtype=torch.float64, generator=gen) for _ in range(6)]
+    names = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
+    state = {k: 1e-3 * torch.randn(D, H, W, dtype=torch.float64, generator=gen) for k in names}
+    kw = dict(dl=DL, dt=dt, omega=2 * math.pi / 1550.0, pml_layers=PML, source=src,
+              monitors=mon, component="Ex")
+    if Wm:
+        state = R.run_3d(eps, n_steps=Wm, init=state, t0=t_start - Wm, **kw)
     t = time.perf_counter()
-    f = list(R.step_3d(*f, eps, prof, dt, DL))  # warm-up
-    t1 = time.perf_counter() - t
-    n = n_steps_hint or max(2, min(20, int(budget_s / max(t1, 1e-3))))
-    t = time.perf_counter()
-    for _ in range(n):
-        f = list(R.step_3d(*f, eps, prof, dt, DL))
+    R.run_3d(eps, n_steps=K, init=state, t0=t_start, **kw)
     el = time.perf_counter() - t
-    return {"value": D * H * W * n / el / 1e9, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{n} time steps of the full 256^3 grid, FP64 torch-CPU restatement of "
-                      f"fdtd3d.py:_time_step (oracle/fdtd_ref.py), {threads} threads"}
+    desc = (f"{K} time steps (after {Wm} warm-up steps) of the full 256^3 grid from a seeded "
+            f"random state, steps {t_start}..{t_start + K - 1}: FP64 torch-CPU restatement of "
+            "the reference's fdtd3d.py:_time_step with the Ex plane source and the Ey DFT "
+            f"monitor (oracle/fdtd_ref.py), {threads} threads")
+    return D * H * W * K / el / 1e9, el / K, desc, threads
 
 
 def run_reference(args):
+    """``--impl reference``: the CPU arm, on rank 0 only (see ``oracle_sample``);
+    a long ``--steps`` is sampled by its first 100 steps (per-step cost is
+    constant)."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    from oracle import fdtd_ref as R
-
-    threads = os.cpu_count() or 1
-    torch.set_num_threads(threads)
-    eps, _, _ = workload()
-    D, H, W = SHAPE
-    # bounded sample (about a minute on 8 cores): full grid while K+W <= 16
-    # steps, else a z-slab of the same grid
-    total = args.steps + args.warmup
-    dz = D if total <= 16 else max(8, int(D * 16 / total))
-    dt = COURANT * DL / math.sqrt(3.0)
-    # the slab keeps all three CPML profiles (cubic "reference" broadcasting)
-    prof = (*R.cpml_profile(W, PML, DL, dt), *R.cpml_profile(H, PML, DL, dt),
-            *R.cpml_profile(W, PML, DL, dt))
-    e = eps[:dz].contiguous()
-    gen = torch.Generator().manual_seed(0)
-    f = [1e-3 * torch.randn(dz, H, W, dtype=torch.float64, generator=gen) for _ in range(6)]
-
-    def step(f):
-        return list(R.step_3d(*f, e, prof, dt, DL))
-
-    for _ in range(args.warmup):
-        f = step(f)
-    t = time.perf_counter()
-    for _ in range(args.steps):
-        f = step(f)
-    el = time.perf_counter() - t
-    v = dz * H * W * args.steps / el / 1e9
+    K, Wm = args.steps, args.warmup
+    preroll, _ = timed_window(K, Wm)
+    t_start = preroll + Wm
+    k_eff, w_eff = min(K, 100), min(Wm, 5)
+    v, s_step, desc, threads = oracle_sample(k_eff, w_eff, t_start)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
+            "steps": K, "warmup": Wm, "ms_per_step": s_step * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": config_dict({"reference_sample": f"z-slab {dz}x{H}x{W} per step"}),
+            "config": config_dict({"timed_steps": [t_start, t_start + K]}),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": f"{args.steps} steps of a {dz}x{H}x{W} slab of the "
-                                       "256^3 grid, FP64 torch-CPU restatement of the "
-                                       "reference's fdtd3d.py:_time_step"},
+                             "sample": desc},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -265,19 +300,19 @@ def run_ours(args):
     # fills the grid the board draws ~950 W and the power cap lowers the clocks,
     # so steps on a still mostly zero field are a few percent faster than the
     # solve's average.  Untimed pre-roll steps bring the state there first.
-    preroll = max(0, (T_SOLVE - K) // 2 - Wm)
-    n_total = max(T_SOLVE, preroll + Wm + K)
+    preroll, n_total = timed_window(K, Wm)
     solver = dn.FDTDSolver3D(grid_shape=SHAPE, dl=DL, wavelength_nm=1550.0, pml_layers=PML,
                              n_steps=n_total, courant=COURANT, device=dev, dtype=torch.float32)
     eng = solver._make_engine(n_total, src, mons)
     eng.set_eps(eps.to(dev))
-    eng.run(0, preroll + Wm)
-    torch.cuda.synchronize(dev)
     stream = torch.cuda.current_stream(dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    barrier(ws)
-    torch.cuda.synchronize(dev)
     with ClockSampler(local) as cs:
+        cs.wait_ready()
+        eng.run(0, preroll + Wm)
+        torch.cuda.synchronize(dev)
+        barrier(ws)
+        torch.cuda.synchronize(dev)
         e0.record(stream)
         eng.run(preroll + Wm, K)
         e1.record(stream)
@@ -315,11 +350,14 @@ def run_ours(args):
         torch.cuda.synchronize(dev)
         el_a = max_over_ranks(e0.elapsed_time(e1) / 1e3, ws, dev)
         rev_s = el_a / Ta
+        moved = ADJ_BYTES_PER_CELL_STEP + sum(ADJ_OVERHEAD_BYTES_PER_CELL_STEP.values())
         adjoint = {"value": ws * cells * Ta / el_a / 1e9, "unit": UNIT,
                    "ms_per_step": rev_s * 1e3, "steps": Ta,
                    "algorithmic_bytes_per_cell_step": ADJ_BYTES_PER_CELL_STEP,
                    "achieved_GBs": ADJ_BYTES_PER_CELL_STEP * cells / rev_s / 1e9,
                    "frac_of_hbm_peak": ADJ_BYTES_PER_CELL_STEP * cells / rev_s / 1e9 / peak,
+                   "overhead_bytes_per_cell_step": ADJ_OVERHEAD_BYTES_PER_CELL_STEP,
+                   "moved_GBs": moved * cells / rev_s / 1e9,
                    "what": f"reverse sweep of a {Ta}-step solve: per step one replay step with "
                            "curl record (k_fdtd3d) + one reverse step (k_adj3d), "
                            f"checkpoints every {runner.K} steps"}
@@ -348,6 +386,24 @@ def run_ours(args):
                "step": f"one FDTDSolver3D.forward(device='cpu') solve of {T_SOLVE} time steps "
                        f"(host eps in, host field + monitor DFT out), mean of {args.e2e_steps}"}
 
+    # the same 4000-step solve through the FP64 build of the kernels (untimed):
+    # the error of the FP32 result that e2e timed
+    fp64_check = None
+    if not args.no_fp64_check and e2e is not None:
+        s64 = dn.FDTDSolver3D(grid_shape=SHAPE, dl=DL, wavelength_nm=1550.0, pml_layers=PML,
+                              n_steps=T_SOLVE, courant=COURANT, device=dev,
+                              dtype=torch.float64)
+        with torch.no_grad():
+            r64 = s64.forward(eps.to(dev), source=dict(src), monitors=mons)
+        fp64_check = {
+            "field_rel_l2": rel_l2_dev(r.field, r64.field),
+            "dft_rel_l2": rel_l2_dev(r.metadata["monitors"][0]["dft"],
+                                     r64.metadata["monitors"][0]["dft"]),
+            "what": f"FP32 result of the timed {T_SOLVE}-step solve vs the same solve on the "
+                    "FP64 kernels: field [Ez, Ex, Ey] and Ey DFT, relative L2"}
+        del r64, s64
+        torch.cuda.empty_cache()
+
     # full gradient of the monitor FOM through the public API, host buffers
     grad_e2e = None
     if not args.no_grad_e2e:
@@ -374,12 +430,30 @@ def run_ours(args):
                             "(forward with checkpoints, replay, reverse sweep), "
                             "FDTDSolver3D(device='cpu', backward='time_reversal'), "
                             "after one untimed call"}
-        del r, fom, e_in
+        if fp64_check is not None:
+            g32 = e_in.grad.to(dev, torch.float64)
+            fom32 = float(fom)
+            del r, fom, e_in
+            torch.cuda.empty_cache()
+            s64 = dn.FDTDSolver3D(grid_shape=SHAPE, dl=DL, wavelength_nm=1550.0,
+                                  pml_layers=PML, n_steps=T_SOLVE, courant=COURANT, device=dev,
+                                  dtype=torch.float64, backward="time_reversal")
+            e64 = eps.to(dev).requires_grad_(True)
+            r64 = s64.forward(e64, source=dict(src), monitors=mons)
+            fom64 = (r64.metadata["monitors"][0]["dft"].abs() ** 2).sum()
+            fom64.backward()
+            fp64_check["fom_rel"] = abs(fom32 / float(fom64) - 1.0)
+            fp64_check["gradient_rel_l2"] = rel_l2_dev(g32, e64.grad)
+            fp64_check["what"] += "; FOM and dFOM/deps of the gradient_e2e solve likewise"
+            del r64, fom64, e64, g32
+        else:
+            del r, fom, e_in
         torch.cuda.empty_cache()
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(eps)
+        v, _, desc, threads = oracle_sample(20, 2, preroll + Wm)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc}
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K,
@@ -392,7 +466,9 @@ def run_ours(args):
                              "algorithmic_bytes_per_launch": BYTES_PER_CELL_STEP * cells,
                              "kernel": "k_fdtd3d (one launch per time step)"},
                 "cpu_baseline": cpu, "e2e": e2e, "adjoint": adjoint, "gradient_e2e": grad_e2e,
-                "clocks": cs.summary(), "gpu_launches": K}
+                "fp64_check": fp64_check,
+                "clocks": cs.summary("untimed pre-roll + timed steps of the same solve"),
+                "gpu_launches": K}
         print(json.dumps(line), flush=True)
     if ws > 1:
         import torch.distributed as dist
@@ -457,6 +533,34 @@ def run_batch2d(args):
     torch.cuda.synchronize(dev)
     f_s, b_s = e0.elapsed_time(e1) / 1e3, e1.elapsed_time(e2) / 1e3
     f_s, b_s = max_over_ranks(f_s, ws, dev), max_over_ranks(b_s, ws, dev)
+    fp64_check = None
+    if not args.no_fp64_check:
+        # the same batch through the FP64 kernels, untimed: fields, DFTs, gradients
+        g32 = [e.grad.detach().double() for e in e_dev]
+        f32 = [f.detach().double() for f in fields]
+        d32 = [d.detach() for d in dfts]
+        del fields, dfts, e_dev
+        b64 = FDTDBatch2D(specs, "TM", torch.float64, dev)
+        e64 = [e.to(dev).requires_grad_(True) for e in eps]
+        f64, d64 = b64.forward(e64)
+        sum((d.abs() ** 2).sum() for d in d64).backward()
+
+        def agg(a, b):
+            num = sum(float(torch.linalg.vector_norm(
+                torch.view_as_real(x.to(torch.complex128)) - torch.view_as_real(y.to(torch.complex128))) ** 2)
+                if x.is_complex() else float(torch.linalg.vector_norm(x.double() - y.double()) ** 2)
+                for x, y in zip(a, b))
+            den = sum(float(torch.linalg.vector_norm(
+                torch.view_as_real(y.to(torch.complex128)) if y.is_complex() else y.double()) ** 2)
+                for y in b)
+            return math.sqrt(num / den)
+
+        fp64_check = {"field_rel_l2": agg(f32, f64), "dft_rel_l2": agg(d32, d64),
+                      "gradient_rel_l2": agg(g32, [e.grad.double() for e in e64]),
+                      "what": "every instance's FP32 field, DFT and dFOM/deps vs the same batch "
+                              "on the FP64 kernels; relative L2 over the whole batch"}
+        del b64, e64, f64, d64
+        torch.cuda.empty_cache()
     cells_steps = int(sum_over_ranks(float(cells_steps), ws, dev))
     if ws > 1:
         import torch.distributed as dist
@@ -476,7 +580,7 @@ def run_batch2d(args):
                        "cell_steps": cells_steps, "tile_rows": batch.tile_rows,
                        "checkpoint_interval": batch.K},
             "forward_s": f_s, "backward_s": b_s,
-            "backward_gcells": cells_steps / b_s / 1e9,
+            "backward_gcells": cells_steps / b_s / 1e9, "fp64_check": fp64_check,
             "kernels": "k_batch2d_fwd / k_batch2d_bwd (one persistent launch each)"}
     print(json.dumps(line), flush=True)
     return 0
@@ -663,6 +767,17 @@ def run_fdtd2d(args):
                     "gbs": 28 * side * side * T / s_solve / 1e9,
                     "kernel": kernel, "warmup_solves": n_warm, "timed_solves": reps,
                     "launches_per_solve": 1 if cluster else T}
+        if not args.no_fp64_check:
+            s64 = FDTDSolver2D(grid_shape=(side, side), dl=st.dl, wavelength_nm=st.center_nm,
+                               pml_layers=st.pml, n_steps=T, courant=st.courant, device=dev,
+                               dtype=torch.float64, monitors=mon)
+            r64 = s64.forward(ed, source=dict(src))
+            out[key]["fp64_check"] = {
+                "field_rel_l2": rel_l2_dev(r.field, r64.field),
+                "dft_rel_l2": rel_l2_dev(r.metadata["monitors"][0]["dft"],
+                                         r64.metadata["monitors"][0]["dft"]),
+                "what": "FP32 result of the timed solve vs the same solve on the FP64 kernels "
+                        "(Ez field, Ez line DFT), relative L2"}
         if key == "cfg0":
             host = FDTDSolver2D(grid_shape=(side, side), dl=st.dl, wavelength_nm=st.center_nm,
                                 pml_layers=st.pml, n_steps=T, courant=st.courant, device="cpu",
@@ -712,6 +827,7 @@ def run_fdtd2d(args):
                          "unit": "GB/s", "frac": out["1024"]["gbs"] / peak,
                          "note": "1024^2 grid (28 B/cell-step); 256^2 is L2-resident"},
             "e2e": out["e2e"], "cpu_baseline": cpu,
+            "fp64_check": c0.get("fp64_check"),
             "gpu_launches": c0_launches,
             "kernels": f"{c0['kernel']} ({c0['launches_per_solve']} launch(es) per solve, {c0['timed_solves']} solves "
                        f"timed); grid_1024: {out['1024']['kernel']}"}
@@ -900,6 +1016,8 @@ def main():
     ap.add_argument("--adjoint-steps", type=int, default=256)
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-grad-e2e", action="store_true")
+    ap.add_argument("--no-fp64-check", action="store_true",
+                    help="skip the untimed FP64 cross-run of the solve and its gradient")
     ap.add_argument("--workload", choices=["fdtd3d", "fdtd2d", "batch2d", "fno", "design",
                                            "gemm", "fno-step", "fdtd3d-phases"],
                     default="fdtd3d",

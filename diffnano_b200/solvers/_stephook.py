@@ -1,0 +1,178 @@
+"""The reference's per-step hooks (``_time_step``, ``_time_step_tm``,
+``_time_step_te``) on the fused step kernels.
+
+The reference's bandwidth harness calls the 3-D hook in a loop on FP64 device
+tensors and divides the bytes it moved by the wall time
+(``diffnano/solvers/fdtd_benchmark.py:321-391``), so the hook must cost one
+kernel step and nothing else.  A :class:`StepHook` keeps, per solver, dtype
+and device, everything that does not change between calls -- the CPML
+profiles on the device, the ABI structs, dt/eps for the last ``eps_r`` seen
+(keyed on the tensor's storage and version), the check that ``mu_r`` is 1 --
+and runs one ``dn_fdtd3d_run`` / ``dn_fdtd2d_run`` step straight from the
+caller's tensors into one freshly allocated output block when their layout
+allows it (contiguous, 16-byte aligned; 3-D rows a multiple of 16 bytes for
+TMA).  Other inputs go through a cached padded :class:`Engine` (copy in,
+step, copy out).
+
+The device status word is read back without a synchronisation: each call
+queues an asynchronous copy into page-locked memory and the next call raises
+if an earlier step reported an error; :meth:`StepHook.check` synchronises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from diffnano_b200 import _lib
+from diffnano_b200.solvers import _setup
+from diffnano_b200.solvers._engine import Engine
+
+F64 = torch.float64
+
+
+class StepHook:
+    def __init__(self, *, is3d: bool, shape, dl: float, dt: float, pml_layers: int,
+                 dtype: torch.dtype, device: torch.device, pol: int = _lib.DN_TM,
+                 axes: int = _lib.DN_AXES_REFERENCE):
+        self.is3d = is3d
+        self.shape = tuple(int(v) for v in shape)
+        self.shape3 = self.shape if is3d else (1, *self.shape)
+        self.dl, self.dt, self.pml_layers = float(dl), float(dt), int(pml_layers)
+        self.dtype, self.device, self.pol, self.axes = dtype, device, pol, axes
+        self.comps = ((_lib.DN_EX, _lib.DN_EY, _lib.DN_EZ, _lib.DN_HX, _lib.DN_HY, _lib.DN_HZ)
+                      if is3d else (_lib.DN_EZ, _lib.DN_HX, _lib.DN_HY) if pol == _lib.DN_TM
+                      else (_lib.DN_HZ, _lib.DN_EX, _lib.DN_EY))
+        D, H, W = self.shape3
+        es = torch.tensor([], dtype=dtype).element_size()
+        self.grid = _lib.DnGrid(D=D, H=H, W=W,
+                                dtype=_lib.DN_F32 if dtype == torch.float32 else _lib.DN_F64,
+                                pitch_y=W, pitch_z=H * W, dt=self.dt, dl=self.dl, axes=axes,
+                                pol=pol)
+        self.rows16 = (W * es) % 16 == 0
+        self.prof = []
+        self.cpml = _lib.DnCpml()
+        for a, n in enumerate(self.shape3):
+            if a == 0 and not is3d:
+                continue
+            b, c = (t.to(device) for t in _setup.cpml_profile(n, pml_layers, dl, dt))
+            self.prof.append((b, c))
+            self.cpml.b[a], self.cpml.c[a] = b.data_ptr(), c.data_ptr()
+        self.status = torch.zeros(1, dtype=torch.int32, device=device)
+        self._host_status = torch.zeros(1, dtype=torch.int32, pin_memory=True)
+        self._event = None
+        self._ce, self._ce_key, self._mu_key = None, None, None
+        self._engine = None
+
+    # ------------------------------------------------------------------
+    @staticmethod
+    def _key(t: torch.Tensor):
+        return (t.data_ptr(), t._version, t.dtype, tuple(t.shape), t.device)
+
+    def _coefficient(self, eps_r: torch.Tensor) -> torch.Tensor:
+        key = self._key(eps_r)
+        if key != self._ce_key:
+            e = eps_r.detach().to(device=self.device, dtype=F64).reshape(self.shape3)
+            self._ce = (self.dt / e).to(self.dtype).contiguous()
+            self._ce_key = key
+        return self._ce
+
+    def _check_mu(self, mu_r) -> None:
+        if mu_r is None:
+            return
+        key = self._key(mu_r)
+        if key != self._mu_key:
+            if not bool((mu_r == 1).all()):
+                raise ValueError("the step kernels assume mu_r = 1 everywhere (as the "
+                                 "reference's solvers pass it)")
+            self._mu_key = key
+
+    def _poll(self) -> None:
+        if self._event is not None and self._event.query():
+            self._event = None
+            s = int(self._host_status[0])
+            if s != _lib.DN_OK:
+                self.status.zero_()
+                _lib.check("per-step hook (an earlier step)", s)
+
+    def check(self) -> None:
+        """Synchronise and raise if any step so far reported an error."""
+        s = int(self.status.item())
+        if s != _lib.DN_OK:
+            self.status.zero_()
+            _lib.check("per-step hook", s)
+
+    def _direct_ok(self, fields) -> bool:
+        if self.is3d and not self.rows16:
+            return False
+        for f in fields:
+            if not (f.is_cuda and f.device == self.device and f.dtype == self.dtype
+                    and f.is_contiguous() and tuple(f.shape) == self.shape
+                    and f.data_ptr() % 16 == 0):
+                return False
+        return True
+
+    # ------------------------------------------------------------------
+    def step(self, fields, eps_r: torch.Tensor, mu_r) -> tuple:
+        """One source-free step of ``fields`` (the solver's components in
+        the order of ``self.comps``); returns new tensors in that order."""
+        self._poll()
+        self._check_mu(mu_r)
+        ce = self._coefficient(eps_r)
+        out_dev = fields[0].device
+        if self._direct_ok(fields):
+            n = len(self.comps)
+            out = torch.empty((n, *self.shape), dtype=self.dtype, device=self.device)
+            fa, fb = [None] * 6, [None] * 6
+            for i, c in enumerate(self.comps):
+                fa[c], fb[c] = fields[i].data_ptr(), out[i].data_ptr()
+            self._launch(_lib.PTR6(*fa), _lib.PTR6(*fb), ce)
+            return tuple(out[i] for i in range(n))
+        eng = self._padded_engine()
+        for i, c in enumerate(self.comps):
+            eng.field(c).copy_(fields[i].reshape(self.shape3))
+        eng.ce[..., : self.shape3[2]] = ce
+        eng.cur_b = False
+        eng.run(0, 1)
+        return tuple(eng.field(c).reshape(self.shape).clone().to(out_dev) for c in self.comps)
+
+    def _launch(self, fa, fb, ce) -> None:
+        L = _lib.lib()
+        fn = "dn_fdtd3d_run" if self.is3d else "dn_fdtd2d_run"
+        out = ctypes.c_int32(0)
+        with torch.cuda.device(self.device):
+            stream = torch.cuda.current_stream(self.device)
+            rc = getattr(L, fn)(ctypes.byref(self.grid), fa, fb, ce.data_ptr(),
+                                ctypes.byref(self.cpml), None, None, 0, None, None, 0, 1,
+                                self.status.data_ptr(), ctypes.c_void_p(stream.cuda_stream),
+                                ctypes.byref(out))
+            _lib.check(fn, rc)
+            self._host_status.copy_(self.status, non_blocking=True)
+            self._event = torch.cuda.Event()
+            self._event.record(stream)
+
+    def _padded_engine(self) -> Engine:
+        if self._engine is None:
+            self._engine = Engine(is3d=self.is3d, shape=self.shape, dl=self.dl, dt=self.dt,
+                                  pml_layers=self.pml_layers, dtype=self.dtype,
+                                  device=self.device, n_steps=1,
+                                  wave=torch.zeros(1, dtype=F64), src_box=None,
+                                  src_comp=_lib.DN_NONE, pol=self.pol, axes=self.axes)
+        return self._engine
+
+
+def hook_for(solver, is3d: bool, dtype, device, pol=_lib.DN_TM, axes=_lib.DN_AXES_REFERENCE):
+    """The solver's cached :class:`StepHook` for this dtype and device (one
+    per combination; rebuilt if the solver's set-up attributes changed)."""
+    key = (dtype, device, tuple(solver.grid_shape), solver.dl, solver.dt, solver.pml_layers,
+           pol, axes)
+    cache = solver.__dict__.setdefault("_step_hooks", {})
+    h = cache.get(key)
+    if h is None:
+        if len(cache) >= 4:
+            cache.clear()
+        h = cache[key] = StepHook(is3d=is3d, shape=solver.grid_shape, dl=solver.dl,
+                                  dt=solver.dt, pml_layers=solver.pml_layers, dtype=dtype,
+                                  device=device, pol=pol, axes=axes)
+    return h

@@ -241,30 +241,26 @@ class FDTDSolver2D:
             m[box[1][0]:box[1][1], box[2][0]:box[2][1]] = 1.0
         return m
 
-    def _single_step(self, fields: dict, eps_r: torch.Tensor):
-        H, W = self.grid_shape
-        inj = _lib.DN_EZ if self.polarization == "TM" else _lib.DN_HZ
+    def _single_step(self, fields: dict, eps_r: torch.Tensor, mu_r=None):
+        """One source-free step through the cached per-step hook
+        (``_stephook.StepHook``): the kernel runs straight from the caller's
+        tensors when they are contiguous CUDA tensors of the compute dtype."""
+        from diffnano_b200.solvers._stephook import hook_for
+
         first = fields[self._fields()[0]]
         dtype = first.dtype if first.dtype in (torch.float32, torch.float64) else self.dtype
-        eng = Engine(is3d=False, shape=(H, W), dl=self.dl, dt=self.dt, pml_layers=self.pml_layers,
-                     dtype=dtype, device=compute_device(first.device), n_steps=1,
-                     wave=torch.zeros(1, dtype=torch.float64), src_box=None, src_comp=inj,
-                     pol=_lib.DN_TM if self.polarization == "TM" else _lib.DN_TE)
-        eng.set_eps(eps_r)
-        for name, t in fields.items():
-            eng.field(_lib.COMPONENTS[name]).copy_(t)
-        eng.run(0, 1)
-        return tuple(eng.field(_lib.COMPONENTS[n])[0].clone().to(fields[n].device)
-                     for n in self._fields())
+        pol = _lib.DN_TM if self.polarization == "TM" else _lib.DN_TE
+        h = hook_for(self, False, dtype, compute_device(first.device), pol=pol)
+        return h.step(tuple(fields[n] for n in self._fields()), eps_r, mu_r)
 
     def _time_step_tm(self, Ez, Hx, Hy, eps_r, mu_r):
         """One TM step without source (``fdtd2d.py:233-267``); mu_r must be 1."""
         if self.polarization != "TM":
             raise ValueError("_time_step_tm on a TE solver")
-        return self._single_step({"Ez": Ez, "Hx": Hx, "Hy": Hy}, eps_r)
+        return self._single_step({"Ez": Ez, "Hx": Hx, "Hy": Hy}, eps_r, mu_r)
 
     def _time_step_te(self, Hz, Ex, Ey, eps_r, mu_r):
         """One TE step without source (``fdtd2d.py:269-303``); mu_r must be 1."""
         if self.polarization != "TE":
             raise ValueError("_time_step_te on a TM solver")
-        return self._single_step({"Hz": Hz, "Ex": Ex, "Ey": Ey}, eps_r)
+        return self._single_step({"Hz": Hz, "Ex": Ex, "Ey": Ey}, eps_r, mu_r)

@@ -171,16 +171,13 @@ class FDTDSolver3D:
         return m
 
     def _time_step(self, Ex, Ey, Ez, Hx, Hy, Hz, eps_r, mu_r):
-        """One step without source (``fdtd3d.py:378-465``), used by the
-        reference's bandwidth harness; mu_r must be 1.  Runs the fused kernel
-        in the inputs' dtype (float32 or float64)."""
+        """One step without source (``fdtd3d.py:378-465``), the hook the
+        reference's bandwidth harness times (``fdtd_benchmark.py:346-363``);
+        mu_r must be 1.  Runs the fused kernel in the inputs' dtype (float32
+        or float64) straight from the caller's tensors when they allow it; the
+        set-up is cached across calls (``_stephook.StepHook``)."""
+        from diffnano_b200.solvers._stephook import hook_for
+
         dtype = Ex.dtype if Ex.dtype in (torch.float32, torch.float64) else self.dtype
-        eng = Engine(is3d=True, shape=tuple(self.grid_shape), dl=self.dl, dt=self.dt,
-                     pml_layers=self.pml_layers, dtype=dtype, device=compute_device(Ex.device),
-                     n_steps=1, wave=torch.zeros(1, dtype=torch.float64), src_box=None,
-                     src_comp=_lib.DN_EZ, axes=self._axes())
-        eng.set_eps(eps_r)
-        for name, t in zip(_FIELDS, (Ex, Ey, Ez, Hx, Hy, Hz)):
-            eng.field(_lib.COMPONENTS[name]).copy_(t)
-        eng.run(0, 1)
-        return tuple(eng.field(_lib.COMPONENTS[n]).clone().to(Ex.device) for n in _FIELDS)
+        h = hook_for(self, True, dtype, compute_device(Ex.device), axes=self._axes())
+        return h.step((Ex, Ey, Ez, Hx, Hy, Hz), eps_r, mu_r)
