@@ -533,6 +533,16 @@ def run_batch2d(args):
     torch.cuda.synchronize(dev)
     f_s, b_s = e0.elapsed_time(e1) / 1e3, e1.elapsed_time(e2) / 1e3
     f_s, b_s = max_over_ranks(f_s, ws, dev), max_over_ranks(b_s, ws, dev)
+    # the same forward + gradient as one CUDA-graph replay (FOM = sum |DFT|^2)
+    e_in = [e.to(dev) for e in eps]
+    batch.fom_gradient_graphed(e_in)  # records the graph
+    torch.cuda.synchronize(dev)
+    barrier(ws)
+    e0.record()
+    batch.fom_gradient_graphed(e_in)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    g_s = max_over_ranks(e0.elapsed_time(e1) / 1e3, ws, dev)
     fp64_check = None
     if not args.no_fp64_check:
         # the same batch through the FP64 kernels, untimed: fields, DFTs, gradients
@@ -580,7 +590,12 @@ def run_batch2d(args):
                        "cell_steps": cells_steps, "tile_rows": batch.tile_rows,
                        "checkpoint_interval": batch.K},
             "forward_s": f_s, "backward_s": b_s,
-            "backward_gcells": cells_steps / b_s / 1e9, "fp64_check": fp64_check,
+            "backward_gcells": cells_steps / b_s / 1e9,
+            "graphed_forward_backward_s": g_s,
+            "graphed_what": "FDTDBatch2D.fom_gradient_graphed: eps upload, forward, adjoint "
+                            "seeding, backward and dFOM/deps replayed as one CUDA graph "
+                            "(includes the watchdog scan and status read after the replay)",
+            "fp64_check": fp64_check,
             "kernels": "k_batch2d_fwd / k_batch2d_bwd (one persistent launch each)"}
     print(json.dumps(line), flush=True)
     return 0

@@ -33,9 +33,14 @@ using namespace zm;
 constexpr int NRING_F = 7;  // Ex Ey Ez Hx Hy Hz ce
 constexpr int A_CE = 6;
 
+// ring depth in planes (FP32: two CTAs per SM must fit 228 KB of shared memory)
+#ifndef DN_FWD3D_STAGES_F32
+#define DN_FWD3D_STAGES_F32 4
+#endif
+
 template <typename T>
 struct FwdCfg {
-  static constexpr int S = sizeof(T) == 4 ? 4 : 3;
+  static constexpr int S = sizeof(T) == 4 ? DN_FWD3D_STAGES_F32 : 3;
   static constexpr int MINB = sizeof(T) == 4 ? 2 : 1;
   using L = Layout<T, NRING_F, 0, S>;
 };

@@ -190,6 +190,7 @@ class FDTDBatch2D:
         self._stack = None
         self._grad_alloc = None
         self._graph = None
+        self._ggraph = None
         self.status = torch.zeros(1, dtype=torch.int32, device=self.device)
         # gradient-free solves: whole grids in thread-block clusters when they fit
         # (None = when possible, False = never)
@@ -248,6 +249,10 @@ class FDTDBatch2D:
         return [(f[b], ce[b], None if acc is None else acc[b]) for b in range(n)]
 
     def _pack(self):
+        # recorded graphs launch with the device table they were captured
+        # with: a new table (new pointers) makes them stale
+        self._graph = None
+        self._ggraph = None
         L = _lib.lib()
         arr = (_lib.DnBatch2dInst * len(self._insts))(*[i.struct(self.pol) for i in self._insts])
         cols = 128 if self.dtype == torch.float32 else 64  # tile width: 32 lanes x 16 bytes
@@ -374,6 +379,57 @@ class FDTDBatch2D:
         self._graph.replay()
         self.check_status()
         return self._outputs()
+
+    def fom_gradient_graphed(self, eps_list):
+        """FOM = sum |DFT|^2 of every instance's monitor and dFOM/deps, as one
+        CUDA-graph replay: the first call records eps upload, state reset,
+        the persistent forward launch (checkpoints on), the seeding of the
+        adjoint with dFOM/dDFT = 2 DFT, the persistent backward launch and
+        dFOM/deps = -(dt/eps^2) dFOM/d(dt/eps); later calls copy the new eps
+        into the recorded input buffers and replay.  Returns (per-instance
+        FOM tensor (FP64), list of dFOM/deps (FP64, one per instance)); the
+        results are views of graph-owned buffers, overwritten by the next
+        call.  No autograd."""
+        self._build(True)
+        if any(i.acc is None for i in self._insts):
+            raise ValueError("fom_gradient_graphed needs a monitor on every instance")
+        if getattr(self, "_ggraph", None) is None:
+            self._g_eps = [e.detach().to(self.device, F64).clone() for e in eps_list]
+            for i in self._insts:
+                i.gmon = torch.zeros_like(i.acc)
+            self._pack()
+            self._g_fom = torch.zeros(len(self._insts), dtype=F64, device=self.device)
+            self._g_out = [torch.zeros(i.H, i.W, dtype=F64, device=self.device)
+                           for i in self._insts]
+            side = torch.cuda.Stream(self.device)
+            side.wait_stream(torch.cuda.current_stream(self.device))
+            with torch.cuda.stream(side):
+                self._grad_body()  # warm-up outside the capture
+            torch.cuda.current_stream(self.device).wait_stream(side)
+            torch.cuda.synchronize(self.device)
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                self._grad_body()
+            self._ggraph = g
+        for dst, e in zip(self._g_eps, eps_list):
+            dst.copy_(e.detach())
+        self._ggraph.replay()
+        self.check_status(grads=True)
+        return self._g_fom, self._g_out
+
+    def _grad_body(self):
+        for i, e in zip(self._insts, self._g_eps):
+            i.ce[:, : i.W] = (i.spec.dt / e).to(self.dtype)
+        self._reset()
+        self._launch(True, True)
+        for n, i in enumerate(self._insts):
+            self._g_fom[n] = (i.acc * i.acc).sum()
+            torch.mul(i.acc, 2.0, out=i.gmon)
+            i.lam.zero_()
+            i.grad.zero_()
+        self._launch(False)
+        for i, e, out in zip(self._insts, self._g_eps, self._g_out):
+            torch.mul(i.grad[:, : i.W], -(i.spec.dt) / (e * e), out=out)
 
     def _graph_body(self):
         for i, e in zip(self._insts, self._static_eps):
