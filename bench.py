@@ -432,7 +432,7 @@ def run_ours(args):
                             "after one untimed call"}
         if fp64_check is not None:
             g32 = e_in.grad.to(dev, torch.float64)
-            fom32 = float(fom)
+            fom32 = float(fom.detach())
             del r, fom, e_in
             torch.cuda.empty_cache()
             s64 = dn.FDTDSolver3D(grid_shape=SHAPE, dl=DL, wavelength_nm=1550.0,

@@ -130,10 +130,10 @@ class StepHook:
             self._launch(_lib.PTR6(*fa), _lib.PTR6(*fb), ce)
             return tuple(out[i] for i in range(n))
         eng = self._padded_engine()
+        eng.cur_b = False  # the inputs go into set A, the step writes set B
         for i, c in enumerate(self.comps):
             eng.field(c).copy_(fields[i].reshape(self.shape3))
         eng.ce[..., : self.shape3[2]] = ce
-        eng.cur_b = False
         eng.run(0, 1)
         return tuple(eng.field(c).reshape(self.shape).clone().to(out_dev) for c in self.comps)
 

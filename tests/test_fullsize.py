@@ -81,7 +81,7 @@ def _gradient(cuda, cfg, dtype):
         e = eps.clone().to(cuda).requires_grad_(True)
         L = _fom(_solver(cuda, dtype).forward(e, source=dict(src), monitors=mons))
         L.backward()
-        _CACHE[key] = (float(L), e.grad.double().cpu())
+        _CACHE[key] = (float(L.detach()), e.grad.double().cpu())
         del e, L
         torch.cuda.empty_cache()
     return _CACHE[key]
