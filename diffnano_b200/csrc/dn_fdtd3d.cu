@@ -33,6 +33,12 @@ using namespace zm;
 constexpr int NRING_F = 7;  // Ex Ey Ez Hx Hy Hz ce
 constexpr int A_CE = 6;
 
+// resident CTAs per SM the work split plans for (a build-time override exists for
+// measurements of the split; the default is the occupancy the kernel is built for)
+#ifndef DN_FWD3D_PLAN_PER_SM
+#define DN_FWD3D_PLAN_PER_SM(minb) (minb)
+#endif
+
 // ring depth in planes (FP32: two CTAs per SM must fit 228 KB of shared memory)
 #ifndef DN_FWD3D_STAGES_F32
 #define DN_FWD3D_STAGES_F32 4
@@ -386,7 +392,7 @@ int run3d(const dn_grid* g, void* const fa[6], void* const fb[6], const void* ce
   DN_CUDA_CHECK(cudaGetDevice(&dev));
   DN_CUDA_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   long long nctas = 0;
-  const Plan plan = make_plan(g, (long long)nsm * FwdCfg<T>::MINB, &nctas);
+  const Plan plan = make_plan(g, (long long)nsm * DN_FWD3D_PLAN_PER_SM(FwdCfg<T>::MINB), &nctas);
   if (nctas > 0x7fffffffLL) return DN_EUNSUPPORTED;
   const size_t smem = L::bytes(plan.maxj);
   if (smem > 227 * 1024) return DN_EUNSUPPORTED;

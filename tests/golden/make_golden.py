@@ -1,7 +1,7 @@
 """Generate the golden fixtures in this folder by running DiffNano itself.
 
-Run once, in a container that has the reference checkout (read-only) at
-``/root/reference``::
+Run once, in a container that has the reference checkout (read-only); its
+location comes from ``DIFFNANO_REFERENCE`` (default ``/root/reference``)::
 
     PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden.py
 
@@ -22,7 +22,7 @@ import time
 import numpy as np
 import torch
 
-REF = "/root/reference"
+REF = os.environ.get("DIFFNANO_REFERENCE", "/root/reference")
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REF)
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
