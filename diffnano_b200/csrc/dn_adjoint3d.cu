@@ -56,13 +56,13 @@ __global__ void __launch_bounds__(NT, AdjCfg<T>::MINB)
   const Range R(plan, D);
   const int z0 = R.z0, z1 = R.z1, k0 = R.k0, j0 = R.j0;
 
-  const int nj = pipe_setup(sm, R, D, H, W, p.b, p.c, p.status);
+  const int nj = pipe_setup(sm, plan, D, H, W, p.b, p.c, p.status);
   if (nj == 0) return;
 
   if (warp == NCW) {
     const int slot = p.t - p.curl_t0;
     if (lane == 0)
-      producer_run<T, L, NRING_A, NTILE_A>(sm, tm, R, nj, p.status,
+      producer_run<T, L, NRING_A, NTILE_A>(sm, tm, plan.ntx, nj, p.status,
                                            [slot](int) { return slot; });
     return;
   }

@@ -65,6 +65,47 @@ class DensityAdam:
         return self.rho
 
 
+class OutputMap:
+    """Output-space map from the cross-section model to the 3-D focal field.
+
+    The 3-D lens is finite in y and the plane wave also passes beside it, so
+    the 3-D focal field is not the 2-D cross-section's; measured over very
+    different designs (uniform, random, cross-section optima) it is close to
+    an affine image of it, E3 = c S + b with complex c and b (7.6 % relative
+    residual over 13 designs, against 9.7 % for E3 = c S).  The map is fitted
+    by complex least squares to the (surrogate value, FDTD value) pairs of
+    every 3-D verification so far: with one pair b = 0 and c = E3 / S; with
+    more, both (Bandler et al.'s output space mapping, IEEE MTT 52, 2004)."""
+
+    def __init__(self):
+        self.s: List[complex] = []
+        self.e: List[complex] = []
+
+    def add(self, s: complex, e: complex) -> None:
+        self.s.append(complex(s))
+        self.e.append(complex(e))
+
+    def coef(self):
+        if not self.s:
+            return 1.0 + 0.0j, 0.0j
+        if len(self.s) == 1:
+            s0 = self.s[0] if abs(self.s[0]) > 0 else 1.0
+            return self.e[0] / s0, 0.0j
+        S = torch.tensor(self.s, dtype=torch.complex128)
+        E = torch.tensor(self.e, dtype=torch.complex128)
+        A = torch.stack([S, torch.ones_like(S)], 1)
+        sol = torch.linalg.lstsq(A, E[:, None]).solution[:, 0]
+        return complex(sol[0]), complex(sol[1])
+
+    def residual(self) -> float:
+        """Relative residual of the current fit over its pairs."""
+        if len(self.s) < 2:
+            return 0.0
+        c, b = self.coef()
+        num = sum(abs(c * s + b - e) ** 2 for s, e in zip(self.s, self.e))
+        return math.sqrt(num / sum(abs(e) ** 2 for e in self.e))
+
+
 @dataclass
 class Record:
     verification: int

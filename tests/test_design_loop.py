@@ -65,3 +65,22 @@ def test_surrogate_assisted_loop_runs(cuda):
     assert all(r.fom > 0 for r in h)
     assert out["timings"]["label_s"] > 0 and out["timings"]["train_s"] > 0
     assert 0.0 <= loop.proxy_error() < 10.0
+
+
+def test_output_map_fits_affine_pairs_exactly():
+    """Host logic of the cross-section -> 3-D output map: one pair gives the
+    ratio, two or more an affine fit; exact data give zero residual."""
+    from diffnano_b200.design.loop import OutputMap
+
+    m = OutputMap()
+    assert m.coef() == (1.0, 0.0)
+    c, b = 0.76 - 0.09j, -1890.0 + 662.0j
+    s0 = 6061.0 + 120.0j
+    m.add(s0, c * s0 + b)
+    c1, b1 = m.coef()
+    assert b1 == 0 and abs(c1 * s0 - (c * s0 + b)) < 1e-9
+    for s in (10121.0 - 50.0j, 63402.0 + 900.0j, 1367.0 + 10.0j):
+        m.add(s, c * s + b)
+    c2, b2 = m.coef()
+    assert abs(c2 - c) < 1e-9 and abs(b2 - b) < 1e-6
+    assert m.residual() < 1e-12

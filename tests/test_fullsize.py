@@ -178,3 +178,39 @@ def test_gradient_fp32_vs_fp64_full_grid(cuda, cfg1):
     assert abs(L32 / L64 - 1) < 1e-5
     assert err < 1e-4
     assert err_blk < 1e-4
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+def test_split_with_slabs_non_cubic_vs_oracle(cuda, dtype):
+    """A 128 x 256 x 256 grid with the physical CPML axes: like the 256^3
+    grid, its column ranges leave resident CTA slots idle, so the ends of the
+    ranges are marched by extra CTAs (several short slabs each).  12 steps
+    from a random state against the oracle."""
+    shape = (128, 256, 256)
+    D, H, W = shape
+    gen = torch.Generator().manual_seed(21)
+    eps = 1.5 + 2.0 * torch.rand(*shape, dtype=torch.float64, generator=gen)
+    src = {"type": "gaussian_pulse", "plane": "xy", "z": 20, "component": "Ex"}
+    mons = [{"component": "Ez", "plane": "xy", "z": 100, "extent": [[40, 200], [30, 220]],
+             "wavelengths_nm": [1500.0, 1600.0]}]
+    names = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
+    init = {k: torch.randn(*shape, dtype=torch.float64, generator=gen) for k in names}
+    t0, n = 600, 12
+    s = dn.FDTDSolver3D(grid_shape=shape, dl=25.0, pml_layers=12, n_steps=t0 + n, device=cuda,
+                        dtype=dtype, cpml_axes="physical")
+    eng = s._make_engine(t0 + n, src, mons)
+    torch.set_num_threads(os.cpu_count() or 1)
+    o = R.run_3d(eps, dl=25.0, dt=s.dt, omega=s.omega, pml_layers=12, n_steps=n, source=src,
+                 monitors=[{"component": "Ez", "box": eng.monitors[0].box,
+                            "wavelengths_nm": [1500.0, 1600.0]}],
+                 axes="physical", component="Ex", init=init, t0=t0)
+    eng.set_eps(eps.to(cuda))
+    for k in names:
+        eng.field(dn._lib.COMPONENTS[k]).copy_(init[k].to(cuda))
+    eng.run(t0, n)
+    eng.check_status()
+    tol = 1e-5 if dtype == torch.float32 else 1e-12
+    for k in names:
+        assert rel_l2(eng.field(dn._lib.COMPONENTS[k]), o[k]) < tol, k
+    dft = torch.view_as_real(eng.monitor_dft(0).cpu()).reshape(o["monitors"][0].shape)
+    assert rel_l2(dft, o["monitors"][0]) < tol
