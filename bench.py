@@ -708,8 +708,11 @@ def run_design(args):
                                            "projection, beta 1->32",
                        "fom": "|DFT Ey(1550 nm)|^2 at the focal point",
                        "plain": f"{args.design_iters} Adam iterations, FDTD forward+adjoint each",
-                       "surrogate": f"FNO on the 2-D cross-section, {cfg.n_train} batched-FDTD "
-                                    f"proxy labels, {cfg.n_candidates} candidates/iteration"},
+                       "surrogate": f"FNO trained on {cfg.n_train} batched-FDTD labels of the "
+                                    f"2-D cross-section prescreens {cfg.n_candidates} candidates "
+                                    f"per verification, the batched cross-section FDTD (mapped to "
+                                    f"3-D by a fitted output map) proposes and checks "
+                                    f"{cfg.n_check}, the 3-D FDTD verifies the best"},
             "plain": {"history": [{"n": r.verification, "t": round(r.wall_s, 2),
                                    "fom": r.fom / plain["fom0"], "beta": round(r.beta, 2)}
                                   for r in plain["history"]],
@@ -723,6 +726,7 @@ def run_design(args):
                          if res["best_fom"] else None,
                          "fdtd_verifications": res["verifications"],
                          "timings": res["timings"], "proxy_heldout_rel_l2": loop.proxy_error(),
+                         "output_map": res["map"], "candidates": res["candidates"],
                          "history": hist},
             "clocks": clocks.summary()}
     print(json.dumps(line), flush=True)

@@ -1,29 +1,21 @@
-"""Inverse-design loops: plain FDTD Adam, and surrogate-assisted (the
-surrogate proposes and prescreens, the FDTD verifies and judges).
+"""Inverse-design loops: plain FDTD Adam, and surrogate-assisted (a learned
+surrogate prescreens, the 3-D FDTD verifies and judges).
 
 The reference's two-stage driver (``diffnano/solvers/proxy_prescreen.py:147-274``,
 ``TwoStageOptimizer``: generate candidates, rank them with a fast proxy,
-evaluate the top ones with the full solver) is the pattern; here it runs
-inside a gradient loop:
+evaluate the top ones with the full solver) and its multi-fidelity designer
+(``diffnano/design/multifidelity.py:277-470``: screen cheaply, verify the top
+ones expensively) are the pattern; here they run inside a gradient loop:
 
 * :func:`plain_loop` -- every iteration evaluates the design with the 3-D FDTD
   forward + adjoint and takes an Adam step on the density (``dn_adam``), with
   the projection sharpness beta raised from ``beta[0]`` to ``beta[1]``
   (``beta_continuation_schedule``).
-* :class:`SurrogateAssistedLoop` -- a Fourier neural operator S trained on the
-  2-D proxy (labelled by the batched FDTD) is corrected to first order at the
-  accepted design rho_k (model m(rho) = f_k + S(rho) - S(rho_k) + (g_k -
-  grad S(rho_k)) . (rho - rho_k), which matches the FDTD value f_k and
-  gradient g_k there: first-order model management, Alexandrov et al.,
-  Structural Optimization 15, 1998).  Adam on m from rho_k (beta ramped to the
-  next outer value) proposes a path; ``n_candidates`` snapshots of it are
-  ranked by m in one batched inference and the best goes to the 3-D FDTD
-  forward + adjoint.  It is accepted when its FDTD figure of merit does not
-  fall more than ``tolerance`` below the last accepted one; otherwise the loop
-  falls back to a plain Adam step from rho_k with g_k.  The inner step size is
-  a trust region: doubled when the FDTD gain is at least 3/4 of the predicted
-  one, quartered on a rejection.  Every verified sample also fine-tunes the
-  network.  Wall time includes the proxy labelling and the training.
+* :class:`SurrogateAssistedLoop` -- candidates proposed on the 2-D cross-
+  section (mapped to the 3-D focal field by :class:`OutputMap`), ranked by a
+  Fourier neural operator trained on batched-FDTD labels, checked by the
+  batched cross-section FDTD, verified by the 3-D FDTD.  Wall time includes the
+  proxy labelling and the network's training.
 """
 from __future__ import annotations
 
@@ -112,7 +104,7 @@ class Record:
     wall_s: float
     fom: float
     beta: float
-    kind: str  # "adam", "surrogate", "fallback"
+    kind: str  # "adam" (plain loop); "start", "warm start", "surrogate" (assisted loop)
     accepted: bool = True
 
 
@@ -140,27 +132,66 @@ def plain_loop(problem: Metalens3D, rho0: torch.Tensor, iters: int = 100, lr: fl
 
 @dataclass
 class SurrogateConfig:
-    n_train: int = 4096
+    n_train: int = 2048          # proxy designs labelled by the batched 2-D FDTD
     epochs: int = 20
     batch: int = 256
     lr: float = 1e-3
-    n_candidates: int = 32
-    inner_steps: int = 32
+    warm_steps: int = 60         # warm start: Adam steps on the mapped cross-section model
+    warm_lr: float = 0.05
+    inner_steps: int = 8         # trust-region path per verification (one snapshot per step)
+    n_scales: int = 4            # step-length variants per snapshot: candidates = steps * scales
+    n_check: int = 4             # candidates the FNO passes on to the 2-D FDTD
     inner_lr: float = 0.02
-    max_inner_lr: float = 0.16
+    max_inner_lr: float = 0.2
     min_inner_lr: float = 1e-4
-    outer_schedule: int = 10  # outer iterations over which beta reaches its end value
     max_verify: int = 40
-    tolerance: float = 0.02
-    ft_steps: int = 10
+    ft_steps: int = 5
     ft_lr: float = 2e-4
-    fallback_lr: float = 0.02
     seed: int = 0
     fno: FNOConfig = field(default_factory=lambda: FNOConfig(H=40, W=256, eps_lo=1.0,
                                                              eps_hi=12.1))
 
+    @property
+    def n_candidates(self) -> int:
+        return self.inner_steps * self.n_scales
+
 
 class SurrogateAssistedLoop:
+    """Surrogate-assisted design loop: the 3-D FDTD judges every accepted step.
+
+    Three models of the FOM, cheapest first:
+
+    * the FNO (trained on batched-FDTD labels of the cross-section, fine-tuned
+      on every cross-section the loop evaluates) prescreens ``n_candidates``
+      candidate steps per verification in one batched inference and passes
+      ``n_check`` on;
+    * the cross-section FDTD (2-D, ~0.07 s for a value and its adjoint
+      gradient; batched for the checks), mapped to the 3-D focal field by an
+      :class:`OutputMap` fitted to every verification so far, proposes the
+      steps and checks the prescreened candidates;
+    * the 3-D FDTD forward + adjoint verifies the best checked candidate.
+
+    Run: (1) the 3-D FOM and gradient at the start design; (2) warm start:
+    Adam on the mapped cross-section model with beta ramped to its end value
+    (the cross-section's optimum is a good 3-D design, about half the 3-D
+    optimum's FOM), verified in 3-D; (3) trust-region steps at the end beta:
+    the cross-section model corrected to first order at the accepted design
+    rho_k, m(rho) = f_k + M(rho) - M(rho_k) + (g_k - grad M(rho_k)) . (rho -
+    rho_k), which matches the 3-D value and gradient there (first-order model
+    management, Alexandrov et al., Structural Optimization 15, 1998); Adam on m
+    gives ``inner_steps`` snapshots, each at ``n_scales`` step lengths; the FNO
+    ranks them, the cross-section FDTD checks the top ``n_check``, the best goes
+    to 3-D.  Accepted when its FOM does not fall; the step size grows when the
+    gain reaches half the predicted one and shrinks on a rejection.  Wall time
+    includes the proxy labelling and the network's training.
+
+    Measured limits that bound the speed-up: the cross-section alone saturates at about x47 of the start's 3-D FOM, so the
+    rest of the way needs 3-D gradients; and the network, held-out error ~0.6
+    on the cross-section labels, cannot propose designs itself (ascending its
+    own prediction leads to designs it overrates by orders of magnitude), so
+    it only ranks.
+    """
+
     def __init__(self, problem: Metalens3D, cfg: SurrogateConfig = SurrogateConfig(),
                  proxy: Optional[Proxy2D] = None):
         self.problem = problem
@@ -171,6 +202,7 @@ class SurrogateAssistedLoop:
         self.proxy = proxy or Proxy2D(s, device=problem.device)
         self.net = FNO2d(cfg.fno, problem.device, seed=cfg.seed)
         self.scale = 1.0
+        self.map = OutputMap()
         self.timings: Dict[str, float] = {}
         self._buf_x: List[torch.Tensor] = []
         self._buf_y: List[torch.Tensor] = []
@@ -211,49 +243,18 @@ class SurrogateAssistedLoop:
         pred = from_targets(self.net.forward(eps).clone(), self.scale, labels.shape[1])
         return float(rel_l2_per_sample(pred, labels).mean())
 
-    def _focal(self, pred: torch.Tensor) -> torch.Tensor:
+    def _fno_focal(self, eps_design: torch.Tensor) -> torch.Tensor:
+        """Network's complex focal value (centre wavelength) for a batch."""
         s = self.problem.setup
         li, fc = s.center_index, s.focus_col
-        return pred[:, fc, 2 * li] ** 2 + pred[:, fc, 2 * li + 1] ** 2
-
-    def predict_fom(self, eps_design: torch.Tensor) -> torch.Tensor:
-        return self._focal(self.net.forward(eps_design)) * self.scale ** 2
-
-    def _value_grad(self, rho: torch.Tensor, beta: float):
-        """Surrogate focal intensity S(rho) and dS/drho (FOM units)."""
-        s = self.problem.setup
-        W = s.design_shape[1]
-        li, fc = s.center_index, s.focus_col
-        x = rho.detach().clone().requires_grad_(True)
-        eps = s.eps_design(x, beta).unsqueeze(0)
-        pred = self.net.forward(eps.detach())
-        value = self._focal(pred)[0] * self.scale ** 2
-        gout = torch.zeros(W, OUT_LD, device=x.device)
-        gout[fc, 2 * li] = -2.0 * pred[0, fc, 2 * li]
-        gout[fc, 2 * li + 1] = -2.0 * pred[0, fc, 2 * li + 1]
-        self.net._bwd_workspace(1)["gout"].copy_(gout.to(torch.bfloat16))
-        deps = self.net.backward(B=1, want_input_grad=True)  # d(-S/scale^2)/d eps
-        eps.backward(deps)
-        return float(value), -x.grad * self.scale ** 2
-
-    def _ascent(self, rho: torch.Tensor, b0: float, b1: float, corr: torch.Tensor,
-                steps: int, lr: float, fom_ref: float) -> List[torch.Tensor]:
-        """Adam (learning rate ``lr``) on the corrected model m = S + corr .
-        (rho - rho_k); density snapshots along the path (the candidates)."""
-        c = self.cfg
-        opt = DensityAdam(rho, lr)
-        every = max(1, steps // c.n_candidates)
-        snaps = []
-        for k in range(steps):
-            b = b0 * (b1 / b0) ** ((k + 1) / steps)
-            _, dS = self._value_grad(opt.rho, b)
-            opt.ascend(dS + corr, 1.0 / fom_ref)
-            if (k + 1) % every == 0:
-                snaps.append(opt.rho.clone())
-        return snaps[-c.n_candidates:]
+        pred = self.net.forward(eps_design)
+        return torch.complex(pred[:, fc, 2 * li].double(),
+                             pred[:, fc, 2 * li + 1].double()) * self.scale
 
     def _fine_tune(self) -> None:
         c = self.cfg
+        if not self._buf_x:
+            return
         X = torch.stack(self._buf_x)
         Y = torch.stack(self._buf_y)
         n = X.shape[0]
@@ -267,9 +268,17 @@ class SurrogateAssistedLoop:
             self.net.backward(B=B)
             self.net.adam_step(lr=c.ft_lr)
 
-    def _record_sample(self, eps_design: torch.Tensor, dft_line: torch.Tensor) -> None:
-        self._buf_x.append(eps_design.detach().to(torch.float32))
-        self._buf_y.append(to_targets(dft_line.unsqueeze(0), self.scale)[0])
+    # ---- models -------------------------------------------------------------------
+    def _mapped(self, rho: torch.Tensor, beta: float, grad: bool):
+        """(cross-section focal value, mapped intensity M, dM/drho)."""
+        cc, bb = self.map.coef()
+        return self.proxy.focal(rho, beta, cc, bb, grad=grad)
+
+    def _verify(self, rho: torch.Tensor, beta: float):
+        """3-D FDTD forward + adjoint: (FOM, gradient, complex focal value)."""
+        s = self.problem.setup
+        f, g, dft = self.problem.evaluate(rho, beta, grad=True)
+        return f, g, complex(dft[s.center_index, s.focus_col])
 
     # ---- loop -------------------------------------------------------------------
     def run(self, rho0: torch.Tensor, target: Optional[float] = None,
@@ -281,64 +290,90 @@ class SurrogateAssistedLoop:
         self.prepare()
         hist: List[Record] = []
         cand_stats = []
-        rho = rho0.to(dev, torch.float32).clone()
-        b = beta[0]
-        fom, grad, dft = p.evaluate(rho, b, grad=True)
-        self._record_sample(s.eps_design(rho, b).detach(), dft)
-        hist.append(Record(1, time.perf_counter() - t0, fom, b, "start"))
-        fallback = DensityAdam(rho, c.fallback_lr)
-        fom0 = fom
         reached = None
-        steps = c.inner_steps
-        lr = c.inner_lr  # trust region: the inner path's step size
-        o = 0
-        while len(hist) < c.max_verify:
-            o += 1
-            b_next = beta_continuation_schedule(o, c.outer_schedule, beta[0], beta[1])
-            # first-order correction: the model matches the FDTD value and
-            # gradient at the accepted design
-            s0, dS0 = self._value_grad(rho, b)
-            corr = grad - dS0
-            snaps = self._ascent(rho, b, b_next, corr, steps, lr, fom0)
+        b_end = beta[1]
+
+        def done(fom, b):
+            return target is not None and b >= b_end * (1 - 1e-9) and fom >= 0.99 * target
+
+        # (1) the start design
+        rho = rho0.to(dev, torch.float32).clone()
+        fom, grad, e3 = self._verify(rho, beta[0])
+        fom0 = fom
+        e2, _, _ = self.proxy.focal(rho, beta[0])
+        self.map.add(e2, e3)
+        hist.append(Record(1, time.perf_counter() - t0, fom, beta[0], "start"))
+        # (2) warm start on the mapped cross-section model, beta ramped
+        opt = DensityAdam(rho, c.warm_lr)
+        _, m_ref, _ = self._mapped(rho, beta[0], grad=False)
+        for k in range(c.warm_steps):
+            b = beta[0] * (b_end / beta[0]) ** (k / max(1, c.warm_steps - 1))
+            _, _, gm = self._mapped(opt.rho, b, grad=True)
+            opt.ascend(gm, 1.0 / max(m_ref, 1e-30))
+        cand = opt.rho.clone()
+        f_w, g_w, e3_w = self._verify(cand, b_end)
+        e2_w, _, _ = self.proxy.focal(cand, b_end)
+        self.map.add(e2_w, e3_w)
+        hist.append(Record(2, time.perf_counter() - t0, f_w, b_end, "warm start"))
+        # the start was judged at beta[0]; the warm start, at the end beta, is the new base
+        b = b_end
+        rho, fom, grad = cand, f_w, g_w
+        if done(fom, b):
+            reached = time.perf_counter() - t0
+        lr = c.inner_lr
+        # (3) trust-region steps on the corrected model
+        while reached is None and len(hist) < c.max_verify:
+            e2_k, m_k, dm_k = self._mapped(rho, b, grad=True)
+            corr = grad - dm_k
+            inner = DensityAdam(rho, lr)
+            snaps = []
+            for _ in range(c.inner_steps):
+                _, _, dm = self._mapped(inner.rho, b, grad=True)
+                inner.ascend(dm + corr, 1.0 / fom0)
+                snaps.append(inner.rho.clone())
+            scales = torch.linspace(0.5, 2.0, c.n_scales).tolist()
+            cands = torch.stack([(rho + sc * (sn - rho)).clamp(0.0, 1.0)
+                                 for sn in snaps for sc in scales])
+            lin = ((cands - rho) * corr).flatten(1).sum(1).double()
+            cc, bb = self.map.coef()
             with torch.no_grad():
-                eps_c = torch.stack([s.eps_design(r, b_next) for r in snaps])
-                S = self.predict_fom(eps_c)
-                lin = torch.stack([(corr * (r - rho)).sum() for r in snaps])
-                model = fom + (S - s0) + lin
-            best = int(torch.argmax(model))
-            cand = snaps[best]
-            f_new, g_new, dft_new = p.evaluate(cand, b_next, grad=True)
-            self._record_sample(eps_c[best], dft_new)
-            ok = f_new >= (1.0 - c.tolerance) * fom
-            hist.append(Record(len(hist) + 1, time.perf_counter() - t0, f_new, b_next,
-                               "surrogate", ok))
-            predicted = float(model[best])
-            cand_stats.append({"model_best": predicted, "fdtd": f_new, "fom_before": fom,
-                               "inner_lr": lr, "pick": best})
-            gain_pred = predicted - fom
-            ratio = (f_new - fom) / gain_pred if gain_pred > 0 else 0.0
+                eps_c = torch.stack([s.eps_design(r, b) for r in cands])
+                fno_e = self._fno_focal(eps_c)
+                fno_k = self._fno_focal(s.eps_design(rho, b).unsqueeze(0))[0]
+                pre = fom + ((cc * fno_e + bb).abs() ** 2 - abs(cc * fno_k + bb) ** 2) + lin
+                top = torch.topk(pre, min(c.n_check, len(cands))).indices
+                labels = self.proxy.label(eps_c[top])  # batched cross-section FDTD
+            e2_top = labels[:, s.center_index, s.focus_col]
+            model = fom + ((cc * e2_top + bb).abs() ** 2 - m_k) + lin[top]
+            j = int(torch.argmax(model))
+            pick = int(top[j])
+            for e_, l_ in zip(eps_c[top], labels):
+                self._buf_x.append(e_.float())
+                self._buf_y.append(to_targets(l_.unsqueeze(0), self.scale)[0])
+            f_new, g_new, e3_new = self._verify(cands[pick], b)
+            self.map.add(complex(e2_top[j]), e3_new)
+            ok = f_new >= fom
+            hist.append(Record(len(hist) + 1, time.perf_counter() - t0, f_new, b, "surrogate",
+                               ok))
+            predicted = float(model[j])
+            cand_stats.append({"predicted": predicted, "fdtd": f_new, "fom_before": fom,
+                               "lr": lr, "pick": pick, "fno_rank_of_pick": int(j),
+                               "map_residual": self.map.residual()})
             if ok:
-                rho, fom, grad, b = cand.clone(), f_new, g_new, b_next
-                if ratio > 0.75:
-                    lr = min(c.max_inner_lr, 2.0 * lr)
+                if f_new - fom >= 0.5 * max(predicted - fom, 0.0):
+                    lr = min(c.max_inner_lr, 1.5 * lr)
+                rho, fom, grad = cands[pick].clone(), f_new, g_new
             else:
-                lr = max(c.min_inner_lr, 0.25 * lr)
-                # plain step from the accepted design with its FDTD gradient
-                fallback.rho.copy_(rho)
-                r2 = fallback.ascend(grad, 1.0 / fom0).clone()
-                f2, g2, d2 = p.evaluate(r2, b_next, grad=True)
-                self._record_sample(s.eps_design(r2, b_next).detach(), d2)
-                hist.append(Record(len(hist) + 1, time.perf_counter() - t0, f2, b_next,
-                                   "fallback"))
-                rho, fom, grad, b = r2, f2, g2, b_next
+                lr = max(c.min_inner_lr, 0.3 * lr)
             self._fine_tune()
-            if target is not None and b >= beta[1] * (1 - 1e-9) and fom >= 0.99 * target:
+            if done(fom, b):
                 reached = time.perf_counter() - t0
-                break
         torch.cuda.synchronize(dev)
-        at_end = [r.fom for r in hist if r.beta >= beta[1] * (1 - 1e-9)]
+        at_end = [r.fom for r in hist if r.beta >= b_end * (1 - 1e-9)]
         return {"rho": rho, "history": hist, "final_fom": fom,
                 "best_fom": max(at_end) if at_end else None,
                 "wall_s": time.perf_counter() - t0, "time_to_target_s": reached,
                 "verifications": p.evaluations, "timings": dict(self.timings),
-                "candidates": cand_stats, "fom0": fom0}
+                "candidates": cand_stats, "fom0": fom0,
+                "map": {"coef": [str(v) for v in self.map.coef()],
+                        "residual": self.map.residual()}}

@@ -180,6 +180,43 @@ class Proxy2D:
             eps_design.to(self.device, torch.float64)
         return eps
 
+    def _solver2d(self):
+        if getattr(self, "_s2d", None) is None:
+            from ..solvers.fdtd2d import FDTDSolver2D
+
+            s = self.setup
+            D, W = self.grid
+            self._s2d = FDTDSolver2D(grid_shape=(D, W), dl=s.dl, wavelength_nm=s.center_nm,
+                                     polarization="TM", pml_layers=s.pml, n_steps=s.n_steps,
+                                     courant=self.courant2d, device=self.device,
+                                     dtype=torch.float32)
+            fc = W // 2
+            self._mon = [{"component": "Ez", "box": [[s.focus_z, s.focus_z + 1], [fc, fc + 1]],
+                          "wavelengths_nm": [s.center_nm]}]
+        return self._s2d
+
+    def focal(self, rho: torch.Tensor, beta: float, c: complex = None, b: complex = 0j,
+              grad: bool = False):
+        """Complex focal-point DFT (centre wavelength) of the cross-section for
+        density ``rho``, by one 2-D FDTD solve; with ``c`` given, also the
+        mapped intensity |c e + b|^2 and, with ``grad``, its gradient with
+        respect to ``rho`` (the 2-D adjoint kernels).  Returns (e, value,
+        gradient or None)."""
+        s = self.setup
+        solver = self._solver2d()
+        x = rho.detach().to(self.device, torch.float32).clone().requires_grad_(grad)
+        with torch.set_grad_enabled(grad):
+            eps = self.full_eps(s.eps_design(x, beta).unsqueeze(0))[0].to(torch.float32)
+            r = solver.forward(eps, source=s.source(False), monitors=self._mon)
+            e = r.metadata["monitors"][0]["dft"].reshape(-1)[0]
+            self.cell_steps += self.grid[0] * self.grid[1] * s.n_steps * (3 if grad else 1)
+            if c is None:
+                return complex(e.detach()), None, None
+            v = (c * e + b).abs() ** 2
+            if grad:
+                v.backward()
+        return complex(e.detach()), float(v.detach()), (x.grad.detach() if grad else None)
+
     @torch.no_grad()
     def label(self, eps_design: torch.Tensor) -> torch.Tensor:
         """(n, 40, 256) design eps -> complex128 (n, L, 256) focal-row DFTs."""
