@@ -1052,7 +1052,7 @@ def main():
                     help="scale the step counts (1 is the workload; smaller for profiling)")
     ap.add_argument("--fno-batch", type=int, default=256)
     ap.add_argument("--design-iters", type=int, default=100)
-    ap.add_argument("--design-max-verify", type=int, default=40)
+    ap.add_argument("--design-max-verify", type=int, default=60)
     ap.add_argument("--design-scale", type=int, default=1,
                     help="shrink the design workload's grid by this factor (tests)")
     ap.add_argument("--fno-samples", type=int, default=20000)

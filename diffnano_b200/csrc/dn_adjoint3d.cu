@@ -34,12 +34,6 @@ constexpr int NRING_A = 7;  // lEx lEy lEz lHx lHy lHz ce
 constexpr int NTILE_A = 3;  // curl x y z of the step
 constexpr int A_CE = 6;
 
-// the work split of dn_zmarch.cuh with slabs for extra CTAs (1) or one z range
-// per CTA (0)
-#ifndef DN_ADJ3D_SLABS
-#define DN_ADJ3D_SLABS 1
-#endif
-
 template <typename T>
 struct AdjCfg {
   static constexpr int S = sizeof(T) == 4 ? 4 : 3;
@@ -59,30 +53,49 @@ __global__ void __launch_bounds__(NT, AdjCfg<T>::MINB)
   const int D = p.D, H = p.H, W = p.W;
   const long long py = p.py, pz = p.pz;
   const T dt = p.dt, idl = p.inv_dl;
+  const Range R(plan, D);
+  const int z0 = R.z0, z1 = R.z1, k0 = R.k0, j0 = R.j0;
 
-  const int nj = pipe_setup(sm, plan, D, H, W, p.b, p.c, p.status);
+  const int nj = pipe_setup(sm, R, D, H, W, p.b, p.c, p.status);
   if (nj == 0) return;
 
   if (warp == NCW) {
     const int slot = p.t - p.curl_t0;
     if (lane == 0)
-      producer_run<T, L, NRING_A, NTILE_A>(sm, tm, plan.ntx, nj, p.status,
+      producer_run<T, L, NRING_A, NTILE_A>(sm, tm, R, nj, p.status,
                                            [slot](int) { return slot; });
     return;
   }
 
   volatile int* s_abort = sm.flags + 1;
   const int w = warp;
+  const int ja = j0 + 2 * w;
+  const int k = k0 + lane;
+  const bool kin = k < W;
   const T dti = dt * idl;
-  // Geometry and coefficients of the forward step for the current segment,
-  // boundary rules folded in (see dn_fdtd3d.cu); "p1" = at the +1 neighbour
-  // along the named axis
-  int z0 = 0, z1 = 0, k0 = 0, j0 = 0, ja = 0, k = 0;
-  bool kin = false;
-  T bK, gK, gKp1, bKh, gKh, gK0, kf, kb, cKf, cKb, cKbp1, cKfh, cKbh;
+  // coefficients of the forward step, boundary rules folded in (see
+  // dn_fdtd3d.cu); "p1" = at the +1 neighbour along the named axis
+  const T bK = sm.sbK[lane + 1], gK = sm.sgK[lane + 1];
+  const T gKp1 = sm.sgK[lane + 2];  // column k+1
+  const T bKh = sm.sbK[0], gKh = sm.sgK[0], gK0 = sm.sgK[1];  // columns k0-1, k0
+  const T kf = (k < W - 1) ? T(1) : T(0);
+  const T kb = (k > 0) ? T(1) : T(0);
+  const T cKf = kf * dti * gK;     // forward x, H update
+  const T cKb = kb * gK * idl;     // backward x, E update
+  const T cKbp1 = gKp1 * idl;      // backward x at column k+1 (k+1 > 0)
+  const T cKfh = dti * gKh;        // forward x at column k0-1 (k0-1 < W-1)
+  const T cKbh = (k0 > 1) ? gKh * idl : T(0);  // backward x at column k0-1
   T bJ[4], gJ[4], cJf[4], cJb[4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {  // rows ja-1 .. ja+2
+    const int j = ja + r - 1;
+    bJ[r] = sm.sbJ[2 * w + r];
+    gJ[r] = sm.sgJ[2 * w + r];
+    cJf[r] = (j < H - 1) ? dti * gJ[r] : T(0);
+    cJb[r] = (j > 0) ? gJ[r] * idl : T(0);
+  }
   // z-1 terms of rows ja, ja+1: vx_i = hx_c2 lHx', vy_i = hy_c1 lHy' of the plane below
-  T pvxi[2], pvyi[2];
+  T pvxi[2] = {T(0), T(0)}, pvyi[2] = {T(0), T(0)};
   int q = 0;
 
   auto wait_full = [&](int qa) -> bool {
@@ -148,180 +161,137 @@ __global__ void __launch_bounds__(NT, AdjCfg<T>::MINB)
     lhz = cur[DN_HZ * AE + e] + (cJb[r] * ux - cJb[r + 1] * ux_j) - (eyc2 * uy - eyc2p1 * uy_k);
   };
 
-#pragma unroll 1
-  for (int gseg = 0; gseg < plan_nseg(plan, blockIdx.x); ++gseg) {
-    const Range R(plan, plan_seg(plan, D, blockIdx.x, gseg));
-    z0 = R.z0;
-    z1 = R.z1;
-    k0 = R.k0;
-    j0 = R.j0;
-    ja = j0 + 2 * w;
-    k = k0 + lane;
-    kin = k < W;
-    // profile values of column x (1 outside the grid, as the tables held)
-    auto colb = [&](int x) { return x >= 0 && x < W ? static_cast<T>(__ldg(p.b[2] + x)) : T(1); };
-    auto colg = [&](int x) {
-      return x >= 0 && x < W ? static_cast<T>(1.0 + __ldg(p.c[2] + x)) : T(1);
-    };
-    bK = colb(k);
-    gK = colg(k);
-    gKp1 = colg(k + 1);  // column k+1
-    bKh = colb(k0 - 1);  // columns k0-1, k0
-    gKh = colg(k0 - 1);
-    gK0 = colg(k0);
-    kf = (k < W - 1) ? T(1) : T(0);
-    kb = (k > 0) ? T(1) : T(0);
-    cKf = kf * dti * gK;     // forward x, H update
-    cKb = kb * gK * idl;     // backward x, E update
-    cKbp1 = gKp1 * idl;      // backward x at column k+1 (k+1 > 0)
-    cKfh = dti * gKh;        // forward x at column k0-1 (k0-1 < W-1)
-    cKbh = (k0 > 1) ? gKh * idl : T(0);  // backward x at column k0-1
+  // ---- warm-up: z-1 terms from plane z0-1 ------------------------------------
+  if (z0 > 0) {
+    if (!(wait_full(q) && wait_full(q + 1))) {
+      fail();
+      return;
+    }
+    const int i = z0 - 1;
+    T e_ci, hx_c2, hy_c1, hy_b, bI;
+    i_roles(i, e_ci, hx_c2, hy_c1, hy_b, bI);
+    const T e_ci_n = e_ci_at(i + 1);
+    const T* cur = sm.arr(q, 0) + 2 * w * BX + lane + 4;
+    const T* nxt = sm.arr(q + 1, 0) + 2 * w * BX + lane + 4;
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {  // rows ja-1 .. ja+2
-      const int j = ja + r - 1;
-      const bool jok = j >= 0 && j < H;
-      bJ[r] = jok ? static_cast<T>(__ldg(p.b[1] + j)) : T(1);
-      gJ[r] = jok ? static_cast<T>(1.0 + __ldg(p.c[1] + j)) : T(1);
-      cJf[r] = (j < H - 1) ? dti * gJ[r] : T(0);
-      cJb[r] = (j > 0) ? gJ[r] * idl : T(0);
+    for (int r = 1; r < 3; ++r) {
+      T lhx, lhy, lhz;
+      lam_h(cur, nxt, r, e_ci, e_ci_n, i > 0 ? T(1) : T(0), T(1), lhx, lhy, lhz);
+      pvxi[r - 1] = hx_c2 * lhx;  // i < D-1 here
+      pvyi[r - 1] = hy_c1 * lhy;
     }
-    pvxi[0] = pvxi[1] = pvyi[0] = pvyi[1] = T(0);
-
-    // ---- warm-up: z-1 terms from plane z0-1 ------------------------------------
-    if (z0 > 0) {
-      if (!(wait_full(q) && wait_full(q + 1))) {
-        fail();
-        return;
-      }
-      const int i = z0 - 1;
-      T e_ci, hx_c2, hy_c1, hy_b, bI;
-      i_roles(i, e_ci, hx_c2, hy_c1, hy_b, bI);
-      const T e_ci_n = e_ci_at(i + 1);
-      const T* cur = sm.arr(q, 0) + 2 * w * BX + lane + 4;
-      const T* nxt = sm.arr(q + 1, 0) + 2 * w * BX + lane + 4;
-  #pragma unroll
-      for (int r = 1; r < 3; ++r) {
-        T lhx, lhy, lhz;
-        lam_h(cur, nxt, r, e_ci, e_ci_n, i > 0 ? T(1) : T(0), T(1), lhx, lhy, lhz);
-        pvxi[r - 1] = hx_c2 * lhx;  // i < D-1 here
-        pvyi[r - 1] = hy_c1 * lhy;
-      }
-      release(q);
-      ++q;
-    }
-
-    // ---- march -----------------------------------------------------------------
-    for (int i = z0; i < z1; ++i) {
-      const bool has_next = (i + 1 < D);
-      if ((i == 0 && !wait_full(q)) || (has_next && !wait_full(q + 1))) {
-        fail();
-        return;
-      }
-      T e_ci, hx_c2, hy_c1, hy_b, bI;
-      i_roles(i, e_ci, hx_c2, hy_c1, hy_b, bI);
-      const T e_ci_n = has_next ? e_ci_at(i + 1) : T(0);
-      const T fi_prev = i > 0 ? T(1) : T(0);
-      const T fi_next = has_next ? T(1) : T(0);
-      const T* cur = sm.arr(q, 0) + 2 * w * BX + lane + 4;
-      const T* nxt = has_next ? sm.arr(q + 1, 0) + 2 * w * BX + lane + 4 : cur;
-      // issue the FP64 gradient loads now; they are consumed after lH'
-      const long long o_plane = i * pz + (long long)ja * py + k;
-      double gpre[2];
-  #pragma unroll
-      for (int r = 1; r < 3; ++r)
-        gpre[r - 1] = (ja + r - 1 < H && kin) ? p.grad[o_plane + (r - 1) * py] : 0.0;
-
-      // ---- lH' of rows ja-1, ja, ja+1 --------------------------------------
-      T LHx[3], LHy[3], LHz[3];
-  #pragma unroll
-      for (int r = 0; r < 3; ++r)
-        lam_h(cur, nxt, r, e_ci, e_ci_n, fi_prev, fi_next, LHx[r], LHy[r], LHz[r]);
-
-      // ---- k0-1 halo column: lHy', lHz' of rows ja, ja+1 (lanes 0, 1) -------
-      // v_k terms there: vy_k = hy_c2 lHy', vz_k = cKf lHz'
-      T hvyk = T(0), hvzk = T(0);
-      if (lane < 2 && k0 > 0) {
-        const int r = 1 + lane;
-        const T gJr = lane == 0 ? gJ[1] : gJ[2];
-        const T cJbr = lane == 0 ? cJb[1] : cJb[2];
-        const T cJbr1 = lane == 0 ? cJb[2] : cJb[3];
-        const int e = r * BX - 1 - lane;  // column k0-1 (pointers sit at k0+lane)
-        const T ce = cur[A_CE * AE + e];
-        const T ux = ce * cur[DN_EX * AE + e], uy = ce * cur[DN_EY * AE + e],
-                uz = ce * cur[DN_EZ * AE + e];
-        const T ce_j = cur[A_CE * AE + e + BX];
-        const T ux_j = ce_j * cur[DN_EX * AE + e + BX];
-        const T ce_k = cur[A_CE * AE + e + 1];
-        const T uy_k = ce_k * cur[DN_EY * AE + e + 1], uz_k = ce_k * cur[DN_EZ * AE + e + 1];
-        const T ce_i = nxt[A_CE * AE + e];
-        const T ux_i = ce_i * nxt[DN_EX * AE + e];
-        const T eci = (AXES == DN_AXES_REFERENCE ? gKh * idl : e_ci) * fi_prev;
-        const T ecin = (AXES == DN_AXES_REFERENCE ? gKh * idl : e_ci_n) * fi_next;
-        const T cKb0 = gK0 * idl;  // backward x at column k0 (> 0)
-        const T eyc2 = AXES == DN_AXES_REFERENCE ? (k0 > 1 ? gJr * idl : T(0)) : cKbh;
-        const T eyc2p1 = AXES == DN_AXES_REFERENCE ? gJr * idl : cKb0;
-        const T lhy = cur[DN_HY * AE + e] - (eci * ux - ecin * ux_i) + (cKbh * uz - cKb0 * uz_k);
-        const T lhz = cur[DN_HZ * AE + e] + (cJbr * ux - cJbr1 * ux_j) - (eyc2 * uy - eyc2p1 * uy_k);
-        const T hyc2 = AXES == DN_AXES_REFERENCE ? dti * gJr : cKfh;
-        hvyk = hyc2 * lhy;
-        hvzk = cKfh * lhz;
-      }
-      const T hvyk0 = __shfl_sync(FULL_MASK, hvyk, 0), hvyk1 = __shfl_sync(FULL_MASK, hvyk, 1);
-      const T hvzk0 = __shfl_sync(FULL_MASK, hvzk, 0), hvzk1 = __shfl_sync(FULL_MASK, hvzk, 1);
-
-      // ---- previous adjoint fields of rows ja, ja+1 ---------------------------
-      const T* ct = sm.tile_arr(q, NRING_A, 0) + (2 * w) * TX + lane;
-      constexpr int TE = L::TILE_ARR / (int)sizeof(T);
-  #pragma unroll
-      for (int r = 1; r < 3; ++r) {
-        const int j = ja + r - 1;
-        const T hyc2 = AXES == DN_AXES_REFERENCE ? kf * dti * gJ[r] : cKf;
-        // v terms of this lane
-        const T vxj = cJf[r] * LHx[r], vzj = cJf[r] * LHz[r];
-        const T vxi = has_next ? hx_c2 * LHx[r] : T(0);
-        const T vyi = has_next ? hy_c1 * LHy[r] : T(0);
-        const T vyk = hyc2 * LHy[r], vzk = cKf * LHz[r];
-        // -1 neighbours
-        const T vxj_m = cJf[r - 1] * LHx[r - 1], vzj_m = cJf[r - 1] * LHz[r - 1];
-        T vyk_m = __shfl_up_sync(FULL_MASK, vyk, 1);
-        T vzk_m = __shfl_up_sync(FULL_MASK, vzk, 1);
-        if (lane == 0) {
-          vyk_m = r == 1 ? hvyk0 : hvyk1;
-          vzk_m = r == 1 ? hvzk0 : hvzk1;
-        }
-        if (j < H && kin) {
-          const int e = r * BX;
-          const T lex = cur[DN_EX * AE + e], ley = cur[DN_EY * AE + e], lez = cur[DN_EZ * AE + e];
-          const T ex_b = AXES == DN_AXES_REFERENCE ? bJ[r] * bK : bJ[r] * bI;
-          const T ey_b = AXES == DN_AXES_REFERENCE ? bK * bJ[r] : bI * bK;
-          const T ez_b = bK * bJ[r];
-          const T nlex = ex_b * lex + (vyi - pvyi[r - 1]) - (vzj - vzj_m);
-          const T nley = ey_b * ley - (vxi - pvxi[r - 1]) + (vzk - vzk_m);
-          const T nlez = ez_b * lez + (vxj - vxj_m) - (vyk - vyk_m);
-          const long long o = o_plane + (r - 1) * py;
-          const int et = (r - 1) * TX;
-          const double gsum = static_cast<double>(lex) * static_cast<double>(ct[et]) +
-                              static_cast<double>(ley) * static_cast<double>(ct[TE + et]) +
-                              static_cast<double>(lez) * static_cast<double>(ct[2 * TE + et]);
-          p.grad[o] = gpre[r - 1] + gsum;
-          p.out[DN_EX][o] = nlex;
-          p.out[DN_EY][o] = nley;
-          p.out[DN_EZ][o] = nlez;
-          p.out[DN_HX][o] = bJ[r] * LHx[r];
-          p.out[DN_HY][o] = hy_b * LHy[r];
-          p.out[DN_HZ][o] = bK * LHz[r];
-        }
-        pvxi[r - 1] = vxi;
-        pvyi[r - 1] = vyi;
-      }
-      release(q);
-      ++q;
-    }
-    if (z1 < D) {
-      release(q);
-      ++q;
-    }
+    release(q);
+    ++q;
   }
+
+  // ---- march -----------------------------------------------------------------
+  for (int i = z0; i < z1; ++i) {
+    const bool has_next = (i + 1 < D);
+    if ((i == 0 && !wait_full(q)) || (has_next && !wait_full(q + 1))) {
+      fail();
+      return;
+    }
+    T e_ci, hx_c2, hy_c1, hy_b, bI;
+    i_roles(i, e_ci, hx_c2, hy_c1, hy_b, bI);
+    const T e_ci_n = has_next ? e_ci_at(i + 1) : T(0);
+    const T fi_prev = i > 0 ? T(1) : T(0);
+    const T fi_next = has_next ? T(1) : T(0);
+    const T* cur = sm.arr(q, 0) + 2 * w * BX + lane + 4;
+    const T* nxt = has_next ? sm.arr(q + 1, 0) + 2 * w * BX + lane + 4 : cur;
+    // issue the FP64 gradient loads now; they are consumed after lH'
+    const long long o_plane = i * pz + (long long)ja * py + k;
+    double gpre[2];
+#pragma unroll
+    for (int r = 1; r < 3; ++r)
+      gpre[r - 1] = (ja + r - 1 < H && kin) ? p.grad[o_plane + (r - 1) * py] : 0.0;
+
+    // ---- lH' of rows ja-1, ja, ja+1 --------------------------------------
+    T LHx[3], LHy[3], LHz[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+      lam_h(cur, nxt, r, e_ci, e_ci_n, fi_prev, fi_next, LHx[r], LHy[r], LHz[r]);
+
+    // ---- k0-1 halo column: lHy', lHz' of rows ja, ja+1 (lanes 0, 1) -------
+    // v_k terms there: vy_k = hy_c2 lHy', vz_k = cKf lHz'
+    T hvyk = T(0), hvzk = T(0);
+    if (lane < 2 && k0 > 0) {
+      const int r = 1 + lane;
+      const T gJr = lane == 0 ? gJ[1] : gJ[2];
+      const T cJbr = lane == 0 ? cJb[1] : cJb[2];
+      const T cJbr1 = lane == 0 ? cJb[2] : cJb[3];
+      const int e = r * BX - 1 - lane;  // column k0-1 (pointers sit at k0+lane)
+      const T ce = cur[A_CE * AE + e];
+      const T ux = ce * cur[DN_EX * AE + e], uy = ce * cur[DN_EY * AE + e],
+              uz = ce * cur[DN_EZ * AE + e];
+      const T ce_j = cur[A_CE * AE + e + BX];
+      const T ux_j = ce_j * cur[DN_EX * AE + e + BX];
+      const T ce_k = cur[A_CE * AE + e + 1];
+      const T uy_k = ce_k * cur[DN_EY * AE + e + 1], uz_k = ce_k * cur[DN_EZ * AE + e + 1];
+      const T ce_i = nxt[A_CE * AE + e];
+      const T ux_i = ce_i * nxt[DN_EX * AE + e];
+      const T eci = (AXES == DN_AXES_REFERENCE ? gKh * idl : e_ci) * fi_prev;
+      const T ecin = (AXES == DN_AXES_REFERENCE ? gKh * idl : e_ci_n) * fi_next;
+      const T cKb0 = gK0 * idl;  // backward x at column k0 (> 0)
+      const T eyc2 = AXES == DN_AXES_REFERENCE ? (k0 > 1 ? gJr * idl : T(0)) : cKbh;
+      const T eyc2p1 = AXES == DN_AXES_REFERENCE ? gJr * idl : cKb0;
+      const T lhy = cur[DN_HY * AE + e] - (eci * ux - ecin * ux_i) + (cKbh * uz - cKb0 * uz_k);
+      const T lhz = cur[DN_HZ * AE + e] + (cJbr * ux - cJbr1 * ux_j) - (eyc2 * uy - eyc2p1 * uy_k);
+      const T hyc2 = AXES == DN_AXES_REFERENCE ? dti * gJr : cKfh;
+      hvyk = hyc2 * lhy;
+      hvzk = cKfh * lhz;
+    }
+    const T hvyk0 = __shfl_sync(FULL_MASK, hvyk, 0), hvyk1 = __shfl_sync(FULL_MASK, hvyk, 1);
+    const T hvzk0 = __shfl_sync(FULL_MASK, hvzk, 0), hvzk1 = __shfl_sync(FULL_MASK, hvzk, 1);
+
+    // ---- previous adjoint fields of rows ja, ja+1 ---------------------------
+    const T* ct = sm.tile_arr(q, NRING_A, 0) + (2 * w) * TX + lane;
+    constexpr int TE = L::TILE_ARR / (int)sizeof(T);
+#pragma unroll
+    for (int r = 1; r < 3; ++r) {
+      const int j = ja + r - 1;
+      const T hyc2 = AXES == DN_AXES_REFERENCE ? kf * dti * gJ[r] : cKf;
+      // v terms of this lane
+      const T vxj = cJf[r] * LHx[r], vzj = cJf[r] * LHz[r];
+      const T vxi = has_next ? hx_c2 * LHx[r] : T(0);
+      const T vyi = has_next ? hy_c1 * LHy[r] : T(0);
+      const T vyk = hyc2 * LHy[r], vzk = cKf * LHz[r];
+      // -1 neighbours
+      const T vxj_m = cJf[r - 1] * LHx[r - 1], vzj_m = cJf[r - 1] * LHz[r - 1];
+      T vyk_m = __shfl_up_sync(FULL_MASK, vyk, 1);
+      T vzk_m = __shfl_up_sync(FULL_MASK, vzk, 1);
+      if (lane == 0) {
+        vyk_m = r == 1 ? hvyk0 : hvyk1;
+        vzk_m = r == 1 ? hvzk0 : hvzk1;
+      }
+      if (j < H && kin) {
+        const int e = r * BX;
+        const T lex = cur[DN_EX * AE + e], ley = cur[DN_EY * AE + e], lez = cur[DN_EZ * AE + e];
+        const T ex_b = AXES == DN_AXES_REFERENCE ? bJ[r] * bK : bJ[r] * bI;
+        const T ey_b = AXES == DN_AXES_REFERENCE ? bK * bJ[r] : bI * bK;
+        const T ez_b = bK * bJ[r];
+        const T nlex = ex_b * lex + (vyi - pvyi[r - 1]) - (vzj - vzj_m);
+        const T nley = ey_b * ley - (vxi - pvxi[r - 1]) + (vzk - vzk_m);
+        const T nlez = ez_b * lez + (vxj - vxj_m) - (vyk - vyk_m);
+        const long long o = o_plane + (r - 1) * py;
+        const int et = (r - 1) * TX;
+        const double gsum = static_cast<double>(lex) * static_cast<double>(ct[et]) +
+                            static_cast<double>(ley) * static_cast<double>(ct[TE + et]) +
+                            static_cast<double>(lez) * static_cast<double>(ct[2 * TE + et]);
+        p.grad[o] = gpre[r - 1] + gsum;
+        p.out[DN_EX][o] = nlex;
+        p.out[DN_EY][o] = nley;
+        p.out[DN_EZ][o] = nlez;
+        p.out[DN_HX][o] = bJ[r] * LHx[r];
+        p.out[DN_HY][o] = hy_b * LHy[r];
+        p.out[DN_HZ][o] = bK * LHz[r];
+      }
+      pvxi[r - 1] = vxi;
+      pvyi[r - 1] = vyi;
+    }
+    release(q);
+    ++q;
+  }
+  if (z1 < D) release(q);
 }
 
 template <typename T, int AXES>
@@ -347,7 +317,7 @@ int launch_adj(AdjParams<T> p, void* const la[6], void* const lb[6], const dn_gr
   DN_CUDA_CHECK(cudaGetDevice(&dev));
   DN_CUDA_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   long long nctas = 0;
-  const Plan plan = make_plan(g, (long long)nsm * AdjCfg<T>::MINB, &nctas, DN_ADJ3D_SLABS != 0);
+  const Plan plan = make_plan(g, (long long)nsm * AdjCfg<T>::MINB, &nctas);
   if (nctas > 0x7fffffffLL) return DN_EUNSUPPORTED;
   const size_t smem = L::bytes(plan.maxj);
   if (smem > 227 * 1024) return DN_EUNSUPPORTED;

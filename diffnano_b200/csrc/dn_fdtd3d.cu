@@ -39,12 +39,6 @@ constexpr int A_CE = 6;
 #define DN_FWD3D_PLAN_PER_SM(minb) (minb)
 #endif
 
-// hand the ends of the column ranges to extra CTAs when the columns leave
-// resident slots idle (1; 0 keeps one z range per CTA)
-#ifndef DN_FWD3D_SLABS
-#define DN_FWD3D_SLABS 1
-#endif
-
 // ring depth in planes (FP32: two CTAs per SM must fit 228 KB of shared memory)
 #ifndef DN_FWD3D_STAGES_F32
 #define DN_FWD3D_STAGES_F32 4
@@ -117,30 +111,45 @@ __global__ void __launch_bounds__(NT, FwdCfg<T>::MINB)
   const int D = p.D, H = p.H, W = p.W;
   const long long py = p.py, pz = p.pz;
   const T dt = p.dt, idl = p.inv_dl;
-  const int nj = pipe_setup(sm, plan, D, H, W, p.b, p.c, p.status);
+  const Range R(plan, D);
+  const int z0 = R.z0, z1 = R.z1, k0 = R.k0, j0 = R.j0;
+
+  const int nj = pipe_setup(sm, R, D, H, W, p.b, p.c, p.status);
   if (nj == 0) return;
 
   if (warp == NCW) {  // producer warp
     if (lane == 0)
-      producer_run<T, L, NRING_F, 0>(sm, tm, plan.ntx, nj, p.status, [](int) { return 0; });
+      producer_run<T, L, NRING_F, 0>(sm, tm, R, nj, p.status, [](int) { return 0; });
     return;
   }
 
   // ======================= consumer warps ===================================
   volatile int* s_abort = sm.flags + 1;
   const int w = warp;
+  const int ja = j0 + 2 * w;  // rows ja, ja+1 are owned; row ja-1 is recomputed
+  const int k = k0 + lane;
+  const bool kin = k < W;
   const T dti = dt * idl;
-  // Geometry and per-lane coefficients of the current segment (a CTA marches
-  // one z range of one tile, or several short ones one after another).  The
-  // boundary rules are folded into the coefficients: a forward difference on
-  // the last index and a backward difference on the first one get a zero
-  // coefficient.  The neighbour read there is a zero-filled TMA element or an
-  // in-range finite value, so 0 * value == 0 exactly.
-  int z0 = 0, z1 = 0, k0 = 0, j0 = 0, ja = 0, k = 0;
-  bool kin = false;
-  T bK, gK, bKh, gKh, kf, kb, cKf, cKb;
+  // Per-lane coefficients with the boundary rules folded in: a forward
+  // difference on the last index and a backward difference on the first one
+  // get a zero coefficient.  The neighbour read there is a zero-filled TMA
+  // element or an in-range finite value, so 0 * value == 0 exactly.
+  const T bK = sm.sbK[lane + 1], gK = sm.sgK[lane + 1];
+  const T bKh = sm.sbK[0], gKh = sm.sgK[0];
+  const T kf = (k < W - 1) ? T(1) : T(0);
+  const T kb = (k > 0) ? T(1) : T(0);
+  const T cKf = kf * dti * gK;  // dt (1+c_k)/dl on a forward x difference
+  const T cKb = kb * gK * idl;  // (1+c_k)/dl on a backward x difference
   T bJ[3], gJ[3], cJf[3], cJb[3];
-  T prevHx[2], prevHy[2];
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    const int j = ja + r - 1;
+    bJ[r] = sm.sbJ[2 * w + r];
+    gJ[r] = sm.sgJ[2 * w + r];
+    cJf[r] = (j < H - 1) ? dti * gJ[r] : T(0);  // dt (1+c_j)/dl, forward y
+    cJb[r] = (j > 0) ? gJ[r] * idl : T(0);       // (1+c_j)/dl, backward y
+  }
+  T prevHx[2] = {T(0), T(0)}, prevHy[2] = {T(0), T(0)};
   int q = 0;
 
   auto wait_full = [&](int qa) -> bool {
@@ -177,177 +186,144 @@ __global__ void __launch_bounds__(NT, FwdCfg<T>::MINB)
     }
   };
 
-#pragma unroll 1
-  for (int gseg = 0; gseg < plan_nseg(plan, blockIdx.x); ++gseg) {
-    const Range R(plan, plan_seg(plan, D, blockIdx.x, gseg));
-    z0 = R.z0;
-    z1 = R.z1;
-    k0 = R.k0;
-    j0 = R.j0;
-    ja = j0 + 2 * w;  // rows ja, ja+1 are owned; row ja-1 is recomputed
-    k = k0 + lane;
-    kin = k < W;
-    bK = kin ? static_cast<T>(__ldg(p.b[2] + k)) : T(1);
-    gK = kin ? static_cast<T>(1.0 + __ldg(p.c[2] + k)) : T(1);
-    bKh = k0 > 0 ? static_cast<T>(__ldg(p.b[2] + k0 - 1)) : T(1);
-    gKh = k0 > 0 ? static_cast<T>(1.0 + __ldg(p.c[2] + k0 - 1)) : T(1);
-    kf = (k < W - 1) ? T(1) : T(0);
-    kb = (k > 0) ? T(1) : T(0);
-    cKf = kf * dti * gK;  // dt (1+c_k)/dl on a forward x difference
-    cKb = kb * gK * idl;  // (1+c_k)/dl on a backward x difference
+  // ---- warm-up: new Hx, Hy of plane z0-1 for the owned rows ----------------
+  if (z0 > 0) {
+    if (!(wait_full(q) && wait_full(q + 1))) {
+      fail();
+      return;
+    }
+    T hx_c2, hy_b, hy_c1, e_ci, bI;
+    i_roles(z0 - 1, hx_c2, hy_b, hy_c1, e_ci, bI);
+    const T* cur = sm.arr(q, 0) + 2 * w * BX + lane + 4;
+    const T* nxt = sm.arr(q + 1, 0) + 2 * w * BX + lane + 4;
+#pragma unroll
+    for (int r = 1; r < 3; ++r) {
+      const int e = r * BX;
+      const T hy_c2 = AXES == DN_AXES_REFERENCE ? kf * dti * gJ[r] : cKf;
+      const T ez = cur[DN_EZ * AE + e];
+      prevHx[r - 1] = bJ[r] * cur[DN_HX * AE + e] - cJf[r] * (cur[DN_EZ * AE + e + BX] - ez) +
+                      hx_c2 * (nxt[DN_EY * AE + e] - cur[DN_EY * AE + e]);
+      prevHy[r - 1] = hy_b * cur[DN_HY * AE + e] -
+                      hy_c1 * (nxt[DN_EX * AE + e] - cur[DN_EX * AE + e]) +
+                      hy_c2 * (cur[DN_EZ * AE + e + 1] - ez);
+    }
+    release(q);
+    ++q;
+  }
+
+  // ---- march -----------------------------------------------------------------
+  for (int i = z0; i < z1; ++i) {
+    const bool has_next = (i + 1 < D);
+    // plane i was already waited for as "next" unless it is the very first
+    if ((i == 0 && !wait_full(q)) || (has_next && !wait_full(q + 1))) {
+      fail();
+      return;
+    }
+    T hx_c2, hy_b, hy_c1, e_ci, bI;
+    i_roles(i, hx_c2, hy_b, hy_c1, e_ci, bI);
+    // this lane's element of row ja-1 in the stage of plane i and of plane
+    // i+1 (on the last plane the forward z difference is 0: "next" = current);
+    // every other access is a compile-time offset from these two pointers
+    const T* cur = sm.arr(q, 0) + 2 * w * BX + lane + 4;
+    const T* nxt = has_next ? sm.arr(q + 1, 0) + 2 * w * BX + lane + 4 : cur;
+    const T* cEx = cur + DN_EX * AE;
+    const T* cEy = cur + DN_EY * AE;
+    const T* cEz = cur + DN_EZ * AE;
+    const T* cHx = cur + DN_HX * AE;
+    const T* cHy = cur + DN_HY * AE;
+    const T* cHz = cur + DN_HZ * AE;
+    const T* cCe = cur + A_CE * AE;
+    const T* nEx = nxt + DN_EX * AE;
+    const T* nEy = nxt + DN_EY * AE;
+
+    // ---- new H of rows ja-1 (Hx, Hz), ja, ja+1 (all three) at column k ----
+    T Hx[3], Hy[3], Hz[3];
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
-      const int j = ja + r - 1;
-      const bool jok = j >= 0 && j < H;
-      bJ[r] = jok ? static_cast<T>(__ldg(p.b[1] + j)) : T(1);
-      gJ[r] = jok ? static_cast<T>(1.0 + __ldg(p.c[1] + j)) : T(1);
-      cJf[r] = (j < H - 1) ? dti * gJ[r] : T(0);  // dt (1+c_j)/dl, forward y
-      cJb[r] = (j > 0) ? gJ[r] * idl : T(0);       // (1+c_j)/dl, backward y
-    }
-    prevHx[0] = prevHx[1] = prevHy[0] = prevHy[1] = T(0);
-
-    // ---- warm-up: new Hx, Hy of plane z0-1 for the owned rows ----------------
-    if (z0 > 0) {
-      if (!(wait_full(q) && wait_full(q + 1))) {
-        fail();
-        return;
-      }
-      T hx_c2, hy_b, hy_c1, e_ci, bI;
-      i_roles(z0 - 1, hx_c2, hy_b, hy_c1, e_ci, bI);
-      const T* cur = sm.arr(q, 0) + 2 * w * BX + lane + 4;
-      const T* nxt = sm.arr(q + 1, 0) + 2 * w * BX + lane + 4;
-  #pragma unroll
-      for (int r = 1; r < 3; ++r) {
-        const int e = r * BX;
+      const int e = r * BX;
+      const T ey = cEy[e], ex = cEx[e], ez = cEz[e];
+      Hx[r] = bJ[r] * cHx[e] - cJf[r] * (cEz[e + BX] - ez) + hx_c2 * (nEy[e] - ey);
+      Hz[r] = bK * cHz[e] - cKf * (cEy[e + 1] - ey) + cJf[r] * (cEx[e + BX] - ex);
+      if (r > 0) {
         const T hy_c2 = AXES == DN_AXES_REFERENCE ? kf * dti * gJ[r] : cKf;
-        const T ez = cur[DN_EZ * AE + e];
-        prevHx[r - 1] = bJ[r] * cur[DN_HX * AE + e] - cJf[r] * (cur[DN_EZ * AE + e + BX] - ez) +
-                        hx_c2 * (nxt[DN_EY * AE + e] - cur[DN_EY * AE + e]);
-        prevHy[r - 1] = hy_b * cur[DN_HY * AE + e] -
-                        hy_c1 * (nxt[DN_EX * AE + e] - cur[DN_EX * AE + e]) +
-                        hy_c2 * (cur[DN_EZ * AE + e + 1] - ez);
+        Hy[r] = hy_b * cHy[e] - hy_c1 * (nEx[e] - ex) + hy_c2 * (cEz[e + 1] - ez);
+      } else {
+        Hy[r] = T(0);
       }
-      release(q);
-      ++q;
     }
 
-    // ---- march -----------------------------------------------------------------
-    for (int i = z0; i < z1; ++i) {
-      const bool has_next = (i + 1 < D);
-      // plane i was already waited for as "next" unless it is the very first
-      if ((i == 0 && !wait_full(q)) || (has_next && !wait_full(q + 1))) {
-        fail();
-        return;
-      }
-      T hx_c2, hy_b, hy_c1, e_ci, bI;
-      i_roles(i, hx_c2, hy_b, hy_c1, e_ci, bI);
-      // this lane's element of row ja-1 in the stage of plane i and of plane
-      // i+1 (on the last plane the forward z difference is 0: "next" = current);
-      // every other access is a compile-time offset from these two pointers
-      const T* cur = sm.arr(q, 0) + 2 * w * BX + lane + 4;
-      const T* nxt = has_next ? sm.arr(q + 1, 0) + 2 * w * BX + lane + 4 : cur;
-      const T* cEx = cur + DN_EX * AE;
-      const T* cEy = cur + DN_EY * AE;
-      const T* cEz = cur + DN_EZ * AE;
-      const T* cHx = cur + DN_HX * AE;
-      const T* cHy = cur + DN_HY * AE;
-      const T* cHz = cur + DN_HZ * AE;
-      const T* cCe = cur + A_CE * AE;
-      const T* nEx = nxt + DN_EX * AE;
-      const T* nEy = nxt + DN_EY * AE;
+    // ---- k0-1 halo column of rows ja, ja+1 (lanes 0 and 1) ----------------
+    T haloHy = T(0), haloHz = T(0);
+    if (lane < 2 && k0 > 0) {
+      // lane 0 takes row ja, lane 1 row ja+1 (selected, not indexed, so the
+      // coefficient arrays stay in registers)
+      const T gJr = lane == 0 ? gJ[1] : gJ[2];
+      const T cJfr = lane == 0 ? cJf[1] : cJf[2];
+      const int e = (1 + lane) * BX - 1 - lane;  // column k0-1 (pointers sit at k0+lane)
+      const T ex = cEx[e], ey = cEy[e], ez = cEz[e];
+      const T b = AXES == DN_AXES_REFERENCE ? bKh : bI;
+      const T c1 = AXES == DN_AXES_REFERENCE ? dti * gKh : hy_c1;
+      const T c2 = AXES == DN_AXES_REFERENCE ? dti * gJr : dti * gKh;
+      haloHy = b * cHy[e] - c1 * (nEx[e] - ex) + c2 * (cEz[e + 1] - ez);
+      haloHz = bKh * cHz[e] - dti * gKh * (cEy[e + 1] - ey) + cJfr * (cEx[e + BX] - ex);
+    }
+    const T hHy0 = __shfl_sync(FULL_MASK, haloHy, 0), hHy1 = __shfl_sync(FULL_MASK, haloHy, 1);
+    const T hHz0 = __shfl_sync(FULL_MASK, haloHz, 0), hHz1 = __shfl_sync(FULL_MASK, haloHz, 1);
 
-      // ---- new H of rows ja-1 (Hx, Hz), ja, ja+1 (all three) at column k ----
-      T Hx[3], Hy[3], Hz[3];
-  #pragma unroll
-      for (int r = 0; r < 3; ++r) {
+    if (i == 0) {  // the backward z difference is 0 on the first plane
+      prevHx[0] = Hx[1];
+      prevHx[1] = Hx[2];
+      prevHy[0] = Hy[1];
+      prevHy[1] = Hy[2];
+    }
+
+    // ---- new E of rows ja, ja+1, source, monitors, stores -----------------
+    const bool special = any_special(p, i);
+    const long long o_plane = i * pz + (long long)ja * py + k;
+#pragma unroll
+    for (int r = 1; r < 3; ++r) {
+      const int j = ja + r - 1;
+      T hyL = __shfl_up_sync(FULL_MASK, Hy[r], 1);
+      T hzL = __shfl_up_sync(FULL_MASK, Hz[r], 1);
+      if (lane == 0) {
+        hyL = r == 1 ? hHy0 : hHy1;
+        hzL = r == 1 ? hHz0 : hHz1;
+      }
+      if (j < H && kin) {
         const int e = r * BX;
-        const T ey = cEy[e], ex = cEx[e], ez = cEz[e];
-        Hx[r] = bJ[r] * cHx[e] - cJf[r] * (cEz[e + BX] - ez) + hx_c2 * (nEy[e] - ey);
-        Hz[r] = bK * cHz[e] - cKf * (cEy[e + 1] - ey) + cJf[r] * (cEx[e + BX] - ex);
-        if (r > 0) {
-          const T hy_c2 = AXES == DN_AXES_REFERENCE ? kf * dti * gJ[r] : cKf;
-          Hy[r] = hy_b * cHy[e] - hy_c1 * (nEx[e] - ex) + hy_c2 * (cEz[e + 1] - ez);
-        } else {
-          Hy[r] = T(0);
+        const T ce = cCe[e];
+        const T ex_b = AXES == DN_AXES_REFERENCE ? bJ[r] * bK : bJ[r] * bI;
+        const T ey_b = AXES == DN_AXES_REFERENCE ? bK * bJ[r] : bI * bK;
+        const T ey_c2 = AXES == DN_AXES_REFERENCE ? kb * gJ[r] * idl : cKb;
+        const T curl_x = cJb[r] * (Hz[r] - Hz[r - 1]) - e_ci * (Hy[r] - prevHy[r - 1]);
+        const T curl_y = e_ci * (Hx[r] - prevHx[r - 1]) - ey_c2 * (Hz[r] - hzL);
+        const T curl_z = cKb * (Hy[r] - hyL) - cJb[r] * (Hx[r] - Hx[r - 1]);
+        T ex = ex_b * cEx[e] + ce * curl_x;
+        T ey = ey_b * cEy[e] + ce * curl_y;
+        T ez = bK * bJ[r] * cEz[e] + ce * curl_z;
+        T hx = Hx[r], hy = Hy[r], hz = Hz[r];
+        if (special) special_cell(p, i, j, k, ex, ey, ez, hx, hy, hz);
+        const long long o = o_plane + (r - 1) * py;
+        p.out[DN_EX][o] = ex;
+        p.out[DN_EY][o] = ey;
+        p.out[DN_EZ][o] = ez;
+        p.out[DN_HX][o] = hx;
+        p.out[DN_HY][o] = hy;
+        p.out[DN_HZ][o] = hz;
+        if (REC) {
+          const long long oc = (long long)(p.t - rec.t0) * rec.stride + o;
+          rec.curl[0][oc] = curl_x;
+          rec.curl[1][oc] = curl_y;
+          rec.curl[2][oc] = curl_z;
         }
       }
-
-      // ---- k0-1 halo column of rows ja, ja+1 (lanes 0 and 1) ----------------
-      T haloHy = T(0), haloHz = T(0);
-      if (lane < 2 && k0 > 0) {
-        // lane 0 takes row ja, lane 1 row ja+1 (selected, not indexed, so the
-        // coefficient arrays stay in registers)
-        const T gJr = lane == 0 ? gJ[1] : gJ[2];
-        const T cJfr = lane == 0 ? cJf[1] : cJf[2];
-        const int e = (1 + lane) * BX - 1 - lane;  // column k0-1 (pointers sit at k0+lane)
-        const T ex = cEx[e], ey = cEy[e], ez = cEz[e];
-        const T b = AXES == DN_AXES_REFERENCE ? bKh : bI;
-        const T c1 = AXES == DN_AXES_REFERENCE ? dti * gKh : hy_c1;
-        const T c2 = AXES == DN_AXES_REFERENCE ? dti * gJr : dti * gKh;
-        haloHy = b * cHy[e] - c1 * (nEx[e] - ex) + c2 * (cEz[e + 1] - ez);
-        haloHz = bKh * cHz[e] - dti * gKh * (cEy[e + 1] - ey) + cJfr * (cEx[e + BX] - ex);
-      }
-      const T hHy0 = __shfl_sync(FULL_MASK, haloHy, 0), hHy1 = __shfl_sync(FULL_MASK, haloHy, 1);
-      const T hHz0 = __shfl_sync(FULL_MASK, haloHz, 0), hHz1 = __shfl_sync(FULL_MASK, haloHz, 1);
-
-      if (i == 0) {  // the backward z difference is 0 on the first plane
-        prevHx[0] = Hx[1];
-        prevHx[1] = Hx[2];
-        prevHy[0] = Hy[1];
-        prevHy[1] = Hy[2];
-      }
-
-      // ---- new E of rows ja, ja+1, source, monitors, stores -----------------
-      const bool special = any_special(p, i);
-      const long long o_plane = i * pz + (long long)ja * py + k;
-  #pragma unroll
-      for (int r = 1; r < 3; ++r) {
-        const int j = ja + r - 1;
-        T hyL = __shfl_up_sync(FULL_MASK, Hy[r], 1);
-        T hzL = __shfl_up_sync(FULL_MASK, Hz[r], 1);
-        if (lane == 0) {
-          hyL = r == 1 ? hHy0 : hHy1;
-          hzL = r == 1 ? hHz0 : hHz1;
-        }
-        if (j < H && kin) {
-          const int e = r * BX;
-          const T ce = cCe[e];
-          const T ex_b = AXES == DN_AXES_REFERENCE ? bJ[r] * bK : bJ[r] * bI;
-          const T ey_b = AXES == DN_AXES_REFERENCE ? bK * bJ[r] : bI * bK;
-          const T ey_c2 = AXES == DN_AXES_REFERENCE ? kb * gJ[r] * idl : cKb;
-          const T curl_x = cJb[r] * (Hz[r] - Hz[r - 1]) - e_ci * (Hy[r] - prevHy[r - 1]);
-          const T curl_y = e_ci * (Hx[r] - prevHx[r - 1]) - ey_c2 * (Hz[r] - hzL);
-          const T curl_z = cKb * (Hy[r] - hyL) - cJb[r] * (Hx[r] - Hx[r - 1]);
-          T ex = ex_b * cEx[e] + ce * curl_x;
-          T ey = ey_b * cEy[e] + ce * curl_y;
-          T ez = bK * bJ[r] * cEz[e] + ce * curl_z;
-          T hx = Hx[r], hy = Hy[r], hz = Hz[r];
-          if (special) special_cell(p, i, j, k, ex, ey, ez, hx, hy, hz);
-          const long long o = o_plane + (r - 1) * py;
-          p.out[DN_EX][o] = ex;
-          p.out[DN_EY][o] = ey;
-          p.out[DN_EZ][o] = ez;
-          p.out[DN_HX][o] = hx;
-          p.out[DN_HY][o] = hy;
-          p.out[DN_HZ][o] = hz;
-          if (REC) {
-            const long long oc = (long long)(p.t - rec.t0) * rec.stride + o;
-            rec.curl[0][oc] = curl_x;
-            rec.curl[1][oc] = curl_y;
-            rec.curl[2][oc] = curl_z;
-          }
-        }
-        prevHx[r - 1] = Hx[r];
-        prevHy[r - 1] = Hy[r];
-      }
-      release(q);
-      ++q;
+      prevHx[r - 1] = Hx[r];
+      prevHy[r - 1] = Hy[r];
     }
-    if (z1 < D) {  // the E-only job of plane z1 was read as "next"
-      release(q);
-      ++q;
-    }
+    release(q);
+    ++q;
   }
+  if (z1 < D) release(q);  // the E-only job of plane z1 was read as "next"
 }
 
 // ---------------------------------------------------------------------------
@@ -416,8 +392,7 @@ int run3d(const dn_grid* g, void* const fa[6], void* const fb[6], const void* ce
   DN_CUDA_CHECK(cudaGetDevice(&dev));
   DN_CUDA_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   long long nctas = 0;
-  const Plan plan = make_plan(g, (long long)nsm * DN_FWD3D_PLAN_PER_SM(FwdCfg<T>::MINB), &nctas,
-                              DN_FWD3D_SLABS != 0);
+  const Plan plan = make_plan(g, (long long)nsm * DN_FWD3D_PLAN_PER_SM(FwdCfg<T>::MINB), &nctas);
   if (nctas > 0x7fffffffLL) return DN_EUNSUPPORTED;
   const size_t smem = L::bytes(plan.maxj);
   if (smem > 227 * 1024) return DN_EUNSUPPORTED;

@@ -57,7 +57,7 @@ int encode_tile4(CUtensorMap* m, const void* base, const dn_grid* g, int elem_by
   return encode(m, base, elem_bytes, 4, dims, strides, box);
 }
 
-Plan make_plan(const dn_grid* g, long long capacity, long long* nctas, bool slabs) {
+Plan make_plan(const dn_grid* g, long long capacity, long long* nctas) {
   Plan plan;
   plan.ntx = (g->W + TX - 1) / TX;
   const int nty = (g->H + TY - 1) / TY;
@@ -68,39 +68,8 @@ Plan make_plan(const dn_grid* g, long long capacity, long long* nctas, bool slab
   if (nsplit > g->D / MIN_CHUNK) nsplit = g->D / MIN_CHUNK;
   if (nsplit < 1) nsplit = 1;
   plan.nsplit = (int)nsplit;
-  plan.ncol = (int)(plan.ntiles * nsplit);
-  plan.nextra = 0;
-  plan.slab = 0;
-  const int L = (int)((g->D + nsplit - 1) / nsplit);  // longest column range
-  plan.maxj = L + 2;
-  // Idle slots: give them the ends of the column ranges.  In staged planes
-  // (each segment also stages a warm-up and a "next" plane), a column range
-  // costs L + 2 - slab and the busiest extra CTA segs * (slab + 2), segs =
-  // ceil(ncol / nextra); take the slab length with the smallest larger of the
-  // two, if it beats the plain split (L + 2) by at least 5 %.  Only for grids
-  // whose columns fill at least half the slots, slabs of at least MIN_CHUNK / 2
-  // planes and column ranges of at least MIN_CHUNK.
-  const long long idle = capacity - plan.ncol;
-  if (slabs && idle > 0 && 2LL * plan.ncol >= capacity) {
-    const int segs = (int)((plan.ncol + idle - 1) / idle);
-    const int Lmin = (int)(g->D / nsplit);  // shortest column range
-    int best = 0, best_cost = L + 2;
-    for (int slab = MIN_CHUNK / 2; Lmin - slab >= MIN_CHUNK; ++slab) {
-      const int col = L + 2 - slab, ext = segs * (slab + 2);
-      const int cost = col > ext ? col : ext;
-      if (cost < best_cost) {
-        best_cost = cost;
-        best = slab;
-      }
-    }
-    if (best > 0 && segs <= MAX_SEGS && 20 * best_cost <= 19 * (L + 2)) {
-      plan.nextra = (int)idle;
-      plan.slab = best;
-      const int extra_jobs = segs * (best + 2);
-      plan.maxj = (L - best + 2) > extra_jobs ? (L - best + 2) : extra_jobs;
-    }
-  }
-  *nctas = (long long)plan.ncol + plan.nextra;
+  *nctas = (long long)plan.ntiles * nsplit;
+  plan.maxj = (int)((g->D + nsplit - 1) / nsplit + 2);
   return plan;
 }
 

@@ -52,61 +52,17 @@ struct alignas(64) TmapSet {
   CUtensorMap m[MAX_MAPS];
 };
 
-// Work split.  Column CTA b < ncol owns tile (b % ntiles) over split range
-// s = b / ntiles, z in [s*D/nsplit, (s+1)*D/nsplit - slab).  Consecutive CTAs
-// are neighbouring tiles over the same z range, so CTAs that run together
-// march through z in lockstep and the halo rows/columns one CTA fetches are L2
-// hits for its neighbours.  When the grid leaves resident slots unused
-// (ncol < slots), the last `slab` planes of every column range go to `nextra`
-// extra CTAs instead: extra CTA e marches the slabs k in
-// [e*ncol/nextra, (e+1)*ncol/nextra) one after another (slab k: split
-// k / ntiles, tile k % ntiles), consecutive tiles of one z slab, so each slab's
-// x halo was fetched by the same CTA one slab earlier.  The slab length makes a
-// column range and an extra CTA's slabs cost about the same, so every slot of
-// the wave does equal work (on a doubly loaded SM a CTA marches ~1.5x slower
-// than alone, so idle slots are lost throughput).
-constexpr int MAX_SEGS = 16;  // slabs per extra CTA (make_plan keeps below)
-
+// Work split: CTA b owns tile (b % ntiles) for z in [split*D/nsplit,
+// (split+1)*D/nsplit), split = b / ntiles.  Consecutive CTAs are neighbouring
+// tiles over the same z range, so CTAs that run together march through z in
+// lockstep and the halo rows/columns one CTA fetches are L2 hits for its
+// neighbours.
 struct Plan {
   int ntx;     // tiles along x
   int ntiles;  // tiles per plane
   int nsplit;  // z ranges per tile
   int maxj;    // job-list capacity
-  int ncol;    // column CTAs (ntiles * nsplit)
-  int nextra;  // extra CTAs (0: no slabs)
-  int slab;    // planes cut from the end of every column range
 };
-
-// One contiguous z range of one tile marched by a CTA.
-struct Seg {
-  int tile, z0, z1;
-};
-
-// Number of segments of CTA b.
-__host__ __device__ inline int plan_nseg(const Plan& pl, int b) {
-  if (b < pl.ncol) return 1;
-  const int e = b - pl.ncol;
-  return (int)((long long)(e + 1) * pl.ncol / pl.nextra) -
-         (int)((long long)e * pl.ncol / pl.nextra);
-}
-
-// Segment g of CTA b.
-__host__ __device__ inline Seg plan_seg(const Plan& pl, int D, int b, int g) {
-  Seg sg;
-  if (b < pl.ncol) {
-    const int s = b / pl.ntiles;
-    sg.tile = b % pl.ntiles;
-    sg.z0 = (int)((long long)s * D / pl.nsplit);
-    sg.z1 = (int)((long long)(s + 1) * D / pl.nsplit) - pl.slab;
-    return sg;
-  }
-  const int k = (int)((long long)(b - pl.ncol) * pl.ncol / pl.nextra) + g;
-  const int s = k / pl.ntiles;
-  sg.tile = k % pl.ntiles;
-  sg.z1 = (int)((long long)(s + 1) * D / pl.nsplit);
-  sg.z0 = sg.z1 - pl.slab;
-  return sg;
-}
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
@@ -170,50 +126,35 @@ struct Smem {
   }
 };
 
-// Geometry of one segment (a tile over a z range).
+// Per-CTA geometry derived from the plan.
 struct Range {
   int tile, z0, z1, k0, j0;
-  __device__ Range(const Plan& plan, const Seg& sg) {
-    tile = sg.tile;
-    z0 = sg.z0;
-    z1 = sg.z1;
-    k0 = (tile % plan.ntx) * TX;
-    j0 = (tile / plan.ntx) * TY;
-  }
-  // a column CTA's segment (the only one in plans without extra CTAs)
   __device__ Range(const Plan& plan, int D) {
     tile = blockIdx.x % plan.ntiles;
     const int split = blockIdx.x / plan.ntiles;
     z0 = (int)((long long)split * D / plan.nsplit);
-    z1 = (int)((long long)(split + 1) * D / plan.nsplit) - plan.slab;
+    z1 = (int)((long long)(split + 1) * D / plan.nsplit);
     k0 = (tile % plan.ntx) * TX;
     j0 = (tile / plan.ntx) * TY;
   }
 };
 
 // Thread 0 builds the job list (planes whose inputs this CTA stages, in
-// consumption order, segment after segment: warm-up plane z0-1, z0..z1-1, and
-// plane z1 read only as the "next" plane), initialises the barriers; all
-// threads fill the CPML profile tables of the first segment's tile (read by
-// kernels whose plans give a CTA one segment).  Ends with the kernel's only
-// CTA-wide barrier.
+// consumption order: warm-up plane z0-1, z0..z1-1, and plane z1 read only as
+// the "next" plane), initialises the barriers; all threads fill the CPML
+// profile tables of the tile.  Ends with the kernel's only CTA-wide barrier.
 // Returns the job count (0 when a previous launch recorded an error, which
 // turns this launch into a no-op).
 template <typename T, typename L>
-__device__ int pipe_setup(const Smem<T, L>& sm, const Plan& plan, int D, int H, int W,
+__device__ int pipe_setup(const Smem<T, L>& sm, const Range& R, int D, int H, int W,
                           const double* const b[3], const double* const c[3],
                           const int* status) {
   const int tid = threadIdx.x;
-  const Range R(plan, plan_seg(plan, D, blockIdx.x, 0));  // the tables below: first segment
   if (tid == 0) {
     int nj = 0;
-    const int nseg = plan_nseg(plan, blockIdx.x);
-    for (int g = 0; g < nseg; ++g) {
-      const Seg sg = plan_seg(plan, D, blockIdx.x, g);
-      if (sg.z0 > 0) sm.jobs[nj++] = make_int2(sg.tile, sg.z0 - 1);
-      for (int z = sg.z0; z < sg.z1; ++z) sm.jobs[nj++] = make_int2(sg.tile, z);
-      if (sg.z1 < D) sm.jobs[nj++] = make_int2(sg.tile, sg.z1);
-    }
+    if (R.z0 > 0) sm.jobs[nj++] = make_int2(R.tile, R.z0 - 1);
+    for (int z = R.z0; z < R.z1; ++z) sm.jobs[nj++] = make_int2(R.tile, z);
+    if (R.z1 < D) sm.jobs[nj++] = make_int2(R.tile, R.z1);
     const bool skip = status != nullptr && *reinterpret_cast<const volatile int*>(status) != 0;
     sm.flags[0] = skip ? 0 : nj;
     sm.flags[1] = 0;
@@ -245,7 +186,7 @@ __device__ int pipe_setup(const Smem<T, L>& sm, const Plan& plan, int D, int H, 
 // `tile_slot(z)`.  Stays until the consumers released the last stages so no
 // copy is still in flight when the shared memory is given back.
 template <typename T, typename L, int NRING, int NTILE, typename SlotFn>
-__device__ void producer_run(const Smem<T, L>& sm, const TmapSet& tm, int ntx, int nj,
+__device__ void producer_run(const Smem<T, L>& sm, const TmapSet& tm, const Range& R, int nj,
                              int* status, SlotFn tile_slot) {
   volatile int* abort = sm.flags + 1;
   bool ok = true;
@@ -254,17 +195,16 @@ __device__ void producer_run(const Smem<T, L>& sm, const TmapSet& tm, int ntx, i
     if (q >= L::S) ok = wait_phase(&sm.empty[q % L::S], ((q / L::S) - 1) & 1, abort);
     if (!ok) break;
     const int z = sm.jobs[q].y;
-    const int k0 = (sm.jobs[q].x % ntx) * TX, j0 = (sm.jobs[q].x / ntx) * TY;
     uint64_t* bar = &sm.full[q % L::S];
     unsigned char* dst = sm.stages + (q % L::S) * L::STAGE_BYTES;
     fence_proxy_async_smem();
     mbar_arrive_expect_tx(bar, L::TX_BYTES);
 #pragma unroll
     for (int a = 0; a < NRING; ++a)
-      tma_load_3d(dst + a * L::RING_ARR, &tm.m[a], bar, k0 - 4, j0 - 1, z);
+      tma_load_3d(dst + a * L::RING_ARR, &tm.m[a], bar, R.k0 - 4, R.j0 - 1, z);
 #pragma unroll
     for (int a = 0; a < NTILE; ++a)
-      tma_load_4d(dst + NRING * L::RING_ARR + a * L::TILE_ARR, &tm.m[NRING + a], bar, k0, j0,
+      tma_load_4d(dst + NRING * L::RING_ARR + a * L::TILE_ARR, &tm.m[NRING + a], bar, R.k0, R.j0,
                   z, tile_slot(z));
     issued = q + 1;
   }
@@ -294,10 +234,8 @@ int encode_ring(CUtensorMap* m, const void* base, const dn_grid* g, int elem_byt
 // `slot_stride` elements apart
 int encode_tile4(CUtensorMap* m, const void* base, const dn_grid* g, int elem_bytes, int nslots,
                  long long slot_stride);
-// work split for `capacity` resident CTAs; `slabs`: hand the ends of the column
-// ranges to extra CTAs when the columns leave slots idle (kernels that march
-// several segments per CTA)
-Plan make_plan(const dn_grid* g, long long capacity, long long* nctas, bool slabs = false);
+// work split for `capacity` resident CTAs
+Plan make_plan(const dn_grid* g, long long capacity, long long* nctas);
 // TMA constraints: 16-byte aligned bases and byte strides
 bool tma_ok(const dn_grid* g, int elem_bytes, const void* const* ptrs, int n);
 

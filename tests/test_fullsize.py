@@ -181,11 +181,10 @@ def test_gradient_fp32_vs_fp64_full_grid(cuda, cfg1):
 
 
 @pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
-def test_split_with_slabs_non_cubic_vs_oracle(cuda, dtype):
-    """A 128 x 256 x 256 grid with the physical CPML axes: like the 256^3
-    grid, its column ranges leave resident CTA slots idle, so the ends of the
-    ranges are marched by extra CTAs (several short slabs each).  12 steps
-    from a random state against the oracle."""
+def test_non_cubic_full_width_vs_oracle(cuda, dtype):
+    """A 128 x 256 x 256 grid with the physical CPML axes (128 tiles x 2 z
+    ranges of 64 planes), 12 steps from a random state in every cell against
+    the oracle, source and monitor on."""
     shape = (128, 256, 256)
     D, H, W = shape
     gen = torch.Generator().manual_seed(21)
