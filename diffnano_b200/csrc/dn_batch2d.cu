@@ -34,6 +34,12 @@
 #include "dn_host.cuh"
 #include "dn_strip.cuh"
 
+// L2 prefetch of the FP64 gradient two rows ahead in the reverse march (1) or
+// none (0)
+#ifndef DN_BATCH2D_PREFETCH
+#define DN_BATCH2D_PREFETCH 1
+#endif
+
 namespace dn {
 namespace {
 
@@ -473,6 +479,11 @@ __device__ void adj_strip(const dn_batch2d_inst& I, int j0, int ia, int ib, int 
     }
     for (int i = ia; i < ib; ++i, o += py) {
       const bool nxt = i + 1 < H;
+#if DN_BATCH2D_PREFETCH
+      // the FP64 gradient row two ahead into L2 (its read-modify-write comes
+      // at the end of a row and would otherwise wait for DRAM)
+      if (any && i + 2 < ib) prefetch_l2(I.grad + o + 2 * py);
+#endif
       const V l_n = ldl0(i + 1, o + py, any && nxt);
       const V c_n = ldv<T, VEC, LD_NC>(ce, o + py, any && nxt, full, jv, W);
       const V l1 = ldl(L1, o, any);
@@ -577,6 +588,9 @@ __device__ void adj_strip(const dn_batch2d_inst& I, int j0, int ia, int ib, int 
     e_row(ia, o, lh_c, lh_u, true, a_c, b_c, ux_c, uy_c);
     for (int i = ia; i < ib; ++i, o += py) {
       const bool nxt = i + 1 < H;
+#if DN_BATCH2D_PREFETCH
+      if (any && i + 2 < ib) prefetch_l2(I.grad + o + 2 * py);  // as in the TM march
+#endif
       const V lh_n = ldl0(i + 1, o + py, any && nxt);
       const T l1_31 = ldl1(L1, o + VEC, edge_r);
       const T c31 = dn::ld<T, LD_NC>(ce, o + VEC, edge_r);

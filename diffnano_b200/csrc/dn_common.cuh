@@ -176,6 +176,11 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const void* tmap, uint64_
       : "memory");
 }
 
+// hint: bring the cache line holding `a` into L2 (no register is written)
+__device__ __forceinline__ void prefetch_l2(const void* a) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
+}
+
 // record the first error code into a device status word
 __device__ __forceinline__ void report_status(int* status, int code) {
   if (status) atomicCAS(status, 0, code);
