@@ -34,11 +34,6 @@ constexpr int NRING_A = 7;  // lEx lEy lEz lHx lHy lHz ce
 constexpr int NTILE_A = 3;  // curl x y z of the step
 constexpr int A_CE = 6;
 
-// L2 prefetch of the next plane's FP64 gradient rows (1) or none (0)
-#ifndef DN_ADJ3D_PREFETCH
-#define DN_ADJ3D_PREFETCH 1
-#endif
-
 template <typename T>
 struct AdjCfg {
   static constexpr int S = sizeof(T) == 4 ? 4 : 3;
@@ -209,16 +204,6 @@ __global__ void __launch_bounds__(NT, AdjCfg<T>::MINB)
 #pragma unroll
     for (int r = 1; r < 3; ++r)
       gpre[r - 1] = (ja + r - 1 < H && kin) ? p.grad[o_plane + (r - 1) * py] : 0.0;
-#if DN_ADJ3D_PREFETCH
-    // and pull the next plane's rows into L2: one plane from now those loads
-    // wait for L2 instead of DRAM (the gradient is the one array this kernel
-    // reads directly, not through the staged ring)
-    if (i + 1 < z1 && kin) {
-#pragma unroll
-      for (int r = 1; r < 3; ++r)
-        if (ja + r - 1 < H) prefetch_l2(p.grad + o_plane + pz + (r - 1) * py);
-    }
-#endif
 
     // ---- lH' of rows ja-1, ja, ja+1 --------------------------------------
     T LHx[3], LHy[3], LHz[3];
