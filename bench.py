@@ -504,6 +504,25 @@ def batch2d_workload(n_inst=64, seed=7, tscale=1.0):
     return specs, eps
 
 
+# FP32 TMz bytes per cell-step: forward reads Ez, Hx, Hy, dt/eps and writes the
+# three fields (28); a reverse step, as the 3-D adjoint is counted, is forward
+# recompute 28 + adjoint update 28 + dL/deps read-modify-write 8 = 64, and moves
+# 16 more (the curl record written and read back, 4 + 4; the FP64 gradient's
+# extra 8)
+B2D_FWD_BYTES, B2D_BWD_BYTES, B2D_BWD_MOVED = 28, 64, 80
+
+
+def batch_bandwidth(cells_steps: float, f_s: float, b_s: float) -> dict:
+    peak, kind = measured_peak_hbm()
+    fwd = B2D_FWD_BYTES * cells_steps / f_s / 1e9
+    bwd = B2D_BWD_BYTES * cells_steps / b_s / 1e9
+    return {"forward_GBs": fwd, "forward_frac": fwd / peak,
+            "backward_algorithmic_bytes_per_cell_step": B2D_BWD_BYTES,
+            "backward_GBs": bwd, "backward_frac": bwd / peak,
+            "backward_moved_GBs": B2D_BWD_MOVED * cells_steps / b_s / 1e9,
+            "peak": peak, "peak_source": f"hbm_gbs of {kind}"}
+
+
 def run_batch2d(args):
     from diffnano_b200.shard import rank_share, sum_over_ranks
     from diffnano_b200.solvers.batch2d import FDTDBatch2D
@@ -591,6 +610,7 @@ def run_batch2d(args):
                        "checkpoint_interval": batch.K},
             "forward_s": f_s, "backward_s": b_s,
             "backward_gcells": cells_steps / b_s / 1e9,
+            "bandwidth": batch_bandwidth(cells_steps, f_s, b_s),
             "graphed_forward_backward_s": g_s,
             "graphed_what": "FDTDBatch2D.fom_gradient_graphed: eps upload, forward, adjoint "
                             "seeding, backward and dFOM/deps replayed as one CUDA graph "
