@@ -319,7 +319,7 @@ int launch_adj(AdjParams<T> p, void* const la[6], void* const lb[6], const dn_gr
   long long nctas = 0;
   const Plan plan = make_plan(g, (long long)nsm * AdjCfg<T>::MINB, &nctas);
   if (nctas > 0x7fffffffLL) return DN_EUNSUPPORTED;
-  const size_t smem = L::bytes(plan.maxj);
+  const size_t smem = L::BYTES;
   if (smem > 227 * 1024) return DN_EUNSUPPORTED;
   auto kern = k_adj3d<T, AXES>;
   DN_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -23,6 +23,8 @@
 //    six results to the other ping-pong buffer (neighbouring CTAs still read
 //    the old one);
 //  * optionally (adjoint replay) the curl term of each E update is recorded.
+#include <cstdlib>
+
 #include "dn_zmarch.cuh"
 
 namespace dn {
@@ -327,13 +329,336 @@ __global__ void __launch_bounds__(NT, FwdCfg<T>::MINB)
 }
 
 // ---------------------------------------------------------------------------
+// FP32, two columns per lane.  The same march on 16 x 64 tiles: lane l owns
+// columns k0+2l and k0+2l+1 of its two rows, reads the staged arrays as
+// float2 (one shared-memory instruction for both columns), takes the x+1
+// neighbour of its second column with a scalar read and the x-1 neighbour of
+// its first column from lane l-1 by shuffle (lanes 0 and 1 recompute the
+// k0-1 halo column as above), and writes float2 to global memory.  Per cell
+// that halves the shared-memory reads, the global store instructions and the
+// halo-column and per-plane overhead; the arithmetic of every column is the
+// one-column kernel's, expression for expression.
+// ---------------------------------------------------------------------------
+constexpr int S_V2 = 3;  // ring depth: two 109 KB CTAs per SM
+using LV2 = Layout<float, NRING_F, 0, S_V2, Geo64>;
+
+__device__ __forceinline__ float2 ld2(const float* a) {
+  return *reinterpret_cast<const float2*>(a);
+}
+__device__ __forceinline__ float sel(const float2 v, int c) { return c == 0 ? v.x : v.y; }
+
+// store one or both columns (the second one only when it is inside the grid)
+__device__ __forceinline__ void st2(float* base, long long o, float a, float b, bool both) {
+  if (both)
+    *reinterpret_cast<float2*>(base + o) = make_float2(a, b);
+  else
+    base[o] = a;
+}
+
+// 112 registers x 288 threads: two CTAs per SM (64,512 of 65,536 registers)
+template <int AXES, bool REC>
+__global__ void __maxnreg__(112)
+    k_fdtd3d_v2(const StepParams<float> p, const __grid_constant__ TmapSet tm, const Plan plan,
+                const CurlRec<float> rec) {
+  using T = float;
+  using L = LV2;
+  using G = Geo64;
+  constexpr int S = L::S;
+  constexpr int AE = L::RING_ARR / (int)sizeof(T);
+  constexpr int RB = G::BX;  // row stride of a staged box
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const Smem<T, L> sm(smem_raw);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int D = p.D, H = p.H, W = p.W;
+  const long long py = p.py, pz = p.pz;
+  const T dt = p.dt, idl = p.inv_dl;
+  const Range R(plan, D);
+  const int z0 = R.z0, z1 = R.z1, k0 = R.k0, j0 = R.j0;
+
+  const int nj = pipe_setup(sm, R, D, H, W, p.b, p.c, p.status);
+  if (nj == 0) return;
+
+  if (warp == G::NCW) {  // producer warp
+    if (lane == 0)
+      producer_run<T, L, NRING_F, 0>(sm, tm, R, nj, p.status, [](int) { return 0; });
+    return;
+  }
+
+  // ======================= consumer warps ===================================
+  volatile int* s_abort = sm.flags + 1;
+  const int w = warp;
+  const int ja = j0 + 2 * w;      // rows ja, ja+1 are owned; row ja-1 is recomputed
+  const int kA = k0 + 2 * lane;   // columns kA (c = 0) and kA+1 (c = 1)
+  const bool inA = kA < W, inB = kA + 1 < W;
+  const T dti = dt * idl;
+  // per-column coefficients, boundary rules folded in (see k_fdtd3d)
+  T bK[2], gK[2], kf[2], kb[2], cKf[2], cKb[2];
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    const int k = kA + c;
+    bK[c] = sm.sbK[2 * lane + 1 + c];
+    gK[c] = sm.sgK[2 * lane + 1 + c];
+    kf[c] = (k < W - 1) ? T(1) : T(0);
+    kb[c] = (k > 0) ? T(1) : T(0);
+    cKf[c] = kf[c] * dti * gK[c];
+    cKb[c] = kb[c] * gK[c] * idl;
+  }
+  const T bKh = sm.sbK[0], gKh = sm.sgK[0];
+  T bJ[3], gJ[3], cJf[3], cJb[3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    const int j = ja + r - 1;
+    bJ[r] = sm.sbJ[2 * w + r];
+    gJ[r] = sm.sgJ[2 * w + r];
+    cJf[r] = (j < H - 1) ? dti * gJ[r] : T(0);
+    cJb[r] = (j > 0) ? gJ[r] * idl : T(0);
+  }
+  T prevHx[2][2] = {{T(0), T(0)}, {T(0), T(0)}};  // [owned row][column]
+  T prevHy[2][2] = {{T(0), T(0)}, {T(0), T(0)}};
+  int q = 0;
+
+  auto wait_full = [&](int qa) -> bool {
+    const bool r = wait_phase(&sm.full[qa % S], (qa / S) & 1, s_abort);
+    __syncwarp();
+    return r;
+  };
+  auto release = [&](int qa) {
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&sm.empty[qa % S]);
+  };
+  auto fail = [&]() {
+    if (lane == 0) {
+      report_status(p.status, DN_ETIMEOUT);
+      *s_abort = 1;
+    }
+  };
+  // z (i) roles per column: per lane for the reference mapping, per plane for
+  // the physical one
+  auto i_roles = [&](int i, T hx_c2[2], T hy_b[2], T hy_c1[2], T e_ci[2], T& bI) {
+    if (AXES == DN_AXES_REFERENCE) {
+      bI = T(1);
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        hx_c2[c] = dti * gK[c];
+        hy_b[c] = bK[c];
+        hy_c1[c] = dti * gK[c];
+        e_ci[c] = gK[c] * idl;
+      }
+    } else {
+      bI = static_cast<T>(__ldg(p.b[0] + i));
+      const T gI = static_cast<T>(1.0 + __ldg(p.c[0] + i));
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        hx_c2[c] = dti * gI;
+        hy_b[c] = bI;
+        hy_c1[c] = dti * gI;
+        e_ci[c] = gI * idl;
+      }
+    }
+  };
+
+  // ---- warm-up: new Hx, Hy of plane z0-1 for the owned rows ----------------
+  if (z0 > 0) {
+    if (!(wait_full(q) && wait_full(q + 1))) {
+      fail();
+      return;
+    }
+    T hx_c2[2], hy_b[2], hy_c1[2], e_ci[2], bI;
+    i_roles(z0 - 1, hx_c2, hy_b, hy_c1, e_ci, bI);
+    const T* cur = sm.arr(q, 0) + 2 * w * RB + 2 * lane + 4;
+    const T* nxt = sm.arr(q + 1, 0) + 2 * w * RB + 2 * lane + 4;
+#pragma unroll
+    for (int r = 1; r < 3; ++r) {
+      const int e = r * RB;
+      const float2 ez = ld2(cur + DN_EZ * AE + e), ezj = ld2(cur + DN_EZ * AE + e + RB);
+      const float2 ey = ld2(cur + DN_EY * AE + e), ney = ld2(nxt + DN_EY * AE + e);
+      const float2 ex = ld2(cur + DN_EX * AE + e), nex = ld2(nxt + DN_EX * AE + e);
+      const float2 hx = ld2(cur + DN_HX * AE + e), hy = ld2(cur + DN_HY * AE + e);
+      const T ezk2 = cur[DN_EZ * AE + e + 2];
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        const T hy_c2 = AXES == DN_AXES_REFERENCE ? kf[c] * dti * gJ[r] : cKf[c];
+        const T ezk = c == 0 ? ez.y : ezk2;
+        prevHx[r - 1][c] = bJ[r] * sel(hx, c) - cJf[r] * (sel(ezj, c) - sel(ez, c)) +
+                           hx_c2[c] * (sel(ney, c) - sel(ey, c));
+        prevHy[r - 1][c] = hy_b[c] * sel(hy, c) - hy_c1[c] * (sel(nex, c) - sel(ex, c)) +
+                           hy_c2 * (ezk - sel(ez, c));
+      }
+    }
+    release(q);
+    ++q;
+  }
+
+  // ---- march -----------------------------------------------------------------
+  for (int i = z0; i < z1; ++i) {
+    const bool has_next = (i + 1 < D);
+    if ((i == 0 && !wait_full(q)) || (has_next && !wait_full(q + 1))) {
+      fail();
+      return;
+    }
+    T hx_c2[2], hy_b[2], hy_c1[2], e_ci[2], bI;
+    i_roles(i, hx_c2, hy_b, hy_c1, e_ci, bI);
+    const T* cur = sm.arr(q, 0) + 2 * w * RB + 2 * lane + 4;
+    const T* nxt = has_next ? sm.arr(q + 1, 0) + 2 * w * RB + 2 * lane + 4 : cur;
+    const T* cEx = cur + DN_EX * AE;
+    const T* cEy = cur + DN_EY * AE;
+    const T* cEz = cur + DN_EZ * AE;
+    const T* cHx = cur + DN_HX * AE;
+    const T* cHy = cur + DN_HY * AE;
+    const T* cHz = cur + DN_HZ * AE;
+    const T* cCe = cur + A_CE * AE;
+    const T* nEx = nxt + DN_EX * AE;
+    const T* nEy = nxt + DN_EY * AE;
+
+    // ---- new H of rows ja-1 (Hx, Hz), ja, ja+1 (all three), both columns --
+    T Hx[3][2], Hy[3][2], Hz[3][2];
+    float2 Ex[3], Ey[3], Ez[3];  // E of rows ja-1 .. ja+1 (reused by the E update)
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      const int e = r * RB;
+      Ex[r] = ld2(cEx + e);
+      Ey[r] = ld2(cEy + e);
+      Ez[r] = ld2(cEz + e);
+      const float2 ezj = ld2(cEz + e + RB), exj = ld2(cEx + e + RB);
+      const float2 hx = ld2(cHx + e), hz = ld2(cHz + e), ney = ld2(nEy + e);
+      const T eyk2 = cEy[e + 2];
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        const T ex = sel(Ex[r], c), ey = sel(Ey[r], c), ez = sel(Ez[r], c);
+        const T eyk = c == 0 ? Ey[r].y : eyk2;
+        Hx[r][c] = bJ[r] * sel(hx, c) - cJf[r] * (sel(ezj, c) - ez) +
+                   hx_c2[c] * (sel(ney, c) - ey);
+        Hz[r][c] = bK[c] * sel(hz, c) - cKf[c] * (eyk - ey) + cJf[r] * (sel(exj, c) - ex);
+      }
+      if (r > 0) {
+        const float2 hy = ld2(cHy + e), nex = ld2(nEx + e);
+        const T ezk2 = cEz[e + 2];
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          const T ex = sel(Ex[r], c), ez = sel(Ez[r], c);
+          const T ezk = c == 0 ? Ez[r].y : ezk2;
+          const T hy_c2 = AXES == DN_AXES_REFERENCE ? kf[c] * dti * gJ[r] : cKf[c];
+          Hy[r][c] = hy_b[c] * sel(hy, c) - hy_c1[c] * (sel(nex, c) - ex) + hy_c2 * (ezk - ez);
+        }
+      } else {
+        Hy[r][0] = Hy[r][1] = T(0);
+      }
+    }
+
+    // ---- k0-1 halo column of rows ja, ja+1 (lanes 0 and 1) ----------------
+    T haloHy = T(0), haloHz = T(0);
+    if (lane < 2 && k0 > 0) {
+      const T gJr = lane == 0 ? gJ[1] : gJ[2];
+      const T cJfr = lane == 0 ? cJf[1] : cJf[2];
+      const int e = (1 + lane) * RB - 1 - 2 * lane;  // column k0-1 (pointers sit at k0+2*lane)
+      const T ex = cEx[e], ey = cEy[e], ez = cEz[e];
+      const T b = AXES == DN_AXES_REFERENCE ? bKh : bI;
+      const T c1 = AXES == DN_AXES_REFERENCE ? dti * gKh : hy_c1[0];
+      const T c2 = AXES == DN_AXES_REFERENCE ? dti * gJr : dti * gKh;
+      haloHy = b * cHy[e] - c1 * (nEx[e] - ex) + c2 * (cEz[e + 1] - ez);
+      haloHz = bKh * cHz[e] - dti * gKh * (cEy[e + 1] - ey) + cJfr * (cEx[e + RB] - ex);
+    }
+    const T hHy0 = __shfl_sync(FULL_MASK, haloHy, 0), hHy1 = __shfl_sync(FULL_MASK, haloHy, 1);
+    const T hHz0 = __shfl_sync(FULL_MASK, haloHz, 0), hHz1 = __shfl_sync(FULL_MASK, haloHz, 1);
+
+    if (i == 0) {  // the backward z difference is 0 on the first plane
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        prevHx[0][c] = Hx[1][c];
+        prevHx[1][c] = Hx[2][c];
+        prevHy[0][c] = Hy[1][c];
+        prevHy[1][c] = Hy[2][c];
+      }
+    }
+
+    // ---- new E of rows ja, ja+1, source, monitors, stores -----------------
+    const bool special = any_special(p, i);
+    const long long o_plane = i * pz + (long long)ja * py + kA;
+#pragma unroll
+    for (int r = 1; r < 3; ++r) {
+      const int j = ja + r - 1;
+      // x-1 neighbours: column kA-1 is lane l-1's second column (the halo on
+      // lane 0), column kA is this lane's first
+      T hyL[2], hzL[2];
+      hyL[0] = __shfl_up_sync(FULL_MASK, Hy[r][1], 1);
+      hzL[0] = __shfl_up_sync(FULL_MASK, Hz[r][1], 1);
+      if (lane == 0) {
+        hyL[0] = r == 1 ? hHy0 : hHy1;
+        hzL[0] = r == 1 ? hHz0 : hHz1;
+      }
+      hyL[1] = Hy[r][0];
+      hzL[1] = Hz[r][0];
+      if (j < H && inA) {
+        const int e = r * RB;
+        const float2 ce2 = ld2(cCe + e);
+        T nE[3][2], nH[3][2], crl[3][2];
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          const T ce = sel(ce2, c);
+          const T ex_b = AXES == DN_AXES_REFERENCE ? bJ[r] * bK[c] : bJ[r] * bI;
+          const T ey_b = AXES == DN_AXES_REFERENCE ? bK[c] * bJ[r] : bI * bK[c];
+          const T ey_c2 = AXES == DN_AXES_REFERENCE ? kb[c] * gJ[r] * idl : cKb[c];
+          const T curl_x =
+              cJb[r] * (Hz[r][c] - Hz[r - 1][c]) - e_ci[c] * (Hy[r][c] - prevHy[r - 1][c]);
+          const T curl_y =
+              e_ci[c] * (Hx[r][c] - prevHx[r - 1][c]) - ey_c2 * (Hz[r][c] - hzL[c]);
+          const T curl_z = cKb[c] * (Hy[r][c] - hyL[c]) - cJb[r] * (Hx[r][c] - Hx[r - 1][c]);
+          T ex = ex_b * sel(Ex[r], c) + ce * curl_x;
+          T ey = ey_b * sel(Ey[r], c) + ce * curl_y;
+          T ez = bK[c] * bJ[r] * sel(Ez[r], c) + ce * curl_z;
+          T hx = Hx[r][c], hy = Hy[r][c], hz = Hz[r][c];
+          if (special) special_cell(p, i, j, kA + c, ex, ey, ez, hx, hy, hz);
+          nE[0][c] = ex;
+          nE[1][c] = ey;
+          nE[2][c] = ez;
+          nH[0][c] = hx;
+          nH[1][c] = hy;
+          nH[2][c] = hz;
+          crl[0][c] = curl_x;
+          crl[1][c] = curl_y;
+          crl[2][c] = curl_z;
+        }
+        const long long o = o_plane + (r - 1) * py;
+        st2(p.out[DN_EX], o, nE[0][0], nE[0][1], inB);
+        st2(p.out[DN_EY], o, nE[1][0], nE[1][1], inB);
+        st2(p.out[DN_EZ], o, nE[2][0], nE[2][1], inB);
+        st2(p.out[DN_HX], o, nH[0][0], nH[0][1], inB);
+        st2(p.out[DN_HY], o, nH[1][0], nH[1][1], inB);
+        st2(p.out[DN_HZ], o, nH[2][0], nH[2][1], inB);
+        if (REC) {
+          const long long oc = (long long)(p.t - rec.t0) * rec.stride + o;
+          st2(rec.curl[0], oc, crl[0][0], crl[0][1], inB);
+          st2(rec.curl[1], oc, crl[1][0], crl[1][1], inB);
+          st2(rec.curl[2], oc, crl[2][0], crl[2][1], inB);
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        prevHx[r - 1][c] = Hx[r][c];
+        prevHy[r - 1][c] = Hy[r][c];
+      }
+    }
+    release(q);
+    ++q;
+  }
+  if (z1 < D) release(q);  // the E-only job of plane z1 was read as "next"
+}
+
+// ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
-template <typename T, int AXES, bool REC>
+template <typename T, int AXES, bool REC, bool TWO_COL>
 int launch_all(const StepParams<T>& base, const TmapSet& ta, const TmapSet& tb, void* const fa[6],
                void* const fb[6], int t0, int nsteps, const Plan& plan, int nctas, size_t smem,
                const CurlRec<T>& rec, cudaStream_t s) {
-  auto kern = k_fdtd3d<T, AXES, REC>;
+  void (*kern)(const StepParams<T>, const TmapSet, const Plan, const CurlRec<T>);
+  int nt = NT;
+  if constexpr (TWO_COL) {
+    kern = k_fdtd3d_v2<AXES, REC>;
+    nt = Geo64::NT;
+  } else {
+    kern = k_fdtd3d<T, AXES, REC>;
+  }
   DN_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)smem));
   StepParams<T> p = base;
@@ -341,10 +666,41 @@ int launch_all(const StepParams<T>& base, const TmapSet& ta, const TmapSet& tb, 
     const bool even = (n % 2) == 0;
     set_io(&p, even ? fa : fb, even ? fb : fa);
     p.t = t0 + n;
-    kern<<<nctas, NT, smem, s>>>(p, even ? ta : tb, plan, rec);
+    kern<<<nctas, nt, smem, s>>>(p, even ? ta : tb, plan, rec);
   }
   DN_CUDA_CHECK(cudaGetLastError());
   return DN_OK;
+}
+
+template <typename T, bool TWO_COL>
+int dispatch(const dn_grid* g, bool record, const StepParams<T>& p, const TmapSet& ta,
+             const TmapSet& tb, void* const fa[6], void* const fb[6], int t0, int nsteps,
+             const Plan& plan, int n, size_t smem, const CurlRec<T>& rec, cudaStream_t s) {
+  if (g->axes == DN_AXES_REFERENCE)
+    return record ? launch_all<T, DN_AXES_REFERENCE, true, TWO_COL>(p, ta, tb, fa, fb, t0, nsteps,
+                                                                    plan, n, smem, rec, s)
+                  : launch_all<T, DN_AXES_REFERENCE, false, TWO_COL>(p, ta, tb, fa, fb, t0,
+                                                                     nsteps, plan, n, smem, rec, s);
+  return record ? launch_all<T, DN_AXES_PHYSICAL, true, TWO_COL>(p, ta, tb, fa, fb, t0, nsteps,
+                                                                 plan, n, smem, rec, s)
+                : launch_all<T, DN_AXES_PHYSICAL, false, TWO_COL>(p, ta, tb, fa, fb, t0, nsteps,
+                                                                  plan, n, smem, rec, s);
+}
+
+// Lane columns of the FP32 kernel: DN_FWD3D_LANE_COLUMNS by default, or the
+// environment variable DN_FDTD3D_LANE_COLUMNS ("1" or "2", read once per
+// process), e.g. to compare the two kernels.
+#ifndef DN_FWD3D_LANE_COLUMNS
+#define DN_FWD3D_LANE_COLUMNS 1
+#endif
+bool two_column_fp32() {
+  static const bool on = [] {
+    const char* v = std::getenv("DN_FDTD3D_LANE_COLUMNS");
+    if (v && v[0] == '1' && v[1] == '\0') return false;
+    if (v && v[0] == '2' && v[1] == '\0') return true;
+    return DN_FWD3D_LANE_COLUMNS == 2;
+  }();
+  return on;
 }
 
 template <typename T>
@@ -380,35 +736,41 @@ int run3d(const dn_grid* g, void* const fa[6], void* const fb[6], const void* ce
     rec.t0 = crec->t0;
   }
 
+  // FP32: two columns per lane (float2 stores need 8-byte aligned curl-record
+  // arrays and an even record stride; otherwise the one-column kernel runs)
+  bool rec_pairs = !record || rec.stride % 2 == 0;
+  for (int c = 0; c < 3 && record; ++c)
+    rec_pairs = rec_pairs && (reinterpret_cast<uintptr_t>(rec.curl[c]) & 7) == 0;
+  const bool two_col = sizeof(T) == 4 && two_column_fp32() && rec_pairs;
+  const int bx = two_col ? Geo64::BX : BX, by = two_col ? Geo64::BY : BY;
   TmapSet ta, tb;
   for (int c = 0; c < 6; ++c) {
-    if ((rc = encode_ring(&ta.m[c], fa[c], g, sizeof(T))) != DN_OK) return rc;
-    if ((rc = encode_ring(&tb.m[c], fb[c], g, sizeof(T))) != DN_OK) return rc;
+    if ((rc = encode_ring(&ta.m[c], fa[c], g, sizeof(T), bx, by)) != DN_OK) return rc;
+    if ((rc = encode_ring(&tb.m[c], fb[c], g, sizeof(T), bx, by)) != DN_OK) return rc;
   }
-  if ((rc = encode_ring(&ta.m[A_CE], ce, g, sizeof(T))) != DN_OK) return rc;
+  if ((rc = encode_ring(&ta.m[A_CE], ce, g, sizeof(T), bx, by)) != DN_OK) return rc;
   tb.m[A_CE] = ta.m[A_CE];
 
   int dev = 0, nsm = 0;
   DN_CUDA_CHECK(cudaGetDevice(&dev));
   DN_CUDA_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   long long nctas = 0;
-  const Plan plan = make_plan(g, (long long)nsm * DN_FWD3D_PLAN_PER_SM(FwdCfg<T>::MINB), &nctas);
+  const Plan plan =
+      two_col ? make_plan(g, (long long)nsm * 2, &nctas, Geo64::TX, Geo64::TY)
+              : make_plan(g, (long long)nsm * DN_FWD3D_PLAN_PER_SM(FwdCfg<T>::MINB), &nctas);
   if (nctas > 0x7fffffffLL) return DN_EUNSUPPORTED;
-  const size_t smem = L::bytes(plan.maxj);
+  const size_t smem = two_col ? LV2::BYTES : L::BYTES;
   if (smem > 227 * 1024) return DN_EUNSUPPORTED;
 
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int n = (int)nctas;
-  if (g->axes == DN_AXES_REFERENCE)
-    rc = record ? launch_all<T, DN_AXES_REFERENCE, true>(p, ta, tb, fa, fb, t0, nsteps, plan, n,
-                                                         smem, rec, s)
-                : launch_all<T, DN_AXES_REFERENCE, false>(p, ta, tb, fa, fb, t0, nsteps, plan, n,
-                                                          smem, rec, s);
-  else
-    rc = record ? launch_all<T, DN_AXES_PHYSICAL, true>(p, ta, tb, fa, fb, t0, nsteps, plan, n,
-                                                        smem, rec, s)
-                : launch_all<T, DN_AXES_PHYSICAL, false>(p, ta, tb, fa, fb, t0, nsteps, plan, n,
-                                                         smem, rec, s);
+  if constexpr (sizeof(T) == 4) {
+    rc = two_col
+             ? dispatch<T, true>(g, record, p, ta, tb, fa, fb, t0, nsteps, plan, n, smem, rec, s)
+             : dispatch<T, false>(g, record, p, ta, tb, fa, fb, t0, nsteps, plan, n, smem, rec, s);
+  } else {
+    rc = dispatch<T, false>(g, record, p, ta, tb, fa, fb, t0, nsteps, plan, n, smem, rec, s);
+  }
   if (rc != DN_OK) return rc;
   *final_in_b = nsteps % 2;
   return DN_OK;

@@ -38,11 +38,12 @@ static int encode(CUtensorMap* m, const void* base, int elem_bytes, int rank,
   return DN_OK;
 }
 
-int encode_ring(CUtensorMap* m, const void* base, const dn_grid* g, int elem_bytes) {
+int encode_ring(CUtensorMap* m, const void* base, const dn_grid* g, int elem_bytes, int bx,
+                int by) {
   const cuuint64_t dims[3] = {(cuuint64_t)g->W, (cuuint64_t)g->H, (cuuint64_t)g->D};
   const cuuint64_t strides[2] = {(cuuint64_t)g->pitch_y * elem_bytes,
                                  (cuuint64_t)g->pitch_z * elem_bytes};
-  const cuuint32_t box[3] = {BX, BY, 1};
+  const cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
   return encode(m, base, elem_bytes, 3, dims, strides, box);
 }
 
@@ -57,10 +58,12 @@ int encode_tile4(CUtensorMap* m, const void* base, const dn_grid* g, int elem_by
   return encode(m, base, elem_bytes, 4, dims, strides, box);
 }
 
-Plan make_plan(const dn_grid* g, long long capacity, long long* nctas) {
+Plan make_plan(const dn_grid* g, long long capacity, long long* nctas, int tx, int ty) {
   Plan plan;
-  plan.ntx = (g->W + TX - 1) / TX;
-  const int nty = (g->H + TY - 1) / TY;
+  plan.tx = tx;
+  plan.ty = ty;
+  plan.ntx = (g->W + tx - 1) / tx;
+  const int nty = (g->H + ty - 1) / ty;
   plan.ntiles = plan.ntx * nty;
   // as many z ranges per tile as keep every CTA resident at once, each at
   // least MIN_CHUNK planes long
@@ -69,7 +72,6 @@ Plan make_plan(const dn_grid* g, long long capacity, long long* nctas) {
   if (nsplit < 1) nsplit = 1;
   plan.nsplit = (int)nsplit;
   *nctas = (long long)plan.ntiles * nsplit;
-  plan.maxj = (int)((g->D + nsplit - 1) / nsplit + 2);
   return plan;
 }
 

@@ -16,12 +16,28 @@
 namespace dn {
 namespace zm {
 
-constexpr int TX = 32;               // tile x (one warp)
-constexpr int TY = 16;               // tile y
-constexpr int NCW = TY / 2;          // consumer warps, two rows each
-constexpr int NT = (NCW + 1) * 32;   // + one producer warp
-constexpr int BX = TX + 8;           // ring box x: k0-4 .. k0+TX+3
-constexpr int BY = TY + 2;           // ring box y: j0-1 .. j0+TY
+// Tile geometry: TX_ columns (one warp: 32 lanes x TX_/32 columns) by TY_
+// rows (TY_/2 consumer warps, two rows each, plus one producer warp); ring
+// boxes are BX x BY = (TX_+8) x (TY_+2): x from k0-4 (16-byte aligned) to
+// k0+TX_+3, y from j0-1 to j0+TY_.
+template <int TX_, int TY_>
+struct Geo {
+  static constexpr int TX = TX_;
+  static constexpr int TY = TY_;
+  static constexpr int NCW = TY_ / 2;
+  static constexpr int NT = (NCW + 1) * 32;
+  static constexpr int BX = TX_ + 8;
+  static constexpr int BY = TY_ + 2;
+};
+using Geo32 = Geo<32, 16>;  // one column per lane (FP64 forward, adjoint)
+using Geo64 = Geo<64, 16>;  // two columns per lane (FP32 forward)
+
+constexpr int TX = Geo32::TX;        // tile x (one warp)
+constexpr int TY = Geo32::TY;        // tile y
+constexpr int NCW = Geo32::NCW;      // consumer warps, two rows each
+constexpr int NT = Geo32::NT;        // + one producer warp
+constexpr int BX = Geo32::BX;        // ring box x: k0-4 .. k0+TX+3
+constexpr int BY = Geo32::BY;        // ring box y: j0-1 .. j0+TY
 constexpr int MIN_CHUNK = 8;         // min planes per CTA range
 constexpr uint32_t WAIT_PROBES = 1u << 16;  // bound on mbarrier probes per wait
 constexpr uint32_t SLEEP_NS = 20000;        // suspend-time hint per probe (~1.3 s bound)
@@ -29,23 +45,23 @@ constexpr unsigned FULL_MASK = 0xffffffffu;
 constexpr int MAX_MAPS = 10;
 
 // Shared-memory layout of one kernel configuration.
-template <typename T, int NRING, int NTILE, int S_>
+template <typename T, int NRING, int NTILE, int S_, typename G_ = Geo32>
 struct Layout {
+  using G = G_;
   static constexpr int S = S_;
-  static constexpr int RING_BYTES = BX * BY * (int)sizeof(T);
-  static constexpr int TILE_BYTES = TX * TY * (int)sizeof(T);
+  static constexpr int RING_BYTES = G::BX * G::BY * (int)sizeof(T);
+  static constexpr int TILE_BYTES = G::TX * G::TY * (int)sizeof(T);
   static constexpr int RING_ARR = (RING_BYTES + 127) / 128 * 128;
   static constexpr int TILE_ARR = (TILE_BYTES + 127) / 128 * 128;
   static constexpr int STAGE_BYTES = NRING * RING_ARR + NTILE * TILE_ARR;
   static constexpr int TX_BYTES = NRING * RING_BYTES + NTILE * TILE_BYTES;
-  static constexpr int TAB_ELEMS = 2 * (TY + 2) + 2 * (TX + 2);
+  static constexpr int TAB_ELEMS = 2 * (G::TY + 2) + 2 * (G::TX + 2);
   static constexpr int TAB_BYTES = TAB_ELEMS * (int)sizeof(T);
   static constexpr int BAR_OFF = ((S * STAGE_BYTES + TAB_BYTES + 15) / 16) * 16;
-  // bytes of dynamic shared memory for a job list of `maxj` entries
-  static size_t bytes(int maxj) {
-    return (size_t)BAR_OFF + 2 * S * sizeof(uint64_t) + 2 * sizeof(int) +
-           (size_t)maxj * sizeof(int2) + 128;
-  }
+  // bytes of dynamic shared memory (stages, profile tables, barriers, flags,
+  // and 128 bytes of slack for aligning the carve)
+  static constexpr size_t BYTES =
+      (size_t)BAR_OFF + 2 * S * sizeof(uint64_t) + 2 * sizeof(int) + 128;
 };
 
 struct alignas(64) TmapSet {
@@ -61,7 +77,7 @@ struct Plan {
   int ntx;     // tiles along x
   int ntiles;  // tiles per plane
   int nsplit;  // z ranges per tile
-  int maxj;    // job-list capacity
+  int tx, ty;  // tile size (columns, rows)
 };
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
@@ -94,12 +110,11 @@ struct Smem {
   unsigned char* stages;
   T* sbJ;  // b_y of rows j0-1 .. j0+TY
   T* sgJ;  // 1 + c_y of the same rows
-  T* sbK;  // b_x of columns k0-1 .. k0+TX
+  T* sbK;  // b_x of columns k0-1 .. k0+TX (the geometry's TX)
   T* sgK;  // 1 + c_x of the same columns
   uint64_t* full;
   uint64_t* empty;
   int* flags;  // [0] job count, [1] abort flag
-  int2* jobs;
 
   __device__ explicit Smem(unsigned char* raw) {
     // TMA destinations must be 128-byte aligned: align the carve explicitly
@@ -107,13 +122,12 @@ struct Smem {
         (reinterpret_cast<uintptr_t>(raw) + 127) & ~static_cast<uintptr_t>(127));
     stages = s;
     sbJ = reinterpret_cast<T*>(s + L::S * L::STAGE_BYTES);
-    sgJ = sbJ + (TY + 2);
-    sbK = sgJ + (TY + 2);
-    sgK = sbK + (TX + 2);
+    sgJ = sbJ + (L::G::TY + 2);
+    sbK = sgJ + (L::G::TY + 2);
+    sgK = sbK + (L::G::TX + 2);
     full = reinterpret_cast<uint64_t*>(s + L::BAR_OFF);
     empty = full + L::S;
     flags = reinterpret_cast<int*>(empty + L::S);
-    jobs = reinterpret_cast<int2*>(flags + 2);
   }
   // ring array a of job q's stage
   __device__ const T* arr(int q, int a) const {
@@ -126,51 +140,49 @@ struct Smem {
   }
 };
 
-// Per-CTA geometry derived from the plan.
+// Per-CTA geometry derived from the plan.  The CTA stages the planes
+// zs .. zs + njobs - 1 in this order: the warm-up plane z0-1 (when z0 > 0),
+// z0 .. z1-1, and plane z1 (when z1 < D), read only as the "next" plane.
 struct Range {
-  int tile, z0, z1, k0, j0;
+  int tile, z0, z1, k0, j0, zs, njobs;
   __device__ Range(const Plan& plan, int D) {
     tile = blockIdx.x % plan.ntiles;
     const int split = blockIdx.x / plan.ntiles;
     z0 = (int)((long long)split * D / plan.nsplit);
     z1 = (int)((long long)(split + 1) * D / plan.nsplit);
-    k0 = (tile % plan.ntx) * TX;
-    j0 = (tile / plan.ntx) * TY;
+    k0 = (tile % plan.ntx) * plan.tx;
+    j0 = (tile / plan.ntx) * plan.ty;
+    zs = z0 > 0 ? z0 - 1 : z0;
+    njobs = (z1 - zs) + (z1 < D ? 1 : 0);
   }
 };
 
-// Thread 0 builds the job list (planes whose inputs this CTA stages, in
-// consumption order: warm-up plane z0-1, z0..z1-1, and plane z1 read only as
-// the "next" plane), initialises the barriers; all threads fill the CPML
-// profile tables of the tile.  Ends with the kernel's only CTA-wide barrier.
-// Returns the job count (0 when a previous launch recorded an error, which
-// turns this launch into a no-op).
+// Thread 0 initialises the barriers and the job count; all threads fill the
+// CPML profile tables of the tile.  Ends with the kernel's only CTA-wide
+// barrier.  Returns the job count (0 when a previous launch recorded an
+// error, which turns this launch into a no-op).
 template <typename T, typename L>
 __device__ int pipe_setup(const Smem<T, L>& sm, const Range& R, int D, int H, int W,
                           const double* const b[3], const double* const c[3],
                           const int* status) {
   const int tid = threadIdx.x;
   if (tid == 0) {
-    int nj = 0;
-    if (R.z0 > 0) sm.jobs[nj++] = make_int2(R.tile, R.z0 - 1);
-    for (int z = R.z0; z < R.z1; ++z) sm.jobs[nj++] = make_int2(R.tile, z);
-    if (R.z1 < D) sm.jobs[nj++] = make_int2(R.tile, R.z1);
     const bool skip = status != nullptr && *reinterpret_cast<const volatile int*>(status) != 0;
-    sm.flags[0] = skip ? 0 : nj;
+    sm.flags[0] = skip ? 0 : R.njobs;
     sm.flags[1] = 0;
     for (int s = 0; s < L::S; ++s) {
       mbar_init(&sm.full[s], 1);
-      mbar_init(&sm.empty[s], NCW);
+      mbar_init(&sm.empty[s], L::G::NCW);
     }
     fence_barrier_init();
   }
-  for (int e = tid; e < TY + 2; e += blockDim.x) {
+  for (int e = tid; e < L::G::TY + 2; e += blockDim.x) {
     const int j = R.j0 - 1 + e;
     const bool ok = j >= 0 && j < H;
     sm.sbJ[e] = ok ? static_cast<T>(b[1][j]) : T(1);
     sm.sgJ[e] = ok ? static_cast<T>(1.0 + c[1][j]) : T(1);
   }
-  for (int e = tid; e < TX + 2; e += blockDim.x) {
+  for (int e = tid; e < L::G::TX + 2; e += blockDim.x) {
     const int kx = R.k0 - 1 + e;
     const bool ok = kx >= 0 && kx < W;
     sm.sbK[e] = ok ? static_cast<T>(b[2][kx]) : T(1);
@@ -194,7 +206,7 @@ __device__ void producer_run(const Smem<T, L>& sm, const TmapSet& tm, const Rang
   for (int q = 0; q < nj && ok; ++q) {
     if (q >= L::S) ok = wait_phase(&sm.empty[q % L::S], ((q / L::S) - 1) & 1, abort);
     if (!ok) break;
-    const int z = sm.jobs[q].y;
+    const int z = R.zs + q;
     uint64_t* bar = &sm.full[q % L::S];
     unsigned char* dst = sm.stages + (q % L::S) * L::STAGE_BYTES;
     fence_proxy_async_smem();
@@ -228,14 +240,16 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
 
 EncodeTiledFn get_encode();
 
-// ring (40 x 18 x 1) map over a (D, H, W) field with the grid's pitches
-int encode_ring(CUtensorMap* m, const void* base, const dn_grid* g, int elem_bytes);
+// ring (bx x by x 1; default 40 x 18) map over a (D, H, W) field with the
+// grid's pitches
+int encode_ring(CUtensorMap* m, const void* base, const dn_grid* g, int elem_bytes, int bx = BX,
+                int by = BY);
 // tile (32 x 16 x 1 x 1) map over `nslots` fields of the grid's shape,
 // `slot_stride` elements apart
 int encode_tile4(CUtensorMap* m, const void* base, const dn_grid* g, int elem_bytes, int nslots,
                  long long slot_stride);
-// work split for `capacity` resident CTAs
-Plan make_plan(const dn_grid* g, long long capacity, long long* nctas);
+// work split for `capacity` resident CTAs over tx x ty tiles
+Plan make_plan(const dn_grid* g, long long capacity, long long* nctas, int tx = TX, int ty = TY);
 // TMA constraints: 16-byte aligned bases and byte strides
 bool tma_ok(const dn_grid* g, int elem_bytes, const void* const* ptrs, int n);
 
