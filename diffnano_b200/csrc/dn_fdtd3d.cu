@@ -23,8 +23,6 @@
 //    six results to the other ping-pong buffer (neighbouring CTAs still read
 //    the old one);
 //  * optionally (adjoint replay) the curl term of each E update is recorded.
-#include <cstdlib>
-
 #include "dn_zmarch.cuh"
 
 namespace dn {
@@ -687,21 +685,6 @@ int dispatch(const dn_grid* g, bool record, const StepParams<T>& p, const TmapSe
                                                                   plan, n, smem, rec, s);
 }
 
-// Lane columns of the FP32 kernel: DN_FWD3D_LANE_COLUMNS by default, or the
-// environment variable DN_FDTD3D_LANE_COLUMNS ("1" or "2", read once per
-// process), e.g. to compare the two kernels.
-#ifndef DN_FWD3D_LANE_COLUMNS
-#define DN_FWD3D_LANE_COLUMNS 1
-#endif
-bool two_column_fp32() {
-  static const bool on = [] {
-    const char* v = std::getenv("DN_FDTD3D_LANE_COLUMNS");
-    if (v && v[0] == '1' && v[1] == '\0') return false;
-    if (v && v[0] == '2' && v[1] == '\0') return true;
-    return DN_FWD3D_LANE_COLUMNS == 2;
-  }();
-  return on;
-}
 
 template <typename T>
 int run3d(const dn_grid* g, void* const fa[6], void* const fb[6], const void* ce,

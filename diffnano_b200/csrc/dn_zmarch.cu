@@ -1,5 +1,6 @@
 // Host helpers of the 3-D z-marching kernels: TMA tensor-map encoding (via
 // the driver entry point, no libcuda link) and the work split.
+#include <cstdlib>
 #include <mutex>
 
 #include "dn_zmarch.cuh"
@@ -73,6 +74,19 @@ Plan make_plan(const dn_grid* g, long long capacity, long long* nctas, int tx, i
   plan.nsplit = (int)nsplit;
   *nctas = (long long)plan.ntiles * nsplit;
   return plan;
+}
+
+#ifndef DN_FWD3D_LANE_COLUMNS
+#define DN_FWD3D_LANE_COLUMNS 1
+#endif
+bool two_column_fp32() {
+  static const bool on = [] {
+    const char* v = std::getenv("DN_FDTD3D_LANE_COLUMNS");
+    if (v && v[0] == '1' && v[1] == '\0') return false;
+    if (v && v[0] == '2' && v[1] == '\0') return true;
+    return DN_FWD3D_LANE_COLUMNS == 2;
+  }();
+  return on;
 }
 
 bool tma_ok(const dn_grid* g, int elem_bytes, const void* const* ptrs, int n) {

@@ -250,6 +250,11 @@ int encode_tile4(CUtensorMap* m, const void* base, const dn_grid* g, int elem_by
                  long long slot_stride);
 // work split for `capacity` resident CTAs over tx x ty tiles
 Plan make_plan(const dn_grid* g, long long capacity, long long* nctas, int tx = TX, int ty = TY);
+// Does FP32 run the two-column kernels (forward and adjoint)?
+// DN_FWD3D_LANE_COLUMNS at build time, or the environment variable
+// DN_FDTD3D_LANE_COLUMNS = "1" or "2" (read once per process), e.g. to compare
+// the one- and two-column kernels.
+bool two_column_fp32();
 // TMA constraints: 16-byte aligned bases and byte strides
 bool tma_ok(const dn_grid* g, int elem_bytes, const void* const* ptrs, int n);
 
