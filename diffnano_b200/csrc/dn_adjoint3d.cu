@@ -314,7 +314,7 @@ __device__ __forceinline__ float2 ld2(const float* a) {
 __device__ __forceinline__ float sel(const float2 v, int c) { return c == 0 ? v.x : v.y; }
 
 template <int AXES>
-__global__ void __maxnreg__(112)
+__global__ void __launch_bounds__(Geo64::NCW * 32, 2)
     k_adj3d_v2(const AdjParams<float> p, const __grid_constant__ TmapSet tm, const Plan plan) {
   using T = float;
   using L = LA2;
@@ -334,11 +334,14 @@ __global__ void __maxnreg__(112)
   const int nj = pipe_setup(sm, R, D, H, W, p.b, p.c, p.status);
   if (nj == 0) return;
 
-  if (warp == G::NCW) {
-    if (lane == 0)
-      producer_run<T, L, NRING_A, 0>(sm, tm, R, nj, p.status, [](int) { return 0; });
-    return;
-  }
+  // lane 0 of warp 0 issues the stage loads: the first S jobs now, job q + S
+  // once every warp released job q (no separate producer warp: eight warps
+  // per CTA keep two CTAs per SM within the register file)
+  const bool producer = warp == 0 && lane == 0;
+  auto slot0 = [](int) { return 0; };
+  int issued = 0;
+  if (producer)
+    for (; issued < S && issued < nj; ++issued) issue_job<T, L, NRING_A, 0>(sm, tm, R, issued, slot0);
 
   volatile int* s_abort = sm.flags + 1;
   const int w = warp;
@@ -378,15 +381,24 @@ __global__ void __maxnreg__(112)
     __syncwarp();
     return r;
   };
-  auto release = [&](int qa) {
+  // release job qa; the producer lane then refills its stage with job qa + S
+  auto release = [&](int qa) -> bool {
     __syncwarp();
     if (lane == 0) mbar_arrive(&sm.empty[qa % S]);
+    bool ok = true;
+    if (producer && qa + S < nj) {
+      ok = wait_phase(&sm.empty[qa % S], (qa / S) & 1, s_abort);
+      if (ok) issue_job<T, L, NRING_A, 0>(sm, tm, R, qa + S, slot0);
+      if (ok) issued = qa + S + 1;
+    }
+    return __shfl_sync(FULL_MASK, ok ? 1 : 0, 0) != 0;
   };
   auto fail = [&]() {
     if (lane == 0) {
       report_status(p.status, DN_ETIMEOUT);
       *s_abort = 1;
     }
+    if (producer) drain_jobs(sm, issued);
   };
   // z roles of plane i per column (reference mapping: per column; physical:
   // per plane)
@@ -475,7 +487,10 @@ __global__ void __maxnreg__(112)
         pvyi[r - 1][c] = hy_c1[c] * lhy[c];
       }
     }
-    release(q);
+    if (!release(q)) {
+      fail();
+      return;
+    }
     ++q;
   }
 
@@ -644,10 +659,13 @@ __global__ void __maxnreg__(112)
         pvyi[r - 1][c] = vyi[c];
       }
     }
-    release(q);
+    if (!release(q)) {
+      fail();
+      return;
+    }
     ++q;
   }
-  if (z1 < D) release(q);
+  if (z1 < D) (void)release(q);  // the last job: nothing left to issue
 }
 
 // FP32 two-column reverse steps (k_adj3d_v2): ring maps with 72 x 18 boxes,
@@ -674,6 +692,8 @@ int launch_adj_v2(AdjParams<float> p, void* const la[6], void* const lb[6], cons
   auto kern = k_adj3d_v2<AXES>;
   DN_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)smem));
+  DN_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     (int)cudaSharedmemCarveoutMaxShared));
   for (int n = 0; n < nsteps; ++n) {
     const bool even = (n % 2) == 0;
     for (int c = 0; c < 6; ++c) {
@@ -682,7 +702,7 @@ int launch_adj_v2(AdjParams<float> p, void* const la[6], void* const lb[6], cons
     }
     p.t = t_end - 1 - n;
     if (n_mon > 0 && (rc = inject_monitors<float>(p, mons, n_mon, true, 0, s)) != DN_OK) return rc;
-    kern<<<(unsigned)nctas, Geo64::NT, smem, s>>>(p, even ? ta : tb, plan);
+    kern<<<(unsigned)nctas, Geo64::NCW * 32, smem, s>>>(p, even ? ta : tb, plan);
   }
   DN_CUDA_CHECK(cudaGetLastError());
   return DN_OK;

@@ -337,7 +337,7 @@ __global__ void __launch_bounds__(NT, FwdCfg<T>::MINB)
 // halo-column and per-plane overhead; the arithmetic of every column is the
 // one-column kernel's, expression for expression.
 // ---------------------------------------------------------------------------
-constexpr int S_V2 = 3;  // ring depth: two 109 KB CTAs per SM
+constexpr int S_V2 = 3;  // ring depth: two 109 KB CTAs per SM (maximum carveout)
 using LV2 = Layout<float, NRING_F, 0, S_V2, Geo64>;
 
 __device__ __forceinline__ float2 ld2(const float* a) {
@@ -353,9 +353,10 @@ __device__ __forceinline__ void st2(float* base, long long o, float a, float b, 
     base[o] = a;
 }
 
-// 112 registers x 288 threads: two CTAs per SM (64,512 of 65,536 registers)
+// eight warps x up to 128 registers: two CTAs per SM (each SM sub-partition
+// holds four warps of 128 x 32 registers)
 template <int AXES, bool REC>
-__global__ void __maxnreg__(112)
+__global__ void __launch_bounds__(Geo64::NCW * 32, 2)
     k_fdtd3d_v2(const StepParams<float> p, const __grid_constant__ TmapSet tm, const Plan plan,
                 const CurlRec<float> rec) {
   using T = float;
@@ -376,11 +377,14 @@ __global__ void __maxnreg__(112)
   const int nj = pipe_setup(sm, R, D, H, W, p.b, p.c, p.status);
   if (nj == 0) return;
 
-  if (warp == G::NCW) {  // producer warp
-    if (lane == 0)
-      producer_run<T, L, NRING_F, 0>(sm, tm, R, nj, p.status, [](int) { return 0; });
-    return;
-  }
+  // lane 0 of warp 0 issues the stage loads: the first S jobs now, job q + S
+  // once every warp released job q (no separate producer warp: eight warps
+  // per CTA keep two CTAs per SM within the register file)
+  const bool producer = warp == 0 && lane == 0;
+  auto slot0 = [](int) { return 0; };
+  int issued = 0;
+  if (producer)
+    for (; issued < S && issued < nj; ++issued) issue_job<T, L, NRING_F, 0>(sm, tm, R, issued, slot0);
 
   // ======================= consumer warps ===================================
   volatile int* s_abort = sm.flags + 1;
@@ -420,15 +424,24 @@ __global__ void __maxnreg__(112)
     __syncwarp();
     return r;
   };
-  auto release = [&](int qa) {
+  // release job qa; the producer lane then refills its stage with job qa + S
+  auto release = [&](int qa) -> bool {
     __syncwarp();
     if (lane == 0) mbar_arrive(&sm.empty[qa % S]);
+    bool ok = true;
+    if (producer && qa + S < nj) {
+      ok = wait_phase(&sm.empty[qa % S], (qa / S) & 1, s_abort);
+      if (ok) issue_job<T, L, NRING_F, 0>(sm, tm, R, qa + S, slot0);
+      if (ok) issued = qa + S + 1;
+    }
+    return __shfl_sync(FULL_MASK, ok ? 1 : 0, 0) != 0;
   };
   auto fail = [&]() {
     if (lane == 0) {
       report_status(p.status, DN_ETIMEOUT);
       *s_abort = 1;
     }
+    if (producer) drain_jobs(sm, issued);
   };
   // z (i) roles per column: per lane for the reference mapping, per plane for
   // the physical one
@@ -483,7 +496,10 @@ __global__ void __maxnreg__(112)
                            hy_c2 * (ezk - sel(ez, c));
       }
     }
-    release(q);
+    if (!release(q)) {
+      fail();
+      return;
+    }
     ++q;
   }
 
@@ -636,10 +652,13 @@ __global__ void __maxnreg__(112)
         prevHy[r - 1][c] = Hy[r][c];
       }
     }
-    release(q);
+    if (!release(q)) {
+      fail();
+      return;
+    }
     ++q;
   }
-  if (z1 < D) release(q);  // the E-only job of plane z1 was read as "next"
+  if (z1 < D) (void)release(q);  // the last job: nothing left to issue  // the E-only job of plane z1 was read as "next"
 }
 
 // ---------------------------------------------------------------------------
@@ -653,7 +672,9 @@ int launch_all(const StepParams<T>& base, const TmapSet& ta, const TmapSet& tb, 
   int nt = NT;
   if constexpr (TWO_COL) {
     kern = k_fdtd3d_v2<AXES, REC>;
-    nt = Geo64::NT;
+    nt = Geo64::NCW * 32;  // eight warps, no separate producer warp
+    DN_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                       (int)cudaSharedmemCarveoutMaxShared));
   } else {
     kern = k_fdtd3d<T, AXES, REC>;
   }

@@ -192,6 +192,36 @@ __device__ int pipe_setup(const Smem<T, L>& sm, const Range& R, int D, int H, in
   return sm.flags[0];
 }
 
+// Issue job q's loads into stage q % S: NRING ring boxes and NTILE tile boxes
+// (4-D tile maps, slot coordinate `tile_slot(z)`), completion counted on the
+// stage's "full" barrier.  The stage must have been released by every
+// consumer warp.
+template <typename T, typename L, int NRING, int NTILE, typename SlotFn>
+__device__ __forceinline__ void issue_job(const Smem<T, L>& sm, const TmapSet& tm,
+                                          const Range& R, int q, SlotFn tile_slot) {
+  const int z = R.zs + q;
+  uint64_t* bar = &sm.full[q % L::S];
+  unsigned char* dst = sm.stages + (q % L::S) * L::STAGE_BYTES;
+  fence_proxy_async_smem();
+  mbar_arrive_expect_tx(bar, L::TX_BYTES);
+#pragma unroll
+  for (int a = 0; a < NRING; ++a)
+    tma_load_3d(dst + a * L::RING_ARR, &tm.m[a], bar, R.k0 - 4, R.j0 - 1, z);
+#pragma unroll
+  for (int a = 0; a < NTILE; ++a)
+    tma_load_4d(dst + NRING * L::RING_ARR + a * L::TILE_ARR, &tm.m[NRING + a], bar, R.k0, R.j0,
+                z, tile_slot(z));
+}
+
+// Wait (bounded) until the copies of the last S issued jobs have landed, so
+// that none is in flight when the CTA gives its shared memory back (error
+// paths; jobs before those were consumed before their stage was reused).
+template <typename T, typename L>
+__device__ __forceinline__ void drain_jobs(const Smem<T, L>& sm, int issued) {
+  for (int q = max(0, issued - L::S); q < issued; ++q)
+    (void)mbar_wait_bounded(&sm.full[q % L::S], (q / L::S) & 1, WAIT_PROBES);
+}
+
 // Producer (lane 0 of the last warp): stream job q's NRING ring boxes and
 // NTILE tile boxes into stage q % S once the consumers released the stage's
 // previous job; tile maps are 4-D (x, y, z, slot) with the slot coordinate
@@ -206,18 +236,7 @@ __device__ void producer_run(const Smem<T, L>& sm, const TmapSet& tm, const Rang
   for (int q = 0; q < nj && ok; ++q) {
     if (q >= L::S) ok = wait_phase(&sm.empty[q % L::S], ((q / L::S) - 1) & 1, abort);
     if (!ok) break;
-    const int z = R.zs + q;
-    uint64_t* bar = &sm.full[q % L::S];
-    unsigned char* dst = sm.stages + (q % L::S) * L::STAGE_BYTES;
-    fence_proxy_async_smem();
-    mbar_arrive_expect_tx(bar, L::TX_BYTES);
-#pragma unroll
-    for (int a = 0; a < NRING; ++a)
-      tma_load_3d(dst + a * L::RING_ARR, &tm.m[a], bar, R.k0 - 4, R.j0 - 1, z);
-#pragma unroll
-    for (int a = 0; a < NTILE; ++a)
-      tma_load_4d(dst + NRING * L::RING_ARR + a * L::TILE_ARR, &tm.m[NRING + a], bar, R.k0, R.j0,
-                  z, tile_slot(z));
+    issue_job<T, L, NRING, NTILE>(sm, tm, R, q, tile_slot);
     issued = q + 1;
   }
   for (int q = max(0, nj - L::S); q < nj && ok; ++q)
@@ -225,8 +244,7 @@ __device__ void producer_run(const Smem<T, L>& sm, const TmapSet& tm, const Rang
   if (!ok) {
     report_status(status, DN_ETIMEOUT);
     *abort = 1;
-    for (int q = max(0, issued - L::S); q < issued; ++q)
-      (void)mbar_wait_bounded(&sm.full[q % L::S], (q / L::S) & 1, WAIT_PROBES);
+    drain_jobs(sm, issued);
   }
 }
 
