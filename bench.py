@@ -708,7 +708,7 @@ def run_design(args):
     prob2 = Metalens3D(setup, dev)
     from diffnano_b200.surrogate.fno import FNOConfig
     dz, dx = setup.design_shape
-    cfg = SurrogateConfig(max_verify=args.design_max_verify,
+    cfg = SurrogateConfig(max_verify=args.design_max_verify, model=args.design_model,
                           fno=FNOConfig(H=dz, W=dx, modes=min(16, dz // 2 - 1),
                                         eps_lo=setup.eps_lo, eps_hi=setup.eps_hi))
     loop = SurrogateAssistedLoop(prob2, cfg)
@@ -728,11 +728,18 @@ def run_design(args):
                                            "projection, beta 1->32",
                        "fom": "|DFT Ey(1550 nm)|^2 at the focal point",
                        "plain": f"{args.design_iters} Adam iterations, FDTD forward+adjoint each",
+                       "assisted": "model (mapped to the 3-D focal field by a fitted output "
+                                   "map) gives the warm start and proposes trust-region steps; "
+                                   f"it checks the FNO's top {cfg.n_check}; the 3-D FDTD "
+                                   "verifies the best and judges every step",
                        "surrogate": f"FNO trained on {cfg.n_train} batched-FDTD labels of the "
                                     f"2-D cross-section prescreens {cfg.n_candidates} candidates "
-                                    f"per verification, the batched cross-section FDTD (mapped to "
-                                    f"3-D by a fitted output map) proposes and checks "
-                                    f"{cfg.n_check}, the 3-D FDTD verifies the best"},
+                                    f"per verification; the {cfg.model} model "
+                                    f"({cfg.coarse_factor}x coarser 3-D cells)"
+                                    if cfg.model == "coarse3d" else
+                                    f"FNO trained on {cfg.n_train} batched-FDTD labels of the "
+                                    f"2-D cross-section prescreens {cfg.n_candidates} candidates "
+                                    f"per verification; the cross-section model"},
             "plain": {"history": [{"n": r.verification, "t": round(r.wall_s, 2),
                                    "fom": r.fom / plain["fom0"], "beta": round(r.beta, 2)}
                                   for r in plain["history"]],
@@ -746,7 +753,8 @@ def run_design(args):
                          if res["best_fom"] else None,
                          "fdtd_verifications": res["verifications"],
                          "timings": res["timings"], "proxy_heldout_rel_l2": loop.proxy_error(),
-                         "output_map": res["map"], "candidates": res["candidates"],
+                         "model": res["model"], "output_map": res["map"],
+                         "network_map": res["net_map"], "candidates": res["candidates"],
                          "history": hist},
             "clocks": clocks.summary()}
     print(json.dumps(line), flush=True)
@@ -1073,6 +1081,8 @@ def main():
     ap.add_argument("--fno-batch", type=int, default=256)
     ap.add_argument("--design-iters", type=int, default=100)
     ap.add_argument("--design-max-verify", type=int, default=60)
+    ap.add_argument("--design-model", choices=["coarse3d", "cross-section"], default="coarse3d",
+                    help="proposing model of the assisted design loop")
     ap.add_argument("--design-scale", type=int, default=1,
                     help="shrink the design workload's grid by this factor (tests)")
     ap.add_argument("--fno-samples", type=int, default=20000)

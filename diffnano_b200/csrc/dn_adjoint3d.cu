@@ -334,14 +334,15 @@ __global__ void __launch_bounds__(Geo64::NCW * 32, 2)
   const int nj = pipe_setup(sm, R, D, H, W, p.b, p.c, p.status);
   if (nj == 0) return;
 
-  // lane 0 of warp 0 issues the stage loads: the first S jobs now, job q + S
-  // once every warp released job q (no separate producer warp: eight warps
-  // per CTA keep two CTAs per SM within the register file)
-  const bool producer = warp == 0 && lane == 0;
+  // No separate producer warp (eight warps per CTA keep two CTAs per SM within
+  // the register file): lane 0 of warp 0 issues the first S jobs, and the
+  // warp that releases job q last issues job q + S into its stage at once.
   auto slot0 = [](int) { return 0; };
-  int issued = 0;
-  if (producer)
-    for (; issued < S && issued < nj; ++issued) issue_job<T, L, NRING_A, 0>(sm, tm, R, issued, slot0);
+  if (warp == 0 && lane == 0) {
+    const int n0 = min(S, nj);
+    for (int qa = 0; qa < n0; ++qa) issue_job<T, L, NRING_A, 0>(sm, tm, R, qa, slot0);
+    atomicMax(&sm.flags[2], n0);
+  }
 
   volatile int* s_abort = sm.flags + 1;
   const int w = warp;
@@ -381,24 +382,29 @@ __global__ void __launch_bounds__(Geo64::NCW * 32, 2)
     __syncwarp();
     return r;
   };
-  // release job qa; the producer lane then refills its stage with job qa + S
+  // release job qa: the warp's reads of its stage are ordered before its
+  // count; the warp whose count completes the stage's (qa / S + 1)-th use
+  // refills it with job qa + S (counts only grow, so no reset races)
   auto release = [&](int qa) -> bool {
     __syncwarp();
-    if (lane == 0) mbar_arrive(&sm.empty[qa % S]);
-    bool ok = true;
-    if (producer && qa + S < nj) {
-      ok = wait_phase(&sm.empty[qa % S], (qa / S) & 1, s_abort);
-      if (ok) issue_job<T, L, NRING_A, 0>(sm, tm, R, qa + S, slot0);
-      if (ok) issued = qa + S + 1;
+    if (lane == 0) {
+      __threadfence_block();
+      const unsigned prev = atomicAdd(&sm.release[qa % S], 1u);
+      if (prev == (unsigned)(G::NCW * (qa / S + 1) - 1) && qa + S < nj) {
+        __threadfence_block();
+        issue_job<T, L, NRING_A, 0>(sm, tm, R, qa + S, slot0);
+        atomicMax(&sm.flags[2], qa + S + 1);
+      }
     }
-    return __shfl_sync(FULL_MASK, ok ? 1 : 0, 0) != 0;
+    return true;
   };
+  // on an error every warp waits (bounded) for the copies still in flight
   auto fail = [&]() {
     if (lane == 0) {
       report_status(p.status, DN_ETIMEOUT);
       *s_abort = 1;
+      drain_jobs(sm, *reinterpret_cast<volatile int*>(&sm.flags[2]));
     }
-    if (producer) drain_jobs(sm, issued);
   };
   // z roles of plane i per column (reference mapping: per column; physical:
   // per plane)

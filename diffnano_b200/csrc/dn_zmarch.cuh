@@ -61,7 +61,7 @@ struct Layout {
   // bytes of dynamic shared memory (stages, profile tables, barriers, flags,
   // and 128 bytes of slack for aligning the carve)
   static constexpr size_t BYTES =
-      (size_t)BAR_OFF + 2 * S * sizeof(uint64_t) + 2 * sizeof(int) + 128;
+      (size_t)BAR_OFF + 2 * S * sizeof(uint64_t) + (4 + S) * sizeof(int) + 128;
 };
 
 struct alignas(64) TmapSet {
@@ -114,7 +114,8 @@ struct Smem {
   T* sgK;  // 1 + c_x of the same columns
   uint64_t* full;
   uint64_t* empty;
-  int* flags;  // [0] job count, [1] abort flag
+  int* flags;         // [0] job count, [1] abort flag, [2] jobs issued
+  unsigned* release;  // per stage: warp releases so far (refill by the last one)
 
   __device__ explicit Smem(unsigned char* raw) {
     // TMA destinations must be 128-byte aligned: align the carve explicitly
@@ -128,6 +129,7 @@ struct Smem {
     full = reinterpret_cast<uint64_t*>(s + L::BAR_OFF);
     empty = full + L::S;
     flags = reinterpret_cast<int*>(empty + L::S);
+    release = reinterpret_cast<unsigned*>(flags + 4);
   }
   // ring array a of job q's stage
   __device__ const T* arr(int q, int a) const {
@@ -170,6 +172,8 @@ __device__ int pipe_setup(const Smem<T, L>& sm, const Range& R, int D, int H, in
     const bool skip = status != nullptr && *reinterpret_cast<const volatile int*>(status) != 0;
     sm.flags[0] = skip ? 0 : R.njobs;
     sm.flags[1] = 0;
+    sm.flags[2] = 0;
+    for (int s = 0; s < L::S; ++s) sm.release[s] = 0;
     for (int s = 0; s < L::S; ++s) {
       mbar_init(&sm.full[s], 1);
       mbar_init(&sm.empty[s], L::G::NCW);

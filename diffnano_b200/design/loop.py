@@ -11,11 +11,12 @@ ones expensively) are the pattern; here they run inside a gradient loop:
   forward + adjoint and takes an Adam step on the density (``dn_adam``), with
   the projection sharpness beta raised from ``beta[0]`` to ``beta[1]``
   (``beta_continuation_schedule``).
-* :class:`SurrogateAssistedLoop` -- candidates proposed on the 2-D cross-
-  section (mapped to the 3-D focal field by :class:`OutputMap`), ranked by a
-  Fourier neural operator trained on batched-FDTD labels, checked by the
-  batched cross-section FDTD, verified by the 3-D FDTD.  Wall time includes the
-  proxy labelling and the network's training.
+* :class:`SurrogateAssistedLoop` -- candidates proposed by a cheaper model of
+  the lens (by default the same 3-D problem on 2x coarser cells; or the 2-D
+  cross-section), mapped to the 3-D focal field by :class:`OutputMap`, ranked
+  by a Fourier neural operator trained on batched-FDTD labels, checked by the
+  model, verified by the 3-D FDTD.  Wall time includes the proxy labelling
+  and the network's training.
 """
 from __future__ import annotations
 
@@ -30,7 +31,7 @@ import torch
 from .. import _lib
 from ..surrogate.data import from_targets, label_scale, to_targets
 from ..surrogate.fno import FNO2d, FNOConfig, OUT_LD
-from .metalens import Metalens3D, Proxy2D, proxy_dataset
+from .metalens import Metalens3D, Proxy2D, coarse_model, proxy_dataset
 from .projection import beta_continuation_schedule
 
 
@@ -58,13 +59,14 @@ class DensityAdam:
 
 
 class OutputMap:
-    """Output-space map from the cross-section model to the 3-D focal field.
+    """Output-space map from a cheaper model's focal value to the 3-D focal field.
 
-    The 3-D lens is finite in y and the plane wave also passes beside it, so
-    the 3-D focal field is not the 2-D cross-section's; measured over very
-    different designs (uniform, random, cross-section optima) it is close to
-    an affine image of it, E3 = c S + b with complex c and b (7.6 % relative
-    residual over 13 designs, against 9.7 % for E3 = c S).  The map is fitted
+    For the 2-D cross-section: the 3-D lens is finite in y and the plane wave
+    also passes beside it, so the 3-D focal field is not the cross-section's;
+    measured over very different designs (uniform, random, cross-section
+    optima) it is close to an affine image of it, E3 = c S + b with complex c
+    and b (7.6 % relative residual over 13 designs, against 9.7 % for E3 =
+    c S).  The same form maps the coarse 3-D model and the network.  The map is fitted
     by complex least squares to the (surrogate value, FDTD value) pairs of
     every 3-D verification so far: with one pair b = 0 and c = E3 / S; with
     more, both (Bandler et al.'s output space mapping, IEEE MTT 52, 2004)."""
@@ -132,15 +134,17 @@ def plain_loop(problem: Metalens3D, rho0: torch.Tensor, iters: int = 100, lr: fl
 
 @dataclass
 class SurrogateConfig:
-    n_train: int = 4096          # proxy designs labelled by the batched 2-D FDTD
-    epochs: int = 20
+    n_train: int = 1024          # proxy designs labelled by the batched 2-D FDTD
+    epochs: int = 12
     batch: int = 256
     lr: float = 1e-3
-    warm_steps: int = 60         # warm start: Adam steps on the mapped cross-section model
+    model: str = "coarse3d"      # proposing model: "coarse3d" or "cross-section"
+    coarse_factor: int = 2       # cell-size factor of the coarse 3-D model
+    warm_steps: int = 60         # warm start: Adam steps on the mapped model, beta ramped
     warm_lr: float = 0.05
-    inner_steps: int = 8         # trust-region path per verification (one snapshot per step)
+    inner_steps: int = 6         # trust-region path per verification (one snapshot per step)
     n_scales: int = 4            # step-length variants per snapshot: candidates = steps * scales
-    n_check: int = 4             # candidates the FNO passes on to the 2-D FDTD
+    n_check: int = 2             # candidates the FNO passes on to the model's check
     inner_lr: float = 0.02
     max_inner_lr: float = 0.2
     min_inner_lr: float = 1e-4
@@ -161,37 +165,39 @@ class SurrogateAssistedLoop:
 
     Three models of the FOM, cheapest first:
 
-    * the FNO (trained on batched-FDTD labels of the cross-section, fine-tuned
-      on every cross-section the loop evaluates) prescreens ``n_candidates``
-      candidate steps per verification in one batched inference and passes
-      ``n_check`` on;
-    * the cross-section FDTD (2-D, ~0.07 s for a value and its adjoint
-      gradient; batched for the checks), mapped to the 3-D focal field by an
-      :class:`OutputMap` fitted to every verification so far, proposes the
-      steps and checks the prescreened candidates;
+    * the FNO (trained on batched-FDTD labels of the lens's 2-D cross-section)
+      prescreens ``n_candidates`` candidate steps per verification in one
+      batched inference and passes ``n_check`` on; its focal value is mapped
+      to the 3-D focal field by its own :class:`OutputMap`, fitted to every
+      verification so far;
+    * the proposing model, mapped to the 3-D focal field by an
+      :class:`OutputMap`: by default (``model="coarse3d"``) the same lens on
+      2x coarser cells (:func:`coarse_model`, ~0.28 s for a value and its
+      adjoint gradient on the workload, 1/12 of the full solve), or the 2-D
+      cross-section (``"cross-section"``, ~0.07 s; its optimum is about half
+      the 3-D one); it proposes the steps and checks the prescreened
+      candidates;
     * the 3-D FDTD forward + adjoint verifies the best checked candidate.
 
-    Run: (1) the 3-D FOM and gradient at the start design; (2) warm start:
-    Adam on the mapped cross-section model with beta ramped to its end value
-    (the cross-section's optimum is a good 3-D design, about half the 3-D
-    optimum's FOM), verified in 3-D; (3) trust-region steps at the end beta:
-    the cross-section model corrected to first order at the accepted design
-    rho_k, m(rho) = f_k + M(rho) - M(rho_k) + (g_k - grad M(rho_k)) . (rho -
-    rho_k), which matches the 3-D value and gradient there (first-order model
-    management, Alexandrov et al., Structural Optimization 15, 1998); Adam on m
-    gives ``inner_steps`` snapshots, each at ``n_scales`` step lengths; the FNO
-    ranks them, the cross-section FDTD checks the top ``n_check``, the best goes
-    to 3-D.  Accepted when its FOM does not fall; the step size grows by half
-    when the gain reaches half the predicted one and shrinks to 0.3 on a
-    rejection (a gentler control, growth at a quarter and halving, accepted 29
-    of 58 steps on the 384x384x192 workload and ended lower).  Wall time
-    includes the proxy labelling and the network's training.
+    Run: (1) the 3-D FOM at the start design (forward only); (2) warm start:
+    Adam on the mapped model with beta ramped to its end value, verified in
+    3-D; (3) trust-region steps at the end beta: the model corrected to first
+    order at the accepted design rho_k, m(rho) = f_k + M(rho) - M(rho_k) +
+    (g_k - grad M(rho_k)) . (rho - rho_k), which matches the 3-D value and
+    gradient there (first-order model management, Alexandrov et al.,
+    Structural Optimization 15, 1998); Adam on m gives ``inner_steps``
+    snapshots, each at ``n_scales`` step lengths; the FNO ranks them, the
+    model checks the top ``n_check``, the best goes to 3-D.  Accepted when its
+    FOM does not fall; the step size grows by half when the gain reaches half
+    the predicted one and shrinks to 0.3 on a rejection.  Wall time includes
+    the proxy labelling and the network's training.
 
-    Measured limits that bound the speed-up: the cross-section alone saturates at about x47 of the start's 3-D FOM, so the
-    rest of the way needs 3-D gradients; and the network, held-out error ~0.6
-    on the cross-section labels, cannot propose designs itself (ascending its
-    own prediction leads to designs it overrates by orders of magnitude), so
-    it only ranks.
+    Measured on the 384x384x192 workload: the cross-section model saturates
+    near x47 of the start's 3-D FOM, the coarse 3-D model's own optimum scores
+    x68-69 on the full grid; the network (held-out error ~0.6 on the
+    cross-section labels) cannot propose designs itself (ascending its own
+    prediction leads to designs it overrates by orders of magnitude), so it
+    only ranks.
     """
 
     def __init__(self, problem: Metalens3D, cfg: SurrogateConfig = SurrogateConfig(),
@@ -201,10 +207,15 @@ class SurrogateAssistedLoop:
         s = problem.setup
         if (cfg.fno.H, cfg.fno.W) != s.design_shape:
             raise ValueError(f"surrogate input {(cfg.fno.H, cfg.fno.W)} != design {s.design_shape}")
+        if cfg.model not in ("coarse3d", "cross-section"):
+            raise ValueError(f"model must be 'coarse3d' or 'cross-section', got {cfg.model!r}")
         self.proxy = proxy or Proxy2D(s, device=problem.device)
+        self.model = (coarse_model(s, cfg.coarse_factor, problem.device)
+                      if cfg.model == "coarse3d" else self.proxy)
         self.net = FNO2d(cfg.fno, problem.device, seed=cfg.seed)
         self.scale = 1.0
-        self.map = OutputMap()
+        self.map = OutputMap()    # model focal value -> 3-D focal field
+        self.nmap = OutputMap()   # network focal value -> 3-D focal field
         self.timings: Dict[str, float] = {}
         self._buf_x: List[torch.Tensor] = []
         self._buf_y: List[torch.Tensor] = []
@@ -236,11 +247,13 @@ class SurrogateAssistedLoop:
         torch.cuda.synchronize(dev)
         self.net.check_status()
         self.timings.update(label_s=t1 - t0, train_s=time.perf_counter() - t1)
-        self._heldout = proxy_dataset(self.proxy, 256, seed=c.seed + 999)
 
     def proxy_error(self) -> float:
-        """Mean relative L2 error of the network on 256 held-out proxy designs."""
+        """Mean relative L2 error of the network on 256 held-out proxy designs
+        (labelled on first use, outside the timed loop)."""
         from ..surrogate.data import rel_l2_per_sample
+        if getattr(self, "_heldout", None) is None:
+            self._heldout = proxy_dataset(self.proxy, 256, seed=self.cfg.seed + 999)
         eps, labels = self._heldout
         pred = from_targets(self.net.forward(eps).clone(), self.scale, labels.shape[1])
         return float(rel_l2_per_sample(pred, labels).mean())
@@ -272,15 +285,34 @@ class SurrogateAssistedLoop:
 
     # ---- models -------------------------------------------------------------------
     def _mapped(self, rho: torch.Tensor, beta: float, grad: bool):
-        """(cross-section focal value, mapped intensity M, dM/drho)."""
+        """(model focal value, mapped intensity M, dM/drho)."""
         cc, bb = self.map.coef()
-        return self.proxy.focal(rho, beta, cc, bb, grad=grad)
+        return self.model.focal(rho, beta, cc, bb, grad=grad)
 
-    def _verify(self, rho: torch.Tensor, beta: float):
-        """3-D FDTD forward + adjoint: (FOM, gradient, complex focal value)."""
+    def _check(self, cands: torch.Tensor, eps_c: torch.Tensor, beta: float) -> torch.Tensor:
+        """Model focal values of the prescreened candidates (complex128)."""
         s = self.problem.setup
-        f, g, dft = self.problem.evaluate(rho, beta, grad=True)
+        if self.cfg.model == "cross-section":
+            labels = self.proxy.label(eps_c)  # one batched cross-section FDTD launch
+            for e_, l_ in zip(eps_c, labels):
+                self._buf_x.append(e_.float())
+                self._buf_y.append(to_targets(l_.unsqueeze(0), self.scale)[0])
+            return labels[:, s.center_index, s.focus_col]
+        vals = [self.model.focal(r, beta)[0] for r in cands]
+        return torch.tensor(vals, dtype=torch.complex128, device=cands.device)
+
+    def _verify(self, rho: torch.Tensor, beta: float, grad: bool = True):
+        """3-D FDTD forward (+ adjoint): (FOM, gradient, complex focal value)."""
+        s = self.problem.setup
+        f, g, dft = self.problem.evaluate(rho, beta, grad=grad)
         return f, g, complex(dft[s.center_index, s.focus_col])
+
+    def _pair(self, rho: torch.Tensor, beta: float, e3: complex, e_model: complex) -> None:
+        """Add a verified design's focal values to both output maps."""
+        self.map.add(e_model, e3)
+        with torch.no_grad():
+            e_net = complex(self._fno_focal(self.problem.setup.eps_design(rho, beta)[None])[0])
+        self.nmap.add(e_net, e3)
 
     # ---- loop -------------------------------------------------------------------
     def run(self, rho0: torch.Tensor, target: Optional[float] = None,
@@ -298,14 +330,14 @@ class SurrogateAssistedLoop:
         def done(fom, b):
             return target is not None and b >= b_end * (1 - 1e-9) and fom >= 0.99 * target
 
-        # (1) the start design
+        # (1) the start design (its FOM is the reference of the step scale)
         rho = rho0.to(dev, torch.float32).clone()
-        fom, grad, e3 = self._verify(rho, beta[0])
+        fom, _, e3 = self._verify(rho, beta[0], grad=False)
         fom0 = fom
-        e2, _, _ = self.proxy.focal(rho, beta[0])
-        self.map.add(e2, e3)
+        e_m, _, _ = self.model.focal(rho, beta[0])
+        self._pair(rho, beta[0], e3, e_m)
         hist.append(Record(1, time.perf_counter() - t0, fom, beta[0], "start"))
-        # (2) warm start on the mapped cross-section model, beta ramped
+        # (2) warm start on the mapped model, beta ramped
         opt = DensityAdam(rho, c.warm_lr)
         _, m_ref, _ = self._mapped(rho, beta[0], grad=False)
         for k in range(c.warm_steps):
@@ -314,8 +346,8 @@ class SurrogateAssistedLoop:
             opt.ascend(gm, 1.0 / max(m_ref, 1e-30))
         cand = opt.rho.clone()
         f_w, g_w, e3_w = self._verify(cand, b_end)
-        e2_w, _, _ = self.proxy.focal(cand, b_end)
-        self.map.add(e2_w, e3_w)
+        e_mw, _, _ = self.model.focal(cand, b_end)
+        self._pair(cand, b_end, e3_w, e_mw)
         hist.append(Record(2, time.perf_counter() - t0, f_w, b_end, "warm start"))
         # the start was judged at beta[0]; the warm start, at the end beta, is the new base
         b = b_end
@@ -325,7 +357,7 @@ class SurrogateAssistedLoop:
         lr = c.inner_lr
         # (3) trust-region steps on the corrected model
         while reached is None and len(hist) < c.max_verify:
-            e2_k, m_k, dm_k = self._mapped(rho, b, grad=True)
+            e_k, m_k, dm_k = self._mapped(rho, b, grad=True)
             corr = grad - dm_k
             inner = DensityAdam(rho, lr)
             snaps = []
@@ -338,22 +370,19 @@ class SurrogateAssistedLoop:
                                  for sn in snaps for sc in scales])
             lin = ((cands - rho) * corr).flatten(1).sum(1).double()
             cc, bb = self.map.coef()
+            cn, bn = self.nmap.coef()
             with torch.no_grad():
                 eps_c = torch.stack([s.eps_design(r, b) for r in cands])
                 fno_e = self._fno_focal(eps_c)
                 fno_k = self._fno_focal(s.eps_design(rho, b).unsqueeze(0))[0]
-                pre = fom + ((cc * fno_e + bb).abs() ** 2 - abs(cc * fno_k + bb) ** 2) + lin
+                pre = fom + ((cn * fno_e + bn).abs() ** 2 - abs(cn * fno_k + bn) ** 2) + lin
                 top = torch.topk(pre, min(c.n_check, len(cands))).indices
-                labels = self.proxy.label(eps_c[top])  # batched cross-section FDTD
-            e2_top = labels[:, s.center_index, s.focus_col]
-            model = fom + ((cc * e2_top + bb).abs() ** 2 - m_k) + lin[top]
+                e_top = self._check(cands[top], eps_c[top], b)
+            model = fom + ((cc * e_top + bb).abs() ** 2 - m_k) + lin[top]
             j = int(torch.argmax(model))
             pick = int(top[j])
-            for e_, l_ in zip(eps_c[top], labels):
-                self._buf_x.append(e_.float())
-                self._buf_y.append(to_targets(l_.unsqueeze(0), self.scale)[0])
             f_new, g_new, e3_new = self._verify(cands[pick], b)
-            self.map.add(complex(e2_top[j]), e3_new)
+            self._pair(cands[pick], b, e3_new, complex(e_top[j]))
             ok = f_new >= fom
             hist.append(Record(len(hist) + 1, time.perf_counter() - t0, f_new, b, "surrogate",
                                ok))
@@ -367,7 +396,8 @@ class SurrogateAssistedLoop:
                 rho, fom, grad = cands[pick].clone(), f_new, g_new
             else:
                 lr = max(c.min_inner_lr, 0.3 * lr)
-            self._fine_tune()
+            if c.model == "cross-section":
+                self._fine_tune()
             if done(fom, b):
                 reached = time.perf_counter() - t0
         torch.cuda.synchronize(dev)
@@ -376,6 +406,8 @@ class SurrogateAssistedLoop:
                 "best_fom": max(at_end) if at_end else None,
                 "wall_s": time.perf_counter() - t0, "time_to_target_s": reached,
                 "verifications": p.evaluations, "timings": dict(self.timings),
-                "candidates": cand_stats, "fom0": fom0,
+                "candidates": cand_stats, "fom0": fom0, "model": c.model,
                 "map": {"coef": [str(v) for v in self.map.coef()],
-                        "residual": self.map.residual()}}
+                        "residual": self.map.residual()},
+                "net_map": {"coef": [str(v) for v in self.nmap.coef()],
+                            "residual": self.nmap.residual()}}
