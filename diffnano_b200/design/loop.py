@@ -140,8 +140,8 @@ class SurrogateConfig:
     lr: float = 1e-3
     model: str = "coarse3d"      # proposing model: "coarse3d" or "cross-section"
     coarse_factor: int = 2       # cell-size factor of the coarse 3-D model
-    warm_steps: int = 60         # warm start: Adam steps on the mapped model, beta ramped
-    warm_lr: float = 0.05
+    warm_steps: int = 100        # warm start: Adam steps on the mapped model, beta ramped
+    warm_lr: float = 0.02
     inner_steps: int = 6         # trust-region path per verification (one snapshot per step)
     n_scales: int = 4            # step-length variants per snapshot: candidates = steps * scales
     n_check: int = 2             # candidates the FNO passes on to the model's check
@@ -188,9 +188,10 @@ class SurrogateAssistedLoop:
     Structural Optimization 15, 1998); Adam on m gives ``inner_steps``
     snapshots, each at ``n_scales`` step lengths; the FNO ranks them, the
     model checks the top ``n_check``, the best goes to 3-D.  Accepted when its
-    FOM does not fall; the step size grows by half when the gain reaches half
-    the predicted one and shrinks to 0.3 on a rejection.  Wall time includes
-    the proxy labelling and the network's training.
+    FOM does not fall; the step size doubles when the gain reaches 3/4 of the
+    predicted one, halves when it falls below 1/4 of it or the step is
+    rejected (the usual trust-region ratio test).  Wall time includes the proxy
+    labelling and the network's training.
 
     Measured on the 384x384x192 workload: the cross-section model saturates
     near x47 of the start's 3-D FOM, the coarse 3-D model's own optimum scores
@@ -390,12 +391,14 @@ class SurrogateAssistedLoop:
             cand_stats.append({"predicted": predicted, "fdtd": f_new, "fom_before": fom,
                                "lr": lr, "pick": pick, "fno_rank_of_pick": int(j),
                                "map_residual": self.map.residual()})
+            # trust-region ratio: achieved / predicted gain
+            ratio = (f_new - fom) / (predicted - fom) if predicted > fom else 0.0
+            if ok and ratio >= 0.75:
+                lr = min(c.max_inner_lr, 2.0 * lr)
+            elif not ok or ratio < 0.25:
+                lr = max(c.min_inner_lr, 0.5 * lr)
             if ok:
-                if f_new - fom >= 0.5 * max(predicted - fom, 0.0):
-                    lr = min(c.max_inner_lr, 1.5 * lr)
                 rho, fom, grad = cands[pick].clone(), f_new, g_new
-            else:
-                lr = max(c.min_inner_lr, 0.3 * lr)
             if c.model == "cross-section":
                 self._fine_tune()
             if done(fom, b):
