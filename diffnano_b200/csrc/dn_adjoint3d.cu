@@ -294,435 +294,11 @@ __global__ void __launch_bounds__(NT, AdjCfg<T>::MINB)
   if (z1 < D) release(q);
 }
 
-// ---------------------------------------------------------------------------
-// FP32, two columns per lane (the forward's 16 x 64 tiles): lane l owns
-// columns k0+2l and k0+2l+1 of its two rows; staged arrays are read as
-// float2, the x+1 neighbour of the second column with a scalar read, the x-1
-// terms of the first column come from lane l-1 by shuffle (lanes 0 and 1
-// compute the k0-1 halo column as above).  The step's curl record is read
-// straight from global memory as float2 (issued at the start of the plane,
-// consumed at its end) instead of being staged: staging it as well would
-// leave room for one CTA per SM.  Per column the arithmetic is the one-column
-// kernel's, expression for expression.
-// ---------------------------------------------------------------------------
-constexpr int S_V2 = 3;
-using LA2 = Layout<float, NRING_A, 0, S_V2, Geo64>;
-
-__device__ __forceinline__ float2 ld2(const float* a) {
-  return *reinterpret_cast<const float2*>(a);
-}
-__device__ __forceinline__ float sel(const float2 v, int c) { return c == 0 ? v.x : v.y; }
-
-template <int AXES>
-__global__ void __launch_bounds__(Geo64::NCW * 32, 2)
-    k_adj3d_v2(const AdjParams<float> p, const __grid_constant__ TmapSet tm, const Plan plan) {
-  using T = float;
-  using L = LA2;
-  using G = Geo64;
-  constexpr int S = L::S;
-  constexpr int AE = L::RING_ARR / (int)sizeof(T);
-  constexpr int RB = G::BX;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  const Smem<T, L> sm(smem_raw);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int D = p.D, H = p.H, W = p.W;
-  const long long py = p.py, pz = p.pz;
-  const T dt = p.dt, idl = p.inv_dl;
-  const Range R(plan, D);
-  const int z0 = R.z0, z1 = R.z1, k0 = R.k0, j0 = R.j0;
-
-  const int nj = pipe_setup(sm, R, D, H, W, p.b, p.c, p.status);
-  if (nj == 0) return;
-
-  // No separate producer warp (eight warps per CTA keep two CTAs per SM within
-  // the register file): lane 0 of warp 0 issues the first S jobs, and the
-  // warp that releases job q last issues job q + S into its stage at once.
-  auto slot0 = [](int) { return 0; };
-  if (warp == 0 && lane == 0) {
-    const int n0 = min(S, nj);
-    for (int qa = 0; qa < n0; ++qa) issue_job<T, L, NRING_A, 0>(sm, tm, R, qa, slot0);
-    atomicMax(&sm.flags[2], n0);
-  }
-
-  volatile int* s_abort = sm.flags + 1;
-  const int w = warp;
-  const int ja = j0 + 2 * w;
-  const int kA = k0 + 2 * lane;
-  const bool inA = kA < W, inB = kA + 1 < W;
-  const T dti = dt * idl;
-  T bK[2], gK[2], kf[2], kb[2], cKf[2], cKb[2], cKbp1[2];
-#pragma unroll
-  for (int c = 0; c < 2; ++c) {
-    const int k = kA + c;
-    bK[c] = sm.sbK[2 * lane + 1 + c];
-    gK[c] = sm.sgK[2 * lane + 1 + c];
-    kf[c] = (k < W - 1) ? T(1) : T(0);
-    kb[c] = (k > 0) ? T(1) : T(0);
-    cKf[c] = kf[c] * dti * gK[c];
-    cKb[c] = kb[c] * gK[c] * idl;
-    cKbp1[c] = sm.sgK[2 * lane + 2 + c] * idl;  // backward x at column k+1 (> 0)
-  }
-  const T bKh = sm.sbK[0], gKh = sm.sgK[0], gK0 = sm.sgK[1];  // columns k0-1, k0
-  const T cKfh = dti * gKh;
-  const T cKbh = (k0 > 1) ? gKh * idl : T(0);
-  T bJ[4], gJ[4], cJf[4], cJb[4];
-#pragma unroll
-  for (int r = 0; r < 4; ++r) {
-    const int j = ja + r - 1;
-    bJ[r] = sm.sbJ[2 * w + r];
-    gJ[r] = sm.sgJ[2 * w + r];
-    cJf[r] = (j < H - 1) ? dti * gJ[r] : T(0);
-    cJb[r] = (j > 0) ? gJ[r] * idl : T(0);
-  }
-  T pvxi[2][2] = {{T(0), T(0)}, {T(0), T(0)}}, pvyi[2][2] = {{T(0), T(0)}, {T(0), T(0)}};
-  int q = 0;
-
-  auto wait_full = [&](int qa) -> bool {
-    const bool r = wait_phase(&sm.full[qa % S], (qa / S) & 1, s_abort);
-    __syncwarp();
-    return r;
-  };
-  // release job qa: the warp's reads of its stage are ordered before its
-  // count; the warp whose count completes the stage's (qa / S + 1)-th use
-  // refills it with job qa + S (counts only grow, so no reset races)
-  auto release = [&](int qa) -> bool {
-    __syncwarp();
-    if (lane == 0) {
-      __threadfence_block();
-      const unsigned prev = atomicAdd(&sm.release[qa % S], 1u);
-      if (prev == (unsigned)(G::NCW * (qa / S + 1) - 1) && qa + S < nj) {
-        __threadfence_block();
-        issue_job<T, L, NRING_A, 0>(sm, tm, R, qa + S, slot0);
-        atomicMax(&sm.flags[2], qa + S + 1);
-      }
-    }
-    return true;
-  };
-  // on an error every warp waits (bounded) for the copies still in flight
-  auto fail = [&]() {
-    if (lane == 0) {
-      report_status(p.status, DN_ETIMEOUT);
-      *s_abort = 1;
-      drain_jobs(sm, *reinterpret_cast<volatile int*>(&sm.flags[2]));
-    }
-  };
-  // z roles of plane i per column (reference mapping: per column; physical:
-  // per plane)
-  auto i_roles = [&](int i, T e_ci[2], T hx_c2[2], T hy_c1[2], T hy_b[2], T& bI) {
-    if (AXES == DN_AXES_REFERENCE) {
-      bI = T(1);
-#pragma unroll
-      for (int c = 0; c < 2; ++c) {
-        e_ci[c] = gK[c] * idl;
-        hx_c2[c] = dti * gK[c];
-        hy_c1[c] = dti * gK[c];
-        hy_b[c] = bK[c];
-      }
-    } else {
-      bI = static_cast<T>(__ldg(p.b[0] + i));
-      const T gI = static_cast<T>(1.0 + __ldg(p.c[0] + i));
-#pragma unroll
-      for (int c = 0; c < 2; ++c) {
-        e_ci[c] = gI * idl;
-        hx_c2[c] = dti * gI;
-        hy_c1[c] = dti * gI;
-        hy_b[c] = bI;
-      }
-    }
-  };
-  auto e_ci_at = [&](int i, T out[2]) {
-#pragma unroll
-    for (int c = 0; c < 2; ++c)
-      out[c] = AXES == DN_AXES_REFERENCE ? gK[c] * idl
-                                         : static_cast<T>(1.0 + __ldg(p.c[0] + i)) * idl;
-  };
-
-  // lH' (all three) of row r (0..2), both columns
-  auto lam_h = [&](const T* cur, const T* nxt, int r, const T e_ci[2], const T e_ci_n[2],
-                   T fi_prev, T fi_next, T lhx[2], T lhy[2], T lhz[2]) {
-    const int e = r * RB;
-    const float2 ce = ld2(cur + A_CE * AE + e);
-    const float2 ex = ld2(cur + DN_EX * AE + e), ey = ld2(cur + DN_EY * AE + e),
-                 ez = ld2(cur + DN_EZ * AE + e);
-    const float2 cej = ld2(cur + A_CE * AE + e + RB);
-    const float2 exj = ld2(cur + DN_EX * AE + e + RB), ezj = ld2(cur + DN_EZ * AE + e + RB);
-    const T ce2 = cur[A_CE * AE + e + 2], ey2 = cur[DN_EY * AE + e + 2],
-            ez2 = cur[DN_EZ * AE + e + 2];
-    const float2 cei = ld2(nxt + A_CE * AE + e);
-    const float2 exi = ld2(nxt + DN_EX * AE + e), eyi = ld2(nxt + DN_EY * AE + e);
-    const float2 hx = ld2(cur + DN_HX * AE + e), hy = ld2(cur + DN_HY * AE + e),
-                 hz = ld2(cur + DN_HZ * AE + e);
-#pragma unroll
-    for (int c = 0; c < 2; ++c) {
-      const T cc = sel(ce, c);
-      const T ux = cc * sel(ex, c), uy = cc * sel(ey, c), uz = cc * sel(ez, c);
-      const T ce_j = sel(cej, c);
-      const T ux_j = ce_j * sel(exj, c), uz_j = ce_j * sel(ezj, c);
-      const T ce_k = c == 0 ? ce.y : ce2;
-      const T uy_k = ce_k * (c == 0 ? ey.y : ey2), uz_k = ce_k * (c == 0 ? ez.y : ez2);
-      const T ce_i = sel(cei, c);
-      const T ux_i = ce_i * sel(exi, c), uy_i = ce_i * sel(eyi, c);
-      const T eci = e_ci[c] * fi_prev, ecin = e_ci_n[c] * fi_next;
-      const T eyc2 = AXES == DN_AXES_REFERENCE ? kb[c] * gJ[r] * idl : cKb[c];
-      const T eyc2p1 = AXES == DN_AXES_REFERENCE ? gJ[r] * idl : cKbp1[c];
-      lhx[c] = sel(hx, c) + (eci * uy - ecin * uy_i) - (cJb[r] * uz - cJb[r + 1] * uz_j);
-      lhy[c] = sel(hy, c) - (eci * ux - ecin * ux_i) + (cKb[c] * uz - cKbp1[c] * uz_k);
-      lhz[c] = sel(hz, c) + (cJb[r] * ux - cJb[r + 1] * ux_j) - (eyc2 * uy - eyc2p1 * uy_k);
-    }
-  };
-
-  // ---- warm-up: z-1 terms from plane z0-1 ------------------------------------
-  if (z0 > 0) {
-    if (!(wait_full(q) && wait_full(q + 1))) {
-      fail();
-      return;
-    }
-    const int i = z0 - 1;
-    T e_ci[2], hx_c2[2], hy_c1[2], hy_b[2], bI, e_ci_n[2];
-    i_roles(i, e_ci, hx_c2, hy_c1, hy_b, bI);
-    e_ci_at(i + 1, e_ci_n);
-    const T* cur = sm.arr(q, 0) + 2 * w * RB + 2 * lane + 4;
-    const T* nxt = sm.arr(q + 1, 0) + 2 * w * RB + 2 * lane + 4;
-#pragma unroll
-    for (int r = 1; r < 3; ++r) {
-      T lhx[2], lhy[2], lhz[2];
-      lam_h(cur, nxt, r, e_ci, e_ci_n, i > 0 ? T(1) : T(0), T(1), lhx, lhy, lhz);
-#pragma unroll
-      for (int c = 0; c < 2; ++c) {
-        pvxi[r - 1][c] = hx_c2[c] * lhx[c];
-        pvyi[r - 1][c] = hy_c1[c] * lhy[c];
-      }
-    }
-    if (!release(q)) {
-      fail();
-      return;
-    }
-    ++q;
-  }
-
-  const long long cslot = (long long)(p.t - p.curl_t0) * p.curl_stride;
-  // ---- march -----------------------------------------------------------------
-  for (int i = z0; i < z1; ++i) {
-    const bool has_next = (i + 1 < D);
-    if ((i == 0 && !wait_full(q)) || (has_next && !wait_full(q + 1))) {
-      fail();
-      return;
-    }
-    T e_ci[2], hx_c2[2], hy_c1[2], hy_b[2], bI, e_ci_n[2];
-    i_roles(i, e_ci, hx_c2, hy_c1, hy_b, bI);
-    if (has_next) {
-      e_ci_at(i + 1, e_ci_n);
-    } else {
-      e_ci_n[0] = e_ci_n[1] = T(0);
-    }
-    const T fi_prev = i > 0 ? T(1) : T(0);
-    const T fi_next = has_next ? T(1) : T(0);
-    const T* cur = sm.arr(q, 0) + 2 * w * RB + 2 * lane + 4;
-    const T* nxt = has_next ? sm.arr(q + 1, 0) + 2 * w * RB + 2 * lane + 4 : cur;
-    // FP64 gradient and curl record of the owned cells: brought into L2 now,
-    // loaded into registers after lH' (holding them across it would spill)
-    const long long o_plane = i * pz + (long long)ja * py + kA;
-#pragma unroll
-    for (int r = 1; r < 3; ++r) {
-      if (ja + r - 1 < H && inA) {
-        const long long o = o_plane + (r - 1) * py;
-        prefetch_l2(p.grad + o);
-#pragma unroll
-        for (int a = 0; a < 3; ++a) prefetch_l2(p.curl[a] + cslot + o);
-      }
-    }
-
-    // ---- lH' of rows ja-1, ja, ja+1 --------------------------------------
-    T LHx[3][2], LHy[3][2], LHz[3][2];
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-      lam_h(cur, nxt, r, e_ci, e_ci_n, fi_prev, fi_next, LHx[r], LHy[r], LHz[r]);
-
-    // ---- k0-1 halo column: v_k terms of rows ja, ja+1 (lanes 0, 1) ---------
-    T hvyk = T(0), hvzk = T(0);
-    if (lane < 2 && k0 > 0) {
-      const int r = 1 + lane;
-      const T gJr = lane == 0 ? gJ[1] : gJ[2];
-      const T cJbr = lane == 0 ? cJb[1] : cJb[2];
-      const T cJbr1 = lane == 0 ? cJb[2] : cJb[3];
-      const int e = r * RB - 1 - 2 * lane;  // column k0-1 (pointers sit at k0+2*lane)
-      const T ce = cur[A_CE * AE + e];
-      const T ux = ce * cur[DN_EX * AE + e], uy = ce * cur[DN_EY * AE + e],
-              uz = ce * cur[DN_EZ * AE + e];
-      const T ce_j = cur[A_CE * AE + e + RB];
-      const T ux_j = ce_j * cur[DN_EX * AE + e + RB];
-      const T ce_k = cur[A_CE * AE + e + 1];
-      const T uy_k = ce_k * cur[DN_EY * AE + e + 1], uz_k = ce_k * cur[DN_EZ * AE + e + 1];
-      const T ce_i = nxt[A_CE * AE + e];
-      const T ux_i = ce_i * nxt[DN_EX * AE + e];
-      const T eci = (AXES == DN_AXES_REFERENCE ? gKh * idl : e_ci[0]) * fi_prev;
-      const T ecin = (AXES == DN_AXES_REFERENCE ? gKh * idl : e_ci_n[0]) * fi_next;
-      const T cKb0 = gK0 * idl;
-      const T eyc2 = AXES == DN_AXES_REFERENCE ? (k0 > 1 ? gJr * idl : T(0)) : cKbh;
-      const T eyc2p1 = AXES == DN_AXES_REFERENCE ? gJr * idl : cKb0;
-      const T lhy = cur[DN_HY * AE + e] - (eci * ux - ecin * ux_i) + (cKbh * uz - cKb0 * uz_k);
-      const T lhz = cur[DN_HZ * AE + e] + (cJbr * ux - cJbr1 * ux_j) - (eyc2 * uy - eyc2p1 * uy_k);
-      const T hyc2 = AXES == DN_AXES_REFERENCE ? dti * gJr : cKfh;
-      hvyk = hyc2 * lhy;
-      hvzk = cKfh * lhz;
-    }
-    const T hvyk0 = __shfl_sync(FULL_MASK, hvyk, 0), hvyk1 = __shfl_sync(FULL_MASK, hvyk, 1);
-    const T hvzk0 = __shfl_sync(FULL_MASK, hvzk, 0), hvzk1 = __shfl_sync(FULL_MASK, hvzk, 1);
-
-    // ---- previous adjoint fields of rows ja, ja+1 ---------------------------
-    double2 gpre[2];
-    float2 crl[2][3];
-#pragma unroll
-    for (int r = 1; r < 3; ++r) {
-      const bool ok = ja + r - 1 < H && inA;
-      const long long o = o_plane + (r - 1) * py;
-      if (ok && inB) {
-        gpre[r - 1] = *reinterpret_cast<const double2*>(p.grad + o);
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-          crl[r - 1][a] = __ldcs(reinterpret_cast<const float2*>(p.curl[a] + cslot + o));
-      } else if (ok) {
-        gpre[r - 1] = make_double2(p.grad[o], 0.0);
-#pragma unroll
-        for (int a = 0; a < 3; ++a) crl[r - 1][a] = make_float2(__ldcs(p.curl[a] + cslot + o), 0.f);
-      } else {
-        gpre[r - 1] = make_double2(0.0, 0.0);
-#pragma unroll
-        for (int a = 0; a < 3; ++a) crl[r - 1][a] = make_float2(0.f, 0.f);
-      }
-    }
-#pragma unroll
-    for (int r = 1; r < 3; ++r) {
-      const int j = ja + r - 1;
-      T vxj[2], vzj[2], vxi[2], vyi[2], vyk[2], vzk[2];
-#pragma unroll
-      for (int c = 0; c < 2; ++c) {
-        const T hyc2 = AXES == DN_AXES_REFERENCE ? kf[c] * dti * gJ[r] : cKf[c];
-        vxj[c] = cJf[r] * LHx[r][c];
-        vzj[c] = cJf[r] * LHz[r][c];
-        vxi[c] = has_next ? hx_c2[c] * LHx[r][c] : T(0);
-        vyi[c] = has_next ? hy_c1[c] * LHy[r][c] : T(0);
-        vyk[c] = hyc2 * LHy[r][c];
-        vzk[c] = cKf[c] * LHz[r][c];
-      }
-      // x-1 terms: column kA-1 is lane l-1's second column (the halo on lane 0)
-      T vyk_m[2], vzk_m[2];
-      vyk_m[0] = __shfl_up_sync(FULL_MASK, vyk[1], 1);
-      vzk_m[0] = __shfl_up_sync(FULL_MASK, vzk[1], 1);
-      if (lane == 0) {
-        vyk_m[0] = r == 1 ? hvyk0 : hvyk1;
-        vzk_m[0] = r == 1 ? hvzk0 : hvzk1;
-      }
-      vyk_m[1] = vyk[0];
-      vzk_m[1] = vzk[0];
-      if (j < H && inA) {
-        const int e = r * RB;
-        const float2 lex2 = ld2(cur + DN_EX * AE + e), ley2 = ld2(cur + DN_EY * AE + e),
-                     lez2 = ld2(cur + DN_EZ * AE + e);
-        T nlex[2], nley[2], nlez[2];
-        double gs[2];
-#pragma unroll
-        for (int c = 0; c < 2; ++c) {
-          const T lex = sel(lex2, c), ley = sel(ley2, c), lez = sel(lez2, c);
-          const T ex_b = AXES == DN_AXES_REFERENCE ? bJ[r] * bK[c] : bJ[r] * bI;
-          const T ey_b = AXES == DN_AXES_REFERENCE ? bK[c] * bJ[r] : bI * bK[c];
-          const T ez_b = bK[c] * bJ[r];
-          const T vxj_m = cJf[r - 1] * LHx[r - 1][c], vzj_m = cJf[r - 1] * LHz[r - 1][c];
-          nlex[c] = ex_b * lex + (vyi[c] - pvyi[r - 1][c]) - (vzj[c] - vzj_m);
-          nley[c] = ey_b * ley - (vxi[c] - pvxi[r - 1][c]) + (vzk[c] - vzk_m[c]);
-          nlez[c] = ez_b * lez + (vxj[c] - vxj_m) - (vyk[c] - vyk_m[c]);
-          const double gsum =
-              static_cast<double>(lex) * static_cast<double>(sel(crl[r - 1][0], c)) +
-              static_cast<double>(ley) * static_cast<double>(sel(crl[r - 1][1], c)) +
-              static_cast<double>(lez) * static_cast<double>(sel(crl[r - 1][2], c));
-          gs[c] = (c == 0 ? gpre[r - 1].x : gpre[r - 1].y) + gsum;
-        }
-        const long long o = o_plane + (r - 1) * py;
-        if (inB) {
-          *reinterpret_cast<double2*>(p.grad + o) = make_double2(gs[0], gs[1]);
-          *reinterpret_cast<float2*>(p.out[DN_EX] + o) = make_float2(nlex[0], nlex[1]);
-          *reinterpret_cast<float2*>(p.out[DN_EY] + o) = make_float2(nley[0], nley[1]);
-          *reinterpret_cast<float2*>(p.out[DN_EZ] + o) = make_float2(nlez[0], nlez[1]);
-          *reinterpret_cast<float2*>(p.out[DN_HX] + o) =
-              make_float2(bJ[r] * LHx[r][0], bJ[r] * LHx[r][1]);
-          *reinterpret_cast<float2*>(p.out[DN_HY] + o) =
-              make_float2(hy_b[0] * LHy[r][0], hy_b[1] * LHy[r][1]);
-          *reinterpret_cast<float2*>(p.out[DN_HZ] + o) =
-              make_float2(bK[0] * LHz[r][0], bK[1] * LHz[r][1]);
-        } else {
-          p.grad[o] = gs[0];
-          p.out[DN_EX][o] = nlex[0];
-          p.out[DN_EY][o] = nley[0];
-          p.out[DN_EZ][o] = nlez[0];
-          p.out[DN_HX][o] = bJ[r] * LHx[r][0];
-          p.out[DN_HY][o] = hy_b[0] * LHy[r][0];
-          p.out[DN_HZ][o] = bK[0] * LHz[r][0];
-        }
-      }
-#pragma unroll
-      for (int c = 0; c < 2; ++c) {
-        pvxi[r - 1][c] = vxi[c];
-        pvyi[r - 1][c] = vyi[c];
-      }
-    }
-    if (!release(q)) {
-      fail();
-      return;
-    }
-    ++q;
-  }
-  if (z1 < D) (void)release(q);  // the last job: nothing left to issue
-}
-
-// FP32 two-column reverse steps (k_adj3d_v2): ring maps with 72 x 18 boxes,
-// the curl record read directly (float2, 8-byte aligned by the TMA checks),
-// the FP64 gradient as double2 (16-byte aligned base)
-template <int AXES>
-int launch_adj_v2(AdjParams<float> p, void* const la[6], void* const lb[6], const dn_grid* g,
-                  const dn_monitor* mons, int n_mon, int t_end, int nsteps, cudaStream_t s) {
-  int rc;
-  TmapSet ta, tb;
-  for (int c = 0; c < 6; ++c) {
-    if ((rc = encode_ring(&ta.m[c], la[c], g, 4, Geo64::BX, Geo64::BY)) != DN_OK) return rc;
-    if ((rc = encode_ring(&tb.m[c], lb[c], g, 4, Geo64::BX, Geo64::BY)) != DN_OK) return rc;
-  }
-  if ((rc = encode_ring(&ta.m[A_CE], p.ce, g, 4, Geo64::BX, Geo64::BY)) != DN_OK) return rc;
-  tb.m[A_CE] = ta.m[A_CE];
-  int dev = 0, nsm = 0;
-  DN_CUDA_CHECK(cudaGetDevice(&dev));
-  DN_CUDA_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  long long nctas = 0;
-  const Plan plan = make_plan(g, (long long)nsm * 2, &nctas, Geo64::TX, Geo64::TY);
-  if (nctas > 0x7fffffffLL) return DN_EUNSUPPORTED;
-  const size_t smem = LA2::BYTES;
-  auto kern = k_adj3d_v2<AXES>;
-  DN_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem));
-  DN_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                     (int)cudaSharedmemCarveoutMaxShared));
-  for (int n = 0; n < nsteps; ++n) {
-    const bool even = (n % 2) == 0;
-    for (int c = 0; c < 6; ++c) {
-      p.in[c] = static_cast<const float*>(even ? la[c] : lb[c]);
-      p.out[c] = static_cast<float*>(even ? lb[c] : la[c]);
-    }
-    p.t = t_end - 1 - n;
-    if (n_mon > 0 && (rc = inject_monitors<float>(p, mons, n_mon, true, 0, s)) != DN_OK) return rc;
-    kern<<<(unsigned)nctas, Geo64::NCW * 32, smem, s>>>(p, even ? ta : tb, plan);
-  }
-  DN_CUDA_CHECK(cudaGetLastError());
-  return DN_OK;
-}
-
 template <typename T, int AXES>
 int launch_adj(AdjParams<T> p, void* const la[6], void* const lb[6], const dn_grid* g,
                const dn_curl_record* curl, const dn_monitor* mons, int n_mon, int t_end,
                int nsteps, cudaStream_t s) {
   using L = typename AdjCfg<T>::L;
-  if constexpr (sizeof(T) == 4) {
-    if (two_column_fp32() && (reinterpret_cast<uintptr_t>(p.grad) & 15) == 0)
-      return launch_adj_v2<AXES>(p, la, lb, g, mons, n_mon, t_end, nsteps, s);
-  }
   int rc;
   TmapSet ta, tb;
   for (int c = 0; c < 6; ++c) {

@@ -23,6 +23,11 @@
 //    six results to the other ping-pong buffer (neighbouring CTAs still read
 //    the old one);
 //  * optionally (adjoint replay) the curl term of each E update is recorded.
+// FP32 runs k_fdtd3d_v2 by default: the same march with two columns per lane
+// on 16 x 64 tiles (float2 shared-memory reads and global stores, ~30 % fewer
+// instructions per cell) in eight-warp CTAs whose stage loads are issued by
+// the warp that releases a stage last (two CTAs per SM at 128 registers);
+// FP64 and the one-column switch run k_fdtd3d.
 #include "dn_zmarch.cuh"
 
 namespace dn {

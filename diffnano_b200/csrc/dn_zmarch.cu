@@ -77,7 +77,7 @@ Plan make_plan(const dn_grid* g, long long capacity, long long* nctas, int tx, i
 }
 
 #ifndef DN_FWD3D_LANE_COLUMNS
-#define DN_FWD3D_LANE_COLUMNS 1
+#define DN_FWD3D_LANE_COLUMNS 2
 #endif
 bool two_column_fp32() {
   static const bool on = [] {

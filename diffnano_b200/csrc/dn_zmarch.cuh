@@ -29,7 +29,7 @@ struct Geo {
   static constexpr int BX = TX_ + 8;
   static constexpr int BY = TY_ + 2;
 };
-using Geo32 = Geo<32, 16>;  // one column per lane (FP64 forward, adjoint)
+using Geo32 = Geo<32, 16>;  // one column per lane (FP64 forward, the adjoint)
 using Geo64 = Geo<64, 16>;  // two columns per lane (FP32 forward)
 
 constexpr int TX = Geo32::TX;        // tile x (one warp)
@@ -272,10 +272,10 @@ int encode_tile4(CUtensorMap* m, const void* base, const dn_grid* g, int elem_by
                  long long slot_stride);
 // work split for `capacity` resident CTAs over tx x ty tiles
 Plan make_plan(const dn_grid* g, long long capacity, long long* nctas, int tx = TX, int ty = TY);
-// Does FP32 run the two-column kernels (forward and adjoint)?
-// DN_FWD3D_LANE_COLUMNS at build time, or the environment variable
-// DN_FDTD3D_LANE_COLUMNS = "1" or "2" (read once per process), e.g. to compare
-// the one- and two-column kernels.
+// Does the FP32 forward step (and the adjoint's replay) run the two-column
+// kernel?  DN_FWD3D_LANE_COLUMNS at build time (default 2), or the
+// environment variable DN_FDTD3D_LANE_COLUMNS = "1" or "2" (read once per
+// process), e.g. to compare the one- and two-column kernels.
 bool two_column_fp32();
 // TMA constraints: 16-byte aligned bases and byte strides
 bool tma_ok(const dn_grid* g, int elem_bytes, const void* const* ptrs, int n);
