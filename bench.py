@@ -46,6 +46,12 @@ METRIC = "FDTD Gcell-updates/s"
 UNIT = "Gcell-updates/s"
 
 
+
+def fwd_kernel_name() -> str:
+    """The FP32 3-D step kernel the library runs (two columns per lane unless
+    DN_FDTD3D_LANE_COLUMNS=1 asks for the one-column kernel)."""
+    return "k_fdtd3d" if os.environ.get("DN_FDTD3D_LANE_COLUMNS") == "1" else "k_fdtd3d_v2"
+
 def workload():
     """eps, source dict and monitor spec of the cubic grid SHAPE."""
     from diffnano_b200.workloads import gaussian_pulse_for_band, slab_eps_3d
@@ -359,7 +365,7 @@ def run_ours(args):
                    "overhead_bytes_per_cell_step": ADJ_OVERHEAD_BYTES_PER_CELL_STEP,
                    "moved_GBs": moved * cells / rev_s / 1e9,
                    "what": f"reverse sweep of a {Ta}-step solve: per step one replay step with "
-                           "curl record (k_fdtd3d) + one reverse step (k_adj3d), "
+                           f"curl record ({fwd_kernel_name()}) + one reverse step (k_adj3d), "
                            f"checkpoints every {runner.K} steps"}
         del runner, eng_a
         torch.cuda.empty_cache()
@@ -464,7 +470,7 @@ def run_ours(args):
                              "frac": achieved / peak, "traffic": traffic,
                              "peak_source": f"hbm_gbs of {peak_kind}",
                              "algorithmic_bytes_per_launch": BYTES_PER_CELL_STEP * cells,
-                             "kernel": "k_fdtd3d (one launch per time step)"},
+                             "kernel": f"{fwd_kernel_name()} (one launch per time step)"},
                 "cpu_baseline": cpu, "e2e": e2e, "adjoint": adjoint, "gradient_e2e": grad_e2e,
                 "fp64_check": fp64_check,
                 "clocks": cs.summary("untimed pre-roll + timed steps of the same solve"),
