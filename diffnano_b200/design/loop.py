@@ -142,7 +142,6 @@ class SurrogateConfig:
     coarse_factor: int = 2       # cell-size factor of the coarse 3-D model
     warm_steps: int = 100        # warm start: Adam steps on the mapped model, beta ramped
     warm_lr: float = 0.02
-    warm_anchor: int = 20        # 3-D forward + adjoint every this many warm steps (0: none)
     inner_steps: int = 6         # trust-region path per verification (one snapshot per step)
     n_scales: int = 4            # step-length variants per snapshot: candidates = steps * scales
     n_check: int = 2             # candidates the FNO passes on to the model's check
@@ -181,10 +180,8 @@ class SurrogateAssistedLoop:
     * the 3-D FDTD forward + adjoint verifies the best checked candidate.
 
     Run: (1) the 3-D FOM at the start design (forward only); (2) warm start:
-    Adam on the mapped model with beta ramped to its end value, with a 3-D
-    forward + adjoint every ``warm_anchor`` steps that refits the output map
-    and corrects the model to first order there, verified in 3-D at the end;
-    (3) trust-region steps at the end beta: the model corrected to first
+    Adam on the mapped model with beta ramped to its end value, verified in
+    3-D; (3) trust-region steps at the end beta: the model corrected to first
     order at the accepted design rho_k, m(rho) = f_k + M(rho) - M(rho_k) +
     (g_k - grad M(rho_k)) . (rho - rho_k), which matches the 3-D value and
     gradient there (first-order model management, Alexandrov et al.,
@@ -341,33 +338,18 @@ class SurrogateAssistedLoop:
         e_m, _, _ = self.model.focal(rho, beta[0])
         self._pair(rho, beta[0], e3, e_m)
         hist.append(Record(1, time.perf_counter() - t0, fom, beta[0], "start"))
-        # (2) warm start: Adam on the mapped model along the beta ramp; every
-        # warm_anchor steps one 3-D forward + adjoint refits the output map and
-        # corrects the model to first order there (that step takes the 3-D
-        # gradient itself), so the cheap trajectory follows the 3-D one while
-        # the design is still grey
+        # (2) warm start on the mapped model, beta ramped
         opt = DensityAdam(rho, c.warm_lr)
         _, m_ref, _ = self._mapped(rho, beta[0], grad=False)
-        corr = None
         for k in range(c.warm_steps):
             b = beta[0] * (b_end / beta[0]) ** (k / max(1, c.warm_steps - 1))
-            if c.warm_anchor > 0 and k > 0 and k % c.warm_anchor == 0 and \
-                    len(hist) + 2 < c.max_verify:
-                f_a, g_a, e3_a = self._verify(opt.rho, b)
-                e_ma, _, _ = self.model.focal(opt.rho, b)
-                self._pair(opt.rho, b, e3_a, e_ma)
-                hist.append(Record(len(hist) + 1, time.perf_counter() - t0, f_a, b, "anchor"))
-                _, _, gm = self._mapped(opt.rho, b, grad=True)
-                corr = g_a - gm
-                opt.ascend(g_a, 1.0 / max(m_ref, 1e-30))
-                continue
             _, _, gm = self._mapped(opt.rho, b, grad=True)
-            opt.ascend(gm if corr is None else gm + corr, 1.0 / max(m_ref, 1e-30))
+            opt.ascend(gm, 1.0 / max(m_ref, 1e-30))
         cand = opt.rho.clone()
         f_w, g_w, e3_w = self._verify(cand, b_end)
         e_mw, _, _ = self.model.focal(cand, b_end)
         self._pair(cand, b_end, e3_w, e_mw)
-        hist.append(Record(len(hist) + 1, time.perf_counter() - t0, f_w, b_end, "warm start"))
+        hist.append(Record(2, time.perf_counter() - t0, f_w, b_end, "warm start"))
         # the start was judged at beta[0]; the warm start, at the end beta, is the new base
         b = b_end
         rho, fom, grad = cand, f_w, g_w

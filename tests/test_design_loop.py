@@ -69,9 +69,7 @@ def test_surrogate_assisted_loop_not_behind_plain_loop(cuda):
     out = loop.run(rho0, target=None, beta=(1.0, 8.0))
     h = out["history"]
     assert len(h) == n and prob.evaluations == n
-    kinds = [r.kind for r in h]
-    assert kinds[0] == "start" and "warm start" in kinds
-    assert kinds.index("warm start") == 1 + kinds.count("anchor")
+    assert [r.kind for r in h[:2]] == ["start", "warm start"]
     assert all(r.fom > 0 for r in h)
     assert out["timings"]["label_s"] > 0 and out["timings"]["train_s"] > 0
     assert 0.0 <= loop.proxy_error() < 10.0
