@@ -142,7 +142,7 @@ class SurrogateConfig:
     coarse_factor: int = 2       # cell-size factor of the coarse 3-D model
     warm_steps: int = 100        # warm start: Adam steps on the mapped model, beta ramped
     warm_lr: float = 0.02
-    inner_steps: int = 6         # trust-region path per verification (one snapshot per step)
+    inner_steps: int = 8         # trust-region path per verification (one snapshot per step)
     n_scales: int = 4            # step-length variants per snapshot: candidates = steps * scales
     n_check: int = 2             # candidates the FNO passes on to the model's check
     inner_lr: float = 0.02
