@@ -94,3 +94,27 @@ def test_output_map_fits_affine_pairs_exactly():
     c2, b2 = m.coef()
     assert abs(c2 - c) < 1e-9 and abs(b2 - b) < 1e-6
     assert m.residual() < 1e-12
+
+
+def test_coarsened_setup_keeps_the_physical_layout():
+    """Host logic of the coarse 3-D model: the 2x coarser setup places the
+    design block, source plane, focal point and domain at the same physical
+    positions, simulates the same physical time, and keeps at least the
+    CPML's physical depth."""
+    from diffnano_b200.design.metalens import MetalensSetup
+
+    for fine in (MetalensSetup(), MetalensSetup().scaled(4)):
+        c = fine.coarsened(2)
+        assert c.dl == 2 * fine.dl
+        assert all(2 * a == b for a, b in zip(c.shape, fine.shape))
+        assert [2 * v for v in c.design_z] == list(fine.design_z)
+        assert [2 * v for v in c.design_xy] == list(fine.design_xy)
+        assert 2 * c.focus_z in (fine.focus_z, fine.focus_z - 1)
+        assert 2 * c.src_z in (fine.src_z, fine.src_z - 1)
+        assert c.src_z > c.pml and c.pml * c.dl >= fine.pml * fine.dl
+        assert abs(c.n_steps * c.dt - fine.n_steps * fine.dt) <= c.dt
+        assert c.focus_col * c.dl == fine.focus_col * fine.dl
+        assert c.design_shape == (fine.design_shape[0] // 2, fine.design_shape[1] // 2)
+    import pytest as _pt
+    with _pt.raises(ValueError):
+        MetalensSetup(shape=(191, 384, 384)).coarsened(2)
