@@ -34,8 +34,8 @@ e = eps.clone().requires_grad_(True)
 r = s.forward(e, source=dict(src))
 dft = r.metadata["monitors"][0]["dft"]
 ((r.field[1].double() * w).sum() + (dft.abs() ** 2).sum() * 1e-6).backward()
-torch.save({{"field": r.field.double().cpu(), "dft": torch.view_as_real(dft).cpu(),
-            "grad": e.grad.cpu()}}, sys.argv[1])
+torch.save({{"field": r.field.detach().double().cpu(),
+            "dft": torch.view_as_real(dft.detach()).cpu(), "grad": e.grad.cpu()}}, sys.argv[1])
 """
 
 
