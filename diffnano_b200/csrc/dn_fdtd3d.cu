@@ -433,7 +433,7 @@ __global__ void __launch_bounds__(Geo64::NCW * 32, 2)
   // release job qa: the warp's reads of its stage are ordered before its
   // count; the warp whose count completes the stage's (qa / S + 1)-th use
   // refills it with job qa + S (counts only grow, so no reset races)
-  auto release = [&](int qa) -> bool {
+  auto release = [&](int qa) {
     __syncwarp();
     if (lane == 0) {
       __threadfence_block();
@@ -444,7 +444,6 @@ __global__ void __launch_bounds__(Geo64::NCW * 32, 2)
         atomicMax(&sm.flags[2], qa + S + 1);
       }
     }
-    return true;
   };
   // on an error every warp waits (bounded) for the copies still in flight
   auto fail = [&]() {
@@ -507,10 +506,7 @@ __global__ void __launch_bounds__(Geo64::NCW * 32, 2)
                            hy_c2 * (ezk - sel(ez, c));
       }
     }
-    if (!release(q)) {
-      fail();
-      return;
-    }
+    release(q);
     ++q;
   }
 
@@ -663,13 +659,10 @@ __global__ void __launch_bounds__(Geo64::NCW * 32, 2)
         prevHy[r - 1][c] = Hy[r][c];
       }
     }
-    if (!release(q)) {
-      fail();
-      return;
-    }
+    release(q);
     ++q;
   }
-  if (z1 < D) (void)release(q);  // the last job: nothing left to issue  // the E-only job of plane z1 was read as "next"
+  if (z1 < D) release(q);  // the E-only job of plane z1 was read as "next"
 }
 
 // ---------------------------------------------------------------------------
