@@ -142,6 +142,8 @@ class SurrogateConfig:
     coarse_factor: int = 2       # cell-size factor of the coarse 3-D model
     warm_steps: int = 100        # warm start: Adam steps on the mapped model, beta ramped
     warm_lr: float = 0.02
+    tr_beta_start: float = 0.0   # > 0: the warm start stops at this beta and the first
+    tr_beta_steps: int = 8       # tr_beta_steps verifications raise it to the end value
     inner_steps: int = 8         # trust-region path per verification (one snapshot per step)
     n_scales: int = 4            # step-length variants per snapshot: candidates = steps * scales
     n_check: int = 2             # candidates the FNO passes on to the model's check
@@ -338,26 +340,36 @@ class SurrogateAssistedLoop:
         e_m, _, _ = self.model.focal(rho, beta[0])
         self._pair(rho, beta[0], e3, e_m)
         hist.append(Record(1, time.perf_counter() - t0, fom, beta[0], "start"))
-        # (2) warm start on the mapped model, beta ramped
+        # (2) warm start on the mapped model, beta ramped to b_w (the end value,
+        # or tr_beta_start when the trust-region steps finish the ramp)
+        b_w = c.tr_beta_start if 0.0 < c.tr_beta_start < b_end else b_end
         opt = DensityAdam(rho, c.warm_lr)
         _, m_ref, _ = self._mapped(rho, beta[0], grad=False)
         for k in range(c.warm_steps):
-            b = beta[0] * (b_end / beta[0]) ** (k / max(1, c.warm_steps - 1))
+            b = beta[0] * (b_w / beta[0]) ** (k / max(1, c.warm_steps - 1))
             _, _, gm = self._mapped(opt.rho, b, grad=True)
             opt.ascend(gm, 1.0 / max(m_ref, 1e-30))
         cand = opt.rho.clone()
-        f_w, g_w, e3_w = self._verify(cand, b_end)
-        e_mw, _, _ = self.model.focal(cand, b_end)
-        self._pair(cand, b_end, e3_w, e_mw)
-        hist.append(Record(2, time.perf_counter() - t0, f_w, b_end, "warm start"))
-        # the start was judged at beta[0]; the warm start, at the end beta, is the new base
-        b = b_end
+        f_w, g_w, e3_w = self._verify(cand, b_w)
+        e_mw, _, _ = self.model.focal(cand, b_w)
+        self._pair(cand, b_w, e3_w, e_mw)
+        hist.append(Record(2, time.perf_counter() - t0, f_w, b_w, "warm start"))
+        # the start was judged at beta[0]; the warm start is the new base
+        b = b_w
+        n_tr = 0
         rho, fom, grad = cand, f_w, g_w
         if done(fom, b):
             reached = time.perf_counter() - t0
         lr = c.inner_lr
         # (3) trust-region steps on the corrected model
         while reached is None and len(hist) < c.max_verify:
+            # beta of this verification: raised geometrically to the end value
+            # over tr_beta_steps verifications when the warm start stopped short
+            b_prev = b
+            n_tr += 1
+            if b < b_end:
+                b = min(b_end, b_w * (b_end / b_w) ** (n_tr / max(1, c.tr_beta_steps)))
+            ramping = b > b_prev
             e_k, m_k, dm_k = self._mapped(rho, b, grad=True)
             corr = grad - dm_k
             inner = DensityAdam(rho, lr)
@@ -384,7 +396,9 @@ class SurrogateAssistedLoop:
             pick = int(top[j])
             f_new, g_new, e3_new = self._verify(cands[pick], b)
             self._pair(cands[pick], b, e3_new, complex(e_top[j]))
-            ok = f_new >= fom
+            # while beta rises the FOMs of consecutive steps are not comparable:
+            # every step is taken (as the plain loop takes every step)
+            ok = ramping or f_new >= fom
             hist.append(Record(len(hist) + 1, time.perf_counter() - t0, f_new, b, "surrogate",
                                ok))
             predicted = float(model[j])
