@@ -755,9 +755,11 @@ def run_design(args):
                        "fom": "|DFT Ey(1550 nm)|^2 at the focal point",
                        "plain": f"{args.design_iters} Adam iterations, FDTD forward+adjoint each",
                        "assisted": "model (mapped to the 3-D focal field by a fitted output "
-                                   "map) gives the warm start and proposes trust-region steps; "
-                                   f"it checks the FNO's top {cfg.n_check}; the 3-D FDTD "
-                                   "verifies the best and judges every step",
+                                   "map) gives the warm start (beta ramped to "
+                                   f"{cfg.tr_beta_frac} of its end value) and proposes "
+                                   f"trust-region steps (the first {cfg.tr_beta_steps} finish "
+                                   f"the beta ramp); it checks the FNO's top {cfg.n_check}; the "
+                                   "3-D FDTD verifies the best and judges every step",
                        "surrogate": f"FNO trained on {cfg.n_train} batched-FDTD labels of the "
                                     f"2-D cross-section prescreens {cfg.n_candidates} candidates "
                                     f"per verification; the {cfg.model} model "

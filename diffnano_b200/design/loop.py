@@ -142,8 +142,8 @@ class SurrogateConfig:
     coarse_factor: int = 2       # cell-size factor of the coarse 3-D model
     warm_steps: int = 100        # warm start: Adam steps on the mapped model, beta ramped
     warm_lr: float = 0.02
-    tr_beta_start: float = 0.0   # > 0: the warm start stops at this beta and the first
-    tr_beta_steps: int = 8       # tr_beta_steps verifications raise it to the end value
+    tr_beta_frac: float = 0.5    # < 1: the warm start stops at this fraction of the end
+    tr_beta_steps: int = 8       # beta; the first tr_beta_steps verifications raise it
     inner_steps: int = 8         # trust-region path per verification (one snapshot per step)
     n_scales: int = 4            # step-length variants per snapshot: candidates = steps * scales
     n_check: int = 2             # candidates the FNO passes on to the model's check
@@ -182,8 +182,12 @@ class SurrogateAssistedLoop:
     * the 3-D FDTD forward + adjoint verifies the best checked candidate.
 
     Run: (1) the 3-D FOM at the start design (forward only); (2) warm start:
-    Adam on the mapped model with beta ramped to its end value, verified in
-    3-D; (3) trust-region steps at the end beta: the model corrected to first
+    Adam on the mapped model with beta ramped to ``tr_beta_frac`` of its end
+    value, verified in 3-D; (3) trust-region steps, the first
+    ``tr_beta_steps`` of them raising beta geometrically to its end value
+    (every step taken while beta rises, as the plain loop takes every step;
+    at beta 32 the landscape admits only tiny steps, so the design is shaped
+    while it is still grey): the model corrected to first
     order at the accepted design rho_k, m(rho) = f_k + M(rho) - M(rho_k) +
     (g_k - grad M(rho_k)) . (rho - rho_k), which matches the 3-D value and
     gradient there (first-order model management, Alexandrov et al.,
@@ -340,9 +344,9 @@ class SurrogateAssistedLoop:
         e_m, _, _ = self.model.focal(rho, beta[0])
         self._pair(rho, beta[0], e3, e_m)
         hist.append(Record(1, time.perf_counter() - t0, fom, beta[0], "start"))
-        # (2) warm start on the mapped model, beta ramped to b_w (the end value,
-        # or tr_beta_start when the trust-region steps finish the ramp)
-        b_w = c.tr_beta_start if 0.0 < c.tr_beta_start < b_end else b_end
+        # (2) warm start on the mapped model, beta ramped to b_w (a fraction of
+        # the end value; the trust-region steps finish the ramp)
+        b_w = max(beta[0], b_end * c.tr_beta_frac) if 0.0 < c.tr_beta_frac < 1.0 else b_end
         opt = DensityAdam(rho, c.warm_lr)
         _, m_ref, _ = self._mapped(rho, beta[0], grad=False)
         for k in range(c.warm_steps):

@@ -63,7 +63,7 @@ def test_surrogate_assisted_loop_not_behind_plain_loop(cuda):
     plain = plain_loop(Metalens3D(s, cuda), rho0, iters=n, lr=0.05, beta=(1.0, 8.0))
     prob = Metalens3D(s, cuda)
     cfg = SurrogateConfig(n_train=512, epochs=3, batch=128, warm_steps=30, inner_steps=4,
-                          n_scales=2, n_check=2, max_verify=n,
+                          n_scales=2, n_check=2, max_verify=n, tr_beta_steps=2,
                           fno=FNOConfig(H=H, W=W, modes=4, eps_lo=s.eps_lo, eps_hi=s.eps_hi))
     loop = SurrogateAssistedLoop(prob, cfg)
     out = loop.run(rho0, target=None, beta=(1.0, 8.0))
