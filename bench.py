@@ -46,11 +46,11 @@ METRIC = "FDTD Gcell-updates/s"
 UNIT = "Gcell-updates/s"
 
 
-
 def fwd_kernel_name() -> str:
     """The FP32 3-D step kernel the library runs (two columns per lane unless
     DN_FDTD3D_LANE_COLUMNS=1 asks for the one-column kernel)."""
     return "k_fdtd3d" if os.environ.get("DN_FDTD3D_LANE_COLUMNS") == "1" else "k_fdtd3d_v2"
+
 
 def workload():
     """eps, source dict and monitor spec of the cubic grid SHAPE."""
