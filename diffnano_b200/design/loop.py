@@ -175,7 +175,7 @@ class SurrogateAssistedLoop:
     * the proposing model, mapped to the 3-D focal field by an
       :class:`OutputMap`: by default (``model="coarse3d"``) the same lens on
       2x coarser cells (:func:`coarse_model`, ~0.28 s for a value and its
-      adjoint gradient on the workload, 1/12 of the full solve), or the 2-D
+      adjoint gradient on the workload, ~1/11 of the full solve), or the 2-D
       cross-section (``"cross-section"``, ~0.07 s; its optimum is about half
       the 3-D one); it proposes the steps and checks the prescreened
       candidates;
@@ -201,7 +201,7 @@ class SurrogateAssistedLoop:
 
     Measured on the 384x384x192 workload: the cross-section model saturates
     near x47 of the start's 3-D FOM, the coarse 3-D model's own optimum scores
-    x68-69 on the full grid; the network (held-out error ~0.6 on the
+    x68-69 on the full grid; the network (held-out error ~0.7 on the
     cross-section labels) cannot propose designs itself (ascending its own
     prediction leads to designs it overrates by orders of magnitude), so it
     only ranks.

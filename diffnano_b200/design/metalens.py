@@ -16,6 +16,9 @@ the lens axis as a 2-D TMz grid (rows = z, 192; columns = x, 384) with the
 same dx, time step, CPML depth, layers, source row and design region; 2-D Ez
 plays the part of 3-D Ey.  The batched 2-D FDTD labels thousands of proxy
 designs per launch with the DFT of Ez along the focal row.
+
+Coarse 3-D model (:func:`coarse_model`, what the assisted loop proposes
+with): the same lens on 2x larger cells, driven by the fine density.
 """
 from __future__ import annotations
 
@@ -191,7 +194,7 @@ def coarse_model(setup: MetalensSetup, factor: int = 2, device="cuda") -> Metale
     """The lens of ``setup`` on ``factor`` times coarser cells, driven by the
     fine density: the fine design eps (filter and projection on the fine
     grid) averaged over each coarse cell.  At factor 2 one forward + adjoint
-    costs ~1/12 of the fine one."""
+    costs ~1/11 of the fine one."""
     cs = setup.coarsened(factor)
 
     def design_map(rho, beta):
