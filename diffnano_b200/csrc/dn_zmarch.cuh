@@ -2,11 +2,14 @@
 // step): tile geometry, the TMA tensor maps, the work split, the staged
 // shared-memory ring with its producer warp, and bounded mbarrier waits.
 //
-// A CTA owns a 16 (y) x 32 (x) tile over a range of z planes.  Per plane it
-// stages NRING arrays as 40 x 18 boxes (x from k0-4, y from j0-1: the tile
-// plus a one-cell ring, x start 16-byte aligned for TMA) and NTILE arrays as
-// 32 x 16 tile boxes, through a ring of S stages filled by one producer warp
-// and drained by eight consumer warps (two rows each).
+// A CTA owns a TY (y) x TX (x) tile over a range of z planes (Geo: 16 x 32
+// with one column per lane, 16 x 64 with two).  Per plane it stages NRING
+// arrays as (TX+8) x (TY+2) boxes (x from k0-4, y from j0-1: the tile plus a
+// one-cell ring, x start 16-byte aligned for TMA) and NTILE arrays as TX x TY
+// tile boxes, through a ring of S stages drained by eight consumer warps (two
+// rows each) and filled either by a producer warp (producer_run) or, in
+// eight-warp CTAs, by the consumer warp that releases a stage last
+// (issue_job).
 #pragma once
 
 #include <cuda.h>
