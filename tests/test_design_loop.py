@@ -147,3 +147,16 @@ def test_coarsened_setup_keeps_the_physical_layout():
     import pytest as _pt
     with _pt.raises(ValueError):
         MetalensSetup(shape=(191, 384, 384)).coarsened(2)
+
+
+def test_assisted_loop_defaults_follow_the_workload():
+    """Config 4 asks for 32 candidates per iteration; the loop's defaults
+    give 8 snapshots x 4 step lengths, propose with the coarse 3-D model and
+    run the beta continuation (warm start to half the end beta, 8 ramp
+    verifications)."""
+    from diffnano_b200.design.loop import SurrogateConfig
+
+    c = SurrogateConfig()
+    assert c.n_candidates == 32 and (c.inner_steps, c.n_scales) == (8, 4)
+    assert c.model == "coarse3d" and c.coarse_factor == 2
+    assert 0.0 < c.tr_beta_frac < 1.0 and c.tr_beta_steps == 8
